@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Headline benchmark: Poisson solves/s to 1e-10 relative residual.
+
+Workload (one "step"): one full MG solve of the level-10 Q1 Poisson system
+(1025 x 1025 nodes, 1,050,625 unknowns, ELL FP64), V(4,4) with damped Jacobi
+(omega 0.7), bilinear prolongation / transposed restriction, coarsest level 3
+solved by CG (iteration cap 100, the reference's own MG test setting), stop at
+||r|| < 1e-10 ||r0||; b = A u*, u* ~ U[-1,1] (splitmix64, seed 42 + rank),
+x0 = 0.  Inputs are resident in HBM when a timed step starts; L2 is flushed
+(256 MiB write) before every step and the flush is outside the step's events.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (torchrun): every rank solves its own independent system (weak scaling,
+no data-path collective); the step time is the max over ranks.
+--impl reference: the reference's own CPU MG solver (compiled from its sources
+into oracle/_ref/) on this host's cores, same workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Poisson solves/s & HBM GB/s to 1e-10 rel. residual, mixed vs FP64; p99 latency"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "honei_ref")
+MIN_LEVEL = 3
+COARSE_CAP = 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--level", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def mg_solve_bytes(level: int, cycles: int, min_level: int = MIN_LEVEL, n_pre: int = 4, n_post: int = 4,
+                   s: int = 8, si: int = 4) -> int:
+    """Algorithmic HBM bytes of one MG solve (each vector / matrix entry touched once per pass).
+
+    Jacobi sweep 9(s+si)+4s per row; defect 9(s+si)+3s; restriction R (coarse rows,
+    <=9 slots) 9(s+si)+2s per coarse row + the fine input; prolongation-add P (fine
+    rows, 4 slots) 4(s+si)+2s per fine row + the coarse input; convergence defect once
+    per cycle plus the initial one; the coarse solve is counted once (it runs in
+    shared memory)."""
+    total = 0
+    for l in range(min_level + 1, level + 1):
+        nf = ((1 << l) + 1) ** 2
+        nc = ((1 << (l - 1)) + 1) ** 2
+        total += (n_pre + n_post) * nf * (9 * (s + si) + 4 * s)
+        total += nf * (9 * (s + si) + 3 * s)
+        total += nc * (9 * (s + si) + 2 * s) + nf * s
+        total += nf * (4 * (s + si) + 2 * s) + nc * s
+    n0 = ((1 << min_level) + 1) ** 2
+    total += n0 * (9 * (s + si) + 2 * s)
+    nF = ((1 << level) + 1) ** 2
+    total += nF * (9 * (s + si) + 3 * s)      # convergence defect + norm
+    return cycles * total + nF * (9 * (s + si) + 3 * s)
+
+
+JACOBI_BYTES_PER_ROW = 9 * (8 + 4) + 4 * 8     # FP64 values, int32 columns: 140 B
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_cpu(level: int, reps: int, warmup: int, tag: str, threads: int):
+    """Run the reference's own MG solver (oracle/_ref/honei_ref) and parse its RESULT line."""
+    env = dict(os.environ)
+    with tempfile.NamedTemporaryFile("w", suffix=".honeirc", delete=False) as f:
+        f.write(f"mc::num_threads = {threads}\nlog::categories = none\nlog::output = /dev/null\n")
+        env["HONEI_CONFIG"] = f.name
+    env["HONEI_COARSE_CAP"] = str(COARSE_CAP)
+    out = subprocess.run([REF_BIN, "bench", "mg", tag, str(level), str(reps), str(warmup)], capture_output=True,
+                         text=True, env=env, timeout=1800)
+    os.unlink(env["HONEI_CONFIG"])
+    for line in out.stdout.splitlines():
+        if line.startswith("RESULT "):
+            return json.loads(line[len("RESULT "):])
+    raise RuntimeError("reference run failed: " + out.stderr[-500:])
+
+
+def oracle_port_cpu(level: int, reps: int):
+    """Fallback CPU baseline: the oracle's C restatement (single thread)."""
+    from honei_b200.inputs import uniform
+    from oracle import oracle as o
+    A = o.q1_ell(level)
+    b = o.ell_spmv(A, uniform(A.rows, 42))
+    t = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        _, it, _ = o.mg_q1(level, b, max_iters_coarse=COARSE_CAP)
+        t.append(time.perf_counter() - t0)
+    return {"seconds_per_solve": sum(t) / len(t), "iters": it, "tag": "oracle-port"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    res = None
+    kind = "reference"
+    try:
+        res = reference_cpu(args.level, args.steps, min(args.warmup, 1), "mc", threads)
+    except Exception:
+        res = oracle_port_cpu(args.level, max(1, args.steps))
+        kind, threads = "port", 1
+    v = 1.0 / res["seconds_per_solve"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * res["seconds_per_solve"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: b = A u*, u* ~ U[-1,1] (splitmix64 seed 42)",
+            "config": workload_config(args, world),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} MG solves at level {args.level} "
+                                       f"(tags::CPU::MultiCore::SSE, {threads} threads)",
+                             "iters": res.get("iters")},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, world):
+    return {"workload": f"mg-v44-fp64-q1-level{args.level}", "level": args.level,
+            "unknowns": ((1 << args.level) + 1) ** 2, "matrix": "SparseMatrixELL (9 slots, int32 columns on device)",
+            "coarse_level": MIN_LEVEL, "coarse_solver": f"CG, cap {COARSE_CAP}", "smoother": "Jacobi omega 0.7, 4+4",
+            "tol": 1e-10, "l2": "flushed (256 MiB write) before every step, flush outside the step events",
+            "parallelism": f"{world} independent systems (one per GPU)" if world > 1 else "single system"}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference_arm(args, rank, world)
+        barrier(world)
+        return rc
+
+    import numpy as np
+    import torch
+
+    import honei_b200 as hb
+    from honei_b200 import _lib
+    from honei_b200.inputs import uniform
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    L = args.level
+    n = ((1 << L) + 1) ** 2
+
+    params = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10, coarse_exact=True)
+    data = hb.MGData.poisson_q1(MIN_LEVEL, L, params=params)
+    A = hb.SparseMatrixELL.poisson_q1(L)
+    u = hb.DenseVector(torch.from_numpy(uniform(n, 42 + rank)).to(dev))
+    b = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
+    hb.Product.value(b, A, u)
+    x = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+
+    def one_solve():
+        hb.fill(x, 0.0)
+        hb.MGSolver.value(data, b, x)
+
+    for _ in range(args.warmup):
+        one_solve()
+    torch.cuda.synchronize()
+
+    # ---------------------------------------------------------------- timed region
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = hb.launch_count()
+    cycles = []
+    with Clocks(local) as clk:
+        t_wall0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            one_solve()
+            ev[i][1].record(stream)
+            cycles.append(data.used_iters)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall0
+    barrier(world)
+    gpu_launches = hb.launch_count() - launches0     # this library's kernels (graph nodes included)
+    step_ms = [a.elapsed_time(b_) for a, b_ in ev]
+    mean_ms = statistics.mean(step_ms)
+    mean_ms_max = max_over_ranks(mean_ms, world, dev)
+    value = world * 1000.0 / mean_ms_max
+
+    # correctness of the timed solve (relative residual, on the device)
+    r = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
+    hb.Defect.value(r, b, A, x)
+    relres = hb.Norm.value(r) / hb.Norm.value(b)
+
+    # ---------------------------------------------------------------- end to end
+    hb_pinned = torch.from_numpy(uniform(n, 42 + rank)).pin_memory()
+    b_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    bd = torch.zeros(n, dtype=torch.float64, device=dev)
+    ud = hb_pinned.to(dev, non_blocking=True)
+    hb.Product.value(hb.DenseVector(bd), A, hb.DenseVector(ud))
+    b_host.copy_(bd.cpu())
+    x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b_dev = b_host.to(dev, non_blocking=True)
+        x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+        hb.MGSolver.value(data, hb.DenseVector(b_dev), hb.DenseVector(x_dev))
+        x_host.copy_(x_dev, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_mean = max_over_ranks(statistics.mean(e2e_ms), world, dev)
+
+    # ---------------------------------------------------------------- dominant kernel
+    P = hb.RISmoother.jacobi_precon(A, 0.7)
+    xa = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
+    xb = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
+    kms = []
+    for i in range(args.warmup + max(args.steps, 10)):
+        flush.zero_()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, b.ptr, xa.ptr, xb.ptr,
+                  ctypes_stream(stream))
+        k1.record(stream)
+        k1.synchronize()
+        if i >= args.warmup:
+            kms.append(k0.elapsed_time(k1))
+        xa, xb = xb, xa
+    k_ms = statistics.mean(kms)
+    k_bytes = JACOBI_BYTES_PER_ROW * n
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    peaks = load_peaks()
+    traffic = load_traffic()
+
+    solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)))
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mean_ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: b = A u*, u* ~ U[-1,1] (splitmix64 seed 42+rank)",
+        "config": workload_config(args, world),
+        "hbm_gbs": solve_bytes / (mean_ms_max * 1e-3) / 1e9,
+        "latency_ms": {"p50": percentile(step_ms, 50), "p99": percentile(step_ms, 99), "max": max(step_ms)},
+        "cycles": int(statistics.median(cycles)), "relres": relres,
+        "wall_ms_per_step_incl_flush": 1000 * t_wall / args.steps,
+        "roofline": {"bound": "hbm", "kernel": "ell_kernel<double,9,kJacobi> (fused Jacobi sweep, level %d)" % L,
+                     "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+                     "peak_source": peaks[1], "traffic": traffic, "algorithmic_bytes": k_bytes,
+                     "launch_us": 1000 * k_ms},
+        "e2e": {"value": world * 1000.0 / e2e_mean, "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(L)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def percentile(vals, p):
+    s = sorted(vals)
+    k = min(len(s) - 1, max(0, int(round((p / 100.0) * (len(s) - 1)))))
+    return s[k]
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def load_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ell_jacobi_sweep_fp64_level10.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except Exception:
+        pass
+    return None
+
+
+def cpu_baseline(level):
+    reps = 2
+    try:
+        res = reference_cpu(level, reps, 0, "sse", 1)
+        return {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "reference",
+                "sample": f"{reps} MG solves at level {level} (reference tags::CPU::SSE, 1 thread)",
+                "iters": res["iters"]}
+    except Exception as e:  # binary absent: the oracle port
+        res = oracle_port_cpu(level, 1)
+        return {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "port",
+                "sample": f"1 MG solve at level {level} (oracle C port; reference binary unavailable: {e})"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

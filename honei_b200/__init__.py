@@ -1,0 +1,18 @@
+"""honei_b200 -- B200 (sm_100a) backend of HONEI's sparse Poisson solver path.
+
+Python mirror of the reference's tag-dispatched operator API over the C ABI in
+include/honei_b200.h (libhonei_b200.so).  There is no CPU fallback: the first
+operator call without the built library raises ImportError.
+"""
+from ._lib import DeviceTimeout, HoneiError, NotFinite, VectorSizeDoesNotMatch, launch_count
+from .la import (BandedMatrixQx, Defect, DenseVector, Difference, DotProduct, ElementProduct, Norm, Product, Scale,
+                 ScaledSum, SparseMatrixELL, Sum, convert, copy, fill, tags)
+from .solvers import (CGSolver, IRSolver, MGData, MGSolver, Prolongation, Restriction, RISmoother, methods,
+                      mg_params)
+
+__all__ = [
+    "BandedMatrixQx", "CGSolver", "Defect", "DenseVector", "DeviceTimeout", "Difference", "DotProduct",
+    "ElementProduct", "HoneiError", "IRSolver", "MGData", "MGSolver", "Norm", "NotFinite", "Product",
+    "Prolongation", "RISmoother", "Restriction", "Scale", "ScaledSum", "SparseMatrixELL", "Sum",
+    "VectorSizeDoesNotMatch", "convert", "copy", "fill", "launch_count", "methods", "mg_params", "tags",
+]

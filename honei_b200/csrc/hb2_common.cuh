@@ -1,0 +1,205 @@
+// Common device/host helpers for the B200 backend of the HONEI sparse solver path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/honei_b200.h"
+
+namespace hb2
+{
+    // Status plumbing: every C-ABI entry point returns an int status; the message
+    // of the last failure on this host thread is kept for hb2_last_error().
+    void set_error(const std::string & msg);
+    int fail(int status, const std::string & msg);
+    int cuda_status(cudaError_t e, const char * where);
+
+#define HB2_CUDA(call)                                                       \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) return ::hb2::cuda_status(e_, #call);         \
+    } while (0)
+
+#define HB2_LAUNCH_CHECK(where)                                              \
+    do {                                                                     \
+        cudaError_t e_ = cudaGetLastError();                                 \
+        if (e_ != cudaSuccess) return ::hb2::cuda_status(e_, where);         \
+    } while (0)
+
+    inline size_t dtype_size(int dt) { return dt == HB2_F64 ? 8 : 4; }
+
+    // ------------------------------------------------------------------
+    // Arithmetic with explicit rounding.  The reference's compiled CPU loops
+    // round a*b and then the sum separately (no fma) for products and
+    // element-wise updates, and contract to fma only in the dot product; the
+    // kernels reproduce that exactly so results are bit-identical.
+    template <typename T> struct Arith;
+    template <> struct Arith<double>
+    {
+        static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+        static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+        static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+        static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+        static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    };
+    template <> struct Arith<float>
+    {
+        static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+        static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+        static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+        static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+        static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    };
+
+    // ------------------------------------------------------------------
+    // Deterministic reductions.  A block reduces its threads' partials with a
+    // fixed shuffle tree, writes one partial per block, and the last block to
+    // finish (ticket counter) reduces the partials in a fixed order.  The result
+    // depends only on the data and the launch shape, never on timing.
+    __device__ __forceinline__ double warp_sum(double v)
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+
+    // block-wide sum; every thread gets the result.  scratch: >= 32 doubles.
+    __device__ __forceinline__ double block_sum(double v, double * scratch)
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+        v = warp_sum(v);
+        __syncthreads();
+        if (lane == 0) scratch[warp] = v;
+        __syncthreads();
+        double t = (threadIdx.x < nwarps) ? scratch[threadIdx.x] : 0.0;
+        if (warp == 0) t = warp_sum(t);
+        if (threadIdx.x == 0) scratch[0] = t;
+        __syncthreads();
+        double r = scratch[0];
+        __syncthreads();
+        return r;
+    }
+
+    // Workspace used by the fused reductions of one stream: block partials and
+    // the ticket counter.  One per (device, stream) user; see workspace.cu.
+    struct ReduceSlot
+    {
+        double * partials;      // >= max_blocks
+        unsigned * ticket;      // zero between launches
+        uint32_t max_blocks;
+    };
+
+    // Called by every block after it computed `v` (valid in all threads).  The
+    // last block writes the total to *out (and optionally sqrt) and re-arms the
+    // ticket.  Returns true in the block that finished the reduction.
+    __device__ __forceinline__ bool grid_sum_finish(double v, ReduceSlot rs, double * out, int want_sqrt,
+            double * scratch)
+    {
+        __shared__ bool is_last;
+        if (threadIdx.x == 0)
+        {
+            rs.partials[blockIdx.x] = v;
+            __threadfence();
+            unsigned t = atomicAdd(rs.ticket, 1u);
+            is_last = (t == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (! is_last) return false;
+        __threadfence();
+        double s = 0.0;
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+            s += ((volatile double *)rs.partials)[i];
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0)
+        {
+            out[0] = want_sqrt ? sqrt(s) : s;
+            *rs.ticket = 0;
+        }
+        return true;
+    }
+
+    // ------------------------------------------------------------------
+    // Grid-wide barrier for cooperative (co-resident) launches, with a bounded
+    // wait: after `limit_ns` of spinning it records an error and returns false
+    // instead of hanging.  count/gen live in device memory, zero-initialised.
+    struct GridBarrier
+    {
+        unsigned * count;
+        unsigned * gen;
+        int * error;
+    };
+
+    __device__ __forceinline__ unsigned long long global_ns()
+    {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+
+    __device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned long long limit_ns = 2000000000ull)
+    {
+        __shared__ int ok;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            ok = 1;
+            volatile unsigned * vgen = b.gen;
+            unsigned g = *vgen;
+            __threadfence();
+            unsigned arrived = atomicAdd(b.count, 1u);
+            if (arrived == gridDim.x - 1)
+            {
+                *b.count = 0;
+                __threadfence();
+                atomicAdd(b.gen, 1u);
+            }
+            else
+            {
+                unsigned long long t0 = global_ns();
+                while (*vgen == g)
+                {
+                    if (*((volatile int *)b.error) != 0) { ok = 0; break; }
+                    if (global_ns() - t0 > limit_ns)
+                    {
+                        atomicExch(b.error, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(20);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        return ok != 0;
+    }
+
+    // ------------------------------------------------------------------
+    // device workspace: reduction slots, barrier words, scalar slots.
+    struct Workspace
+    {
+        int device;
+        double * partials;       // max_blocks doubles
+        unsigned * ticket;       // 1
+        unsigned * bar_words;    // 2 (count, gen)
+        int * error;             // 1
+        double * scalars;        // 64 doubles of solver scalars
+        uint32_t max_blocks;
+        double * host_scalars;   // pinned, 64 doubles
+        ReduceSlot slot() const { ReduceSlot r; r.partials = partials; r.ticket = ticket; r.max_blocks = max_blocks; return r; }
+        GridBarrier barrier() const { GridBarrier g; g.count = bar_words; g.gen = bar_words + 1; g.error = error; return g; }
+    };
+
+    // Per-device default workspace, created on first use (cudaMalloc) and kept
+    // until process exit.  Not thread-safe across concurrent streams: calls
+    // that use the default workspace must be stream-ordered.
+    int default_workspace(Workspace ** out);
+    int workspace_create(Workspace ** out, uint32_t max_blocks);
+    void workspace_destroy(Workspace * w);
+
+    inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+    extern int g_num_sms;
+    int num_sms();
+}

@@ -1,0 +1,104 @@
+// Internal host-side structures shared by the backend's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hb2_common.cuh"
+
+namespace hb2
+{
+    // Launch shape of the ELL family: blocks of 256 threads, each thread owns
+    // kRowsPerThread consecutive rows (one 128-bit load of values per slot for
+    // FP64, two rows; four rows for FP32).
+    constexpr int kEllThreads = 256;
+    constexpr uint32_t kMaxReduceBlocks = 1u << 16;
+
+    void count_launches(uint64_t n);
+    void set_launch_count(uint64_t n);   // undo the counting of captured (not launched) kernels
+    int stream_workspace(cudaStream_t stream, Workspace ** out);
+
+    template <typename T> struct RowsPerThread;
+    template <> struct RowsPerThread<double> { static constexpr int value = 2; };
+    template <> struct RowsPerThread<float> { static constexpr int value = 4; };
+
+    // Device view of an ELL matrix in the B200 layout: slot-major like the
+    // reference (coalesced across rows), int32 column indices, -1 marking the
+    // slots past a row's length, leading dimension padded to 64 rows so each
+    // slot column starts 256-byte aligned and every vector load is in bounds.
+    template <typename T>
+    struct EllView
+    {
+        const T * val;
+        const int32_t * col;
+        uint64_t rows;
+        uint64_t ld;
+        uint32_t K;
+    };
+}
+
+struct hb2_ell_s
+{
+    int dtype;
+    int device;
+    uint64_t rows, cols;
+    uint32_t K;        // device slots per row (reference num_cols_per_row * threads)
+    uint64_t ld;       // device leading dimension
+    void * val;        // K * ld values
+    int32_t * col;     // K * ld column indices (-1 = empty)
+    uint64_t ref_stride, ref_K, ref_T;
+    uint64_t bytes;
+
+    template <typename T> hb2::EllView<T> view() const
+    {
+        hb2::EllView<T> v;
+        v.val = (const T *)val;
+        v.col = col;
+        v.rows = rows;
+        v.ld = ld;
+        v.K = K;
+        return v;
+    }
+};
+
+struct hb2_q1_s
+{
+    int dtype;
+    uint64_t n, m;
+    void * bands;      // 9 * n, band-major LL LD LU DL DD DU UL UD UU
+};
+
+namespace hb2
+{
+    // ELL kernel family (ell.cu).  Modes of the fused epilogue:
+    enum EllMode
+    {
+        kPlain = 0,     // y = A x
+        kDefect = 1,    // y = aux - A x             (+ optional ||y||^2)
+        kDot = 2,       // y = A x, red = <y, x>
+        kAdd = 3,       // y = y + A x
+        kJacobi = 4,    // y = x + P (.) (aux - A x) (ping-pong sweep)
+        kRestrict = 5   // y = A x, zero[0..rows) = 0
+    };
+
+    // Launch one ELL kernel on `stream`.  aux: rhs / b; aux2: Jacobi P; zero:
+    // vector cleared by kRestrict; red: device double receiving the fused
+    // reduction (nullable, kDefect / kDot); ws: workspace for the reduction.
+    int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
+                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream);
+
+    // BLAS-1 helpers (blas1.cu) usable from other translation units.
+    int launch_fill(int dt, void * x, double value, uint64_t n, cudaStream_t stream);
+    int launch_copy(int dt, void * dst, const void * src, uint64_t n, cudaStream_t stream);
+    int launch_norm(int dt, const void * x, uint64_t n, int root, double * dev_out, const Workspace * ws,
+                    cudaStream_t stream);
+    int launch_convert(int dst_dt, void * dst, int src_dt, const void * src, uint64_t n, cudaStream_t stream);
+    // x64 += (double) c  (IR update, math/ir.hh:73-75)
+    int launch_add_converted(void * x64, int c_dt, const void * c, uint64_t n, cudaStream_t stream);
+
+    // small-system CG in one thread block (cg.cu); returns HB2_ERR_UNSUPPORTED
+    // when the system does not fit in shared memory.
+    int launch_cg_small(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
+                        uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
+    bool cg_small_fits(const hb2_ell_s * A);
+}

@@ -1,0 +1,381 @@
+// Geometric multigrid on the device: MGData + MGCycleCreation<V::STATIC,
+// CGSolver<NONE>, RISmoother, Restriction<PROLMAT>, Prolongation<PROLMAT>>
+// (math/mg.hh:57-240, 567-656), MGSolver (math/mg.hh:1094-1127) and IRSolver
+// (math/ir.hh:31-80).
+//
+// The reference walks a vector of virtual Operator objects per cycle, each a
+// tag-dispatched call (math/operator_list.hh:69-76).  Here the same operator
+// sequence is recorded once into a CUDA graph with fused kernels:
+//   smoother sweep  = Defect + ElementProduct + Sum     -> one Jacobi pass
+//   Defect + Restriction + Fill(c = 0)                  -> defect pass + restrict pass
+//   Prolongation + Sum                                  -> one SpMV-add pass
+//   coarsest CGSolver                                   -> one thread block, shared memory
+//   convergence Defect + Norm                           -> one pass
+// and a V-cycle costs one graph launch.  Each kernel is bit-identical to the
+// reference's operator; with coarse_exact the coarse CG is too, so the MG
+// iterates match the reference's tags::CPU solver bit for bit.
+#include "hb2_common.cuh"
+#include "hb2_internal.hh"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace hb2
+{
+    struct MgLevel
+    {
+        hb2_ell_s * A = 0;
+        hb2_ell_s * P = 0;   // prolongation from the next coarser level (levels > 0)
+        hb2_ell_s * R = 0;   // restriction to the next coarser level
+        uint64_t n = 0;
+        void * x = 0;        // finest: solution; coarser: c
+        void * b = 0;        // finest: rhs; coarser: d
+        void * store = 0;
+        void * tmp = 0;      // Jacobi ping-pong
+        void * jac = 0;      // omega / diag(A)
+    };
+}
+
+struct hb2_mg_s
+{
+    int dtype;
+    int device;
+    uint32_t nlev;
+    std::vector<hb2::MgLevel> lev;
+    hb2_mg_params prm;
+    bool owns_matrices;
+    hb2::Workspace * ws;
+    void * vec_block;        // one allocation for all level vectors
+    void * rfine;            // finest-level defect
+    cudaStream_t cap;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    uint64_t graph_kernels;
+    double * norm_dev;       // sqrt(r.r) after the cycle
+    uint64_t * coarse_used_dev;
+    double * coarse_def_dev;
+};
+
+namespace hb2
+{
+    static int smooth(hb2_mg_s * mg, MgLevel & L, uint64_t sweeps, cudaStream_t s)
+    {
+        void * cur = L.x, * nxt = L.tmp;
+        for (uint64_t k = 0; k < sweeps; ++k)
+        {
+            int st = launch_ell(L.A, kJacobi, cur, nxt, L.b, L.jac, 0, 0, 0, mg->ws, s);
+            if (st) return st;
+            std::swap(cur, nxt);
+        }
+        if (cur != L.x) return launch_copy(mg->dtype, L.x, cur, L.n, s);
+        return HB2_OK;
+    }
+
+    // MGCycleCreation::_build_cycle (math/mg.hh:577-640)
+    static int record_cycle(hb2_mg_s * mg, uint32_t i, cudaStream_t s)
+    {
+        MgLevel & L = mg->lev[i];
+        if (i == 0)
+            return launch_cg_small(L.A, L.b, L.x, mg->prm.max_iters_coarse, mg->prm.coarse_eps, mg->prm.coarse_exact,
+                                   mg->coarse_used_dev, mg->coarse_def_dev, s);
+        MgLevel & C = mg->lev[i - 1];
+        int st = smooth(mg, L, mg->prm.n_pre_smooth, s);
+        if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s);
+        if (! st) st = launch_ell(L.R, kRestrict, L.store, C.b, 0, 0, C.x, 0, 0, mg->ws, s);
+        if (! st) st = record_cycle(mg, i - 1, s);
+        if (! st) st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, mg->ws, s);
+        if (! st) st = smooth(mg, L, mg->prm.n_post_smooth, s);
+        return st;
+    }
+
+    static int finest_norm(hb2_mg_s * mg, cudaStream_t s)
+    {
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        return launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, s);
+    }
+
+    static int build_graph(hb2_mg_s * mg)
+    {
+        HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
+        uint64_t before = hb2_launch_count();
+        int st = record_cycle(mg, mg->nlev - 1, mg->cap);
+        if (! st) st = finest_norm(mg, mg->cap);
+        if (! st)
+        {
+            cudaError_t e = cudaMemcpyAsync(mg->ws->host_scalars, mg->norm_dev, sizeof(double), cudaMemcpyDeviceToHost, mg->cap);
+            if (e != cudaSuccess) st = cuda_status(e, "capture D2H");
+        }
+        cudaGraph_t g = 0;
+        cudaError_t e = cudaStreamEndCapture(mg->cap, &g);
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+        mg->graph_kernels = hb2_launch_count() - before;
+        set_launch_count(before);
+        mg->graph = g;
+        e = cudaGraphInstantiate(&mg->exec, g, 0);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+        return HB2_OK;
+    }
+
+    static int mg_alloc(hb2_mg_s * mg, cudaStream_t stream)
+    {
+        const size_t es = dtype_size(mg->dtype);
+        size_t total = 0;
+        for (uint32_t i = 0; i < mg->nlev; ++i) total += 5 * ((mg->lev[i].n * es + 255) / 256 * 256);
+        total += (mg->lev[mg->nlev - 1].n * es + 255) / 256 * 256;
+        HB2_CUDA(cudaMalloc(&mg->vec_block, total));
+        HB2_CUDA(cudaMemsetAsync(mg->vec_block, 0, total, stream));
+        char * p = (char *)mg->vec_block;
+        for (uint32_t i = 0; i < mg->nlev; ++i)
+        {
+            size_t sz = (mg->lev[i].n * es + 255) / 256 * 256;
+            MgLevel & L = mg->lev[i];
+            L.x = p; p += sz;
+            L.b = p; p += sz;
+            L.store = p; p += sz;
+            L.tmp = p; p += sz;
+            L.jac = p; p += sz;
+            int st = hb2_jacobi_precon(L.A, mg->prm.omega, L.jac, stream);
+            if (st) return st;
+        }
+        mg->rfine = p;
+        int st = workspace_create(&mg->ws, kMaxReduceBlocks);
+        if (st) return st;
+        mg->norm_dev = mg->ws->scalars + 0;
+        mg->coarse_used_dev = (uint64_t *)(mg->ws->scalars + 1);
+        mg->coarse_def_dev = mg->ws->scalars + 2;
+        HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap, cudaStreamNonBlocking));
+        return HB2_OK;
+    }
+
+    static int mg_finish_create(hb2_mg_s * mg, cudaStream_t stream)
+    {
+        int st = mg_alloc(mg, stream);
+        if (st) return st;
+        HB2_CUDA(cudaStreamSynchronize(stream));
+        // prime the coarse kernel's shared-memory attribute outside the capture
+        MgLevel & C = mg->lev[0];
+        st = launch_cg_small(C.A, C.b, C.x, 0, mg->prm.coarse_eps, mg->prm.coarse_exact, mg->coarse_used_dev,
+                             mg->coarse_def_dev, mg->cap);
+        if (st) return st;
+        HB2_CUDA(cudaStreamSynchronize(mg->cap));
+        return build_graph(mg);
+    }
+
+    static hb2_mg_params default_params()
+    {
+        hb2_mg_params p;
+        p.n_pre_smooth = 4;
+        p.n_post_smooth = 4;
+        p.max_iters = 100;
+        p.max_iters_coarse = 100;
+        p.eps_relative = 1e-10;
+        p.coarse_eps = 1e-10;
+        p.omega = 0.7;
+        p.coarse_exact = 1;
+        return p;
+    }
+
+    static int validate(uint32_t nlev, const hb2_ell * A, const hb2_ell * prol, const hb2_ell * res)
+    {
+        if (nlev < 1 || ! A) return fail(HB2_ERR_ARG, "hb2_mg_create: no levels");
+        for (uint32_t i = 0; i < nlev; ++i)
+        {
+            if (! A[i] || A[i]->rows != A[i]->cols) return fail(HB2_ERR_SIZE, "hb2_mg_create: level matrix not square");
+            if (A[i]->dtype != A[0]->dtype) return fail(HB2_ERR_ARG, "hb2_mg_create: mixed element types");
+            if (i > 0)
+            {
+                const hb2_ell_s * P = prol[i - 1], * R = res[i - 1];
+                if (! P || ! R) return fail(HB2_ERR_ARG, "hb2_mg_create: missing transfer matrix");
+                if (P->rows != A[i]->rows || P->cols != A[i - 1]->rows || R->rows != A[i - 1]->rows || R->cols != A[i]->rows)
+                    return fail(HB2_ERR_SIZE, "hb2_mg_create: MatrixRowsDoNotMatch (transfer vs level sizes)");
+                if (P->dtype != A[0]->dtype || R->dtype != A[0]->dtype) return fail(HB2_ERR_ARG, "hb2_mg_create: mixed element types");
+            }
+        }
+        if (! cg_small_fits(A[0])) return fail(HB2_ERR_UNSUPPORTED, "hb2_mg_create: coarsest level too large for the one-block CG");
+        return HB2_OK;
+    }
+
+    // MGSolver::value on the hierarchy's own finest vectors (b, x already in place)
+    static int solve_internal(hb2_mg_s * mg, double * stats, cudaStream_t stream)
+    {
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        int st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, stream);
+        if (st) return st;
+        HB2_CUDA(cudaMemcpyAsync(mg->ws->host_scalars, mg->norm_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        HB2_CUDA(cudaStreamSynchronize(stream));
+        const double r0 = mg->ws->host_scalars[0];
+        double rc = 1e16;
+        uint64_t used = 0;
+        for (uint64_t i = 0; i < mg->prm.max_iters; ++i)
+        {
+            HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
+            count_launches(mg->graph_kernels);
+            HB2_CUDA(cudaStreamSynchronize(stream));
+            rc = mg->ws->host_scalars[0];
+            used = i + 1;
+            if (rc < mg->prm.eps_relative * r0) break;
+            if (! (rc == rc)) break;
+        }
+        if (stats)
+        {
+            uint64_t cu = 0;
+            HB2_CUDA(cudaMemcpy(&cu, mg->coarse_used_dev, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+            stats[0] = (double)used;
+            stats[1] = r0;
+            stats[2] = rc;
+            stats[3] = (double)cu;
+        }
+        if (! (rc == rc) || ! (r0 == r0)) return fail(HB2_ERR_NOT_FINITE, "MG solve: NaN defect norm");
+        return HB2_OK;
+    }
+}
+
+using namespace hb2;
+
+extern "C" int hb2_mg_create(hb2_mg * out, uint32_t num_levels, const hb2_ell * A, const hb2_ell * prol,
+                             const hb2_ell * res, const hb2_mg_params * params, cudaStream_t stream)
+{
+    if (! out) return fail(HB2_ERR_ARG, "hb2_mg_create: null output");
+    int st = validate(num_levels, A, prol, res);
+    if (st) return st;
+    hb2_mg_s * mg = new hb2_mg_s();
+    mg->dtype = A[0]->dtype;
+    cudaGetDevice(&mg->device);
+    mg->nlev = num_levels;
+    mg->prm = params ? *params : default_params();
+    mg->owns_matrices = false;
+    mg->lev.resize(num_levels);
+    for (uint32_t i = 0; i < num_levels; ++i)
+    {
+        mg->lev[i].A = A[i];
+        mg->lev[i].n = A[i]->rows;
+        if (i > 0) { mg->lev[i].P = prol[i - 1]; mg->lev[i].R = res[i - 1]; }
+    }
+    st = mg_finish_create(mg, stream);
+    if (st) { hb2_mg_destroy(mg); return st; }
+    *out = mg;
+    return HB2_OK;
+}
+
+extern "C" int hb2_mg_create_q1(hb2_mg * out, hb2_dtype dtype, unsigned min_level, unsigned max_level, double aniso,
+                                const hb2_mg_params * params, cudaStream_t stream)
+{
+    if (! out || min_level < 1 || max_level < min_level || max_level > 14) return fail(HB2_ERR_ARG, "hb2_mg_create_q1: bad levels");
+    const uint32_t nlev = max_level - min_level + 1;
+    std::vector<hb2_ell> A(nlev, (hb2_ell)0), P(nlev, (hb2_ell)0), R(nlev, (hb2_ell)0);
+    int st = HB2_OK;
+    for (uint32_t i = 0; i < nlev && ! st; ++i)
+    {
+        st = hb2_ell_create_q1(&A[i], dtype, min_level + i, aniso, stream);
+        if (! st && i > 0) st = hb2_ell_create_transfer(&P[i - 1], &R[i - 1], dtype, min_level + i, stream);
+    }
+    hb2_mg mg = 0;
+    if (! st) st = hb2_mg_create(&mg, nlev, A.data(), P.data(), R.data(), params, stream);
+    if (st)
+    {
+        for (uint32_t i = 0; i < nlev; ++i) { hb2_ell_destroy(A[i]); hb2_ell_destroy(P[i]); hb2_ell_destroy(R[i]); }
+        return st;
+    }
+    mg->owns_matrices = true;
+    *out = mg;
+    return HB2_OK;
+}
+
+extern "C" int hb2_mg_destroy(hb2_mg mg)
+{
+    if (! mg) return HB2_OK;
+    if (mg->exec) cudaGraphExecDestroy(mg->exec);
+    if (mg->graph) cudaGraphDestroy(mg->graph);
+    if (mg->cap) cudaStreamDestroy(mg->cap);
+    if (mg->vec_block) cudaFree(mg->vec_block);
+    workspace_destroy(mg->ws);
+    if (mg->owns_matrices)
+        for (uint32_t i = 0; i < mg->nlev; ++i)
+        {
+            hb2_ell_destroy(mg->lev[i].A);
+            hb2_ell_destroy(mg->lev[i].P);
+            hb2_ell_destroy(mg->lev[i].R);
+        }
+    delete mg;
+    return HB2_OK;
+}
+
+extern "C" int hb2_mg_solve(hb2_mg mg, const void * b, void * x, double * stats, cudaStream_t stream)
+{
+    if (! mg || ! b || ! x) return fail(HB2_ERR_ARG, "hb2_mg_solve: null argument");
+    MgLevel & F = mg->lev[mg->nlev - 1];
+    int st = launch_copy(mg->dtype, F.b, b, F.n, stream);
+    if (! st) st = launch_copy(mg->dtype, F.x, x, F.n, stream);
+    if (st) return st;
+    int solve_st = solve_internal(mg, stats, stream);
+    st = launch_copy(mg->dtype, x, F.x, F.n, stream);
+    if (! st) { cudaError_t e = cudaStreamSynchronize(stream); if (e != cudaSuccess) st = cuda_status(e, "hb2_mg_solve"); }
+    return solve_st ? solve_st : st;
+}
+
+extern "C" int hb2_mg_cycle(hb2_mg mg, const void * b, void * x, cudaStream_t stream)
+{
+    if (! mg || ! b || ! x) return fail(HB2_ERR_ARG, "hb2_mg_cycle: null argument");
+    MgLevel & F = mg->lev[mg->nlev - 1];
+    int st = launch_copy(mg->dtype, F.b, b, F.n, stream);
+    if (! st) st = launch_copy(mg->dtype, F.x, x, F.n, stream);
+    if (st) return st;
+    HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
+    count_launches(mg->graph_kernels);
+    return launch_copy(mg->dtype, x, F.x, F.n, stream);
+}
+
+extern "C" int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void * b, void * x, double eps, uint64_t max_iters,
+                            int reset_inner, double * stats, cudaStream_t stream)
+{
+    if (! A || ! inner || ! b || ! x) return fail(HB2_ERR_ARG, "hb2_ir_solve: null argument");
+    if (A->dtype != HB2_F64) return fail(HB2_ERR_ARG, "hb2_ir_solve: the outer system must be F64");
+    MgLevel & F = inner->lev[inner->nlev - 1];
+    if (F.n != A->rows || A->rows != A->cols) return fail(HB2_ERR_SIZE, "hb2_ir_solve: VectorSizeDoesNotMatch (inner finest level)");
+    Workspace * ws = 0;
+    int st = stream_workspace(stream, &ws);
+    if (st) return st;
+    void * r = 0;
+    HB2_CUDA(cudaMallocAsync(&r, A->rows * 8 + 16, stream));
+    double r0 = 1e16, rc = 1e16;
+    uint64_t used = 0, inner_total = 0;
+    for (uint64_t i = 0; i < max_iters && ! st; ++i)
+    {
+        // Defect<OuterTag>(r, b, A, x) with the norm fused in
+        st = launch_ell(A, kDefect, x, r, b, 0, 0, ws->scalars + 16, 1, ws, stream);
+        if (st) break;
+        cudaError_t e = cudaMemcpyAsync(ws->host_scalars + 16, ws->scalars + 16, sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) { st = cuda_status(e, "hb2_ir_solve"); break; }
+        const double nr = ws->host_scalars[16];
+        if (i == 0) r0 = nr;
+        else
+        {
+            rc = nr;
+            used = i;
+            if (rc < eps * r0) break;
+            if (! (rc == rc)) break;
+        }
+        // convert<OuterTag>(inner b, r); inner MGSolver; convert + Sum
+        st = launch_convert(inner->dtype, F.b, HB2_F64, r, F.n, stream);
+        if (! st && reset_inner) st = launch_fill(inner->dtype, F.x, 0.0, F.n, stream);
+        double ist[4] = {0, 0, 0, 0};
+        if (! st) st = solve_internal(inner, ist, stream);
+        inner_total += (uint64_t)ist[0];
+        if (! st) st = launch_add_converted(x, inner->dtype, F.x, F.n, stream);
+    }
+    cudaFreeAsync(r, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (! st && e != cudaSuccess) st = cuda_status(e, "hb2_ir_solve");
+    if (stats)
+    {
+        stats[0] = (double)used;
+        stats[1] = r0;
+        stats[2] = rc;
+        stats[3] = (double)inner_total;
+    }
+    if (! st && ! (rc == rc)) st = fail(HB2_ERR_NOT_FINITE, "hb2_ir_solve: NaN defect norm");
+    return st;
+}

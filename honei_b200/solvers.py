@@ -1,0 +1,175 @@
+"""HONEI's solver layer for the B200 tag: grid transfer, smoother, CG, MG, IR.
+
+Mirrors math/prolongation.hh, math/restriction.hh, math/ri.hh, math/cg.hh,
+math/mg.hh and math/ir.hh.  Each solver is one call into libhonei_b200.so; the
+MG cycle runs as a captured CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import MgParams, call
+from .la import DenseVector, SparseMatrixELL, _check_size, _stream, _vec, dtype_code
+
+
+class methods:
+    """math/methods.hh"""
+
+    class NONE:
+        pass
+
+    class PROLMAT:
+        pass
+
+
+ALL_DIRICHLET = np.full(8, 2, np.uint64)
+
+
+class Prolongation:
+    """Prolongation<tags::B200, NONE|PROLMAT>::value(fine, coarse, mask, prolmat)."""
+
+    @staticmethod
+    def value(fine, coarse, mask=ALL_DIRICHLET, prolmat=None, method=methods.NONE, stream=None):
+        fine, coarse = _vec(fine), _vec(coarse)
+        if method is methods.PROLMAT:
+            call("hb2_product_ell", prolmat.handle, coarse.ptr, fine.ptr, _stream(stream))
+            return fine
+        m = np.ascontiguousarray(mask, np.uint64)
+        call("hb2_prolongation", fine.dtype, fine.ptr, fine.size(), coarse.ptr, coarse.size(),
+             m.ctypes.data_as(ctypes.c_void_p), _stream(stream))
+        return fine
+
+
+class Restriction:
+    """Restriction<tags::B200, NONE|PROLMAT>::value(coarse, fine, mask, resmat)."""
+
+    @staticmethod
+    def value(coarse, fine, mask=ALL_DIRICHLET, resmat=None, method=methods.NONE, stream=None):
+        fine, coarse = _vec(fine), _vec(coarse)
+        if method is methods.PROLMAT:
+            call("hb2_product_ell", resmat.handle, fine.ptr, coarse.ptr, _stream(stream))
+            return coarse
+        m = np.ascontiguousarray(mask, np.uint64)
+        call("hb2_restriction", coarse.dtype, coarse.ptr, coarse.size(), fine.ptr, fine.size(),
+             m.ctypes.data_as(ctypes.c_void_p), _stream(stream))
+        return coarse
+
+
+class RISmoother:
+    """RISmoother<tags::B200>::value(A, P, b, x, temps, max_iters) (math/ri.hh:97-133)."""
+
+    @staticmethod
+    def value(A, P, b, x, temps=None, max_iters=1, stream=None):
+        P, b, x = _vec(P), _vec(b), _vec(x)
+        _check_size(x.size(), A.columns())
+        tmp = temps[0] if temps else DenseVector(torch.empty_like(x.elements))
+        call("hb2_jacobi_ell", A.handle, P.ptr, b.ptr, x.ptr, _vec(tmp).ptr, int(max_iters), _stream(stream))
+        return x
+
+    @staticmethod
+    def jacobi_precon(A, omega=0.7, stream=None) -> DenseVector:
+        """PreconFill "jac": P = omega / diag(A) (math/mg.hh:266-273)."""
+        P = DenseVector(A.rows(), dtype=torch.float64 if A.dtype == _lib.HB2_F64 else torch.float32)
+        call("hb2_jacobi_precon", A.handle, float(omega), P.ptr, _stream(stream))
+        return P
+
+
+class CGSolver:
+    """CGSolver<tags::B200, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps) (math/cg.hh:64-135).
+
+    Returns (x, used_iters, final_defect)."""
+
+    @staticmethod
+    def value(A, P, b, x, max_iters, eps_relative=1e-8, stream=None):
+        b, x = _vec(b), _vec(x)
+        _check_size(b.size(), A.rows())
+        _check_size(x.size(), A.columns())
+        used = ctypes.c_uint64()
+        defect = ctypes.c_double()
+        call("hb2_cg_solve", A.handle, b.ptr, x.ptr, int(max_iters), float(eps_relative), ctypes.byref(used),
+             ctypes.byref(defect), _stream(stream))
+        return x, used.value, defect.value
+
+
+def mg_params(n_pre=4, n_post=4, max_iters=100, max_iters_coarse=100, eps=1e-10, coarse_eps=None, omega=0.7,
+              coarse_exact=True) -> MgParams:
+    return MgParams(n_pre, n_post, max_iters, max_iters_coarse, eps, eps if coarse_eps is None else coarse_eps,
+                    omega, int(coarse_exact))
+
+
+class MGData:
+    """MGData + the V-cycle OperatorList resident on the device (math/mg.hh:57-240, 567-656).
+
+    ``MGData.poisson_q1(min_level, max_level, ...)`` assembles the Q1 hierarchy on
+    the device; ``MGData(A, prol, res, params)`` takes matrices coarsest first
+    (prol[i] / res[i] connect level i and i+1)."""
+
+    def __init__(self, A=None, prol=None, res=None, params: MgParams | None = None, stream=None, _handle=None):
+        self.params = params or mg_params()
+        self._keep = (A, prol, res)
+        if _handle is not None:
+            self._h = _handle
+        else:
+            n = len(A)
+            arr = (ctypes.c_void_p * n)(*[m.handle.value for m in A])
+            parr = (ctypes.c_void_p * max(1, n - 1))(*[m.handle.value for m in prol])
+            rarr = (ctypes.c_void_p * max(1, n - 1))(*[m.handle.value for m in res])
+            h = ctypes.c_void_p()
+            call("hb2_mg_create", ctypes.byref(h), n, arr, parr, rarr, ctypes.byref(self.params), _stream(stream))
+            self._h = h
+        self.used_iters = 0
+        self.used_iters_coarse = 0
+        self.rnorm_initial = self.rnorm_final = float("nan")
+
+    @classmethod
+    def poisson_q1(cls, min_level, max_level, dtype=torch.float64, aniso=1.0, params: MgParams | None = None,
+                   stream=None):
+        params = params or mg_params()
+        h = ctypes.c_void_p()
+        call("hb2_mg_create_q1", ctypes.byref(h), dtype_code(dtype), min_level, max_level, float(aniso),
+             ctypes.byref(params), _stream(stream))
+        return cls(params=params, _handle=h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.load().hb2_mg_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
+class MGSolver:
+    """MGSolver<tags::B200, Norm<vnt_l_two, true>>::value(data, b, x) (math/mg.hh:1094-1127)."""
+
+    @staticmethod
+    def value(data: MGData, b, x, stream=None):
+        b, x = _vec(b), _vec(x)
+        stats = (ctypes.c_double * 4)()
+        call("hb2_mg_solve", data.handle, b.ptr, x.ptr, stats, _stream(stream))
+        data.used_iters = int(stats[0])
+        data.rnorm_initial, data.rnorm_final = stats[1], stats[2]
+        data.used_iters_coarse = int(stats[3])
+        return x
+
+
+class IRSolver:
+    """IRSolver<B200 FP64, B200 inner, Norm<l2, true>>::value (math/ir.hh:31-80).
+
+    Returns (x, outer_iters, stats[4])."""
+
+    @staticmethod
+    def value(A: SparseMatrixELL, b, x, inner: MGData, eps=1e-10, max_iters=100, reset_inner=False, stream=None):
+        b, x = _vec(b), _vec(x)
+        stats = (ctypes.c_double * 4)()
+        call("hb2_ir_solve", A.handle, inner.handle, b.ptr, x.ptr, float(eps), int(max_iters), int(bool(reset_inner)),
+             stats, _stream(stream))
+        return x, int(stats[0]), list(stats)

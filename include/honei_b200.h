@@ -1,0 +1,236 @@
+/*
+ * honei_b200 -- C ABI of the B200 (sm_100a) backend for HONEI's sparse Poisson
+ * solver path.
+ *
+ * This is the drop-in boundary.  It replaces the old CUDA backend's launcher
+ * table (honei/backends/cuda/operations.hh:29-128) and the tag glue in
+ * honei/la/ *-cuda.cc and honei/math/ *-cuda.cc.  A new HONEI tag (tags::B200,
+ * see INTEGRATION.md) specialises Product, Defect, ScaledSum, DotProduct, Norm,
+ * Sum, Scale, Difference, ElementProduct, copy/fill/convert, Prolongation,
+ * Restriction and the CG / MG / IR solvers with thin shims over these calls.
+ *
+ * Conventions
+ *   - Plain C: pointers, sizes, enums.  No exceptions cross this boundary.
+ *   - Every function returns an int status: HB2_OK (0) or a negative code;
+ *     hb2_last_error() gives the message of the last failure on this thread.
+ *     Size mismatches that the reference reports as VectorSizeDoesNotMatch /
+ *     MatrixRowsDoNotMatch (e.g. la/product.hh:155-162) return
+ *     HB2_ERR_SIZE before anything is launched.
+ *   - Vector arguments are device pointers of the matrix's element type;
+ *     `stream` orders the work (0 = legacy default stream).  Operators are
+ *     asynchronous; functions returning host scalars synchronise `stream`.
+ *   - Reductions are deterministic: the same inputs and sizes give the same
+ *     bits on every run, alone or interleaved with other work.
+ *   - Matrices live on the device in a B200 layout (hb2_ell / hb2_q1 handles),
+ *     built once from the reference's arrays or assembled on the device.
+ */
+#ifndef HONEI_B200_H
+#define HONEI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define HB2_API __attribute__((visibility("default")))
+#else
+#define HB2_API
+#endif
+
+#ifndef __CUDA_RUNTIME_H__
+typedef struct CUstream_st *cudaStream_t;
+#endif
+
+typedef enum
+{
+    HB2_F64 = 0, /* double */
+    HB2_F32 = 1  /* float  */
+} hb2_dtype;
+
+enum
+{
+    HB2_OK = 0,
+    HB2_ERR_ARG = -1,       /* invalid argument / null pointer */
+    HB2_ERR_SIZE = -2,      /* VectorSizeDoesNotMatch / MatrixRowsDoNotMatch */
+    HB2_ERR_CUDA = -3,      /* CUDA runtime error */
+    HB2_ERR_NOMEM = -4,     /* device allocation failed or over budget */
+    HB2_ERR_TIMEOUT = -5,   /* a bounded device-side wait expired */
+    HB2_ERR_UNSUPPORTED = -6,
+    HB2_ERR_NOT_FINITE = -7 /* a solver produced a NaN/Inf norm */
+};
+
+typedef struct hb2_ell_s *hb2_ell; /* SparseMatrixELL<DT> resident on the device */
+typedef struct hb2_q1_s *hb2_q1;   /* BandedMatrixQx<Q1Type, DT> resident on the device */
+typedef struct hb2_mg_s *hb2_mg;   /* MGData + V-cycle OperatorList resident on the device */
+
+/* ---------------------------------------------------------------- runtime */
+HB2_API const char *hb2_last_error(void);
+HB2_API const char *hb2_version(void);
+/* number of kernels this library launched on this host thread since load */
+HB2_API uint64_t hb2_launch_count(void);
+
+/* ---------------------------------------------------------------- matrices */
+/* Upload a SparseMatrixELL in the reference layout (la/sparse_matrix_ell-impl.hh:42-72:
+ * Aj/Ax of num_cols_per_row*stride slots, slot k of row r at (k%T)+r*T+(k/T)*stride,
+ * Arl[r] used slot groups).  Replaces the MemoryArbiter upload of Aj/Ax/Arl that
+ * Product<tags::GPU::CUDA>(DV, SMELL, DV) performs (la/product-cuda.cc:197-231).
+ * host_ptrs != 0: Aj/Ax/Arl are host pointers; else device pointers. */
+HB2_API int hb2_ell_create(hb2_ell *out, hb2_dtype dtype, uint64_t rows, uint64_t cols, uint64_t stride,
+                   uint64_t num_cols_per_row, uint64_t threads, const uint64_t *Aj, const void *Ax,
+                   const uint64_t *Arl, int host_ptrs, cudaStream_t stream);
+/* Assemble on the device the level-L Q1 Poisson operator that
+ * FillMatrix<Tag, POISSON, DIRICHLET_0> (math/fill_matrix.hh:37-79) followed by
+ * SparseMatrixELL(SparseMatrix(BandedMatrixQx)) (la/sparse_matrix_ell-impl.hh:75-122)
+ * produces; aniso != 1 scales the x-coupling (DL/DU) and the diagonal. */
+HB2_API int hb2_ell_create_q1(hb2_ell *out, hb2_dtype dtype, unsigned level, double aniso, cudaStream_t stream);
+/* Assemble on the device P = ProlongationMatrix (level-1 -> level) with identity
+ * index maps (math/prolongation_matrix.hh:44-100) and its transpose R
+ * (math/transposition.hh:36-50), both as ELL. */
+HB2_API int hb2_ell_create_transfer(hb2_ell *prol, hb2_ell *res, hb2_dtype dtype, unsigned fine_level,
+                            cudaStream_t stream);
+/* Same matrix in another element type (values rounded like DT(double)). */
+HB2_API int hb2_ell_convert(hb2_ell *out, hb2_ell src, hb2_dtype dtype, cudaStream_t stream);
+HB2_API int hb2_ell_destroy(hb2_ell A);
+/* rows, cols, reference stride / num_cols_per_row / threads, device bytes */
+HB2_API int hb2_ell_info(hb2_ell A, uint64_t *rows, uint64_t *cols, uint64_t *stride, uint64_t *num_cols_per_row,
+                 uint64_t *threads, uint64_t *device_bytes);
+/* Download the matrix in the reference layout (host arrays of K*stride, K*stride
+ * and rows elements); Arl as the reference computes it. */
+HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);
+
+/* BandedMatrixQx<Q1Type, DT> (la/banded_matrix_qx-impl.hh:45-466): 9 bands of n,
+ * band-major LL LD LU DL DD DU UL UD UU; n must be (2^L+1)^2. */
+HB2_API int hb2_q1_create(hb2_q1 *out, hb2_dtype dtype, uint64_t n, const void *bands, int host_ptrs,
+                  cudaStream_t stream);
+HB2_API int hb2_q1_create_poisson(hb2_q1 *out, hb2_dtype dtype, unsigned level, double aniso, cudaStream_t stream);
+HB2_API int hb2_q1_destroy(hb2_q1 A);
+
+/* ---------------------------------------------------------------- operators */
+/* Product<Tag>::value(y, A, x) on ELL (la/product.hh:148-206; old CUDA launcher
+ * cuda_product_smell_dv_{float,double}, backends/cuda/operations.hh:93-99). */
+HB2_API int hb2_product_ell(hb2_ell A, const void *x, void *y, cudaStream_t stream);
+/* Defect<Tag>::value(r, rhs, A, x) = rhs - A x (math/defect.hh:357-383; old launcher
+ * cuda_defect_smell_dv_*, operations.hh:40-46).  norm2_dev (nullable, device double):
+ * receives ||r||_2^2 computed in the same pass (Norm<vnt_l_two,false>, la/norm.hh:290-305). */
+HB2_API int hb2_defect_ell(hb2_ell A, const void *rhs, const void *x, void *r, double *norm2_dev,
+                   cudaStream_t stream);
+/* y = A x and dot_dev = <y, x> in one pass (the CG step Product + DotProduct, math/cg.hh:97-98) */
+HB2_API int hb2_product_dot_ell(hb2_ell A, const void *x, void *y, double *dot_dev, cudaStream_t stream);
+/* y += A x (Prolongation<PROLMAT> followed by Sum, math/mg.hh:627-629) */
+HB2_API int hb2_product_add_ell(hb2_ell A, const void *x, void *y, cudaStream_t stream);
+/* Product<Tag>(y, BandedMatrixQx<Q1>, x) (la/product.hh:370-403; old launcher
+ * cuda_product_bmdv_q1_*, operations.hh:82-90) and Defect on Q1 (math/defect.hh:194-198;
+ * cuda_defect_q1_*, operations.hh:30-38). */
+HB2_API int hb2_product_q1(hb2_q1 A, const void *x, void *y, cudaStream_t stream);
+HB2_API int hb2_defect_q1(hb2_q1 A, const void *rhs, const void *x, void *r, cudaStream_t stream);
+
+/* BLAS-1 on DenseVector<DT> (n elements, device pointers):
+ *   ScaledSum x += b*y        la/scaled_sum.hh:73-88   (cuda_scaled_sum_*, operations.hh:117-120)
+ *   ScaledSum r = b*y + x     la/scaled_sum.hh:91-110
+ *   Sum x += y                la/sum.hh                (cuda_sum_two_*, operations.hh:125-126)
+ *   Difference x -= y; r = x - y   la/difference.hh    (cuda_difference_*, operations.hh:54-57)
+ *   Scale x *= a              la/scale.hh              (cuda_scale_one_*, operations.hh:122-123)
+ *   ElementProduct r = a (.) b la/element_product.hh / la/product.hh:1198-1204
+ *   fill, copy, convert       la/algorithm.hh:50-86, 370-440, 163-245 (transfer.cu:28-46)
+ * DotProduct / Norm write a device double (nullable) and, when host_out is
+ * non-null, synchronise and store it on the host (la/dot_product.hh:72-89,
+ * la/norm.hh:290-381; the old launchers finished the sum on the host,
+ * backends/cuda/dot_product.cu:101-105). */
+HB2_API int hb2_scaled_sum(hb2_dtype dt, void *x, const void *y, double b, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_scaled_sum3(hb2_dtype dt, void *r, const void *x, const void *y, double b, uint64_t n,
+                    cudaStream_t stream);
+HB2_API int hb2_sum(hb2_dtype dt, void *x, const void *y, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_difference(hb2_dtype dt, void *x, const void *y, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_difference3(hb2_dtype dt, void *r, const void *x, const void *y, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_scale(hb2_dtype dt, void *x, double a, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_element_product(hb2_dtype dt, void *r, const void *a, const void *b, uint64_t n,
+                        cudaStream_t stream);
+HB2_API int hb2_fill(hb2_dtype dt, void *x, double value, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_copy(hb2_dtype dt, void *dst, const void *src, uint64_t n, cudaStream_t stream);
+HB2_API int hb2_convert(hb2_dtype dst_dt, void *dst, hb2_dtype src_dt, const void *src, uint64_t n,
+                cudaStream_t stream);
+HB2_API int hb2_dot(hb2_dtype dt, const void *x, const void *y, uint64_t n, double *dev_out, double *host_out,
+            cudaStream_t stream);
+HB2_API int hb2_norm_l2(hb2_dtype dt, const void *x, uint64_t n, int root, double *dev_out, double *host_out,
+                cudaStream_t stream);
+
+/* ---------------------------------------------------------------- grid transfer */
+/* Matrix-free Prolongation<Tag, NONE> (math/prolongation.hh:42-139) and
+ * Restriction<Tag, NONE> (math/restriction.hh:41-173), each followed by
+ * ApplyDirichletBoundaries with the 8-entry mask (host array; 2 = Dirichlet,
+ * math/apply_dirichlet_boundaries.hh:29-84).  Old launchers:
+ * cuda_prolongation_* / cuda_restriction_* (operations.hh:101-111).
+ * Bit-identical to the reference (same summation order per node). */
+HB2_API int hb2_prolongation(hb2_dtype dt, void *fine, uint64_t n_fine, const void *coarse, uint64_t n_coarse,
+                     const uint64_t *mask, cudaStream_t stream);
+HB2_API int hb2_restriction(hb2_dtype dt, void *coarse, uint64_t n_coarse, const void *fine, uint64_t n_fine,
+                    const uint64_t *mask, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- solvers */
+/* RISmoother<Tag>::value(A, P, b, x, temps, iters) (math/ri.hh:110-133): `sweeps`
+ * damped-Jacobi sweeps x += P (.) (b - A x), fused into one pass per sweep.
+ * tmp: device vector of A.rows (ping-pong buffer). */
+HB2_API int hb2_jacobi_ell(hb2_ell A, const void *P, const void *b, void *x, void *tmp, uint64_t sweeps,
+                   cudaStream_t stream);
+/* One sweep of RISmoother (math/ri.hh:125-129) into a separate output:
+ * x_out = x_in + P (.) (b - A x_in), one fused pass (no copy). */
+HB2_API int hb2_jacobi_sweep_ell(hb2_ell A, const void *P, const void *b, const void *x_in, void *x_out,
+                                 cudaStream_t stream);
+/* P = omega / diag(A): PreconFill "jac" (math/mg.hh:266-273) */
+HB2_API int hb2_jacobi_precon(hb2_ell A, double omega, void *P, cudaStream_t stream);
+
+/* CGSolver<Tag, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps)
+ * (math/cg.hh:64-135): unpreconditioned CG with the reference's relative-or-
+ * absolute stop sqrt(r.r) < eps*||r0|| or < eps.  One cooperative launch per
+ * solve; all scalars stay on the device.  final_defect: sqrt(r.r) at exit.
+ * Synchronises `stream`. */
+HB2_API int hb2_cg_solve(hb2_ell A, const void *b, void *x, uint64_t max_iters, double eps, uint64_t *used_iters,
+                 double *final_defect, cudaStream_t stream);
+
+/* MG hierarchy: MGData (math/mg.hh:57-240) + MGCycleCreation<V::STATIC,
+ * CGSolver<NONE>, RISmoother, Restriction<PROLMAT>, Prolongation<PROLMAT>>
+ * (math/mg.hh:567-656), captured once as a CUDA graph.  Levels are given
+ * coarsest first: A[0..nlev-1]; prol[i], res[i] connect level i and i+1
+ * (i = 0..nlev-2).  Jacobi P = omega/diag(A) per level.  The handle keeps
+ * references to the matrices (they must outlive it) and owns its vectors. */
+typedef struct
+{
+    uint64_t n_pre_smooth, n_post_smooth;   /* 4, 4 */
+    uint64_t max_iters;                     /* MG cycles */
+    uint64_t max_iters_coarse;              /* coarse CG iterations */
+    double eps_relative;                    /* MG stop: ||r|| < eps * ||r0|| */
+    double coarse_eps;                      /* coarse CG eps (reference: = eps_relative) */
+    double omega;                           /* Jacobi damping, 0.7 */
+    int coarse_exact;                       /* 1: coarse CG dots in the reference's sequential fma order */
+} hb2_mg_params;
+
+HB2_API int hb2_mg_create(hb2_mg *out, uint32_t num_levels, const hb2_ell *A, const hb2_ell *prol, const hb2_ell *res,
+                  const hb2_mg_params *params, cudaStream_t stream);
+/* Q1 Poisson hierarchy min_level..max_level assembled on the device */
+HB2_API int hb2_mg_create_q1(hb2_mg *out, hb2_dtype dtype, unsigned min_level, unsigned max_level, double aniso,
+                     const hb2_mg_params *params, cudaStream_t stream);
+HB2_API int hb2_mg_destroy(hb2_mg mg);
+/* MGSolver<Tag, Norm<vnt_l_two, true>>::value(data, cycle) (math/mg.hh:1094-1127):
+ * b, x: finest-level device vectors (x = initial guess in, solution out).
+ * stats (nullable, host, 4 doubles): used_iters, ||r0||, ||r_final||, coarse iters
+ * of the last cycle.  Synchronises `stream`. */
+HB2_API int hb2_mg_solve(hb2_mg mg, const void *b, void *x, double *stats, cudaStream_t stream);
+/* one V-cycle on the finest level (OperatorList::value, math/operator_list.hh:69-76) */
+HB2_API int hb2_mg_cycle(hb2_mg mg, const void *b, void *x, cudaStream_t stream);
+
+/* IRSolver<OuterTag, InnerTag, Norm> (math/ir.hh:31-80): FP64 outer defect, norm
+ * and update around an inner MG solve on `inner` (an F32 or F64 hierarchy whose
+ * finest level matches A).  reset_inner = 0 keeps the reference's behaviour
+ * (inner initial guess carried over); 1 restarts it from zero each outer step.
+ * stats (nullable, host, 4 doubles): outer iters, ||r0||, ||r_final||, total
+ * inner cycles.  Synchronises `stream`. */
+HB2_API int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void *b, void *x, double eps, uint64_t max_iters,
+                 int reset_inner, double *stats, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,257 @@
+"""ctypes access to the CPU oracle (oracle/liboracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of bench.py
+import this module, and only as the checker or the timed CPU baseline.  The
+product (``honei_b200``) never imports it.  Every function mirrors the C
+restatement in honei_oracle.c, which cites the reference file:line it follows.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "honei_ref")
+
+_u64 = ctypes.c_uint64
+_dbl = ctypes.c_double
+_ptr = ctypes.c_void_p
+
+
+def build(force: bool = False) -> str:
+    """Compile honei_oracle.c into liboracle.so (no FMA contraction)."""
+    src = os.path.join(HERE, "honei_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-std=c99", "-O2", "-ffp-contract=off", "-fPIC", "-shared",
+                               "-o", LIB_PATH, src, "-lm"])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        L = _lib
+        L.hbo_uniform.restype = _dbl
+        L.hbo_uniform.argtypes = [_u64, _u64, _dbl, _dbl]
+        L.hbo_q1_m.restype = _u64
+        L.hbo_q1_n.restype = _u64
+        L.hbo_q1_csr_f64.restype = _u64
+        L.hbo_q1_csr_f32.restype = _u64
+        L.hbo_prolmat_csr_f64.restype = _u64
+        L.hbo_dot_f64.restype = _dbl
+        L.hbo_dot_f64.argtypes = [_u64, _ptr, _ptr]
+        L.hbo_cg_q1_f64.restype = _u64
+        L.hbo_cg_q1_f64.argtypes = [ctypes.c_uint, _dbl, _ptr, _ptr, _u64, _dbl]
+        L.hbo_jacobi_q1_f64.argtypes = [ctypes.c_uint, _dbl, _dbl, _ptr, _ptr, _u64]
+        for sfx in ("f64", "f32"):
+            f = getattr(L, "hbo_mg_q1_" + sfx)
+            f.restype = _u64
+            f.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
+                          _ptr, _ptr, _ptr]
+        L.hbo_ir_q1.restype = _u64
+        L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
+                                _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _sfx(dtype) -> str:
+    return {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32"}[np.dtype(dtype)]
+
+
+def q1_m(L: int) -> int:
+    return (1 << L) + 1
+
+
+def q1_n(L: int) -> int:
+    return q1_m(L) ** 2
+
+
+def uniform(n: int, seed: int, dtype=np.float64, lo=-1.0, hi=1.0) -> np.ndarray:
+    out = np.empty(n, dtype=dtype)
+    getattr(lib(), "hbo_uniform_fill_" + _sfx(dtype))(_p(out), _u64(n), _u64(seed), _dbl(lo), _dbl(hi))
+    return out
+
+
+def q1_bands(L: int, dtype=np.float64, aniso: float = 1.0) -> np.ndarray:
+    """9 x n bands LL LD LU DL DD DU UL UD UU of FillMatrix<POISSON, DIRICHLET_0>."""
+    n = q1_n(L)
+    out = np.empty((9, n), dtype=dtype)
+    getattr(lib(), "hbo_q1_bands_" + _sfx(dtype))(ctypes.c_uint(L), _dbl(aniso), _p(out))
+    return out
+
+
+def q1_csr(L: int, dtype=np.float64, aniso: float = 1.0):
+    n = q1_n(L)
+    bands = q1_bands(L, dtype, aniso)
+    rp = np.empty(n + 1, np.uint64)
+    ci = np.empty(9 * n, np.uint64)
+    v = np.empty(9 * n, dtype)
+    nnz = getattr(lib(), "hbo_q1_csr_" + _sfx(dtype))(ctypes.c_uint(L), _p(bands), _p(rp), _p(ci), _p(v))
+    return rp, ci[:nnz].copy(), v[:nnz].copy()
+
+
+class Ell:
+    """Reference ELL arrays: Aj (uint64), Ax, Arl (uint64), stride, K, T."""
+
+    def __init__(self, rows, cols, stride, K, T, Aj, Ax, Arl):
+        self.rows, self.cols, self.stride, self.K, self.T = int(rows), int(cols), int(stride), int(K), int(T)
+        self.Aj, self.Ax, self.Arl = Aj, Ax, Arl
+
+    @property
+    def dtype(self):
+        return self.Ax.dtype
+
+
+def ell_from_csr(rows, cols, rp, ci, v, T: int = 1) -> Ell:
+    stride = _u64()
+    K = _u64()
+    lib().hbo_ell_dims(_u64(rows), _p(rp), _u64(T), ctypes.byref(stride), ctypes.byref(K))
+    Aj = np.empty(K.value * stride.value, np.uint64)
+    Ax = np.empty(K.value * stride.value, v.dtype)
+    Arl = np.empty(rows, np.uint64)
+    getattr(lib(), "hbo_ell_from_csr_" + _sfx(v.dtype))(
+        _u64(rows), _p(rp), _p(ci), _p(v), _u64(T), stride, K, _p(Aj), _p(Ax), _p(Arl))
+    return Ell(rows, cols, stride.value, K.value, T, Aj, Ax, Arl)
+
+
+def q1_ell(L: int, dtype=np.float64, T: int = 1, aniso: float = 1.0) -> Ell:
+    n = q1_n(L)
+    rp, ci, v = q1_csr(L, dtype, aniso)
+    return ell_from_csr(n, n, rp, ci, v, T)
+
+
+def prolmat_csr(Lf: int):
+    nf = q1_n(Lf)
+    rp = np.empty(nf + 1, np.uint64)
+    ci = np.empty(4 * nf, np.uint64)
+    v = np.empty(4 * nf, np.float64)
+    nnz = lib().hbo_prolmat_csr_f64(ctypes.c_uint(Lf), _p(rp), _p(ci), _p(v))
+    return rp, ci[:nnz].copy(), v[:nnz].copy()
+
+
+def transfer_ell(Lf: int, dtype=np.float64):
+    """(P, R) as ELL: P = ProlongationMatrix(Lf <- Lf-1), R = Transposition(P)."""
+    nf, nc = q1_n(Lf), q1_n(Lf - 1)
+    rp, ci, v = prolmat_csr(Lf)
+    nnz = len(ci)
+    rpt = np.empty(nc + 1, np.uint64)
+    cit = np.empty(nnz, np.uint64)
+    vt = np.empty(nnz, np.float64)
+    lib().hbo_csr_transpose_f64(_u64(nf), _u64(nc), _p(rp), _p(ci), _p(v), _p(rpt), _p(cit), _p(vt))
+    P = ell_from_csr(nf, nc, rp, ci, v.astype(dtype))
+    R = ell_from_csr(nc, nf, rpt, cit, vt.astype(dtype))
+    return P, R
+
+
+def ell_spmv(A: Ell, x: np.ndarray) -> np.ndarray:
+    y = np.empty(A.rows, A.dtype)
+    getattr(lib(), "hbo_ell_spmv_" + _sfx(A.dtype))(
+        _u64(A.rows), _u64(A.stride), _u64(A.T), _p(A.Aj), _p(A.Ax), _p(A.Arl), _p(np.ascontiguousarray(x)), _p(y))
+    return y
+
+
+def ell_defect(A: Ell, rhs: np.ndarray, x: np.ndarray) -> np.ndarray:
+    r = np.empty(A.rows, A.dtype)
+    getattr(lib(), "hbo_ell_defect_" + _sfx(A.dtype))(
+        _u64(A.rows), _u64(A.stride), _u64(A.T), _p(A.Aj), _p(A.Ax), _p(A.Arl), _p(rhs), _p(x), _p(r))
+    return r
+
+
+def ell_row_length(A: Ell) -> np.ndarray:
+    Arl = np.empty(A.rows, np.uint64)
+    lib().hbo_ell_row_length_f64(_u64(A.rows), _u64(A.stride), _u64(A.K), _u64(A.T), _p(A.Ax), _p(Arl))
+    return Arl
+
+
+def q1_spmv(bands: np.ndarray, x: np.ndarray) -> np.ndarray:
+    n = bands.shape[1]
+    m = int(round(n ** 0.5))
+    y = np.empty(n, bands.dtype)
+    getattr(lib(), "hbo_q1_spmv_" + _sfx(bands.dtype))(_u64(n), _u64(m), _p(bands), _p(x), _p(y))
+    return y
+
+
+def q1_defect(bands: np.ndarray, rhs: np.ndarray, x: np.ndarray) -> np.ndarray:
+    n = bands.shape[1]
+    m = int(round(n ** 0.5))
+    r = np.empty(n, bands.dtype)
+    getattr(lib(), "hbo_q1_defect_" + _sfx(bands.dtype))(_u64(n), _u64(m), _p(bands), _p(rhs), _p(x), _p(r))
+    return r
+
+
+def dot(x: np.ndarray, y: np.ndarray) -> float:
+    if x.dtype == np.float64:
+        return lib().hbo_dot_f64(_u64(len(x)), _p(x), _p(y))
+    f = lib().hbo_dot_f32
+    f.restype = ctypes.c_float
+    return f(_u64(len(x)), _p(x), _p(y))
+
+
+ALL_DIRICHLET = np.full(8, 2, np.uint64)
+
+
+def prolongation(coarse: np.ndarray, n_fine: int, mask=ALL_DIRICHLET) -> np.ndarray:
+    fine = np.empty(n_fine, coarse.dtype)
+    mask = np.ascontiguousarray(mask, np.uint64)
+    getattr(lib(), "hbo_prolongation_" + _sfx(coarse.dtype))(_u64(n_fine), _p(fine), _u64(len(coarse)),
+                                                              _p(coarse), _p(mask))
+    return fine
+
+
+def restriction(fine: np.ndarray, n_coarse: int, mask=ALL_DIRICHLET) -> np.ndarray:
+    coarse = np.empty(n_coarse, fine.dtype)
+    mask = np.ascontiguousarray(mask, np.uint64)
+    getattr(lib(), "hbo_restriction_" + _sfx(fine.dtype))(_u64(n_coarse), _p(coarse), _u64(len(fine)),
+                                                           _p(fine), _p(mask))
+    return coarse
+
+
+def cg_q1(L: int, b: np.ndarray, x0=None, max_iters=2000, eps=1e-8, aniso=1.0):
+    x = np.zeros(q1_n(L)) if x0 is None else np.array(x0, np.float64)
+    it = lib().hbo_cg_q1_f64(L, aniso, _p(b), _p(x), max_iters, eps)
+    return x, int(it)
+
+
+def jacobi_q1(L: int, b: np.ndarray, x0, sweeps: int, omega=0.7, aniso=1.0):
+    x = np.array(x0, np.float64)
+    lib().hbo_jacobi_q1_f64(L, aniso, omega, _p(b), _p(x), sweeps)
+    return x
+
+
+def mg_q1(max_level: int, b: np.ndarray, x0=None, min_level=3, omega=0.7, n_pre=4, n_post=4, max_iters=100,
+          max_iters_coarse=1000, eps=1e-10, coarse_eps=None, aniso=1.0):
+    """MG V-cycle solver; returns (x, used_iters, stats[4])."""
+    dtype = b.dtype
+    x = np.zeros(q1_n(max_level), dtype) if x0 is None else np.array(x0, dtype)
+    stats = np.zeros(4)
+    f = getattr(lib(), "hbo_mg_q1_" + _sfx(dtype))
+    it = f(min_level, max_level, aniso, omega, n_pre, n_post, max_iters, max_iters_coarse, eps,
+           eps if coarse_eps is None else coarse_eps, _p(b), _p(x), _p(stats))
+    return x, int(it), stats
+
+
+def ir_q1(max_level: int, b: np.ndarray, x0=None, min_level=3, omega=0.7, n_pre=4, n_post=4, max_inner=100,
+          max_iters_coarse=1000, inner_eps=1e-3, coarse_eps=None, max_outer=100, eps=1e-10, reset_inner=False,
+          aniso=1.0):
+    """FP64-outer / FP32-inner-MG iterative refinement; returns (x, outer_iters, stats[4])."""
+    x = np.zeros(q1_n(max_level)) if x0 is None else np.array(x0, np.float64)
+    stats = np.zeros(4)
+    it = lib().hbo_ir_q1(min_level, max_level, aniso, omega, n_pre, n_post, max_inner, max_iters_coarse, inner_eps,
+                         inner_eps if coarse_eps is None else coarse_eps, max_outer, eps, int(reset_inner),
+                         _p(b), _p(x), _p(stats))
+    return x, int(it), stats

@@ -1,0 +1,430 @@
+// Driver around the reference implementation's own CPU path (test infrastructure
+// only; compiled with the reference sources by oracle/ref.mk into oracle/_ref/).
+//
+//   honei_ref golden <outdir>
+//       writes golden fixtures computed by the reference's tags::CPU code
+//       (raw little-endian arrays + scalars.txt); tests/golden/make_golden.py
+//       packs them into the committed fixtures.
+//   honei_ref bench <cg|mg|ir|spmv> <cpu|generic|sse|mc> <level> <reps> [warmup]
+//       times the solve phase (operator setup excluded; `warmup` untimed solves
+//       first) and prints one "RESULT {json}" line.  The thread count of the MultiCore tag comes from
+//       the honeirc named by $HONEI_CONFIG (mc::num_threads).
+#include "ref_common.hh"
+
+#include <honei/la/dot_product.hh>
+#include <honei/la/norm.hh>
+#include <honei/la/product.hh>
+#include <honei/la/scaled_sum.hh>
+#include <honei/la/sum.hh>
+#include <honei/math/cg.hh>
+#include <honei/math/defect.hh>
+#include <honei/math/ir.hh>
+#include <honei/math/mg.hh>
+#include <honei/math/prolongation.hh>
+#include <honei/math/restriction.hh>
+#include <honei/math/ri.hh>
+#include <honei/util/configuration.hh>
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <algorithm>
+
+using namespace honei;
+using namespace hbref;
+
+namespace
+{
+    std::ofstream scalars;
+    std::string outdir;
+    // coarse CG iteration cap of the timed MG solves: the value the reference's
+    // own MG tests use (math/mg_TEST.cc:421); overridable with $HONEI_COARSE_CAP
+    unsigned long coarse_cap = 100;
+
+    template <typename DT_>
+    void put_vec(const std::string & name, const DenseVector<DT_> & v)
+    {
+        write_raw(outdir + "/" + name, v.elements(), v.size());
+    }
+
+    template <typename DT_>
+    void put_ell(const std::string & name, const SparseMatrixELL<DT_> & A)
+    {
+        put_vec(name + ".Aj", A.Aj());
+        put_vec(name + ".Ax", A.Ax());
+        put_vec(name + ".Arl", A.Arl());
+        scalars << name << ".rows " << A.rows() << "\n" << name << ".cols " << A.columns() << "\n"
+                << name << ".stride " << A.stride() << "\n" << name << ".K " << A.num_cols_per_row() << "\n"
+                << name << ".T " << A.threads() << "\n";
+    }
+
+    std::string key(const char * fmt, unsigned a, const char * b = "")
+    {
+        char buf[128];
+        snprintf(buf, sizeof buf, fmt, a, b);
+        return buf;
+    }
+
+    // MGData over levels 1..L (internal index = level - 1), V(n_pre, n_post),
+    // Jacobi preconditioner "jac" (math/mg.hh:255-288), PROLMAT transfers.
+    template <typename DT_>
+    struct Hierarchy
+    {
+        std::vector<SparseMatrixELL<DT_> > A, Res, Prol;
+        std::vector<DenseVector<DT_> > P, b, x, d, c, store;
+        std::vector<std::vector<DenseVector<DT_> > > temps;
+
+        Hierarchy(unsigned L, double omega, bool assembled, double aniso = 1.0)
+        {
+            for (unsigned l(1); l <= L; ++l)
+            {
+                SparseMatrixELL<DT_> Al(assembled ? q1_ell_assembled<DT_>(l) : q1_ell_fast<DT_>(l, aniso));
+                A.push_back(Al);
+                DenseVector<DT_> Pl(Al.rows(), DT_(omega));
+                for (unsigned long j(0); j < Pl.size(); ++j)
+                    Pl[j] /= Al(j, j);
+                P.push_back(Pl);
+                if (l >= 2)
+                {
+                    SparseMatrixELL<DT_> * p, * r;
+                    if (assembled) transfer_assembled<DT_>(l, p, r); else transfer_fast<DT_>(l, p, r);
+                    Prol.push_back(*p);
+                    Res.push_back(*r);
+                    delete p;
+                    delete r;
+                }
+                DenseVector<DT_> z(Al.rows(), DT_(0));
+                b.push_back(z.copy());
+                x.push_back(z.copy());
+                d.push_back(z.copy());
+                c.push_back(z.copy());
+                store.push_back(z.copy());
+                temps.push_back(std::vector<DenseVector<DT_> >());
+            }
+        }
+
+        MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_>
+        data(unsigned long max_iters, unsigned long max_iters_coarse, unsigned long n_pre, unsigned long n_post,
+             unsigned long min_level, DT_ eps)
+        {
+            return MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_>(
+                    A, Res, Prol, P, b, x, d, c, store, temps, max_iters, max_iters_coarse, n_pre, n_post,
+                    min_level, eps);
+        }
+    };
+
+    template <typename Tag_, typename DT_>
+    OperatorList v_cycle(MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_> & data)
+    {
+        return MGCycleCreation<Tag_, methods::CYCLE::V::STATIC, CGSolver<Tag_, methods::NONE>, RISmoother<Tag_>,
+               Restriction<Tag_, methods::PROLMAT>, Prolongation<Tag_, methods::PROLMAT>, DT_>::value(data);
+    }
+
+    double rel_residual(const SparseMatrixELL<double> & A, const DenseVector<double> & b, const DenseVector<double> & x)
+    {
+        DenseVector<double> r(b.size());
+        Defect<tags::CPU>::value(r, b, A, x);
+        return Norm<vnt_l_two, true, tags::CPU>::value(r) / Norm<vnt_l_two, true, tags::CPU>::value(b);
+    }
+
+    // ---------------------------------------------------------------- golden
+    int golden()
+    {
+        scalars.open((outdir + "/scalars.txt").c_str());
+        scalars.precision(17);
+
+        // ELL assembly, T = 1 (and T = 2, 3 through the ell::threads key)
+        for (unsigned L(1); L <= 8; ++L)
+        {
+            put_ell(key("ell_L%u_T1_f64", L), q1_ell_assembled<double>(L));
+            if (L <= 6) put_ell(key("ell_L%u_T1_f32", L), q1_ell_assembled<float>(L));
+        }
+        for (unsigned T(2); T <= 3; ++T)
+        {
+            Configuration::instance()->set_value("ell::threads", int(T));
+            for (unsigned L(2); L <= 4; ++L)
+            {
+                char nm[64];
+                snprintf(nm, sizeof nm, "ell_L%u_T%u_f64", L, T);
+                SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+                put_ell(nm, A);
+                DenseVector<double> xv(uniform<double>(A.columns(), 7)), yv(A.rows());
+                Product<tags::CPU>::value(yv, A, xv);
+                snprintf(nm, sizeof nm, "spmv_L%u_T%u_f64", L, T);
+                put_vec(nm, yv);
+            }
+        }
+        Configuration::instance()->set_value("ell::threads", 1);
+
+        // grid transfer matrices
+        for (unsigned L(2); L <= 8; ++L)
+        {
+            SparseMatrixELL<double> * P, * R;
+            transfer_assembled<double>(L, P, R);
+            put_ell(key("prol_L%u_f64", L), *P);
+            put_ell(key("res_L%u_f64", L), *R);
+            delete P;
+            delete R;
+        }
+
+        // SpMV / defect on ELL and on the banded Q1 matrix
+        for (unsigned L(1); L <= 7; ++L)
+        {
+            SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+            DenseVector<double> xv(uniform<double>(A.columns(), 7)), rhs(uniform<double>(A.rows(), 11));
+            DenseVector<double> y(A.rows()), r(A.rows());
+            Product<tags::CPU>::value(y, A, xv);
+            Defect<tags::CPU>::value(r, rhs, A, xv);
+            put_vec(key("spmv_L%u_f64", L), y);
+            put_vec(key("defect_L%u_f64", L), r);
+
+            SparseMatrixELL<float> Af(q1_ell_assembled<float>(L));
+            DenseVector<float> xf(uniform<float>(A.columns(), 7)), rf(uniform<float>(A.rows(), 11));
+            DenseVector<float> yf(A.rows()), df(A.rows());
+            Product<tags::CPU>::value(yf, Af, xf);
+            Defect<tags::CPU>::value(df, rf, Af, xf);
+            put_vec(key("spmv_L%u_f32", L), yf);
+            put_vec(key("defect_L%u_f32", L), df);
+
+            BandedMatrixQx<Q1Type, double> Q(q1_banded<double>(L));
+            DenseVector<double> yq(A.rows()), rq(A.rows());
+            Product<tags::CPU>::value(yq, Q, xv);
+            Defect<tags::CPU>::value(rq, rhs, Q, xv);
+            put_vec(key("q1spmv_L%u_f64", L), yq);
+            put_vec(key("q1defect_L%u_f64", L), rq);
+        }
+
+        // BLAS-1 on seeded vectors (n = 1000)
+        {
+            DenseVector<double> a(uniform<double>(1000, 21)), b(uniform<double>(1000, 22));
+            scalars << "dot_1000_f64 " << DotProduct<tags::CPU>::value(a, b) << "\n";
+            scalars << "norm2sq_1000_f64 " << Norm<vnt_l_two, false, tags::CPU>::value(a) << "\n";
+            scalars << "norm2_1000_f64 " << Norm<vnt_l_two, true, tags::CPU>::value(a) << "\n";
+            DenseVector<double> s1(a.copy());
+            ScaledSum<tags::CPU>::value(s1, b, 0.375);
+            put_vec("scaledsum2_1000_f64", s1);
+            DenseVector<double> s2(1000);
+            ScaledSum<tags::CPU>::value(s2, a, b, -1.25);
+            put_vec("scaledsum3_1000_f64", s2);
+        }
+
+        // matrix-free and PROLMAT grid transfer outputs (mask: all Dirichlet)
+        for (unsigned L(2); L <= 7; ++L)
+        {
+            unsigned long nf(hbo_q1_n(L)), nc(hbo_q1_n(L - 1));
+            DenseVector<unsigned long> mask(8, 2ul);
+            DenseVector<double> coarse(uniform<double>(nc, 31)), fine(uniform<double>(nf, 32));
+            DenseVector<double> pf(nf), rc(nc), pfm(nf), rcm(nc);
+            SparseMatrixELL<double> * P, * R;
+            transfer_assembled<double>(L, P, R);
+            Prolongation<tags::CPU, methods::NONE>::value(pf, coarse, mask, *P);
+            Restriction<tags::CPU, methods::NONE>::value(rc, fine, mask, *R);
+            Prolongation<tags::CPU, methods::PROLMAT>::value(pfm, coarse, mask, *P);
+            Restriction<tags::CPU, methods::PROLMAT>::value(rcm, fine, mask, *R);
+            put_vec(key("prolong_L%u_f64", L), pf);
+            put_vec(key("restrict_L%u_f64", L), rc);
+            put_vec(key("prolmat_L%u_f64", L), pfm);
+            put_vec(key("resmat_L%u_f64", L), rcm);
+            delete P;
+            delete R;
+        }
+
+        // CG, FP64, b = A u*, x0 = 0, rel. tol 1e-8 (config 0 shape at L = 5, 7)
+        for (unsigned L(5); L <= 7; L += 2)
+        {
+            SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+            DenseVector<double> u(uniform<double>(A.rows(), 42)), b(A.rows()), x(A.rows(), 0.0);
+            Product<tags::CPU>::value(b, A, u);
+            unsigned long used(0);
+            DenseVector<double> dummy(1);
+            CGSolver<tags::CPU, methods::NONE>::value(A, dummy, b, x, 2000ul, used, 1e-8);
+            scalars << key("cg_L%u.iters", L) << " " << used << "\n";
+            scalars << key("cg_L%u.relres", L) << " " << rel_residual(A, b, x) << "\n";
+            put_vec(key("cg_L%u.x", L), x);
+            put_vec(key("cg_L%u.b", L), b);
+        }
+
+        // Jacobi smoothing: 4 sweeps, omega 0.7, from x = 0
+        for (unsigned L(3); L <= 6; ++L)
+        {
+            SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+            DenseVector<double> P(A.rows(), 0.7);
+            for (unsigned long j(0); j < P.size(); ++j) P[j] /= A(j, j);
+            DenseVector<double> b(uniform<double>(A.rows(), 5)), x(A.rows(), 0.0);
+            std::vector<DenseVector<double> > temps;
+            temps.push_back(DenseVector<double>(A.rows()));
+            temps.push_back(DenseVector<double>(A.rows()));
+            RISmoother<tags::CPU>::value(A, P, b, x, temps, 4);
+            put_vec(key("jacobi_L%u_f64", L), x);
+        }
+
+        // MG V(4,4), omega 0.7, coarse CG on level 3, eps 1e-10 shared with the coarse CG
+        for (unsigned L(5); L <= 7; ++L)
+        {
+            Hierarchy<double> h(L, 0.7, true);
+            DenseVector<double> u(uniform<double>(h.A.back().rows(), 42));
+            Product<tags::CPU>::value(h.b.back(), h.A.back(), u);
+            MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
+                data(h.data(100, 1000, 4, 4, 3, 1e-10));
+            OperatorList cycle(v_cycle<tags::CPU, double>(data));
+            MGSolver<tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(data, cycle);
+            scalars << key("mg_L%u.iters", L) << " " << data.used_iters << "\n";
+            scalars << key("mg_L%u.coarse_iters", L) << " " << data.used_iters_coarse << "\n";
+            scalars << key("mg_L%u.relres", L) << " " << rel_residual(h.A.back(), h.b.back(), data.x.back()) << "\n";
+            put_vec(key("mg_L%u.x", L), data.x.back());
+        }
+
+        // MG FP32 at level 6, eps 1e-5
+        {
+            Hierarchy<float> h(6, 0.7, true);
+            DenseVector<float> u(uniform<float>(h.A.back().rows(), 42));
+            Product<tags::CPU>::value(h.b.back(), h.A.back(), u);
+            MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
+                data(h.data(100, 1000, 4, 4, 3, 1e-5f));
+            OperatorList cycle(v_cycle<tags::CPU, float>(data));
+            MGSolver<tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(data, cycle);
+            scalars << "mg32_L6.iters " << data.used_iters << "\n";
+            put_vec("mg32_L6.x", data.x.back());
+        }
+
+        // IR: FP64 outer (eps 1e-10), FP32 inner MG V(4,4) with eps 1e-3 (shared with the coarse CG)
+        for (unsigned L(5); L <= 6; ++L)
+        {
+            SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+            DenseVector<double> u(uniform<double>(A.rows(), 42)), b(A.rows()), x(A.rows(), 0.0);
+            Product<tags::CPU>::value(b, A, u);
+            Hierarchy<float> h(L, 0.7, true);
+            MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
+                data(h.data(100, 1000, 4, 4, 3, 1e-3f));
+            OperatorList cycle(v_cycle<tags::CPU, float>(data));
+            unsigned long used(0);
+            IRSolver<tags::CPU, tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(A, b, x, data, cycle, 1e-10, 100ul, used);
+            scalars << key("ir_L%u.iters", L) << " " << used << "\n";
+            scalars << key("ir_L%u.relres", L) << " " << rel_residual(A, b, x) << "\n";
+            put_vec(key("ir_L%u.x", L), x);
+        }
+        scalars.close();
+        return 0;
+    }
+
+    // ---------------------------------------------------------------- bench
+    template <typename Tag_>
+    int bench(const std::string & which, unsigned L, unsigned reps, unsigned warmup, const char * tagname)
+    {
+        std::vector<double> times;
+        double t_setup0(now());
+        double secs(0), relres(0);
+        unsigned long iters(0);
+        if (which == "cg")
+        {
+            SparseMatrixELL<double> A(q1_ell_fast<double>(L));
+            DenseVector<double> u(uniform<double>(A.rows(), 42)), b(A.rows());
+            Product<tags::CPU>::value(b, A, u);
+            DenseVector<double> dummy(1);
+            double setup(now() - t_setup0);
+            for (unsigned r(0); r < reps; ++r)
+            {
+                DenseVector<double> x(A.rows(), 0.0);
+                double t0(now());
+                CGSolver<Tag_, methods::NONE>::value(A, dummy, b, x, 2000ul, iters, 1e-8);
+                secs += now() - t0;
+                relres = rel_residual(A, b, x);
+            }
+            printf("RESULT {\"which\": \"cg\", \"tag\": \"%s\", \"level\": %u, \"reps\": %u, \"seconds_per_solve\": %.6g, "
+                   "\"iters\": %lu, \"relres\": %.6g, \"setup_s\": %.3g}\n", tagname, L, reps, secs / reps, iters, relres, setup);
+        }
+        else if (which == "mg")
+        {
+            Hierarchy<double> h(L, 0.7, false);
+            DenseVector<double> u(uniform<double>(h.A.back().rows(), 42));
+            Product<tags::CPU>::value(h.b.back(), h.A.back(), u);
+            double setup(now() - t_setup0);
+            for (unsigned r(0); r < reps + warmup; ++r)
+            {
+                for (unsigned long i(0); i < h.x.back().size(); ++i) h.x.back()[i] = 0.0;
+                MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
+                    data(h.data(100, coarse_cap, 4, 4, 3, 1e-10));
+                OperatorList cycle(v_cycle<Tag_, double>(data));
+                double t0(now());
+                MGSolver<Tag_, Norm<vnt_l_two, true, Tag_> >::value(data, cycle);
+                if (r >= warmup) { secs += now() - t0; times.push_back(now() - t0); }
+                iters = data.used_iters;
+                relres = rel_residual(h.A.back(), h.b.back(), data.x.back());
+            }
+            std::sort(times.begin(), times.end());
+            printf("RESULT {\"which\": \"mg\", \"tag\": \"%s\", \"level\": %u, \"reps\": %u, \"seconds_per_solve\": %.6g, "
+                   "\"min_s\": %.6g, \"max_s\": %.6g, \"iters\": %lu, \"relres\": %.6g, \"setup_s\": %.3g, "
+                   "\"coarse_cap\": %lu}\n", tagname, L, reps, secs / reps, times.front(), times.back(), iters, relres,
+                   setup, coarse_cap);
+        }
+        else if (which == "ir")
+        {
+            SparseMatrixELL<double> A(q1_ell_fast<double>(L));
+            DenseVector<double> u(uniform<double>(A.rows(), 42)), b(A.rows());
+            Product<tags::CPU>::value(b, A, u);
+            Hierarchy<float> h(L, 0.7, false);
+            double setup(now() - t_setup0);
+            for (unsigned r(0); r < reps; ++r)
+            {
+                for (unsigned long i(0); i < h.x.back().size(); ++i) h.x.back()[i] = 0.f;
+                DenseVector<double> x(A.rows(), 0.0);
+                MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
+                    data(h.data(100, 1000, 4, 4, 3, 1e-3f));
+                OperatorList cycle(v_cycle<Tag_, float>(data));
+                double t0(now());
+                IRSolver<Tag_, Tag_, Norm<vnt_l_two, true, Tag_> >::value(A, b, x, data, cycle, 1e-10, 100ul, iters);
+                secs += now() - t0;
+                relres = rel_residual(A, b, x);
+            }
+            printf("RESULT {\"which\": \"ir\", \"tag\": \"%s\", \"level\": %u, \"reps\": %u, \"seconds_per_solve\": %.6g, "
+                   "\"iters\": %lu, \"relres\": %.6g, \"setup_s\": %.3g}\n", tagname, L, reps, secs / reps, iters, relres, setup);
+        }
+        else if (which == "spmv")
+        {
+            SparseMatrixELL<double> A(q1_ell_fast<double>(L));
+            DenseVector<double> x(uniform<double>(A.rows(), 7)), y(A.rows());
+            double setup(now() - t_setup0);
+            Product<Tag_>::value(y, A, x);
+            double t0(now());
+            for (unsigned r(0); r < reps; ++r)
+                Product<Tag_>::value(y, A, x);
+            secs = now() - t0;
+            printf("RESULT {\"which\": \"spmv\", \"tag\": \"%s\", \"level\": %u, \"reps\": %u, \"seconds_per_spmv\": %.6g, "
+                   "\"setup_s\": %.3g}\n", tagname, L, reps, secs / reps, setup);
+        }
+        else
+        {
+            fprintf(stderr, "unknown benchmark '%s'\n", which.c_str());
+            return 2;
+        }
+        fflush(stdout);
+        return 0;
+    }
+}
+
+int main(int argc, char ** argv)
+{
+    if (argc >= 3 && std::string(argv[1]) == "golden")
+    {
+        outdir = argv[2];
+        return golden();
+    }
+    if (argc >= 6 && std::string(argv[1]) == "bench")
+    {
+        if (getenv("HONEI_COARSE_CAP")) coarse_cap = strtoul(getenv("HONEI_COARSE_CAP"), 0, 10);
+        std::string which(argv[2]), tag(argv[3]);
+        unsigned L(atoi(argv[4])), reps(atoi(argv[5])), warmup(argc > 6 ? atoi(argv[6]) : 0);
+        if (reps == 0) reps = 1;
+        if (tag == "cpu") return bench<tags::CPU>(which, L, reps, warmup, "cpu");
+        if (tag == "generic") return bench<tags::CPU::Generic>(which, L, reps, warmup, "generic");
+        if (tag == "sse") return bench<tags::CPU::SSE>(which, L, reps, warmup, "sse");
+        if (tag == "mc") return bench<tags::CPU::MultiCore::SSE>(which, L, reps, warmup, "mc");
+        fprintf(stderr, "unknown tag '%s'\n", tag.c_str());
+        return 2;
+    }
+    fprintf(stderr, "usage: %s golden <outdir> | bench <cg|mg|ir|spmv> <cpu|generic|sse|mc> <level> <reps>\n", argv[0]);
+    return 2;
+}

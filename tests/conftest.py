@@ -1,0 +1,73 @@
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); parity tests through the C ABI")
+
+
+def pytest_collection_modifyitems(config, items):
+    try:
+        import torch
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        have_gpu = False
+    if have_gpu:
+        return
+    skip = pytest.mark.skip(reason="no CUDA device in this environment")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)
+
+
+class Golden:
+    """Fixtures produced by the reference's own tags::CPU code (tests/golden/make_golden.py)."""
+
+    def __init__(self):
+        with open(os.path.join(GOLDEN, "reference_cpu.json")) as f:
+            meta = json.load(f)
+        self.scalars = meta["scalars"]
+        self.digests = meta["digests"]
+        self.full = dict(np.load(os.path.join(GOLDEN, "reference_cpu.npz")))
+
+    def has(self, name):
+        return name in self.digests
+
+    def matches(self, name, arr) -> bool:
+        """bit-exact comparison: full array when stored, else SHA-256 of the raw bytes"""
+        d = self.digests[name]
+        arr = np.ascontiguousarray(arr, dtype=np.dtype(d["dtype"]))
+        if arr.size != d["size"]:
+            return False
+        if name in self.full:
+            return np.array_equal(arr.view(np.uint8), self.full[name].view(np.uint8))
+        return hashlib.sha256(arr.tobytes()).hexdigest() == d["sha256"]
+
+    def array(self, name):
+        return self.full[name]
+
+    def scalar(self, key):
+        return self.scalars[key]
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return Golden()
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as o
+    o.lib()
+    return o
