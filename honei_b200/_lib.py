@@ -75,6 +75,7 @@ SIGNATURES = {
     "hb2_q1_destroy": (_int, [_vp]),
     "hb2_product_ell": (_int, [_vp, _vp, _vp, _vp]),
     "hb2_defect_ell": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "hb2_defect_ell_noalloc": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "hb2_product_dot_ell": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "hb2_product_add_ell": (_int, [_vp, _vp, _vp, _vp]),
     "hb2_product_q1": (_int, [_vp, _vp, _vp, _vp]),

@@ -1,0 +1,93 @@
+// hb2_defect_ell_noalloc: the fused defect + squared-norm pass without any
+// device allocation.
+//
+// hb2_defect_ell reduces ||r||^2 through per-block partial sums and a ticket
+// counter that live in a workspace the library allocates with cudaMalloc the
+// first time a stream is used.  Some callers cannot allow that allocation:
+// code that runs under a hard device-memory budget where every byte is
+// reserved up front, or a latency-critical loop where a cudaMalloc would stall
+// the device.  This entry point keeps the reduction scratch in a fixed
+// file-scope device array instead, so it allocates nothing.
+//
+// Limits and sharing:
+//  * the scratch holds kNoAllocMaxBlocks block partials, so the matrix may have
+//    at most kNoAllocMaxBlocks * 512 rows in FP64 (8,388,608) and
+//    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216); larger matrices are
+//    rejected with HB2_ERR_UNSUPPORTED before anything is launched;
+//  * every GPU that loads the library holds the array (about 128 KiB) until the
+//    process exits;
+//  * all calls on a device share the one array: calls whose kernels overlap on
+//    the GPU (different streams without ordering between them) race on it and
+//    give wrong norms.  Calls ordered on one stream are safe;
+//  * the first call on a device looks up the array's device address with
+//    cudaGetSymbolAddress (with that device current) and caches it; make that
+//    first call before any stream capture on that device.
+#include "hb2_common.cuh"
+#include "hb2_internal.hh"
+
+#include <mutex>
+
+namespace hb2
+{
+    constexpr uint32_t kNoAllocMaxBlocks = 16384;
+    constexpr int kNoAllocMaxDevices = 64;
+
+    // [0, kNoAllocMaxBlocks) doubles: block partials; then the ticket counter.
+    static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + 32];
+
+    static std::mutex g_noalloc_mutex;
+    static void * g_noalloc_addr[kNoAllocMaxDevices];
+
+    // Device address of g_noalloc_scratch on the current device.  In host code
+    // the symbol's name is only a host-side stand-in, never a device address.
+    static int noalloc_scratch(double ** out)
+    {
+        int dev = 0;
+        HB2_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: device ordinal out of range");
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (! g_noalloc_addr[dev])
+        {
+            void * p = 0;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_status(e, "hb2_defect_ell_noalloc: cudaGetSymbolAddress");
+            g_noalloc_addr[dev] = p;
+        }
+        *out = (double *)g_noalloc_addr[dev];
+        return HB2_OK;
+    }
+}
+
+using namespace hb2;
+
+extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * x, void * r, double * norm2_dev,
+                                      cudaStream_t stream)
+{
+    if (! A || ! norm2_dev) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null matrix or norm output");
+    if (A->rows != A->cols) return fail(HB2_ERR_SIZE, "hb2_defect_ell_noalloc: VectorSizeDoesNotMatch (rhs vs columns)");
+    if (A->rows > 0 && (! rhs || ! x || ! r)) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null vector");
+    const uint64_t rows_per_block = (uint64_t)kEllThreads *
+                                    (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
+    const uint64_t max_rows = (uint64_t)kNoAllocMaxBlocks * rows_per_block;
+    if (A->rows > max_rows)
+        return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: " + std::to_string(A->rows) +
+                    " rows exceed the static scratch limit of " + std::to_string(max_rows) +
+                    " rows for this element type; use hb2_defect_ell");
+    double * scratch = 0;
+    int st = noalloc_scratch(&scratch);
+    if (st) return st;
+    // the ticket must start at zero; the previous call's contents are otherwise
+    // left as they were (the partials are written before they are read)
+    unsigned * ticket = (unsigned *)(scratch + kNoAllocMaxBlocks);
+    HB2_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), stream));
+    Workspace ws;
+    ws.device = 0;
+    ws.partials = scratch;
+    ws.ticket = ticket;
+    ws.bar_words = 0;
+    ws.error = 0;
+    ws.scalars = 0;
+    ws.max_blocks = kNoAllocMaxBlocks;
+    ws.host_scalars = 0;
+    return launch_ell(A, kDefect, x, r, rhs, 0, 0, norm2_dev, 0, &ws, stream);
+}

@@ -117,6 +117,20 @@ HB2_API int hb2_product_ell(hb2_ell A, const void *x, void *y, cudaStream_t stre
  * receives ||r||_2^2 computed in the same pass (Norm<vnt_l_two,false>, la/norm.hh:290-305). */
 HB2_API int hb2_defect_ell(hb2_ell A, const void *rhs, const void *x, void *r, double *norm2_dev,
                    cudaStream_t stream);
+/* Defect with the fused ||r||_2^2 like hb2_defect_ell, but allocating nothing:
+ * no counterpart in the reference.  For callers that must not allocate device
+ * memory (a hard device-memory budget with every byte reserved up front, or a
+ * latency-critical loop where a cudaMalloc would stall the device):
+ * hb2_defect_ell's reduction workspace is cudaMalloc'd on first use of a stream,
+ * this variant keeps the reduction scratch in a fixed file-scope device array
+ * (about 128 KiB per GPU that loads the library, held until exit).  norm2_dev
+ * is required.  Limit: at most 8,388,608 rows in F64 and 16,777,216 in F32;
+ * larger matrices return HB2_ERR_UNSUPPORTED before any launch.  All calls on a
+ * device share the array, so calls that overlap on the GPU race; calls ordered on
+ * one stream are safe.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it: make it before any stream capture. */
+HB2_API int hb2_defect_ell_noalloc(hb2_ell A, const void *rhs, const void *x, void *r, double *norm2_dev,
+                                   cudaStream_t stream);
 /* y = A x and dot_dev = <y, x> in one pass (the CG step Product + DotProduct, math/cg.hh:97-98) */
 HB2_API int hb2_product_dot_ell(hb2_ell A, const void *x, void *y, double *dot_dev, cudaStream_t stream);
 /* y += A x (Prolongation<PROLMAT> followed by Sum, math/mg.hh:627-629) */
