@@ -1,0 +1,103 @@
+"""Per-kernel timing of the hot kernels on one Q1 level.
+
+    python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong]
+                                      [--level 10] [--iters 20] [--dtype f64|f32]
+
+Each launch is preceded by an L2 flush (256 MiB write) and timed alone with CUDA
+events on the launching stream; the line reports the mean launch time and the
+algorithmic bandwidth (bytes per row as in the design notes) against the
+measured HBM peak.  The first launch of each kernel is a warm-up.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+
+import torch
+
+from . import _lib
+from .inputs import uniform
+from .la import BandedMatrixQx, DenseVector, SparseMatrixELL
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def peak_gbs() -> float:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel", default="all")
+    ap.add_argument("--level", type=int, default=10)
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    a = ap.parse_args(argv)
+    dt = torch.float64 if a.dtype == "f64" else torch.float32
+    s = 8 if a.dtype == "f64" else 4
+    import numpy as np
+    npdt = np.float64 if a.dtype == "f64" else np.float32
+    dev = torch.device("cuda")
+    L = a.level
+    n = ((1 << L) + 1) ** 2
+    nc = ((1 << (L - 1)) + 1) ** 2
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+
+    def vec(m, seed):
+        return DenseVector(torch.from_numpy(uniform(m, seed, dtype=npdt)).to(dev))
+
+    A = SparseMatrixELL.poisson_q1(L, dt)
+    x, b, y, y2 = vec(n, 1), vec(n, 2), vec(n, 3), vec(n, 4)
+    _lib.call("hb2_product_ell", A.handle, x.ptr, b.ptr, stream)        # b = A x (setup)
+    P = DenseVector(n, dtype=dt)
+    _lib.call("hb2_jacobi_precon", A.handle, 0.7, P.ptr, stream)
+    nrm = torch.zeros(1, dtype=torch.float64, device=dev)
+    kernels = {
+        "jacobi": (lambda: _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, b.ptr, x.ptr, y.ptr, stream),
+                   n * (9 * (s + 4) + 4 * s)),
+        "spmv": (lambda: _lib.call("hb2_product_ell", A.handle, x.ptr, y.ptr, stream), n * (9 * (s + 4) + 2 * s)),
+        "defect": (lambda: _lib.call("hb2_defect_ell", A.handle, b.ptr, x.ptr, y.ptr,
+                                     ctypes.c_void_p(nrm.data_ptr()), stream), n * (9 * (s + 4) + 3 * s)),
+    }
+    if a.kernel in ("all", "q1"):
+        Q = BandedMatrixQx.poisson_q1(L, dt)
+        kernels["q1"] = (lambda: _lib.call("hb2_product_q1", Q.handle, x.ptr, y.ptr, stream), n * (9 * s + 2 * s))
+    if a.kernel in ("all", "restrict", "prolong"):
+        Pm, Rm = SparseMatrixELL.transfer(L, dt)
+        c = vec(nc, 5)
+        kernels["restrict"] = (lambda: _lib.call("hb2_product_ell", Rm.handle, x.ptr, c.ptr, stream),
+                               nc * (9 * (s + 4) + s) + n * s)
+        kernels["prolong"] = (lambda: _lib.call("hb2_product_add_ell", Pm.handle, c.ptr, y2.ptr, stream),
+                              n * (4 * (s + 4) + 2 * s) + nc * s)
+    names = list(kernels) if a.kernel == "all" else [a.kernel]
+    peak = peak_gbs()
+    for name in names:
+        fn, nbytes = kernels[name]
+        times = []
+        for i in range(a.iters + 1):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            if i > 0:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.mean(times)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "launch_us": 1000 * ms,
+                          "algorithmic_bytes": nbytes, "gbs": gbs, "frac_of_measured_peak": gbs / peak}),
+              flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
