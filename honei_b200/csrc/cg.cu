@@ -154,6 +154,268 @@ namespace hb2
         }
     }
 
+    // ------------------------------------------------------------------ one warp
+    // Latency-bound coarse solves (the MG coarsest level has 81 unknowns and runs
+    // a hundred iterations per V-cycle): one warp, no block barriers, reductions
+    // by shuffles.  The reference-order dot is one fma chain in lane 0 with the
+    // operands fetched ahead of the chain.
+    template <typename T>
+    __device__ __forceinline__ T warp_dot_exact(const T * a, const T * b, int n)
+    {
+        T s = T(0);
+        if ((threadIdx.x & 31) == 0)
+        {
+            int i = 0;
+            for (; i + 8 <= n; i += 8)
+            {
+                T a0 = a[i], a1 = a[i + 1], a2 = a[i + 2], a3 = a[i + 3], a4 = a[i + 4], a5 = a[i + 5], a6 = a[i + 6],
+                  a7 = a[i + 7];
+                T b0 = b[i], b1 = b[i + 1], b2 = b[i + 2], b3 = b[i + 3], b4 = b[i + 4], b5 = b[i + 5], b6 = b[i + 6],
+                  b7 = b[i + 7];
+                s = Arith<T>::fma(a0, b0, s);
+                s = Arith<T>::fma(a1, b1, s);
+                s = Arith<T>::fma(a2, b2, s);
+                s = Arith<T>::fma(a3, b3, s);
+                s = Arith<T>::fma(a4, b4, s);
+                s = Arith<T>::fma(a5, b5, s);
+                s = Arith<T>::fma(a6, b6, s);
+                s = Arith<T>::fma(a7, b7, s);
+            }
+            for (; i < n; ++i) s = Arith<T>::fma(a[i], b[i], s);
+        }
+        return __shfl_sync(0xffffffffu, s, 0);
+    }
+
+    template <typename T>
+    __device__ __forceinline__ T warp_dot_tree(const T * a, const T * b, int n)
+    {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < n; i += 32) s = fma((double)a[i], (double)b[i], s);
+        return (T)warp_sum(s);   // xor butterfly: every lane ends with the same bits
+    }
+
+    template <typename T>
+    __global__ void __launch_bounds__(32)
+    cg_warp_kernel(EllView<T> Ag, const T * __restrict__ b, T * __restrict__ xg, uint64_t max_iters, double eps_d,
+                   int exact, int mat_in_smem, uint64_t * used_out, double * defect_out)
+    {
+        typedef Arith<T> M;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        const int n = (int)Ag.rows, lane = threadIdx.x;
+        T * x = (T *)smem_raw;
+        T * r = x + n;
+        T * p = r + n;
+        T * v = p + n;
+        SmallMat<T> A;
+        if (mat_in_smem)
+        {
+            T * sval = v + n;
+            int32_t * scol = (int32_t *)(sval + (size_t)Ag.K * n);
+            for (uint32_t k = 0; k < Ag.K; ++k)
+                for (int i = lane; i < n; i += 32)
+                {
+                    sval[k * n + i] = Ag.val[(uint64_t)k * Ag.ld + i];
+                    scol[k * n + i] = Ag.col[(uint64_t)k * Ag.ld + i];
+                }
+            A.val = sval;
+            A.col = scol;
+            A.ld = n;
+        }
+        else
+        {
+            A.val = Ag.val;
+            A.col = Ag.col;
+            A.ld = Ag.ld;
+        }
+        for (int i = lane; i < n; i += 32) x[i] = xg[i];
+        __syncwarp();
+        for (int i = lane; i < n; i += 32)
+        {
+            T d = M::sub(b[i], row_product(A, Ag.K, i, x));
+            r[i] = d;
+            p[i] = d;
+        }
+        __syncwarp();
+        const T eps = T(eps_d);
+        T alpha = exact ? warp_dot_exact(r, r, n) : warp_dot_tree(r, r, n);
+        const T initial = sqrt(alpha);
+        T current = initial;
+        uint64_t it = 0, used = 0;
+        while (it < max_iters)
+        {
+            for (int i = lane; i < n; i += 32) v[i] = row_product(A, Ag.K, i, p);
+            __syncwarp();
+            const T temp = exact ? warp_dot_exact(v, p, n) : warp_dot_tree(v, p, n);
+            const T lambda = M::div(alpha, guard(temp));
+            const T mlambda = -lambda;
+            for (int i = lane; i < n; i += 32)
+            {
+                x[i] = M::add(x[i], M::mul(lambda, p[i]));
+                r[i] = M::add(r[i], M::mul(mlambda, v[i]));
+            }
+            __syncwarp();
+            const T alpha_old = alpha;
+            alpha = exact ? warp_dot_exact(r, r, n) : warp_dot_tree(r, r, n);
+            const T talpha = M::div(alpha, guard(alpha_old));
+            for (int i = lane; i < n; i += 32) p[i] = M::add(M::mul(p[i], talpha), r[i]);
+            __syncwarp();
+            ++it;
+            current = sqrt(alpha);
+            if (current < M::mul(eps, initial) || current < eps) { used = it; break; }
+            if (it == max_iters) used = it;
+        }
+        for (int i = lane; i < n; i += 32) xg[i] = x[i];
+        if (lane == 0)
+        {
+            if (used_out) *used_out = used;
+            if (defect_out) *defect_out = (double)current;
+        }
+    }
+
+    // Register-resident variant for the smallest systems (n <= 32 * RPL, K = 9):
+    // each lane keeps its RPL rows of A and of x, r, p, v in registers; only p
+    // (gathered by the SpMV) and, for the reference-order dots, the dot operands
+    // go through shared memory.
+    template <typename T, int RPL>
+    __global__ void __launch_bounds__(32)
+    cg_warp_reg_kernel(EllView<T> Ag, const T * __restrict__ b, T * __restrict__ xg, uint64_t max_iters, double eps_d,
+                       int exact, uint64_t * used_out, double * defect_out)
+    {
+        typedef Arith<T> M;
+        constexpr int K = 9;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        const int n = (int)Ag.rows, lane = threadIdx.x;
+        T * sp = (T *)smem_raw;   // p (and x for the initial defect)
+        T * sa = sp + n;          // first dot operand (exact mode)
+        T * sb = sa + n;          // second dot operand (exact mode)
+        T av[RPL][K];
+        int ac[RPL][K];
+        T xr[RPL], rr[RPL], pr[RPL], vr[RPL];
+#pragma unroll
+        for (int j = 0; j < RPL; ++j)
+        {
+            const int row = lane + 32 * j;
+            const bool ok = row < n;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+            {
+                av[j][k] = ok ? Ag.val[(uint64_t)k * Ag.ld + row] : T(0);
+                ac[j][k] = ok ? Ag.col[(uint64_t)k * Ag.ld + row] : -1;
+            }
+            xr[j] = ok ? xg[row] : T(0);
+            if (ok) sp[row] = xr[j];
+        }
+        __syncwarp();
+        auto spmv = [&](T (&out)[RPL]) {
+#pragma unroll
+            for (int j = 0; j < RPL; ++j)
+            {
+                T s = T(0);
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    if (ac[j][k] >= 0) s = M::add(s, M::mul(av[j][k], sp[ac[j][k]]));
+                out[j] = s;
+            }
+        };
+        // dot of per-lane register vectors a, b over the valid rows
+        auto dot = [&](const T (&a)[RPL], const T (&bb)[RPL]) -> T {
+            if (exact)
+            {
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                {
+                    const int row = lane + 32 * j;
+                    if (row < n) { sa[row] = a[j]; sb[row] = bb[j]; }
+                }
+                __syncwarp();
+                T s = warp_dot_exact(sa, sb, n);
+                __syncwarp();
+                return s;
+            }
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j)
+                if (lane + 32 * j < n) s = fma((double)a[j], (double)bb[j], s);
+            return (T)warp_sum(s);
+        };
+        T tmp[RPL];
+        spmv(tmp);
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < RPL; ++j)
+        {
+            const int row = lane + 32 * j;
+            rr[j] = row < n ? M::sub(b[row], tmp[j]) : T(0);
+            pr[j] = rr[j];
+            if (row < n) sp[row] = pr[j];
+        }
+        __syncwarp();
+        const T eps = T(eps_d);
+        T alpha = dot(rr, rr);
+        const T initial = sqrt(alpha);
+        T current = initial;
+        uint64_t it = 0, used = 0;
+        while (it < max_iters)
+        {
+            spmv(vr);
+            const T temp = dot(vr, pr);
+            const T lambda = M::div(alpha, guard(temp));
+            const T mlambda = -lambda;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j)
+            {
+                xr[j] = M::add(xr[j], M::mul(lambda, pr[j]));
+                rr[j] = M::add(rr[j], M::mul(mlambda, vr[j]));
+            }
+            const T alpha_old = alpha;
+            alpha = dot(rr, rr);
+            const T talpha = M::div(alpha, guard(alpha_old));
+            __syncwarp();   // every lane is done gathering the old p
+#pragma unroll
+            for (int j = 0; j < RPL; ++j)
+            {
+                const int row = lane + 32 * j;
+                pr[j] = M::add(M::mul(pr[j], talpha), rr[j]);
+                if (row < n) sp[row] = pr[j];
+            }
+            __syncwarp();
+            ++it;
+            current = sqrt(alpha);
+            if (current < M::mul(eps, initial) || current < eps) { used = it; break; }
+            if (it == max_iters) used = it;
+        }
+#pragma unroll
+        for (int j = 0; j < RPL; ++j)
+            if (lane + 32 * j < n) xg[lane + 32 * j] = xr[j];
+        if (lane == 0)
+        {
+            if (used_out) *used_out = used;
+            if (defect_out) *defect_out = (double)current;
+        }
+    }
+
+    template <typename T>
+    static bool launch_warp_reg(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
+                                uint64_t * used_dev, double * defect_dev, cudaStream_t stream)
+    {
+        if (A->K != 9 || A->rows > 128) return false;
+        const int rpl = (int)((A->rows + 31) / 32);
+        const size_t smem = 3 * A->rows * sizeof(T) + 16;
+        EllView<T> v = A->view<T>();
+        const T * bp = (const T *)b;
+        T * xp = (T *)x;
+        switch (rpl)
+        {
+            case 1: cg_warp_reg_kernel<T, 1><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 2: cg_warp_reg_kernel<T, 2><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 3: cg_warp_reg_kernel<T, 3><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            default: cg_warp_reg_kernel<T, 4><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+        }
+        return true;
+    }
+
+    constexpr uint64_t kWarpCgMaxRows = 1024;
+
     static size_t small_smem(const hb2_ell_s * A, bool with_matrix)
     {
         size_t es = dtype_size(A->dtype), n = A->rows;
@@ -181,7 +443,30 @@ namespace hb2
         {
             HB2_CUDA(cudaFuncSetAttribute(cg_small_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemLimit + 64));
             HB2_CUDA(cudaFuncSetAttribute(cg_small_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemLimit + 64));
+            HB2_CUDA(cudaFuncSetAttribute(cg_warp_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemLimit + 64));
+            HB2_CUDA(cudaFuncSetAttribute(cg_warp_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemLimit + 64));
             attr_set = true;
+        }
+        const bool reg = A->dtype == HB2_F64
+                             ? launch_warp_reg<double>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream)
+                             : launch_warp_reg<float>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream);
+        if (reg)
+        {
+            count_launches(1);
+            HB2_LAUNCH_CHECK("cg_warp_reg_kernel");
+            return HB2_OK;
+        }
+        if (A->rows <= kWarpCgMaxRows)
+        {
+            if (A->dtype == HB2_F64)
+                cg_warp_kernel<double><<<1, 32, smem, stream>>>(A->view<double>(), (const double *)b, (double *)x,
+                                                                max_iters, eps, exact, mat, used_dev, defect_dev);
+            else
+                cg_warp_kernel<float><<<1, 32, smem, stream>>>(A->view<float>(), (const float *)b, (float *)x,
+                                                               max_iters, eps, exact, mat, used_dev, defect_dev);
+            count_launches(1);
+            HB2_LAUNCH_CHECK("cg_warp_kernel");
+            return HB2_OK;
         }
         if (A->dtype == HB2_F64)
         {

@@ -34,21 +34,21 @@ namespace hb2
     union ILoad { typename Vec<double>::I v2; int4 v4; int a[R]; };
 
     template <typename T, int R>
-    __device__ __forceinline__ void load_slot(const T * val, const int32_t * col, T (&v)[R], int (&c)[R])
+    __device__ __forceinline__ void load_slot(const T * val, const int32_t * col, T (&v)[R], int (&c)[R], bool keep)
     {
         VLoad<T, R> lv;
-        lv.v = __ldcs((const typename Vec<T>::V *)val);
+        lv.v = keep ? __ldcg((const typename Vec<T>::V *)val) : __ldcs((const typename Vec<T>::V *)val);
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = lv.a[i];
         if (R == 2)
         {
-            int2 t = __ldcs((const int2 *)col);
+            int2 t = keep ? __ldcg((const int2 *)col) : __ldcs((const int2 *)col);
             c[0] = t.x;
             c[1] = t.y;
         }
         else
         {
-            int4 t = __ldcs((const int4 *)col);
+            int4 t = keep ? __ldcg((const int4 *)col) : __ldcs((const int4 *)col);
             c[0] = t.x;
             if (R > 1) c[1] = t.y;
             if (R > 2) c[2] = t.z;
@@ -60,11 +60,14 @@ namespace hb2
     template <typename T, int KT, int MODE>
     __global__ void __launch_bounds__(kEllThreads)
     ell_kernel(EllView<T> A, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ aux,
-               const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt)
+               const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt,
+               int flags)
     {
         constexpr int R = RowsPerThread<T>::value;
         typedef Arith<T> M;
-        const uint64_t r0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * R;
+        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x;
+        const bool keep = (flags & kKeepL2) != 0;
+        const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
         const int K = KT > 0 ? KT : (int)A.K;
         T acc[R];
 #pragma unroll
@@ -73,15 +76,32 @@ namespace hb2
         {
             const T * vp = A.val + r0;
             const int32_t * cp = A.col + r0;
-#pragma unroll(KT > 0 ? KT : 1)
-            for (int k = 0; k < K; ++k)
+            if constexpr (KT > 0)
             {
-                T v[R];
-                int c[R];
-                load_slot<T, R>(vp + (uint64_t)k * A.ld, cp + (uint64_t)k * A.ld, v, c);
+                // issue every slot load of the thread before the first gather:
+                // K * 24 (FP64) / K * 32 (FP32) bytes in flight per thread
+                T v[KT][R];
+                int c[KT][R];
 #pragma unroll
-                for (int i = 0; i < R; ++i)
-                    if (c[i] >= 0) acc[i] = M::add(acc[i], M::mul(v[i], __ldg(x + c[i])));
+                for (int k = 0; k < KT; ++k)
+                    load_slot<T, R>(vp + (uint64_t)k * A.ld, cp + (uint64_t)k * A.ld, v[k], c[k], keep);
+#pragma unroll
+                for (int k = 0; k < KT; ++k)
+#pragma unroll
+                    for (int i = 0; i < R; ++i)
+                        if (c[k][i] >= 0) acc[i] = M::add(acc[i], M::mul(v[k][i], __ldg(x + c[k][i])));
+            }
+            else
+            {
+                for (int k = 0; k < K; ++k)
+                {
+                    T v[R];
+                    int c[R];
+                    load_slot<T, R>(vp + (uint64_t)k * A.ld, cp + (uint64_t)k * A.ld, v, c, keep);
+#pragma unroll
+                    for (int i = 0; i < R; ++i)
+                        if (c[i] >= 0) acc[i] = M::add(acc[i], M::mul(v[i], __ldg(x + c[i])));
+                }
             }
         }
         double part = 0.0;
@@ -116,40 +136,41 @@ namespace hb2
 
     template <typename T, int MODE>
     static void launch_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
-                            void * zero, double * red, int want_sqrt, ReduceSlot rs, unsigned grid, cudaStream_t s)
+                            void * zero, double * red, int want_sqrt, ReduceSlot rs, unsigned grid, cudaStream_t s,
+                            int flags)
     {
         EllView<T> v = A->view<T>();
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         if (A->K == 9)
             ell_kernel<T, 9, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt);
+                                                                (T *)zero, rs, red, want_sqrt, flags);
         else if (A->K == 4)
             ell_kernel<T, 4, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt);
+                                                                (T *)zero, rs, red, want_sqrt, flags);
         else
             ell_kernel<T, 0, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt);
+                                                                (T *)zero, rs, red, want_sqrt, flags);
     }
 
     template <typename T>
     static void launch_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                              const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs,
-                             unsigned grid, cudaStream_t s)
+                             unsigned grid, cudaStream_t s, int f)
     {
         switch (mode)
         {
-            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
-            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
-            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
-            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
-            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
-            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s); break;
+            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
         }
     }
 
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
-                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream)
+                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags)
     {
         if (A->rows == 0)
         {
@@ -169,8 +190,8 @@ namespace hb2
             if (grid > ws->max_blocks) return fail(HB2_ERR_UNSUPPORTED, "matrix too large for the reduction workspace");
             rs = ws->slot();
         }
-        if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream);
-        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream);
+        if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags);
+        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags);
         count_launches(1);
         HB2_LAUNCH_CHECK("ell kernel launch");
         return HB2_OK;

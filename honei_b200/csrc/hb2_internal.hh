@@ -81,11 +81,22 @@ namespace hb2
         kRestrict = 5   // y = A x, zero[0..rows) = 0
     };
 
+    // Pass flags of the ELL family: kReverse walks the row blocks from the end
+    // (consecutive passes over one matrix in alternating directions start where
+    // the previous pass left its lines in L2); kKeepL2 caches the matrix stream
+    // in L2 (ld.cg) instead of marking it evict-first (ld.cs).
+    enum EllFlags
+    {
+        kReverse = 1,
+        kKeepL2 = 2
+    };
+
     // Launch one ELL kernel on `stream`.  aux: rhs / b; aux2: Jacobi P; zero:
     // vector cleared by kRestrict; red: device double receiving the fused
     // reduction (nullable, kDefect / kDot); ws: workspace for the reduction.
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
-                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream);
+                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream,
+                   int flags = 0);
 
     // BLAS-1 helpers (blas1.cu) usable from other translation units.
     int launch_fill(int dt, void * x, double value, uint64_t n, cudaStream_t stream);

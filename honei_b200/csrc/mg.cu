@@ -11,7 +11,11 @@
 //   Prolongation + Sum                                  -> one SpMV-add pass
 //   coarsest CGSolver                                   -> one thread block, shared memory
 //   convergence Defect + Norm                           -> one pass
-// and a V-cycle costs one graph launch.  Each kernel is bit-identical to the
+// and the MGSolver loop itself runs on the device: the solve graph is the
+// initial defect, a conditional WHILE node whose body is one V-cycle plus the
+// convergence defect and a one-thread decision kernel, and the copy of the
+// statistics to pinned host memory -- one graph launch and one host
+// synchronisation per solve.  Each kernel is bit-identical to the
 // reference's operator; with coarse_exact the coarse CG is too, so the MG
 // iterates match the reference's tags::CPU solver bit for bit.
 #include "hb2_common.cuh"
@@ -34,6 +38,15 @@ namespace hb2
         void * store = 0;
         void * tmp = 0;      // Jacobi ping-pong
         void * jac = 0;      // omega / diag(A)
+        int keep = 0;        // kKeepL2 when the level's working set is near the L2 size
+        bool rev_A = false, rev_R = false, rev_P = false;   // direction of the next pass
+
+        int pass(bool & rev)
+        {
+            int f = keep | (rev ? kReverse : 0);
+            rev = ! rev;
+            return f;
+        }
     };
 }
 
@@ -48,13 +61,18 @@ struct hb2_mg_s
     hb2::Workspace * ws;
     void * vec_block;        // one allocation for all level vectors
     void * rfine;            // finest-level defect
-    cudaStream_t cap;
-    cudaGraph_t graph;
+    cudaStream_t cap, cap2;
+    cudaGraph_t graph;       // one V-cycle + convergence defect (hb2_mg_cycle)
     cudaGraphExec_t exec;
     uint64_t graph_kernels;
+    cudaGraph_t solve_graph; // the whole MGSolver loop
+    cudaGraphExec_t solve_exec;
+    uint64_t body_kernels;
     double * norm_dev;       // sqrt(r.r) after the cycle
     uint64_t * coarse_used_dev;
     double * coarse_def_dev;
+    double * r0_dev;         // sqrt(r0.r0)
+    uint64_t * iters_dev;    // cycles done
 };
 
 namespace hb2
@@ -64,7 +82,7 @@ namespace hb2
         void * cur = L.x, * nxt = L.tmp;
         for (uint64_t k = 0; k < sweeps; ++k)
         {
-            int st = launch_ell(L.A, kJacobi, cur, nxt, L.b, L.jac, 0, 0, 0, mg->ws, s);
+            int st = launch_ell(L.A, kJacobi, cur, nxt, L.b, L.jac, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
             if (st) return st;
             std::swap(cur, nxt);
         }
@@ -81,10 +99,10 @@ namespace hb2
                                    mg->coarse_used_dev, mg->coarse_def_dev, s);
         MgLevel & C = mg->lev[i - 1];
         int st = smooth(mg, L, mg->prm.n_pre_smooth, s);
-        if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s);
-        if (! st) st = launch_ell(L.R, kRestrict, L.store, C.b, 0, 0, C.x, 0, 0, mg->ws, s);
+        if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
+        if (! st) st = launch_ell(L.R, kRestrict, L.store, C.b, 0, 0, C.x, 0, 0, mg->ws, s, L.pass(L.rev_R));
         if (! st) st = record_cycle(mg, i - 1, s);
-        if (! st) st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, mg->ws, s);
+        if (! st) st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_P));
         if (! st) st = smooth(mg, L, mg->prm.n_post_smooth, s);
         return st;
     }
@@ -92,13 +110,107 @@ namespace hb2
     static int finest_norm(hb2_mg_s * mg, cudaStream_t s)
     {
         MgLevel & F = mg->lev[mg->nlev - 1];
-        return launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, s);
+        return launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, s, F.pass(F.rev_A));
+    }
+
+    static void reset_directions(hb2_mg_s * mg)
+    {
+        for (MgLevel & L : mg->lev) L.rev_A = L.rev_R = L.rev_P = false;
+    }
+
+    // MGSolver loop control (math/mg.hh:1109-1121): after each cycle, stop when
+    // ||r|| < eps ||r0|| or max_iters cycles are done (also on a NaN norm).
+    __global__ void mg_loop_init_kernel(uint64_t * iters, uint64_t max_iters, cudaGraphConditionalHandle h)
+    {
+        *iters = 0;
+        cudaGraphSetConditional(h, max_iters > 0 ? 1u : 0u);
+    }
+
+    __global__ void mg_loop_decide_kernel(const double * norm, const double * r0, uint64_t * iters, uint64_t max_iters,
+                                          double eps, cudaGraphConditionalHandle h)
+    {
+        const uint64_t it = *iters + 1;
+        *iters = it;
+        const double rc = *norm;
+        const bool stop = rc < eps * *r0 || ! (rc == rc) || it >= max_iters;
+        cudaGraphSetConditional(h, stop ? 0u : 1u);
+    }
+
+    static int capture_error(cudaError_t e, const char * what, hb2_mg_s * mg)
+    {
+        cudaGraph_t g = 0;
+        cudaStreamEndCapture(mg->cap2, &g);
+        cudaStreamEndCapture(mg->cap, &g);
+        if (g) cudaGraphDestroy(g);
+        return cuda_status(e, what);
+    }
+
+    static int build_solve_graph(hb2_mg_s * mg)
+    {
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
+        const uint64_t before = hb2_launch_count();
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t capg = 0;
+        const cudaGraphNode_t * deps = 0;
+        size_t ndeps = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(mg->cap, &cs, 0, &capg, &deps, &ndeps);
+        if (e != cudaSuccess) return capture_error(e, "cudaStreamGetCaptureInfo", mg);
+        cudaGraphConditionalHandle h;
+        e = cudaGraphConditionalHandleCreate(&h, capg, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return capture_error(e, "cudaGraphConditionalHandleCreate", mg);
+        reset_directions(mg);
+        int st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->r0_dev, 1, mg->ws, mg->cap, F.pass(F.rev_A));
+        if (st) { capture_error(cudaSuccess, "", mg); return st; }
+        mg_loop_init_kernel<<<1, 1, 0, mg->cap>>>(mg->iters_dev, mg->prm.max_iters, h);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(mg->cap, &cs, 0, &capg, &deps, &ndeps);
+        if (e != cudaSuccess) return capture_error(e, "capture (loop init)", mg);
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        e = cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp);
+        if (e != cudaSuccess) return capture_error(e, "cudaGraphAddNode (while)", mg);
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamUpdateCaptureDependencies(mg->cap, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(mg->cap2, body, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return capture_error(e, "capture of the loop body", mg);
+        const uint64_t body0 = hb2_launch_count();
+        st = record_cycle(mg, mg->nlev - 1, mg->cap2);
+        if (! st) st = finest_norm(mg, mg->cap2);
+        if (! st)
+        {
+            mg_loop_decide_kernel<<<1, 1, 0, mg->cap2>>>(mg->norm_dev, mg->r0_dev, mg->iters_dev, mg->prm.max_iters,
+                                                          mg->prm.eps_relative, h);
+            count_launches(1);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return capture_error(e, "decide kernel", mg);
+        }
+        if (st) { capture_error(cudaSuccess, "", mg); return st; }
+        mg->body_kernels = hb2_launch_count() - body0;
+        e = cudaStreamEndCapture(mg->cap2, &body);
+        if (e != cudaSuccess) return capture_error(e, "cudaStreamEndCapture (body)", mg);
+        // statistics: norm, coarse iterations, coarse defect, r0, iterations
+        e = cudaMemcpyAsync(mg->ws->host_scalars, mg->ws->scalars, 5 * sizeof(double), cudaMemcpyDeviceToHost, mg->cap);
+        if (e != cudaSuccess) return capture_error(e, "stats copy", mg);
+        cudaGraph_t g = 0;
+        e = cudaStreamEndCapture(mg->cap, &g);
+        set_launch_count(before);
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture (solve)");
+        mg->solve_graph = g;
+        e = cudaGraphInstantiate(&mg->solve_exec, g, 0);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate (solve)");
+        return HB2_OK;
     }
 
     static int build_graph(hb2_mg_s * mg)
     {
         HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
         uint64_t before = hb2_launch_count();
+        reset_directions(mg);
         int st = record_cycle(mg, mg->nlev - 1, mg->cap);
         if (! st) st = finest_norm(mg, mg->cap);
         if (! st)
@@ -140,12 +252,26 @@ namespace hb2
             if (st) return st;
         }
         mg->rfine = p;
+        // L2 policy per level: keep the matrix stream in L2 when the level's
+        // working set (matrix + five vectors) is at most twice the L2 size
+        int l2 = 0;
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, mg->device);
+        if (l2 <= 0) l2 = 126 << 20;
+        for (uint32_t i = 0; i < mg->nlev; ++i)
+        {
+            MgLevel & L = mg->lev[i];
+            uint64_t ws_bytes = L.A->bytes + 5 * L.n * es;
+            L.keep = ws_bytes <= 2ull * (uint64_t)l2 ? kKeepL2 : 0;
+        }
         int st = workspace_create(&mg->ws, kMaxReduceBlocks);
         if (st) return st;
         mg->norm_dev = mg->ws->scalars + 0;
         mg->coarse_used_dev = (uint64_t *)(mg->ws->scalars + 1);
         mg->coarse_def_dev = mg->ws->scalars + 2;
+        mg->r0_dev = mg->ws->scalars + 3;
+        mg->iters_dev = (uint64_t *)(mg->ws->scalars + 4);
         HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap, cudaStreamNonBlocking));
+        HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap2, cudaStreamNonBlocking));
         return HB2_OK;
     }
 
@@ -160,7 +286,9 @@ namespace hb2
                              mg->coarse_def_dev, mg->cap);
         if (st) return st;
         HB2_CUDA(cudaStreamSynchronize(mg->cap));
-        return build_graph(mg);
+        st = build_graph(mg);
+        if (! st) st = build_solve_graph(mg);
+        return st;
     }
 
     static hb2_mg_params default_params()
@@ -197,31 +325,20 @@ namespace hb2
         return HB2_OK;
     }
 
-    // MGSolver::value on the hierarchy's own finest vectors (b, x already in place)
+    // MGSolver::value on the hierarchy's own finest vectors (b, x already in
+    // place): one launch of the solve graph, one synchronisation.
     static int solve_internal(hb2_mg_s * mg, double * stats, cudaStream_t stream)
     {
-        MgLevel & F = mg->lev[mg->nlev - 1];
-        int st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, stream);
-        if (st) return st;
-        HB2_CUDA(cudaMemcpyAsync(mg->ws->host_scalars, mg->norm_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        HB2_CUDA(cudaGraphLaunch(mg->solve_exec, stream));
         HB2_CUDA(cudaStreamSynchronize(stream));
-        const double r0 = mg->ws->host_scalars[0];
-        double rc = 1e16;
-        uint64_t used = 0;
-        for (uint64_t i = 0; i < mg->prm.max_iters; ++i)
-        {
-            HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
-            count_launches(mg->graph_kernels);
-            HB2_CUDA(cudaStreamSynchronize(stream));
-            rc = mg->ws->host_scalars[0];
-            used = i + 1;
-            if (rc < mg->prm.eps_relative * r0) break;
-            if (! (rc == rc)) break;
-        }
+        const double * h = mg->ws->host_scalars;
+        uint64_t used = 0, cu = 0;
+        memcpy(&used, h + 4, sizeof(uint64_t));
+        memcpy(&cu, h + 1, sizeof(uint64_t));
+        const double r0 = h[3], rc = used ? h[0] : 1e16;
+        count_launches(2 + used * mg->body_kernels);
         if (stats)
         {
-            uint64_t cu = 0;
-            HB2_CUDA(cudaMemcpy(&cu, mg->coarse_used_dev, sizeof(uint64_t), cudaMemcpyDeviceToHost));
             stats[0] = (double)used;
             stats[1] = r0;
             stats[2] = rc;
@@ -288,7 +405,10 @@ extern "C" int hb2_mg_destroy(hb2_mg mg)
     if (! mg) return HB2_OK;
     if (mg->exec) cudaGraphExecDestroy(mg->exec);
     if (mg->graph) cudaGraphDestroy(mg->graph);
+    if (mg->solve_exec) cudaGraphExecDestroy(mg->solve_exec);
+    if (mg->solve_graph) cudaGraphDestroy(mg->solve_graph);
     if (mg->cap) cudaStreamDestroy(mg->cap);
+    if (mg->cap2) cudaStreamDestroy(mg->cap2);
     if (mg->vec_block) cudaFree(mg->vec_block);
     workspace_destroy(mg->ws);
     if (mg->owns_matrices)
