@@ -35,6 +35,7 @@ METRIC = "Poisson solves/s & HBM GB/s to 1e-10 rel. residual, mixed vs FP64; p99
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "honei_ref")
 MIN_LEVEL = 3
 COARSE_CAP = 100
+MIXED_LEVEL = 11
 
 
 def parse():
@@ -45,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--level", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     return ap.parse_args()
 
 
@@ -211,7 +213,7 @@ def run_reference_arm(args, rank, world):
 def workload_config(args, world):
     return {"workload": f"mg-v44-fp64-q1-level{args.level}", "level": args.level,
             "unknowns": ((1 << args.level) + 1) ** 2, "matrix": "SparseMatrixELL (9 slots, int32 columns on device)",
-            "coarse_level": MIN_LEVEL, "coarse_solver": f"CG, cap {COARSE_CAP}", "smoother": "Jacobi omega 0.7, 4+4",
+            "coarse_level": MIN_LEVEL, "coarse_solver": f"CG, cap {COARSE_CAP}, tree-ordered dots", "smoother": "Jacobi omega 0.7, 4+4",
             "tol": 1e-10, "l2": "flushed (256 MiB write) before every step, flush outside the step events",
             "parallelism": f"{world} independent systems (one per GPU)" if world > 1 else "single system"}
 
@@ -237,7 +239,7 @@ def main():
     L = args.level
     n = ((1 << L) + 1) ** 2
 
-    params = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10, coarse_exact=True)
+    params = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10, coarse_exact=False)
     data = hb.MGData.poisson_q1(MIN_LEVEL, L, params=params)
     A = hb.SparseMatrixELL.poisson_q1(L)
     u = hb.DenseVector(torch.from_numpy(uniform(n, 42 + rank)).to(dev))
@@ -346,6 +348,9 @@ def main():
         "gpu_launches": gpu_launches,
         "clocks": clk.summary(),
     }
+    if not args.no_mixed:
+        line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5), min(args.warmup, 2),
+                                              rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(L)
     if rank == 0:
@@ -355,6 +360,69 @@ def main():
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
+    """Config 2: level-11 Q1 Poisson (4,198,401 unknowns) to 1e-10 relative residual,
+    plain FP64 MG vs iterative refinement (FP64 defect / update / norm around an FP32
+    MG V(4,4) inner solve to 1e-3, restarted from zero each outer step, coarse CG
+    cap 100 at eps 1e-10).  Times are CUDA-event times per solve, L2 flushed before each."""
+    import statistics
+
+    import torch
+
+    from honei_b200.inputs import uniform
+    n = ((1 << level) + 1) ** 2
+    A = hb.SparseMatrixELL.poisson_q1(level)
+    u = hb.DenseVector(torch.from_numpy(uniform(n, 42 + rank)).to(dev))
+    b = hb.DenseVector(n)
+    hb.Product.value(b, A, u)
+    fp64 = hb.MGData.poisson_q1(MIN_LEVEL, level, params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10,
+                                                                        coarse_exact=False))
+    inner = hb.MGData.poisson_q1(MIN_LEVEL, level, dtype=torch.float32,
+                                 params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-3, coarse_eps=1e-10,
+                                                     coarse_exact=False, coarse_fp64=True))
+    x64 = hb.DenseVector(n)
+    xir = hb.DenseVector(n)
+
+    def timed(fn):
+        ts = []
+        for i in range(warmup + steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            if i >= warmup:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts)
+
+    info = {}
+
+    def run64():
+        hb.fill(x64, 0.0)
+        hb.MGSolver.value(fp64, b, x64)
+
+    def runir():
+        hb.fill(xir, 0.0)
+        _, it, st = hb.IRSolver.value(A, b, xir, inner, eps=1e-10, reset_inner=True)
+        info["outer"], info["inner"] = it, int(st[3])
+
+    t64 = timed(run64)
+    tir = timed(runir)
+    r = hb.DenseVector(n)
+    nb = hb.Norm.value(b)
+    hb.Defect.value(r, b, A, x64)
+    rel64 = hb.Norm.value(r) / nb
+    hb.Defect.value(r, b, A, xir)
+    relir = hb.Norm.value(r) / nb
+    d = hb.DenseVector(x64.elements - xir.elements)
+    err = hb.Norm.value(d) / hb.Norm.value(x64)
+    return {"level": level, "unknowns": n, "fp64_mg_ms": t64, "fp64_cycles": fp64.used_iters, "fp64_relres": rel64,
+            "mixed_ir_ms": tir, "ir_outer_iters": info["outer"], "ir_inner_fp32_cycles": info["inner"],
+            "mixed_relres": relir, "mixed_rel_error_vs_fp64": err, "speedup_mixed_over_fp64": t64 / tir,
+            "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-10"}
 
 
 def ctypes_stream(stream):

@@ -55,7 +55,7 @@ class MgParams(ctypes.Structure):
     """hb2_mg_params"""
     _fields_ = [("n_pre_smooth", _u64), ("n_post_smooth", _u64), ("max_iters", _u64),
                 ("max_iters_coarse", _u64), ("eps_relative", _dbl), ("coarse_eps", _dbl), ("omega", _dbl),
-                ("coarse_exact", _int)]
+                ("coarse_exact", _int), ("no_fused_levels", _int), ("coarse_fp64", _int)]
 
 
 # name -> (restype, argtypes)

@@ -276,9 +276,12 @@ namespace hb2
     // each lane keeps its RPL rows of A and of x, r, p, v in registers; only p
     // (gathered by the SpMV) and, for the reference-order dots, the dot operands
     // go through shared memory.
-    template <typename T, int RPL>
+    // T: arithmetic and matrix type; S: element type of b and x in memory (an
+    // FP32 hierarchy can run its coarsest solve in FP64 on an FP64 copy of the
+    // coarse operator: b is widened on load, x rounded on store).
+    template <typename T, typename S, int RPL>
     __global__ void __launch_bounds__(32)
-    cg_warp_reg_kernel(EllView<T> Ag, const T * __restrict__ b, T * __restrict__ xg, uint64_t max_iters, double eps_d,
+    cg_warp_reg_kernel(EllView<T> Ag, const S * __restrict__ b, S * __restrict__ xg, uint64_t max_iters, double eps_d,
                        int exact, uint64_t * used_out, double * defect_out)
     {
         typedef Arith<T> M;
@@ -302,7 +305,7 @@ namespace hb2
                 av[j][k] = ok ? Ag.val[(uint64_t)k * Ag.ld + row] : T(0);
                 ac[j][k] = ok ? Ag.col[(uint64_t)k * Ag.ld + row] : -1;
             }
-            xr[j] = ok ? xg[row] : T(0);
+            xr[j] = ok ? T(xg[row]) : T(0);
             if (ok) sp[row] = xr[j];
         }
         __syncwarp();
@@ -345,7 +348,7 @@ namespace hb2
         for (int j = 0; j < RPL; ++j)
         {
             const int row = lane + 32 * j;
-            rr[j] = row < n ? M::sub(b[row], tmp[j]) : T(0);
+            rr[j] = row < n ? M::sub(T(b[row]), tmp[j]) : T(0);
             pr[j] = rr[j];
             if (row < n) sp[row] = pr[j];
         }
@@ -386,7 +389,7 @@ namespace hb2
         }
 #pragma unroll
         for (int j = 0; j < RPL; ++j)
-            if (lane + 32 * j < n) xg[lane + 32 * j] = xr[j];
+            if (lane + 32 * j < n) xg[lane + 32 * j] = S(xr[j]);
         if (lane == 0)
         {
             if (used_out) *used_out = used;
@@ -394,7 +397,7 @@ namespace hb2
         }
     }
 
-    template <typename T>
+    template <typename T, typename S>
     static bool launch_warp_reg(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
                                 uint64_t * used_dev, double * defect_dev, cudaStream_t stream)
     {
@@ -402,16 +405,29 @@ namespace hb2
         const int rpl = (int)((A->rows + 31) / 32);
         const size_t smem = 3 * A->rows * sizeof(T) + 16;
         EllView<T> v = A->view<T>();
-        const T * bp = (const T *)b;
-        T * xp = (T *)x;
+        const S * bp = (const S *)b;
+        S * xp = (S *)x;
         switch (rpl)
         {
-            case 1: cg_warp_reg_kernel<T, 1><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            case 2: cg_warp_reg_kernel<T, 2><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            case 3: cg_warp_reg_kernel<T, 3><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            default: cg_warp_reg_kernel<T, 4><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 1: cg_warp_reg_kernel<T, S, 1><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 2: cg_warp_reg_kernel<T, S, 2><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 3: cg_warp_reg_kernel<T, S, 3><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            default: cg_warp_reg_kernel<T, S, 4><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
         }
         return true;
+    }
+
+    bool cg_mixed_supported(const hb2_ell_s * A64) { return A64->dtype == HB2_F64 && A64->K == 9 && A64->rows <= 128; }
+
+    // coarsest solve of an FP32 level in FP64: A64 is the FP64 operator, b / x are FP32
+    int launch_cg_small_f32io(const hb2_ell_s * A64, const void * b32, void * x32, uint64_t max_iters, double eps,
+                              int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream)
+    {
+        if (! launch_warp_reg<double, float>(A64, b32, x32, max_iters, eps, exact, used_dev, defect_dev, stream))
+            return fail(HB2_ERR_UNSUPPORTED, "FP64 coarse solve of an FP32 level needs <= 128 rows and 9 slots");
+        count_launches(1);
+        HB2_LAUNCH_CHECK("cg_warp_reg_kernel (FP32 vectors, FP64 arithmetic)");
+        return HB2_OK;
     }
 
     constexpr uint64_t kWarpCgMaxRows = 1024;
@@ -448,8 +464,8 @@ namespace hb2
             attr_set = true;
         }
         const bool reg = A->dtype == HB2_F64
-                             ? launch_warp_reg<double>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream)
-                             : launch_warp_reg<float>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream);
+                             ? launch_warp_reg<double, double>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream)
+                             : launch_warp_reg<float, float>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream);
         if (reg)
         {
             count_launches(1);

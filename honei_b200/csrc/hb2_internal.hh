@@ -107,9 +107,29 @@ namespace hb2
     // x64 += (double) c  (IR update, math/ir.hh:73-75)
     int launch_add_converted(void * x64, int c_dt, const void * c, uint64_t n, cudaStream_t stream);
 
+    // small levels of a V-cycle as cluster kernels (subcycle.cu)
+    struct SubLevelDesc
+    {
+        const hb2_ell_s * A;
+        const hb2_ell_s * R;   // restriction to the next coarser level (levels > 0)
+        const hb2_ell_s * P;   // prolongation from the next coarser level (levels > 0)
+        void * x;
+        void * b;
+        void * store;
+        void * tmp;
+        const void * jac;
+    };
+    constexpr uint64_t kSubMaxRows = 20000;
+    int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int n_pre, int n_post, bool down,
+                        cudaStream_t stream);
+    int subcycle_prepare();
+
     // small-system CG in one thread block (cg.cu); returns HB2_ERR_UNSUPPORTED
     // when the system does not fit in shared memory.
     int launch_cg_small(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
                         uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
     bool cg_small_fits(const hb2_ell_s * A);
+    bool cg_mixed_supported(const hb2_ell_s * A64);
+    int launch_cg_small_f32io(const hb2_ell_s * A64, const void * b32, void * x32, uint64_t max_iters, double eps,
+                              int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
 }

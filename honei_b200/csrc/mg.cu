@@ -22,6 +22,7 @@
 #include "hb2_internal.hh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -73,6 +74,8 @@ struct hb2_mg_s
     double * coarse_def_dev;
     double * r0_dev;         // sqrt(r0.r0)
     uint64_t * iters_dev;    // cycles done
+    int sub_top;             // levels 1..sub_top run as cluster kernels (-1: none)
+    hb2_ell_s * coarse64;    // FP64 copy of the coarsest operator (F32 hierarchies with coarse_fp64)
 };
 
 namespace hb2
@@ -90,13 +93,48 @@ namespace hb2
         return HB2_OK;
     }
 
+    // the coarsest-level CG (math/mg.hh:585-594); FP64 arithmetic for an FP32
+    // hierarchy when coarse_fp64 is set
+    static int coarse_solve(hb2_mg_s * mg, cudaStream_t s)
+    {
+        MgLevel & C = mg->lev[0];
+        if (mg->coarse64)
+            return launch_cg_small_f32io(mg->coarse64, C.b, C.x, mg->prm.max_iters_coarse, mg->prm.coarse_eps,
+                                         mg->prm.coarse_exact, mg->coarse_used_dev, mg->coarse_def_dev, s);
+        return launch_cg_small(C.A, C.b, C.x, mg->prm.max_iters_coarse, mg->prm.coarse_eps, mg->prm.coarse_exact,
+                               mg->coarse_used_dev, mg->coarse_def_dev, s);
+    }
+
+    // levels 0..sub_top: down leg (cluster kernel), coarse CG, up leg (cluster kernel)
+    static int record_small_levels(hb2_mg_s * mg, cudaStream_t s)
+    {
+        SubLevelDesc d[16];
+        for (int i = 0; i <= mg->sub_top; ++i)
+        {
+            MgLevel & L = mg->lev[i];
+            d[i].A = L.A;
+            d[i].R = L.R;
+            d[i].P = L.P;
+            d[i].x = L.x;
+            d[i].b = L.b;
+            d[i].store = L.store;
+            d[i].tmp = L.tmp;
+            d[i].jac = L.jac;
+        }
+        int st = launch_subcycle(mg->dtype, d, mg->sub_top, (int)mg->prm.n_pre_smooth, (int)mg->prm.n_post_smooth,
+                                 true, s);
+        if (! st) st = coarse_solve(mg, s);
+        if (! st) st = launch_subcycle(mg->dtype, d, mg->sub_top, (int)mg->prm.n_pre_smooth,
+                                       (int)mg->prm.n_post_smooth, false, s);
+        return st;
+    }
+
     // MGCycleCreation::_build_cycle (math/mg.hh:577-640)
     static int record_cycle(hb2_mg_s * mg, uint32_t i, cudaStream_t s)
     {
         MgLevel & L = mg->lev[i];
-        if (i == 0)
-            return launch_cg_small(L.A, L.b, L.x, mg->prm.max_iters_coarse, mg->prm.coarse_eps, mg->prm.coarse_exact,
-                                   mg->coarse_used_dev, mg->coarse_def_dev, s);
+        if ((int)i == mg->sub_top) return record_small_levels(mg, s);
+        if (i == 0) return coarse_solve(mg, s);
         MgLevel & C = mg->lev[i - 1];
         int st = smooth(mg, L, mg->prm.n_pre_smooth, s);
         if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
@@ -279,6 +317,26 @@ namespace hb2
     {
         int st = mg_alloc(mg, stream);
         if (st) return st;
+        // the small levels (at most kSubMaxRows rows, above the coarsest) run as
+        // cluster kernels unless disabled
+        mg->sub_top = -1;
+        if (! mg->prm.no_fused_levels && mg->prm.n_pre_smooth < (1u << 20) && mg->prm.n_post_smooth < (1u << 20))
+            for (uint32_t i = 1; i < mg->nlev && i < 10; ++i)
+                if (mg->lev[i].n <= kSubMaxRows) mg->sub_top = (int)i;
+        if (mg->sub_top >= 1)
+        {
+            st = subcycle_prepare();
+            if (st) return st;
+        }
+        if (mg->dtype == HB2_F32 && mg->prm.coarse_fp64)
+        {
+            hb2_ell c64 = 0;
+            st = hb2_ell_convert(&c64, mg->lev[0].A, HB2_F64, stream);
+            if (st) return st;
+            mg->coarse64 = c64;
+            if (! cg_mixed_supported(c64)) return fail(HB2_ERR_UNSUPPORTED, "coarse_fp64: coarsest level has more than 128 rows");
+            HB2_CUDA(cudaStreamSynchronize(stream));
+        }
         HB2_CUDA(cudaStreamSynchronize(stream));
         // prime the coarse kernel's shared-memory attribute outside the capture
         MgLevel & C = mg->lev[0];
@@ -302,6 +360,8 @@ namespace hb2
         p.coarse_eps = 1e-10;
         p.omega = 0.7;
         p.coarse_exact = 1;
+        p.no_fused_levels = 0;
+        p.coarse_fp64 = 0;
         return p;
     }
 
@@ -325,10 +385,53 @@ namespace hb2
         return HB2_OK;
     }
 
+    // The same solve with the loop on the host: one launch of the plain cycle
+    // graph per V-cycle and a synchronisation to read its norm.  Identical
+    // kernels and results; selected with HB2_MG_LOOP=host, for profilers that
+    // do not descend into conditional graph bodies.
+    static int solve_host_loop(hb2_mg_s * mg, double * stats, cudaStream_t stream)
+    {
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        int st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, stream);
+        if (st) return st;
+        HB2_CUDA(cudaMemcpyAsync(mg->ws->host_scalars, mg->norm_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        HB2_CUDA(cudaStreamSynchronize(stream));
+        const double r0 = mg->ws->host_scalars[0];
+        double rc = 1e16;
+        uint64_t used = 0;
+        for (uint64_t i = 0; i < mg->prm.max_iters; ++i)
+        {
+            HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
+            count_launches(mg->graph_kernels);
+            HB2_CUDA(cudaStreamSynchronize(stream));
+            rc = mg->ws->host_scalars[0];
+            used = i + 1;
+            if (rc < mg->prm.eps_relative * r0 || ! (rc == rc)) break;
+        }
+        if (stats)
+        {
+            uint64_t cu = 0;
+            HB2_CUDA(cudaMemcpy(&cu, mg->coarse_used_dev, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+            stats[0] = (double)used;
+            stats[1] = r0;
+            stats[2] = rc;
+            stats[3] = (double)cu;
+        }
+        if (! (rc == rc) || ! (r0 == r0)) return fail(HB2_ERR_NOT_FINITE, "MG solve: NaN defect norm");
+        return HB2_OK;
+    }
+
+    static bool host_loop_requested()
+    {
+        const char * v = getenv("HB2_MG_LOOP");
+        return v && strcmp(v, "host") == 0;
+    }
+
     // MGSolver::value on the hierarchy's own finest vectors (b, x already in
     // place): one launch of the solve graph, one synchronisation.
     static int solve_internal(hb2_mg_s * mg, double * stats, cudaStream_t stream)
     {
+        if (host_loop_requested()) return solve_host_loop(mg, stats, stream);
         HB2_CUDA(cudaGraphLaunch(mg->solve_exec, stream));
         HB2_CUDA(cudaStreamSynchronize(stream));
         const double * h = mg->ws->host_scalars;
@@ -409,6 +512,7 @@ extern "C" int hb2_mg_destroy(hb2_mg mg)
     if (mg->solve_graph) cudaGraphDestroy(mg->solve_graph);
     if (mg->cap) cudaStreamDestroy(mg->cap);
     if (mg->cap2) cudaStreamDestroy(mg->cap2);
+    if (mg->coarse64) hb2_ell_destroy(mg->coarse64);
     if (mg->vec_block) cudaFree(mg->vec_block);
     workspace_destroy(mg->ws);
     if (mg->owns_matrices)

@@ -96,9 +96,9 @@ class CGSolver:
 
 
 def mg_params(n_pre=4, n_post=4, max_iters=100, max_iters_coarse=100, eps=1e-10, coarse_eps=None, omega=0.7,
-              coarse_exact=True) -> MgParams:
+              coarse_exact=True, fused_levels=True, coarse_fp64=False) -> MgParams:
     return MgParams(n_pre, n_post, max_iters, max_iters_coarse, eps, eps if coarse_eps is None else coarse_eps,
-                    omega, int(coarse_exact))
+                    omega, int(coarse_exact), int(not fused_levels), int(coarse_fp64))
 
 
 class MGData:

@@ -219,6 +219,10 @@ typedef struct
     double coarse_eps;                      /* coarse CG eps (reference: = eps_relative) */
     double omega;                           /* Jacobi damping, 0.7 */
     int coarse_exact;                       /* 1: coarse CG dots in the reference's sequential fma order */
+    int no_fused_levels;                    /* 1: one kernel per operator on every level (0: levels below
+                                               ~20k rows run as two thread-block-cluster kernels per cycle) */
+    int coarse_fp64;                        /* F32 hierarchies: 1 runs the coarsest CG in FP64 on an FP64 copy
+                                               of the coarse operator (<= 128 rows); 0: FP32 as the reference */
 } hb2_mg_params;
 
 HB2_API int hb2_mg_create(hb2_mg *out, uint32_t num_levels, const hb2_ell *A, const hb2_ell *prol, const hb2_ell *res,

@@ -375,3 +375,55 @@ def test_mg_determinism():
         hb.MGSolver.value(data, DenseVector(b), x)
         out.append(host(x))
     assert same_bits(out[0], out[1])
+
+
+def test_mg_host_loop_mode_identical(monkeypatch):
+    """HB2_MG_LOOP=host (loop on the host over the plain cycle graph) gives the same bits."""
+    L = 7
+    n = ((1 << L) + 1) ** 2
+    data = hb.MGData.poisson_q1(3, L)
+    b = DenseVector(torch.rand(n, dtype=torch.float64, device=DEV, generator=torch.Generator(device=DEV).manual_seed(5)))
+    xs = []
+    for mode in (None, "host"):
+        if mode:
+            monkeypatch.setenv("HB2_MG_LOOP", mode)
+        x = DenseVector(torch.zeros(n, dtype=torch.float64, device=DEV))
+        hb.MGSolver.value(data, b, x)
+        xs.append((host(x), data.used_iters))
+    assert xs[0][1] == xs[1][1]
+    assert same_bits(xs[0][0], xs[1][0])
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_mg_fused_small_levels_identical(dt):
+    """Small levels as cluster kernels give the same bits as one kernel per operator."""
+    L = 9
+    n = ((1 << L) + 1) ** 2
+    b = DenseVector(torch.rand(n, dtype=dt, device=DEV, generator=torch.Generator(device=DEV).manual_seed(9)))
+    out = []
+    for fused in (True, False):
+        data = hb.MGData.poisson_q1(3, L, dtype=dt, params=hb.mg_params(eps=1e-6 if dt == torch.float32 else 1e-10,
+                                                                         fused_levels=fused))
+        x = DenseVector(torch.zeros(n, dtype=dt, device=DEV))
+        hb.MGSolver.value(data, b, x)
+        out.append((host(x), data.used_iters))
+    assert out[0][1] == out[1][1]
+    assert same_bits(out[0][0], out[1][0])
+
+
+def test_ir_mixed_fp64_coarse(oracle):
+    """Mixed IR with the north_star's FP64 coarsest solve inside the FP32 inner MG:
+    converges to the FP64 stop and agrees with the FP64 MG solution."""
+    L = 7
+    Ao = oracle.q1_ell(L)
+    b = oracle.ell_spmv(Ao, oracle.uniform(Ao.rows, 42))
+    A = SparseMatrixELL.poisson_q1(L)
+    inner = hb.MGData.poisson_q1(3, L, dtype=torch.float32,
+                                 params=hb.mg_params(eps=1e-3, coarse_eps=1e-10, coarse_exact=False, coarse_fp64=True))
+    x = dvec(np.zeros(Ao.rows))
+    _, it, st = hb.IRSolver.value(A, dvec(b), x, inner, eps=1e-10, reset_inner=True)
+    xs = host(x)
+    assert np.linalg.norm(b - oracle.ell_spmv(Ao, xs)) < 1e-10 * st[1] * 1.001
+    x64, _, _ = oracle.mg_q1(L, b, max_iters_coarse=100)
+    assert np.linalg.norm(xs - x64) / np.linalg.norm(x64) < 1e-6
+    assert it <= 6
