@@ -51,15 +51,17 @@ def parse():
 
 
 def mg_solve_bytes(level: int, cycles: int, min_level: int = MIN_LEVEL, n_pre: int = 4, n_post: int = 4,
-                   s: int = 8, si: int = 4) -> int:
+                   s: int = 8, si: int = 4, s_mat: int = 8) -> int:
     """Algorithmic HBM bytes of one MG solve (each vector / matrix entry touched once per pass).
 
-    Jacobi sweep 9(s+si)+4s per row; defect 9(s+si)+3s; restriction R (coarse rows,
-    <=9 slots) 9(s+si)+2s per coarse row + the fine input; prolongation-add P (fine
-    rows, 4 slots) 4(s+si)+2s per fine row + the coarse input; convergence defect once
+    Jacobi sweep 9(m)+4s per row; defect 9(m)+3s; restriction R (coarse rows,
+    <=9 slots) 9(m)+2s per coarse row + the fine input; prolongation-add P (fine
+    rows, 4 slots) 4(m)+2s per fine row + the coarse input; convergence defect once
     per cycle plus the initial one; the coarse solve is counted once (it runs in
-    shared memory)."""
+    registers).  m = bytes per stored matrix slot: s_mat + si (plain: value +
+    int32 column = 12 in FP64; compressed: 1-byte code + 2-byte offset = 3)."""
     total = 0
+    si = s_mat + si - s           # so that (s + si) below is the slot size
     for l in range(min_level + 1, level + 1):
         nf = ((1 << l) + 1) ** 2
         nc = ((1 << (l - 1)) + 1) ** 2
@@ -324,12 +326,14 @@ def main():
             kms.append(k0.elapsed_time(k1))
         xa, xb = xb, xa
     k_ms = statistics.mean(kms)
-    k_bytes = JACOBI_BYTES_PER_ROW * n
+    compact, table_size, slot_bytes = A.layout()
+    k_bytes = (9 * slot_bytes + 4 * 8) * n
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
     peaks = load_peaks()
     traffic = load_traffic()
 
-    solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)))
+    solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)), si=4 if not compact else 0,
+                                 s_mat=8 if not compact else 3)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean_ms_max, "higher_is_better": True, "scaling": "weak",
@@ -339,7 +343,10 @@ def main():
         "latency_ms": {"p50": percentile(step_ms, 50), "p99": percentile(step_ms, 99), "max": max(step_ms)},
         "cycles": int(statistics.median(cycles)), "relres": relres,
         "wall_ms_per_step_incl_flush": 1000 * t_wall / args.steps,
-        "roofline": {"bound": "hbm", "kernel": "ell_kernel<double,9,kJacobi> (fused Jacobi sweep, level %d)" % L,
+        "roofline": {"bound": "hbm", "kernel": "%s<double,9,kJacobi> (fused Jacobi sweep, level %d)" % (
+                         "ell_compact_kernel" if compact else "ell_kernel", L),
+                     "layout": "%d-byte value codes (table of %d) + int16 column offsets, %d B/row" % (1, table_size,
+                                9 * slot_bytes + 32) if compact else "FP64 values + int32 columns, 140 B/row",
                      "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
                      "peak_source": peaks[1], "traffic": traffic, "algorithmic_bytes": k_bytes,
                      "launch_us": 1000 * k_ms},

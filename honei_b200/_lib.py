@@ -70,6 +70,7 @@ SIGNATURES = {
     "hb2_ell_destroy": (_int, [_vp]),
     "hb2_ell_info": (_int, [_vp, _pu64, _pu64, _pu64, _pu64, _pu64, _pu64]),
     "hb2_ell_export": (_int, [_vp, _vp, _vp, _vp]),
+    "hb2_ell_layout": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "hb2_q1_create": (_int, [_pvp, _int, _u64, _vp, _int, _vp]),
     "hb2_q1_create_poisson": (_int, [_pvp, _int, ctypes.c_uint, _dbl, _vp]),
     "hb2_q1_destroy": (_int, [_vp]),

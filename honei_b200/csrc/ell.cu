@@ -61,10 +61,19 @@ namespace hb2
     __global__ void __launch_bounds__(kEllThreads)
     ell_kernel(EllView<T> A, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ aux,
                const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt,
-               int flags)
+               int flags, Batch bt)
     {
         constexpr int R = RowsPerThread<T>::value;
         typedef Arith<T> M;
+        if (bt.active && ! bt.active[blockIdx.y]) return;
+        {
+            const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
+            x += vo;
+            y += vo;
+            if (aux) aux += vo;
+            if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;
+            if (red) red += blockIdx.y;   // grid_sum_finish offsets its partials / counters itself
+        }
         const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x;
         const bool keep = (flags & kKeepL2) != 0;
         const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
@@ -136,42 +145,44 @@ namespace hb2
 
     template <typename T, int MODE>
     static void launch_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
-                            void * zero, double * red, int want_sqrt, ReduceSlot rs, unsigned grid, cudaStream_t s,
-                            int flags)
+                            void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
+                            int flags, Batch b)
     {
         EllView<T> v = A->view<T>();
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         if (A->K == 9)
             ell_kernel<T, 9, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags);
+                                                                (T *)zero, rs, red, want_sqrt, flags, b);
         else if (A->K == 4)
             ell_kernel<T, 4, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags);
+                                                                (T *)zero, rs, red, want_sqrt, flags, b);
         else
             ell_kernel<T, 0, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags);
+                                                                (T *)zero, rs, red, want_sqrt, flags, b);
     }
 
     template <typename T>
     static void launch_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                              const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs,
-                             unsigned grid, cudaStream_t s, int f)
+                             dim3 grid, cudaStream_t s, int f, Batch b)
     {
         switch (mode)
         {
-            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
-            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
-            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
-            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
-            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
-            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f); break;
+            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
         }
     }
 
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
-                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags)
+                   void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags,
+                   const Batch * batch)
     {
+        const Batch b = batch ? *batch : Batch();
         if (A->rows == 0)
         {
             // empty matrix: defined results without a launch
@@ -179,19 +190,26 @@ namespace hb2
             return HB2_OK;
         }
         const int R = A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value;
-        unsigned grid = ceil_div(A->rows, (uint64_t)kEllThreads * R);
+        const unsigned gx = A->code ? compact_grid(A, red != 0) : ceil_div(A->rows, (uint64_t)kEllThreads * R);
+        if (b.nvec == 0 || b.nvec > 65535) return fail(HB2_ERR_ARG, "ELL batch: 1..65535 vectors");
+        const dim3 grid(gx, b.nvec);
         ReduceSlot rs;
         rs.partials = 0;
+        rs.gpart = 0;
         rs.ticket = 0;
         rs.max_blocks = 0;
         if (red)
         {
             if (! ws) return fail(HB2_ERR_ARG, "fused reduction without a workspace");
-            if (grid > ws->max_blocks) return fail(HB2_ERR_UNSUPPORTED, "matrix too large for the reduction workspace");
+            const uint64_t ngroups = (gx + kReduceGroup - 1) / kReduceGroup;
+            if ((uint64_t)gx * b.nvec > ws->max_blocks || (ngroups + 1) * b.nvec > ws->max_tickets ||
+                ngroups * b.nvec > ws->max_blocks / kReduceGroup + 4096)
+                return fail(HB2_ERR_UNSUPPORTED, "matrix / batch too large for the reduction workspace");
             rs = ws->slot();
         }
-        if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags);
-        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags);
+        if (A->code) launch_ell_compact(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+        else if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
         count_launches(1);
         HB2_LAUNCH_CHECK("ell kernel launch");
         return HB2_OK;
@@ -467,6 +485,8 @@ extern "C" int hb2_ell_create(hb2_ell * out, hb2_dtype dtype, uint64_t rows, uin
         return fail(HB2_ERR_ARG, hbad == 1 ? "hb2_ell_create: Arl exceeds num_cols_per_row"
                                            : "hb2_ell_create: column index >= columns");
     }
+    int cst = ell_build_compact(A, stream);
+    if (cst) { hb2_ell_destroy(A); return cst; }
     *out = A;
     return HB2_OK;
 }
@@ -487,6 +507,8 @@ extern "C" int hb2_ell_create_q1(hb2_ell * out, hb2_dtype dtype, unsigned level,
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { hb2_ell_destroy(A); return cuda_status(e, "hb2_ell_create_q1"); }
+    int cst = ell_build_compact(A, stream);
+    if (cst) { hb2_ell_destroy(A); return cst; }
     *out = A;
     return HB2_OK;
 }
@@ -520,6 +542,9 @@ extern "C" int hb2_ell_create_transfer(hb2_ell * prol, hb2_ell * res, hb2_dtype 
     count_launches(2);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { hb2_ell_destroy(P); hb2_ell_destroy(R); return cuda_status(e, "hb2_ell_create_transfer"); }
+    int cst = ell_build_compact(P, stream);
+    if (! cst) cst = ell_build_compact(R, stream);
+    if (cst) { hb2_ell_destroy(P); hb2_ell_destroy(R); return cst; }
     *prol = P;
     *res = R;
     return HB2_OK;
@@ -546,6 +571,8 @@ extern "C" int hb2_ell_convert(hb2_ell * out, hb2_ell src, hb2_dtype dtype, cuda
     cudaError_t e = cudaMemcpyAsync(A->col, src->col, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) { hb2_ell_destroy(A); return cuda_status(e, "hb2_ell_convert"); }
+    int cst = ell_build_compact(A, stream);
+    if (cst) { hb2_ell_destroy(A); return cst; }
     *out = A;
     return HB2_OK;
 }
@@ -555,6 +582,7 @@ extern "C" int hb2_ell_destroy(hb2_ell A)
     if (! A) return HB2_OK;
     cudaFree(A->val);
     cudaFree(A->col);
+    ell_free_compact(A);
     delete A;
     return HB2_OK;
 }
@@ -568,7 +596,16 @@ extern "C" int hb2_ell_info(hb2_ell A, uint64_t * rows, uint64_t * cols, uint64_
     if (stride) *stride = A->ref_stride;
     if (K) *K = A->ref_K;
     if (threads) *threads = A->ref_T;
-    if (device_bytes) *device_bytes = A->bytes;
+    if (device_bytes) *device_bytes = A->bytes + A->compact_bytes;
+    return HB2_OK;
+}
+
+extern "C" int hb2_ell_layout(hb2_ell A, int * compact, uint32_t * table_size, uint32_t * slot_bytes)
+{
+    if (! A) return fail(HB2_ERR_ARG, "hb2_ell_layout: null matrix");
+    if (compact) *compact = A->code ? 1 : 0;
+    if (table_size) *table_size = A->ntable;
+    if (slot_bytes) *slot_bytes = A->code ? 3u : (uint32_t)(dtype_size(A->dtype) + 4);
     return HB2_OK;
 }
 

@@ -1,0 +1,477 @@
+// Compressed device layout for SparseMatrixELL: value dictionary + 16-bit
+// column offsets.
+//
+// FEM and stencil operators have few distinct values and bounded column
+// offsets.  When a matrix has at most 255 distinct value bit patterns and every
+// column lies within +-32767 of its row's base column (base = row for square
+// matrices, floor(row * cols / rows) otherwise), each slot is stored as a 1-byte
+// index into a per-matrix value table plus a 2-byte offset: 3 bytes per slot
+// instead of 12 (FP64 value + int32 column) or 8 (FP32).  The kernels look the
+// value up in shared memory and perform exactly the products and sums of the
+// plain layout, so results are bit-identical.  The plain arrays are kept (the
+// small-level, CG and export paths read them); launch_ell uses the compressed
+// arrays when present.  Set HB2_ELL_COMPACT=0 to keep matrices plain,
+// HB2_ELL_COMPACT=force2|force4|force8 to skip the autotuner.
+#include "hb2_common.cuh"
+#include "hb2_internal.hh"
+
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+namespace hb2
+{
+    constexpr int16_t kEmptyOffset = -32768;
+    constexpr uint32_t kDictSlots = 4096;
+    constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+    constexpr int kCompactRowsMax = 8;                // rows per thread: 2, 4 or 8 (autotuned)
+    constexpr uint64_t kCompactMinRows = 32768;       // smaller matrices stay plain
+
+    template <typename T> __device__ __forceinline__ unsigned long long key_of(T v);
+    template <> __device__ __forceinline__ unsigned long long key_of<double>(double v) { return (unsigned long long)__double_as_longlong(v); }
+    template <> __device__ __forceinline__ unsigned long long key_of<float>(float v) { return (unsigned long long)__float_as_uint(v); }
+
+    __device__ __forceinline__ uint32_t dict_hash(unsigned long long k)
+    {
+        k ^= k >> 33;
+        k *= 0xff51afd7ed558ccdull;
+        k ^= k >> 33;
+        return (uint32_t)k & (kDictSlots - 1);
+    }
+
+    __device__ __forceinline__ int64_t row_base(uint64_t r, uint64_t rows, uint64_t cols)
+    {
+        return rows == cols ? (int64_t)r : (int64_t)((r * cols) / rows);
+    }
+
+    template <typename T>
+    __global__ void dict_insert_kernel(const T * __restrict__ val, const int32_t * __restrict__ col, uint64_t n,
+                                       unsigned long long * keys, int * flag)
+    {
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        {
+            if (col[i] < 0) continue;
+            const unsigned long long k = key_of(val[i]);
+            if (k == kEmptyKey) { atomicExch(flag, 3); continue; }
+            uint32_t h = dict_hash(k);
+            bool placed = false;
+            for (uint32_t p = 0; p < kDictSlots; ++p)
+            {
+                const unsigned long long prev = atomicCAS(keys + h, kEmptyKey, k);
+                if (prev == kEmptyKey || prev == k) { placed = true; break; }
+                h = (h + 1) & (kDictSlots - 1);
+            }
+            if (! placed) atomicExch(flag, 1);
+        }
+    }
+
+    template <typename T>
+    __global__ void ell_encode_kernel(const T * __restrict__ val, const int32_t * __restrict__ col, uint64_t rows,
+                                      uint64_t cols, uint64_t ld, uint32_t K, const unsigned long long * __restrict__ keys,
+                                      const uint16_t * __restrict__ code_of_slot, uint8_t * code, int16_t * delta,
+                                      int * flag)
+    {
+        const uint64_t n = (uint64_t)K * ld;
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        {
+            const uint64_t r = i % ld;
+            const int32_t c = col[i];
+            if (c < 0 || r >= rows)
+            {
+                code[i] = 0;
+                delta[i] = kEmptyOffset;
+                continue;
+            }
+            const unsigned long long k = key_of(val[i]);
+            uint32_t h = dict_hash(k);
+            uint32_t p = 0;
+            while (keys[h] != k && p < kDictSlots) { h = (h + 1) & (kDictSlots - 1); ++p; }
+            if (p == kDictSlots) { atomicExch(flag, 4); code[i] = 0; delta[i] = kEmptyOffset; continue; }
+            code[i] = (uint8_t)code_of_slot[h];
+            const int64_t d = (int64_t)c - row_base(r, rows, cols);
+            if (d <= -32768 || d > 32767) { atomicExch(flag, 2); delta[i] = kEmptyOffset; continue; }
+            delta[i] = (int16_t)d;
+        }
+    }
+
+    template <typename T>
+    struct EllCompactView
+    {
+        const uint8_t * code;
+        const int16_t * delta;
+        const T * table;
+        uint64_t rows, cols, ld;
+        uint32_t K, ntable;
+    };
+
+    // one thread: R consecutive rows; per slot it loads R one-byte codes and R
+    // 16-bit offsets (R = 2: 16 + 32 bits, 4: 32 + 64 bits, 8: 64 + 128 bits)
+    template <int R> struct CodeWord;
+    template <> struct CodeWord<2> { typedef uint16_t C; typedef int32_t D; };
+    template <> struct CodeWord<4> { typedef uint32_t C; typedef int2 D; };
+    template <> struct CodeWord<8> { typedef uint2 C; typedef int4 D; };
+
+    template <int R>
+    __device__ __forceinline__ void unpack(const typename CodeWord<R>::C & c, const typename CodeWord<R>::D & d,
+                                           uint32_t (&code)[R], int (&off)[R])
+    {
+        uint32_t cw[(R + 3) / 4];
+        int32_t dw[(R + 1) / 2];
+        if constexpr (R == 2) { cw[0] = c; dw[0] = d; }
+        else if constexpr (R == 4) { cw[0] = c; dw[0] = d.x; dw[1] = d.y; }
+        else { cw[0] = c.x; cw[1] = c.y; dw[0] = d.x; dw[1] = d.y; dw[2] = d.z; dw[3] = d.w; }
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+        {
+            code[i] = (cw[i >> 2] >> ((i & 3) * 8)) & 0xffu;
+            off[i] = (int16_t)(dw[i >> 1] >> ((i & 1) * 16));
+        }
+    }
+
+    template <typename V>
+    __device__ __forceinline__ V ld_policy(const V * p, bool keep) { return keep ? __ldcg(p) : __ldcs(p); }
+    template <>
+    __device__ __forceinline__ uint16_t ld_policy<uint16_t>(const uint16_t * p, bool keep)
+    {
+        return keep ? __ldcg((const unsigned short *)p) : __ldcs((const unsigned short *)p);
+    }
+
+    template <typename T, int KT, int MODE, int R>
+    __global__ void __launch_bounds__(kEllThreads)
+    ell_compact_kernel(EllCompactView<T> A, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ aux,
+                       const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt,
+                       int flags, Batch bt)
+    {
+        typedef Arith<T> M;
+        typedef typename CodeWord<R>::C CW;
+        typedef typename CodeWord<R>::D DW;
+        if (bt.active && ! bt.active[blockIdx.y]) return;
+        {
+            const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
+            x += vo;
+            y += vo;
+            if (aux) aux += vo;
+            if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;
+            if (red) red += blockIdx.y;   // grid_sum_finish offsets its partials / counters itself
+        }
+        __shared__ T table[256];
+        for (uint32_t i = threadIdx.x; i < A.ntable; i += blockDim.x) table[i] = A.table[i];
+        __syncthreads();
+        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x;
+        const bool keep = (flags & kKeepL2) != 0;
+        const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
+        const int K = KT > 0 ? KT : (int)A.K;
+        T acc[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) acc[i] = T(0);
+        if (r0 < A.rows)
+        {
+            int64_t base[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i) base[i] = row_base(r0 + i, A.rows, A.cols);
+            if constexpr (KT > 0)
+            {
+                CW cw[KT];
+                DW dw[KT];
+#pragma unroll
+                for (int k = 0; k < KT; ++k)
+                {
+                    cw[k] = ld_policy((const CW *)(A.code + (uint64_t)k * A.ld + r0), keep);
+                    dw[k] = ld_policy((const DW *)(A.delta + (uint64_t)k * A.ld + r0), keep);
+                }
+#pragma unroll
+                for (int k = 0; k < KT; ++k)
+                {
+                    uint32_t code[R];
+                    int off[R];
+                    unpack<R>(cw[k], dw[k], code, off);
+#pragma unroll
+                    for (int i = 0; i < R; ++i)
+                        if (off[i] != kEmptyOffset) acc[i] = M::add(acc[i], M::mul(table[code[i]], __ldg(x + base[i] + off[i])));
+                }
+            }
+            else
+            {
+                for (int k = 0; k < K; ++k)
+                {
+                    uint32_t code[R];
+                    int off[R];
+                    unpack<R>(ld_policy((const CW *)(A.code + (uint64_t)k * A.ld + r0), keep),
+                              ld_policy((const DW *)(A.delta + (uint64_t)k * A.ld + r0), keep), code, off);
+#pragma unroll
+                    for (int i = 0; i < R; ++i)
+                        if (off[i] != kEmptyOffset) acc[i] = M::add(acc[i], M::mul(table[code[i]], __ldg(x + base[i] + off[i])));
+                }
+            }
+        }
+        double part = 0.0;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+        {
+            const uint64_t r = r0 + i;
+            if (r >= A.rows) break;
+            if (MODE == kPlain) y[r] = acc[i];
+            else if (MODE == kDefect)
+            {
+                T d = M::sub(aux[r], acc[i]);
+                y[r] = d;
+                part = fma((double)d, (double)d, part);
+            }
+            else if (MODE == kDot)
+            {
+                y[r] = acc[i];
+                part = fma((double)acc[i], (double)x[r], part);
+            }
+            else if (MODE == kAdd) y[r] = M::add(y[r], acc[i]);
+            else if (MODE == kJacobi) y[r] = M::add(x[r], M::mul(aux2[r], M::sub(aux[r], acc[i])));
+            else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
+        }
+        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        {
+            __shared__ double scratch[32];
+            double s = block_sum(part, scratch);
+            grid_sum_finish(s, rs, red, want_sqrt, scratch);
+        }
+    }
+
+    template <typename T, int MODE>
+    static void compact_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
+                             void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
+                             int flags, Batch b)
+    {
+        EllCompactView<T> v;
+        v.code = A->code;
+        v.delta = A->delta;
+        v.table = (const T *)A->table;
+        v.rows = A->rows;
+        v.cols = A->cols;
+        v.ld = A->ld;
+        v.K = A->K;
+        v.ntable = A->ntable;
+        const T * xp = (const T *)x;
+        T * yp = (T *)y;
+        const T * ap = (const T *)aux;
+        const T * a2 = (const T *)aux2;
+        T * zp = (T *)zero;
+#define HB2_COMPACT_LAUNCH(KT_, R_)                                                                          \
+        ell_compact_kernel<T, KT_, MODE, R_><<<grid, kEllThreads, 0, s>>>(v, xp, yp, ap, a2, zp, rs, red,      \
+                                                                          want_sqrt, flags, b)
+        const int R = red ? A->compact_rpt_red : A->compact_rpt;
+        if (A->K == 9) { if (R == 2) HB2_COMPACT_LAUNCH(9, 2); else if (R == 4) HB2_COMPACT_LAUNCH(9, 4); else HB2_COMPACT_LAUNCH(9, 8); }
+        else if (A->K == 4) { if (R == 2) HB2_COMPACT_LAUNCH(4, 2); else if (R == 4) HB2_COMPACT_LAUNCH(4, 4); else HB2_COMPACT_LAUNCH(4, 8); }
+        else { if (R == 2) HB2_COMPACT_LAUNCH(0, 2); else if (R == 4) HB2_COMPACT_LAUNCH(0, 4); else HB2_COMPACT_LAUNCH(0, 8); }
+#undef HB2_COMPACT_LAUNCH
+    }
+
+    template <typename T>
+    static void compact_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                              const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                              cudaStream_t s, int f, Batch b)
+    {
+        switch (mode)
+        {
+            case kPlain: compact_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kDefect: compact_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kDot: compact_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kAdd: compact_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kJacobi: compact_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kRestrict: compact_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+        }
+    }
+
+    unsigned compact_grid(const hb2_ell_s * A, bool reducing)
+    {
+        return ceil_div(A->rows, (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt));
+    }
+
+    void launch_ell_compact(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                            const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                            cudaStream_t stream, int flags, Batch b)
+    {
+        if (A->dtype == HB2_F64) compact_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+        else compact_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+    }
+
+    static bool compact_enabled()
+    {
+        const char * v = getenv("HB2_ELL_COMPACT");
+        return ! (v && strcmp(v, "0") == 0);
+    }
+
+    template <typename T>
+    static int build_compact_typed(hb2_ell_s * A, cudaStream_t s)
+    {
+        const uint64_t n = (uint64_t)A->K * A->ld;
+        unsigned long long * keys = 0;
+        int * flag = 0;
+        uint16_t * cos = 0;
+        HB2_CUDA(cudaMalloc(&keys, kDictSlots * sizeof(unsigned long long)));
+        cudaError_t e = cudaMalloc(&flag, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(keys, 0xFF, kDictSlots * sizeof(unsigned long long), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), s);
+        const unsigned grid = (unsigned)std::min<uint64_t>(4096, (n + 255) / 256);
+        if (e == cudaSuccess)
+        {
+            dict_insert_kernel<T><<<grid, 256, 0, s>>>((const T *)A->val, A->col, n, keys, flag);
+            count_launches(1);
+            e = cudaGetLastError();
+        }
+        std::vector<unsigned long long> hk(kDictSlots);
+        int hflag = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hk.data(), keys, kDictSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        int st = e == cudaSuccess ? HB2_OK : cuda_status(e, "ELL compaction (dictionary)");
+        std::vector<T> table;
+        std::vector<uint16_t> code_of_slot(kDictSlots, 0);
+        bool ok = st == HB2_OK && hflag == 0;
+        if (ok)
+            for (uint32_t h = 0; h < kDictSlots && ok; ++h)
+                if (hk[h] != kEmptyKey)
+                {
+                    if (table.size() == 255) { ok = false; break; }
+                    T v;
+                    if (sizeof(T) == 8) { unsigned long long b = hk[h]; memcpy(&v, &b, 8); }
+                    else { uint32_t b = (uint32_t)hk[h]; memcpy(&v, &b, 4); }
+                    code_of_slot[h] = (uint16_t)table.size();
+                    table.push_back(v);
+                }
+        if (ok && ! table.empty())
+        {
+            e = cudaMalloc(&cos, kDictSlots * sizeof(uint16_t));
+            if (e == cudaSuccess) e = cudaMemcpyAsync(cos, code_of_slot.data(), kDictSlots * sizeof(uint16_t), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaMalloc(&A->table, table.size() * sizeof(T));
+            if (e == cudaSuccess) e = cudaMemcpyAsync(A->table, table.data(), table.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaMalloc(&A->code, n);
+            if (e == cudaSuccess) e = cudaMalloc(&A->delta, n * sizeof(int16_t));
+            if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), s);
+            if (e == cudaSuccess)
+            {
+                ell_encode_kernel<T><<<grid, 256, 0, s>>>((const T *)A->val, A->col, A->rows, A->cols, A->ld, A->K, keys,
+                                                          cos, A->code, A->delta, flag);
+                count_launches(1);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) st = cuda_status(e, "ELL compaction (encode)");
+            ok = st == HB2_OK && hflag == 0;
+            A->ntable = (uint32_t)table.size();
+        }
+        else ok = false;
+        if (! ok)
+        {
+            // not eligible (too many distinct values, offsets beyond 16 bits) or failed: stay plain
+            cudaFree(A->table);
+            cudaFree(A->code);
+            cudaFree(A->delta);
+            A->table = 0;
+            A->code = 0;
+            A->delta = 0;
+            A->ntable = 0;
+        }
+        else A->compact_bytes = n * 3 + table.size() * sizeof(T);
+        cudaFree(keys);
+        cudaFree(flag);
+        cudaFree(cos);
+        return st;
+    }
+
+    // Autotuner: time y = A x and the defect with its fused norm, with the plain
+    // layout and with the compressed layout at 2, 4 and 8 rows per thread (three
+    // timed launches each, after one warm-up), and keep the fastest for each of
+    // the two kernel classes; the compressed arrays are freed when the plain
+    // layout wins both.  Runs once per matrix, at creation, on `stream`.
+    static int autotune(hb2_ell_s * A, cudaStream_t s)
+    {
+        const size_t es = dtype_size(A->dtype);
+        const bool square = A->rows == A->cols;
+        Workspace * ws = 0;
+        int st = square ? stream_workspace(s, &ws) : HB2_OK;
+        if (st) return st;
+        void * buf = 0;
+        const size_t vb = ((std::max(A->rows, A->cols) * es + 255) / 256) * 256;
+        HB2_CUDA(cudaMalloc(&buf, 3 * vb + 256));
+        HB2_CUDA(cudaMemsetAsync(buf, 0, 3 * vb + 256, s));
+        void * xv = buf, * yv = (char *)buf + vb, * bv = (char *)buf + 2 * vb;
+        double * nrm = (double *)((char *)buf + 3 * vb);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        uint8_t * code = A->code;
+        const int variants[4] = {0, 2, 4, 8};   // 0: plain layout
+        float best[2] = {1e30f, 1e30f};
+        int best_v[2] = {0, 0};
+        for (int cls = 0; cls < (square ? 2 : 1); ++cls)
+            for (int v : variants)
+            {
+                A->code = v ? code : 0;
+                A->compact_rpt = A->compact_rpt_red = v ? v : 8;
+                float total = 0.f;
+                for (int rep = 0; rep < 4; ++rep)
+                {
+                    cudaEventRecord(e0, s);
+                    st = cls == 0 ? launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s)
+                                  : launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s);
+                    cudaEventRecord(e1, s);
+                    if (st) break;
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) total += ms;
+                }
+                if (st) break;
+                if (total < best[cls]) { best[cls] = total; best_v[cls] = v; }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamSynchronize(s);
+        cudaFree(buf);
+        A->code = code;
+        if (st) return st;
+        if (! square) best_v[1] = best_v[0];
+        if (best_v[0] == 0 && best_v[1] == 0)
+        {
+            ell_free_compact(A);
+            A->compact_bytes = 0;
+        }
+        else
+        {
+            // one layout serves both classes: if only one class prefers plain,
+            // the compressed kernel runs at that class's fastest compressed shape
+            A->compact_rpt = best_v[0] ? best_v[0] : (best_v[1] ? best_v[1] : 2);
+            A->compact_rpt_red = best_v[1] ? best_v[1] : A->compact_rpt;
+        }
+        HB2_LAUNCH_CHECK("ELL layout autotuning");
+        return HB2_OK;
+    }
+
+    int ell_build_compact(hb2_ell_s * A, cudaStream_t stream)
+    {
+        if (! compact_enabled() || A->rows < kCompactMinRows) return HB2_OK;
+        int st = A->dtype == HB2_F64 ? build_compact_typed<double>(A, stream) : build_compact_typed<float>(A, stream);
+        if (st || ! A->code) return st;
+        const char * v = getenv("HB2_ELL_COMPACT");
+        if (v && strncmp(v, "force", 5) == 0)
+        {
+            // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
+            // rows per thread, no autotuning
+            const int r = atoi(v + 5);
+            A->compact_rpt = A->compact_rpt_red = (r == 4 || r == 8) ? r : 2;
+            return HB2_OK;
+        }
+        return autotune(A, stream);
+    }
+
+    void ell_free_compact(hb2_ell_s * A)
+    {
+        cudaFree(A->table);
+        cudaFree(A->code);
+        cudaFree(A->delta);
+        A->table = 0;
+        A->code = 0;
+        A->delta = 0;
+    }
+}

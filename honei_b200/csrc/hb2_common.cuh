@@ -81,40 +81,65 @@ namespace hb2
         return r;
     }
 
-    // Workspace used by the fused reductions of one stream: block partials and
-    // the ticket counter.  One per (device, stream) user; see workspace.cu.
+    // Workspace used by the fused reductions of one stream: block partials,
+    // group partials and ticket counters.
     struct ReduceSlot
     {
-        double * partials;      // >= max_blocks
-        unsigned * ticket;      // zero between launches
+        double * partials;      // >= blocks * vectors
+        double * gpart;         // >= groups * vectors
+        unsigned * ticket;      // >= (groups + 1) * vectors, zero between launches
         uint32_t max_blocks;
     };
 
-    // Called by every block after it computed `v` (valid in all threads).  The
-    // last block writes the total to *out (and optionally sqrt) and re-arms the
-    // ticket.  Returns true in the block that finished the reduction.
+    constexpr unsigned kReduceGroup = 32;
+
+    // Called by every block after it computed `v` (valid in all threads).  Two
+    // levels: the last block of each group of kReduceGroup blocks sums the
+    // group's partials, the last group sums the group partials -- each in a
+    // fixed order, so the result depends only on the data and the launch
+    // shape, and no counter takes more than kReduceGroup atomics.  Vector
+    // blockIdx.y of a batched launch uses its own partials and counters.  The
+    // finishing block writes *out (sqrt when asked) and re-arms the counters.
     __device__ __forceinline__ bool grid_sum_finish(double v, ReduceSlot rs, double * out, int want_sqrt,
             double * scratch)
     {
-        __shared__ bool is_last;
+        __shared__ int stage;
+        const unsigned G = gridDim.x, ngroups = (G + kReduceGroup - 1) / kReduceGroup;
+        const unsigned group = blockIdx.x / kReduceGroup;
+        const unsigned gsize = min(kReduceGroup, G - group * kReduceGroup);
+        double * partials = rs.partials + (uint64_t)blockIdx.y * G;
+        double * gpart = rs.gpart + (uint64_t)blockIdx.y * ngroups;
+        unsigned * ticket = rs.ticket + (uint64_t)blockIdx.y * (ngroups + 1);
         if (threadIdx.x == 0)
         {
-            rs.partials[blockIdx.x] = v;
+            partials[blockIdx.x] = v;
             __threadfence();
-            unsigned t = atomicAdd(rs.ticket, 1u);
-            is_last = (t == gridDim.x - 1);
+            const unsigned t = atomicAdd(ticket + 1 + group, 1u);
+            stage = (t == gsize - 1);
         }
         __syncthreads();
-        if (! is_last) return false;
+        if (! stage) return false;
         __threadfence();
-        double s = 0.0;
-        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
-            s += ((volatile double *)rs.partials)[i];
+        double s = threadIdx.x < gsize ? ((volatile double *)partials)[group * kReduceGroup + threadIdx.x] : 0.0;
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0)
+        {
+            gpart[group] = s;
+            ticket[1 + group] = 0;
+            __threadfence();
+            const unsigned t = atomicAdd(ticket, 1u);
+            stage = (t == ngroups - 1);
+        }
+        __syncthreads();
+        if (! stage) return false;
+        __threadfence();
+        s = 0.0;
+        for (unsigned i = threadIdx.x; i < ngroups; i += blockDim.x) s += ((volatile double *)gpart)[i];
         s = block_sum(s, scratch);
         if (threadIdx.x == 0)
         {
             out[0] = want_sqrt ? sqrt(s) : s;
-            *rs.ticket = 0;
+            ticket[0] = 0;
         }
         return true;
     }
@@ -181,13 +206,23 @@ namespace hb2
     {
         int device;
         double * partials;       // max_blocks doubles
-        unsigned * ticket;       // 1
+        double * gpart;          // max_blocks / kReduceGroup + 4096 doubles
+        unsigned * ticket;       // max_tickets
         unsigned * bar_words;    // 2 (count, gen)
         int * error;             // 1
         double * scalars;        // 64 doubles of solver scalars
         uint32_t max_blocks;
+        uint32_t max_tickets;
         double * host_scalars;   // pinned, 64 doubles
-        ReduceSlot slot() const { ReduceSlot r; r.partials = partials; r.ticket = ticket; r.max_blocks = max_blocks; return r; }
+        ReduceSlot slot() const
+        {
+            ReduceSlot r;
+            r.partials = partials;
+            r.gpart = gpart;
+            r.ticket = ticket;
+            r.max_blocks = max_blocks;
+            return r;
+        }
         GridBarrier barrier() const { GridBarrier g; g.count = bar_words; g.gen = bar_words + 1; g.error = error; return g; }
     };
 

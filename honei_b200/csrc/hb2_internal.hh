@@ -48,6 +48,15 @@ struct hb2_ell_s
     int32_t * col;     // K * ld column indices (-1 = empty)
     uint64_t ref_stride, ref_K, ref_T;
     uint64_t bytes;
+    // optional compressed layout (ell_compact.cu): 1-byte value codes into
+    // `table`, 16-bit column offsets from the row's base column
+    uint8_t * code = nullptr;
+    int16_t * delta = nullptr;
+    void * table = nullptr;
+    uint32_t ntable = 0;
+    uint64_t compact_bytes = 0;
+    int compact_rpt = 2;       // rows per thread of the compressed kernel (autotuned)
+    int compact_rpt_red = 2;   // the same for the modes with a fused reduction
 
     template <typename T> hb2::EllView<T> view() const
     {
@@ -91,12 +100,33 @@ namespace hb2
         kKeepL2 = 2
     };
 
+    // Batch dimension of the ELL family: nvec vectors stored one after another
+    // (vector j of x / y / aux / zero at element offset j * vstride, of red at j);
+    // the matrix and aux2 (the Jacobi vector) are shared; a vector whose
+    // active[j] is 0 is skipped entirely.
+    struct Batch
+    {
+        uint32_t nvec = 1;
+        uint64_t vstride = 0;
+        uint64_t zstride = 0;          // element offset between the `zero` vectors
+        const uint8_t * active = nullptr;
+    };
+
     // Launch one ELL kernel on `stream`.  aux: rhs / b; aux2: Jacobi P; zero:
     // vector cleared by kRestrict; red: device double receiving the fused
-    // reduction (nullable, kDefect / kDot); ws: workspace for the reduction.
+    // reduction (nullable, kDefect / kDot); ws: workspace for the reduction
+    // (max_blocks must cover the grid times nvec).
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
                    void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream,
-                   int flags = 0);
+                   int flags = 0, const Batch * batch = nullptr);
+
+    // compressed ELL layout (ell_compact.cu)
+    int ell_build_compact(hb2_ell_s * A, cudaStream_t stream);
+    void ell_free_compact(hb2_ell_s * A);
+    unsigned compact_grid(const hb2_ell_s * A, bool reducing);
+    void launch_ell_compact(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                            const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                            cudaStream_t stream, int flags, Batch b);
 
     // BLAS-1 helpers (blas1.cu) usable from other translation units.
     int launch_fill(int dt, void * x, double value, uint64_t n, cudaStream_t stream);

@@ -14,7 +14,7 @@
 //    at most kNoAllocMaxBlocks * 512 rows in FP64 (8,388,608) and
 //    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216); larger matrices are
 //    rejected with HB2_ERR_UNSUPPORTED before anything is launched;
-//  * every GPU that loads the library holds the array (about 128 KiB) until the
+//  * every GPU that loads the library holds the array (about 136 KiB) until the
 //    process exits;
 //  * all calls on a device share the one array: calls whose kernels overlap on
 //    the GPU (different streams without ordering between them) race on it and
@@ -32,8 +32,11 @@ namespace hb2
     constexpr uint32_t kNoAllocMaxBlocks = 16384;
     constexpr int kNoAllocMaxDevices = 64;
 
-    // [0, kNoAllocMaxBlocks) doubles: block partials; then the ticket counter.
-    static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + 32];
+    // Layout (in doubles): [0, kNoAllocMaxBlocks) block partials, then
+    // kNoAllocGroups group partials, then kNoAllocGroups + 1 ticket counters.
+    constexpr uint32_t kNoAllocGroups = kNoAllocMaxBlocks / kReduceGroup;
+    constexpr uint32_t kNoAllocTicketDoubles = (kNoAllocGroups + 1 + 1) / 2 + 1;
+    static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + kNoAllocGroups + kNoAllocTicketDoubles];
 
     static std::mutex g_noalloc_mutex;
     static void * g_noalloc_addr[kNoAllocMaxDevices];
@@ -76,18 +79,20 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
     double * scratch = 0;
     int st = noalloc_scratch(&scratch);
     if (st) return st;
-    // the ticket must start at zero; the previous call's contents are otherwise
-    // left as they were (the partials are written before they are read)
-    unsigned * ticket = (unsigned *)(scratch + kNoAllocMaxBlocks);
-    HB2_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), stream));
+    // the ticket counters must start at zero; the previous call's contents are
+    // otherwise left as they were (the partials are written before they are read)
+    unsigned * ticket = (unsigned *)(scratch + kNoAllocMaxBlocks + kNoAllocGroups);
+    HB2_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * (kNoAllocGroups + 1), stream));
     Workspace ws;
     ws.device = 0;
     ws.partials = scratch;
+    ws.gpart = scratch + kNoAllocMaxBlocks;
     ws.ticket = ticket;
     ws.bar_words = 0;
     ws.error = 0;
     ws.scalars = 0;
     ws.max_blocks = kNoAllocMaxBlocks;
+    ws.max_tickets = kNoAllocGroups + 1;
     ws.host_scalars = 0;
     return launch_ell(A, kDefect, x, r, rhs, 0, 0, norm2_dev, 0, &ws, stream);
 }

@@ -47,19 +47,23 @@ namespace hb2
         Workspace * w = new Workspace();
         w->max_blocks = max_blocks;
         cudaGetDevice(&w->device);
-        // one allocation: partials | scalars | ticket, barrier words, error flag
-        size_t bytes = sizeof(double) * (max_blocks + 64) + 64;
+        // one allocation: partials | group partials | scalars | tickets | barrier words, error flag
+        const uint32_t max_tickets = 1u << 16;
+        const uint32_t ngpart = max_blocks / kReduceGroup + 4096;
+        size_t bytes = sizeof(double) * (max_blocks + ngpart + 64) + sizeof(unsigned) * max_tickets + 64;
         char * base = 0;
         cudaError_t e = cudaMalloc(&base, bytes);
         if (e != cudaSuccess) { delete w; return cuda_status(e, "workspace cudaMalloc"); }
         e = cudaMemset(base, 0, bytes);
         if (e != cudaSuccess) { cudaFree(base); delete w; return cuda_status(e, "workspace cudaMemset"); }
         w->partials = (double *)base;
-        w->scalars = w->partials + max_blocks;
+        w->gpart = w->partials + max_blocks;
+        w->scalars = w->gpart + ngpart;
         unsigned * words = (unsigned *)(w->scalars + 64);
         w->ticket = words;
-        w->bar_words = words + 4;
-        w->error = (int *)(words + 8);
+        w->max_tickets = max_tickets;
+        w->bar_words = words + max_tickets;
+        w->error = (int *)(words + max_tickets + 4);
         e = cudaMallocHost(&w->host_scalars, sizeof(double) * 64);
         if (e != cudaSuccess) { cudaFree(base); delete w; return cuda_status(e, "workspace cudaMallocHost"); }
         *out = w;

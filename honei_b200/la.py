@@ -147,6 +147,12 @@ class SparseMatrixELL:
     def columns(self) -> int:
         return self._cols
 
+    def layout(self):
+        """(compact, table_size, bytes_per_slot) of the device layout in use."""
+        c, t, sb = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_uint32()
+        call("hb2_ell_layout", self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(sb))
+        return bool(c.value), t.value, sb.value
+
     def stride(self) -> int:
         return self._stride
 

@@ -97,6 +97,11 @@ HB2_API int hb2_ell_destroy(hb2_ell A);
 /* rows, cols, reference stride / num_cols_per_row / threads, device bytes */
 HB2_API int hb2_ell_info(hb2_ell A, uint64_t *rows, uint64_t *cols, uint64_t *stride, uint64_t *num_cols_per_row,
                  uint64_t *threads, uint64_t *device_bytes);
+/* Device layout in use: *compact = 1 when slots are stored as 1-byte value codes
+ * (a per-matrix table of *table_size distinct values) plus 16-bit column offsets,
+ * 0 for plain values + int32 columns; *slot_bytes = bytes per stored slot.
+ * No counterpart in the reference (its device copy is the raw arrays). */
+HB2_API int hb2_ell_layout(hb2_ell A, int *compact, uint32_t *table_size, uint32_t *slot_bytes);
 /* Download the matrix in the reference layout (host arrays of K*stride, K*stride
  * and rows elements); Arl as the reference computes it. */
 HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);

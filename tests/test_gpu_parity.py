@@ -427,3 +427,58 @@ def test_ir_mixed_fp64_coarse(oracle):
     x64, _, _ = oracle.mg_q1(L, b, max_iters_coarse=100)
     assert np.linalg.norm(xs - x64) / np.linalg.norm(x64) < 1e-6
     assert it <= 6
+
+
+@pytest.mark.parametrize("rpt", [2, 4, 8])
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, rpt):
+    """Value-dictionary + 16-bit offset layout: same bits as the plain layout (and the oracle)
+    for every ELL kernel mode, square and rectangular."""
+    from honei_b200 import _lib
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    L = 9
+    monkeypatch.setenv("HB2_ELL_COMPACT", f"force{rpt}")   # compressed layout, no autotuning
+    A = SparseMatrixELL.poisson_q1(L, dt)
+    P, R = SparseMatrixELL.transfer(L, dt)
+    assert A.layout()[0] and A.layout()[1] == 3 and P.layout()[0] and R.layout()[0]
+    monkeypatch.setenv("HB2_ELL_COMPACT", "0")
+    A0 = SparseMatrixELL.poisson_q1(L, dt)
+    P0, R0 = SparseMatrixELL.transfer(L, dt)
+    assert not A0.layout()[0] and not P0.layout()[0]
+    n, nc = A.rows(), R.rows()
+    x, b = oracle.uniform(n, 3, npdt), oracle.uniform(n, 4, npdt)
+    c = oracle.uniform(nc, 5, npdt)
+    Pj = hb.RISmoother.jacobi_precon(A0)
+    outs = []
+    for (M, Pm, Rm) in ((A, P, R), (A0, P0, R0)):
+        y, r, s = dvec(np.zeros(n, npdt)), dvec(np.zeros(n, npdt)), dvec(np.zeros(n, npdt))
+        hb.Product.value(y, M, dvec(x))
+        nrm = torch.zeros(1, dtype=torch.float64, device=DEV)
+        hb.Defect.value(r, dvec(b), M, dvec(x), norm2_out=nrm)
+        _lib.call("hb2_jacobi_sweep_ell", M.handle, Pj.ptr, dvec(b).ptr, dvec(x).ptr, s.ptr, None)
+        f, cc = dvec(x.copy()), dvec(np.zeros(nc, npdt))
+        _lib.call("hb2_product_add_ell", Pm.handle, dvec(c).ptr, f.ptr, None)
+        hb.Restriction.value(cc, dvec(x), resmat=Rm, method=hb.methods.PROLMAT)
+        outs.append([host(v) for v in (y, r, s, f, cc)] + [nrm.item()])
+    for a, b_ in zip(outs[0][:5], outs[1][:5]):
+        assert same_bits(a, b_)
+    # the fused norm's tree order follows the launch shape (rows per thread)
+    assert abs(outs[0][5] - outs[1][5]) <= 1e-12 * outs[1][5]
+    assert same_bits(outs[0][0], oracle.ell_spmv(oracle.q1_ell(L, npdt), x))
+
+
+def test_compressed_layout_falls_back_when_not_eligible(oracle):
+    """More than 255 distinct values -> plain layout, still correct."""
+    L = 8
+    ref = oracle.q1_ell(L)
+    Ax = ref.Ax.copy()
+    nz = ref.Aj >= 0
+    Ax[Ax != 0] = oracle.uniform(int((Ax != 0).sum()), 77) + 2.0   # many distinct values
+    Arl = ref.Arl
+    A = SparseMatrixELL.from_arrays(ref.rows, ref.cols, ref.stride, ref.K, ref.Aj, Ax, Arl)
+    assert not A.layout()[0]
+    ref2 = oracle.Ell(ref.rows, ref.cols, ref.stride, ref.K, 1, ref.Aj, Ax, Arl)
+    x = oracle.uniform(ref.cols, 1)
+    y = dvec(np.zeros(ref.rows))
+    hb.Product.value(y, A, dvec(x))
+    assert same_bits(host(y), oracle.ell_spmv(ref2, x))
