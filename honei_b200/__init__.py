@@ -7,12 +7,12 @@ operator call without the built library raises ImportError.
 from ._lib import DeviceTimeout, HoneiError, NotFinite, VectorSizeDoesNotMatch, launch_count
 from .la import (BandedMatrixQx, Defect, DenseVector, Difference, DotProduct, ElementProduct, Norm, Product, Scale,
                  ScaledSum, SparseMatrixELL, Sum, convert, copy, fill, tags)
-from .solvers import (CGSolver, IRSolver, MGData, MGSolver, Prolongation, Restriction, RISmoother, methods,
-                      mg_params)
+from .solvers import (BatchedPoissonSolver, CGSolver, IRSolver, MGData, MGSolver, Prolongation, Restriction,
+                      RISmoother, batch_params, methods, mg_params)
 
 __all__ = [
-    "BandedMatrixQx", "CGSolver", "Defect", "DenseVector", "DeviceTimeout", "Difference", "DotProduct",
+    "BandedMatrixQx", "BatchedPoissonSolver", "CGSolver", "Defect", "DenseVector", "DeviceTimeout", "Difference", "DotProduct",
     "ElementProduct", "HoneiError", "IRSolver", "MGData", "MGSolver", "Norm", "NotFinite", "Product",
     "Prolongation", "RISmoother", "Restriction", "Scale", "ScaledSum", "SparseMatrixELL", "Sum",
-    "VectorSizeDoesNotMatch", "convert", "copy", "fill", "launch_count", "methods", "mg_params", "tags",
+    "VectorSizeDoesNotMatch", "batch_params", "convert", "copy", "fill", "launch_count", "methods", "mg_params", "tags",
 ]

@@ -58,6 +58,12 @@ class MgParams(ctypes.Structure):
                 ("coarse_exact", _int), ("no_fused_levels", _int), ("coarse_fp64", _int)]
 
 
+class BatchParams(ctypes.Structure):
+    """hb2_batch_params"""
+    _fields_ = [("max_iters", _u64), ("eps_relative", _dbl), ("n_pre_smooth", _u64), ("n_post_smooth", _u64),
+                ("max_iters_coarse", _u64), ("coarse_eps", _dbl), ("omega", _dbl)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "hb2_last_error": (ctypes.c_char_p, []),
@@ -105,6 +111,14 @@ SIGNATURES = {
     "hb2_mg_solve": (_int, [_vp, _vp, _vp, _pdbl, _vp]),
     "hb2_mg_cycle": (_int, [_vp, _vp, _vp, _vp]),
     "hb2_ir_solve": (_int, [_vp, _vp, _vp, _vp, _dbl, _u64, _int, _pdbl, _vp]),
+    "hb2_batch_create_q1": (_int, [_pvp, _u32, _vp, _vp, ctypes.c_uint, ctypes.POINTER(BatchParams), _vp]),
+    "hb2_batch_destroy": (_int, [_vp]),
+    "hb2_batch_info": (_int, [_vp, ctypes.POINTER(_u32), _pu64, _pu64]),
+    "hb2_batch_copy": (_int, [_vp, _u32, _int, _vp, _vp]),
+    "hb2_batch_start": (_int, [_vp, _u32, _dbl, _int, _vp]),
+    "hb2_batch_step": (_int, [_vp, _u32, _vp, _vp]),
+    "hb2_batch_solve": (_int, [_vp, _int, _pu64, _vp]),
+    "hb2_batch_result": (_int, [_vp, _u32, _u32, _pu64, _pdbl]),
 }
 
 _lib = None

@@ -282,10 +282,14 @@ namespace hb2
     template <typename T, typename S, int RPL>
     __global__ void __launch_bounds__(32)
     cg_warp_reg_kernel(EllView<T> Ag, const S * __restrict__ b, S * __restrict__ xg, uint64_t max_iters, double eps_d,
-                       int exact, uint64_t * used_out, double * defect_out)
+                       int exact, uint64_t * used_out, double * defect_out, uint64_t vstride, const uint8_t * active)
     {
         typedef Arith<T> M;
         constexpr int K = 9;
+        // batched launches: block j solves the system of vector j (b, x at j * vstride)
+        if (active && ! active[blockIdx.x]) return;
+        b += (uint64_t)blockIdx.x * vstride;
+        xg += (uint64_t)blockIdx.x * vstride;
         extern __shared__ __align__(16) unsigned char smem_raw[];
         const int n = (int)Ag.rows, lane = threadIdx.x;
         T * sp = (T *)smem_raw;   // p (and x for the initial defect)
@@ -399,7 +403,8 @@ namespace hb2
 
     template <typename T, typename S>
     static bool launch_warp_reg(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
-                                uint64_t * used_dev, double * defect_dev, cudaStream_t stream)
+                                uint64_t * used_dev, double * defect_dev, cudaStream_t stream, uint32_t nvec = 1,
+                                uint64_t vstride = 0, const uint8_t * active = nullptr)
     {
         if (A->K != 9 || A->rows > 128) return false;
         const int rpl = (int)((A->rows + 31) / 32);
@@ -409,12 +414,33 @@ namespace hb2
         S * xp = (S *)x;
         switch (rpl)
         {
-            case 1: cg_warp_reg_kernel<T, S, 1><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            case 2: cg_warp_reg_kernel<T, S, 2><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            case 3: cg_warp_reg_kernel<T, S, 3><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
-            default: cg_warp_reg_kernel<T, S, 4><<<1, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev); break;
+            case 1: cg_warp_reg_kernel<T, S, 1><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
+            case 2: cg_warp_reg_kernel<T, S, 2><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
+            case 3: cg_warp_reg_kernel<T, S, 3><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
+            default: cg_warp_reg_kernel<T, S, 4><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
         }
         return true;
+    }
+
+    // nvec independent coarse systems with one operator, one warp each: FP64
+    // arithmetic on FP32 vectors (A64 FP64) or in the operator's own type
+    int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
+                               uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
+                               cudaStream_t stream)
+    {
+        if (nvec == 0) return HB2_OK;
+        bool ok;
+        if (A->dtype == HB2_F64 && vec_dtype == HB2_F32)
+            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+        else if (A->dtype == HB2_F64 && vec_dtype == HB2_F64)
+            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+        else if (A->dtype == HB2_F32 && vec_dtype == HB2_F32)
+            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+        else return fail(HB2_ERR_ARG, "batched coarse CG: unsupported element types");
+        if (! ok) return fail(HB2_ERR_UNSUPPORTED, "batched coarse CG: the coarsest level needs <= 128 rows and 9 slots");
+        count_launches(1);
+        HB2_LAUNCH_CHECK("cg_warp_reg_kernel (batched)");
+        return HB2_OK;
     }
 
     bool cg_mixed_supported(const hb2_ell_s * A64) { return A64->dtype == HB2_F64 && A64->K == 9 && A64->rows <= 128; }

@@ -68,7 +68,7 @@ namespace hb2
         if (bt.active && ! bt.active[blockIdx.y]) return;
         {
             const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
-            x += vo;
+            x += (uint64_t)blockIdx.y * (bt.xstride ? bt.xstride : bt.vstride);
             y += vo;
             if (aux) aux += vo;
             if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;

@@ -17,6 +17,9 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace hb2
@@ -150,7 +153,7 @@ namespace hb2
         if (bt.active && ! bt.active[blockIdx.y]) return;
         {
             const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
-            x += vo;
+            x += (uint64_t)blockIdx.y * (bt.xstride ? bt.xstride : bt.vstride);
             y += vo;
             if (aux) aux += vo;
             if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;
@@ -384,8 +387,51 @@ namespace hb2
     // timed launches each, after one warm-up), and keep the fastest for each of
     // the two kernel classes; the compressed arrays are freed when the plain
     // layout wins both.  Runs once per matrix, at creation, on `stream`.
+    // The decision is kept per (device, element type, shape, slots, table size)
+    // for the life of the process: matrices of one shape always run the same
+    // launch shape, so a reduction over them sums in the same order whichever
+    // matrix instance (or solver built on it) computes it.
+    struct TuneKey
+    {
+        int device, dtype;
+        uint64_t rows, cols;
+        uint32_t K, ntable;
+        bool operator<(const TuneKey & o) const
+        {
+            return std::tie(device, dtype, rows, cols, K, ntable) < std::tie(o.device, o.dtype, o.rows, o.cols, o.K, o.ntable);
+        }
+    };
+    static std::mutex g_tune_mutex;
+    static std::map<TuneKey, std::pair<int, int>> g_tune;
+
+    static void apply_decision(hb2_ell_s * A, int plain_v, int red_v)
+    {
+        if (plain_v == 0 && red_v == 0)
+        {
+            ell_free_compact(A);
+            A->compact_bytes = 0;
+        }
+        else
+        {
+            // one layout serves both classes: if only one class prefers plain,
+            // the compressed kernel runs at that class's fastest compressed shape
+            A->compact_rpt = plain_v ? plain_v : (red_v ? red_v : 2);
+            A->compact_rpt_red = red_v ? red_v : A->compact_rpt;
+        }
+    }
+
     static int autotune(hb2_ell_s * A, cudaStream_t s)
     {
+        const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable};
+        {
+            std::lock_guard<std::mutex> lock(g_tune_mutex);
+            auto it = g_tune.find(key);
+            if (it != g_tune.end())
+            {
+                apply_decision(A, it->second.first, it->second.second);
+                return HB2_OK;
+            }
+        }
         const size_t es = dtype_size(A->dtype);
         const bool square = A->rows == A->cols;
         Workspace * ws = 0;
@@ -432,18 +478,11 @@ namespace hb2
         A->code = code;
         if (st) return st;
         if (! square) best_v[1] = best_v[0];
-        if (best_v[0] == 0 && best_v[1] == 0)
         {
-            ell_free_compact(A);
-            A->compact_bytes = 0;
+            std::lock_guard<std::mutex> lock(g_tune_mutex);
+            g_tune[key] = std::make_pair(best_v[0], best_v[1]);
         }
-        else
-        {
-            // one layout serves both classes: if only one class prefers plain,
-            // the compressed kernel runs at that class's fastest compressed shape
-            A->compact_rpt = best_v[0] ? best_v[0] : (best_v[1] ? best_v[1] : 2);
-            A->compact_rpt_red = best_v[1] ? best_v[1] : A->compact_rpt;
-        }
+        apply_decision(A, best_v[0], best_v[1]);
         HB2_LAUNCH_CHECK("ELL layout autotuning");
         return HB2_OK;
     }

@@ -100,19 +100,21 @@ namespace hb2
     // shape, and no counter takes more than kReduceGroup atomics.  Vector
     // blockIdx.y of a batched launch uses its own partials and counters.  The
     // finishing block writes *out (sqrt when asked) and re-arms the counters.
-    __device__ __forceinline__ bool grid_sum_finish(double v, ReduceSlot rs, double * out, int want_sqrt,
-            double * scratch)
+    //
+    // sum_finish is the same reduction over G blocks of one vector whose block
+    // index `blk` (0..G-1) and scratch (partials: G doubles, gpart: groups
+    // doubles, ticket: groups + 1 counters) the caller chose, for launches that
+    // map blocks to vectors through a work list.
+    __device__ __forceinline__ bool sum_finish(double v, double * partials, double * gpart, unsigned * ticket,
+                                               unsigned G, unsigned blk, double * out, int want_sqrt, double * scratch)
     {
         __shared__ int stage;
-        const unsigned G = gridDim.x, ngroups = (G + kReduceGroup - 1) / kReduceGroup;
-        const unsigned group = blockIdx.x / kReduceGroup;
+        const unsigned ngroups = (G + kReduceGroup - 1) / kReduceGroup;
+        const unsigned group = blk / kReduceGroup;
         const unsigned gsize = min(kReduceGroup, G - group * kReduceGroup);
-        double * partials = rs.partials + (uint64_t)blockIdx.y * G;
-        double * gpart = rs.gpart + (uint64_t)blockIdx.y * ngroups;
-        unsigned * ticket = rs.ticket + (uint64_t)blockIdx.y * (ngroups + 1);
         if (threadIdx.x == 0)
         {
-            partials[blockIdx.x] = v;
+            partials[blk] = v;
             __threadfence();
             const unsigned t = atomicAdd(ticket + 1 + group, 1u);
             stage = (t == gsize - 1);
@@ -142,6 +144,14 @@ namespace hb2
             ticket[0] = 0;
         }
         return true;
+    }
+
+    __device__ __forceinline__ bool grid_sum_finish(double v, ReduceSlot rs, double * out, int want_sqrt,
+            double * scratch)
+    {
+        const unsigned G = gridDim.x, ngroups = (G + kReduceGroup - 1) / kReduceGroup;
+        return sum_finish(v, rs.partials + (uint64_t)blockIdx.y * G, rs.gpart + (uint64_t)blockIdx.y * ngroups,
+                          rs.ticket + (uint64_t)blockIdx.y * (ngroups + 1), G, blockIdx.x, out, want_sqrt, scratch);
     }
 
     // ------------------------------------------------------------------

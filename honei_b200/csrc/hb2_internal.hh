@@ -101,13 +101,16 @@ namespace hb2
     };
 
     // Batch dimension of the ELL family: nvec vectors stored one after another
-    // (vector j of x / y / aux / zero at element offset j * vstride, of red at j);
+    // (vector j of y / aux at element offset j * vstride, of x at j * xstride
+    // -- xstride 0 means vstride; a rectangular transfer matrix reads and
+    // writes vectors of two levels --, of zero at j * zstride, of red at j);
     // the matrix and aux2 (the Jacobi vector) are shared; a vector whose
     // active[j] is 0 is skipped entirely.
     struct Batch
     {
         uint32_t nvec = 1;
         uint64_t vstride = 0;
+        uint64_t xstride = 0;
         uint64_t zstride = 0;          // element offset between the `zero` vectors
         const uint8_t * active = nullptr;
     };
@@ -162,4 +165,7 @@ namespace hb2
     bool cg_mixed_supported(const hb2_ell_s * A64);
     int launch_cg_small_f32io(const hb2_ell_s * A64, const void * b32, void * x32, uint64_t max_iters, double eps,
                               int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
+    int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
+                               uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
+                               cudaStream_t stream);
 }

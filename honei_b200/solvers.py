@@ -173,3 +173,88 @@ class IRSolver:
         call("hb2_ir_solve", A.handle, inner.handle, b.ptr, x.ptr, float(eps), int(max_iters), int(bool(reset_inner)),
              stats, _stream(stream))
         return x, int(stats[0]), list(stats)
+
+
+def batch_params(max_iters=100, eps=1e-8, n_pre=4, n_post=4, max_iters_coarse=100, coarse_eps=1e-10,
+                 omega=0.7) -> _lib.BatchParams:
+    return _lib.BatchParams(max_iters, eps, n_pre, n_post, max_iters_coarse, coarse_eps, omega)
+
+
+class BatchedPoissonSolver:
+    """Many Q1 Poisson systems (different levels, one or more right-hand sides
+    each) solved together: CGSolver<B200, methods::VAR> (math/cg.hh:142-210)
+    preconditioned by one mixed-precision MG V-cycle, every PCG step of the
+    whole batch one CUDA graph.
+
+    ``systems``: list of (level, nrhs).  Vectors are FP64 torch tensors of shape
+    (nrhs, (2^level+1)^2), on the device or on the host."""
+
+    def __init__(self, systems, coarse_level=3, params: _lib.BatchParams | None = None, stream=None):
+        self.systems = [(int(l), int(k)) for l, k in systems]
+        self.params = params or batch_params()
+        n = len(self.systems)
+        levels = (ctypes.c_uint32 * n)(*[l for l, _ in self.systems])
+        nrhs = (ctypes.c_uint32 * n)(*[k for _, k in self.systems])
+        h = ctypes.c_void_p()
+        call("hb2_batch_create_q1", ctypes.byref(h), n, levels, nrhs, int(coarse_level), ctypes.byref(self.params),
+             _stream(stream))
+        self._h = h
+        self.steps = 0
+
+    @staticmethod
+    def unknowns(level):
+        return ((1 << level) + 1) ** 2
+
+    def info(self):
+        nv, nb, nl = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64()
+        call("hb2_batch_info", self._h, ctypes.byref(nv), ctypes.byref(nb), ctypes.byref(nl))
+        return {"vectors": nv.value, "device_bytes": nb.value, "launches_per_step": nl.value}
+
+    def _buf(self, system, t):
+        level, k = self.systems[system]
+        if t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != k * self.unknowns(level):
+            raise _lib.VectorSizeDoesNotMatch(_lib.HB2_ERR_SIZE,
+                                              f"system {system}: expected {k} x {self.unknowns(level)} contiguous FP64")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def set_rhs(self, system, b, stream=None):
+        call("hb2_batch_copy", self._h, system, 0, self._buf(system, b), _stream(stream))
+
+    def set_guess(self, system, x, stream=None):
+        call("hb2_batch_copy", self._h, system, 1, self._buf(system, x), _stream(stream))
+
+    def solution(self, system, out=None, stream=None):
+        level, k = self.systems[system]
+        if out is None:
+            out = torch.empty((k, self.unknowns(level)), dtype=torch.float64, device="cuda")
+        call("hb2_batch_copy", self._h, system, 2, self._buf(system, out), _stream(stream))
+        return out
+
+    def start(self, system, eps=0.0, zero_guess=True, stream=None):
+        call("hb2_batch_start", self._h, system, float(eps), int(bool(zero_guess)), _stream(stream))
+
+    def step(self, steps=1, stream=None):
+        """Runs `steps` PCG steps; returns the indices of the systems with nothing left to do."""
+        done = (ctypes.c_uint8 * len(self.systems))()
+        call("hb2_batch_step", self._h, int(steps), done, _stream(stream))
+        return [i for i in range(len(self.systems)) if done[i]]
+
+    def solve(self, zero_guess=True, stream=None):
+        steps = ctypes.c_uint64()
+        call("hb2_batch_solve", self._h, int(bool(zero_guess)), ctypes.byref(steps), _stream(stream))
+        self.steps = steps.value
+        return self.steps
+
+    def result(self, system, rhs=0):
+        """(iterations, final ||r|| / ||r0||) of one right-hand side."""
+        it, rel = ctypes.c_uint64(), ctypes.c_double()
+        call("hb2_batch_result", self._h, system, rhs, ctypes.byref(it), ctypes.byref(rel))
+        return it.value, rel.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.load().hb2_batch_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass

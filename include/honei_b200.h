@@ -65,6 +65,7 @@ enum
 typedef struct hb2_ell_s *hb2_ell; /* SparseMatrixELL<DT> resident on the device */
 typedef struct hb2_q1_s *hb2_q1;   /* BandedMatrixQx<Q1Type, DT> resident on the device */
 typedef struct hb2_mg_s *hb2_mg;   /* MGData + V-cycle OperatorList resident on the device */
+typedef struct hb2_batch_s *hb2_batch; /* many Q1 systems solved together (batched PCG) */
 
 /* ---------------------------------------------------------------- runtime */
 HB2_API const char *hb2_last_error(void);
@@ -252,6 +253,50 @@ HB2_API int hb2_mg_cycle(hb2_mg mg, const void *b, void *x, cudaStream_t stream)
  * inner cycles.  Synchronises `stream`. */
 HB2_API int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void *b, void *x, double eps, uint64_t max_iters,
                  int reset_inner, double *stats, cudaStream_t stream);
+
+/* Batched solves: num_systems Q1 Poisson systems (level levels[s], nrhs[s]
+ * right-hand sides each, nrhs NULL = 1) solved together by
+ * CGSolver<Tag, methods::VAR> (math/cg.hh:142-210) with an MG V-cycle as the
+ * variable preconditioner.  Outer recurrence, dots, norms and stop test FP64 on
+ * the FP64 operator; the preconditioner is one V-cycle (Jacobi omega,
+ * n_pre/n_post sweeps, bilinear transfers) in FP32 with the coarsest-level CG
+ * (level coarse_level, 1..3) in FP64 arithmetic.  Each PCG step of the whole
+ * batch is one CUDA graph whose launch count depends on the deepest hierarchy,
+ * not on the number of systems: every stage is one launch over the (row block,
+ * right-hand side) pairs of all systems at that level.  A right-hand side's
+ * iterates do not depend on which other systems share the batch. */
+typedef struct
+{
+    uint64_t max_iters;                     /* PCG iterations per right-hand side (100) */
+    double eps_relative;                    /* default stop ||r|| < eps ||r0|| or ||r|| < eps (1e-8) */
+    uint64_t n_pre_smooth, n_post_smooth;   /* 4, 4 */
+    uint64_t max_iters_coarse;              /* coarse CG iterations (100) */
+    double coarse_eps;                      /* coarse CG relative tolerance (1e-10) */
+    double omega;                           /* Jacobi damping (0.7) */
+} hb2_batch_params;
+
+HB2_API int hb2_batch_create_q1(hb2_batch *out, uint32_t num_systems, const uint32_t *levels, const uint32_t *nrhs,
+                        unsigned coarse_level, const hb2_batch_params *params, cudaStream_t stream);
+HB2_API int hb2_batch_destroy(hb2_batch B);
+/* right-hand sides in total, device bytes held, kernel launches per PCG step */
+HB2_API int hb2_batch_info(hb2_batch B, uint32_t *num_vectors, uint64_t *device_bytes, uint64_t *launches_per_step);
+/* which = 0: set b, 1: set x (initial guess), 2: read x.  buf (host or device)
+ * holds the system's nrhs vectors of (2^level+1)^2 doubles one after another. */
+HB2_API int hb2_batch_copy(hb2_batch B, uint32_t system, int which, void *buf, cudaStream_t stream);
+/* queue a system for solving at the next step (eps_relative <= 0: the default);
+ * zero_guess = 1 starts from x = 0, else from the x it holds */
+HB2_API int hb2_batch_start(hb2_batch B, uint32_t system, double eps_relative, int zero_guess, cudaStream_t stream);
+/* run `steps` PCG steps of every queued or running system; done (nullable, host,
+ * num_systems bytes) receives 1 for each system with nothing left to do.
+ * Synchronises `stream`. */
+HB2_API int hb2_batch_step(hb2_batch B, uint32_t steps, uint8_t *done, cudaStream_t stream);
+/* start every system and step until all are done, in one graph launch (the loop
+ * runs on the device); steps (nullable) receives the number of steps.
+ * Synchronises `stream`. */
+HB2_API int hb2_batch_solve(hb2_batch B, int zero_guess, uint64_t *steps, cudaStream_t stream);
+/* iterations and final ||r||/||r0|| of one right-hand side, as of the last
+ * hb2_batch_step / hb2_batch_solve */
+HB2_API int hb2_batch_result(hb2_batch B, uint32_t system, uint32_t rhs, uint64_t *iters, double *rel_defect);
 
 #ifdef __cplusplus
 }
