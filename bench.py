@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--level", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     return ap.parse_args()
 
 
@@ -358,6 +359,8 @@ def main():
     if not args.no_mixed:
         line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5), min(args.warmup, 2),
                                               rank)
+    if not args.no_batch:
+        line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(L)
     if rank == 0:
@@ -430,6 +433,111 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
             "mixed_ir_ms": tir, "ir_outer_iters": info["outer"], "ir_inner_fp32_cycles": info["inner"],
             "mixed_relres": relir, "mixed_rel_error_vs_fp64": err, "speedup_mixed_over_fp64": t64 / tir,
             "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-10"}
+
+
+def batch_workload(seed, nsys=512, lo=4, hi=9, multi_frac=0.25, multi_rhs=8):
+    """Config 3: levels uniform in lo..hi, exactly multi_frac of the systems with multi_rhs RHS."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    levels = rng.integers(lo, hi + 1, nsys)
+    nrhs = np.ones(nsys, dtype=np.int64)
+    nrhs[rng.permutation(nsys)[:int(round(multi_frac * nsys))]] = multi_rhs
+    return [(int(l), int(k)) for l, k in zip(levels, nrhs)]
+
+
+def batched_solves(hb, dev, flush, steps, warmup, rank):
+    """Config 3: 512 Q1 systems (levels U{4..9}, 25 % with 8 RHS, RHS ~ U[-1,1]) solved
+    together by the batched mixed-precision MG-preconditioned CG to 1e-8, against
+    looping the single-system FP64 MG solver (V(4,4), coarse CG cap 100) to 1e-8 over
+    the same right-hand sides.  Device time per batch solve with CUDA events (L2
+    flushed before each; the batch's vectors exceed L2); end to end adds the pinned
+    host->device copies of every RHS and the device->host copies of every solution."""
+    import statistics
+
+    import numpy as np
+    import torch
+
+    from honei_b200.inputs import uniform
+    systems = batch_workload(2024 + rank)
+    B = hb.BatchedPoissonSolver(systems)
+    info = B.info()
+    host_b, host_x, dev_b = [], [], []
+    for s, (level, k) in enumerate(systems):
+        n = B.unknowns(level)
+        hbuf = torch.from_numpy(np.stack([uniform(n, 7919 * s + j + 1) for j in range(k)])).pin_memory()
+        host_b.append(hbuf)
+        host_x.append(torch.empty_like(hbuf).pin_memory())
+        dev_b.append(hbuf.to(dev))
+    nvec = sum(k for _, k in systems)
+
+    def load_rhs(src):
+        for s in range(len(systems)):
+            B.set_rhs(s, src[s])
+
+    def timed(fn):
+        ts = []
+        for i in range(warmup + steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            if i >= warmup:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts)
+
+    load_rhs(dev_b)
+    l0 = hb.launch_count()
+    t_dev = timed(lambda: B.solve())
+    launches = (hb.launch_count() - l0) // (warmup + steps)
+    iters = [B.result(s, j)[0] for s, (_, k) in enumerate(systems) for j in range(k)]
+    rels = [B.result(s, j)[1] for s, (_, k) in enumerate(systems) for j in range(k)]
+
+    def e2e():
+        load_rhs(host_b)
+        B.solve()
+        for s in range(len(systems)):
+            B.solution(s, out=host_x[s])
+
+    t_e2e = timed(e2e)
+    # true residual of a sample of solutions, FP64 on the device
+    worst = 0.0
+    for s in range(0, len(systems), 37):
+        level, k = systems[s]
+        A = hb.SparseMatrixELL.poisson_q1(level)
+        x = B.solution(s)
+        for j in range(k):
+            r = hb.DenseVector(B.unknowns(level))
+            bj = hb.DenseVector(dev_b[s][j].clone())
+            hb.Defect.value(r, bj, A, hb.DenseVector(x[j].clone()))
+            worst = max(worst, hb.Norm.value(r) / hb.Norm.value(bj))
+    # the loop of the single-system solver: per-level median solve time x RHS count
+    per_level = {}
+    params = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-8, coarse_exact=False)
+    for level in sorted({l for l, _ in systems}):
+        data = hb.MGData.poisson_q1(MIN_LEVEL, level, params=params)
+        s = next(i for i, (l, _) in enumerate(systems) if l == level)
+        b = hb.DenseVector(dev_b[s][0].clone())
+        x = hb.DenseVector(B.unknowns(level))
+
+        def one():
+            hb.fill(x, 0.0)
+            hb.MGSolver.value(data, b, x)
+        per_level[level] = timed(one)
+        del data
+    t_loop = sum(per_level[l] * k for l, k in systems)
+    return {"systems": len(systems), "rhs": nvec, "levels": "U{4..9}", "multi_rhs_systems": sum(k > 1 for _, k in systems),
+            "device_ms": t_dev, "rhs_per_s": nvec * 1000.0 / t_dev,
+            "e2e_ms": t_e2e, "e2e_rhs_per_s": nvec * 1000.0 / t_e2e,
+            "h2d_bytes": 8 * sum(B.unknowns(l) * k for l, k in systems),
+            "pcg_steps": B.steps, "max_iters": max(iters), "mean_iters": statistics.mean(iters),
+            "max_rel_defect": max(rels), "worst_true_relres_sampled": worst,
+            "launches_per_step": info["launches_per_step"], "launches_per_solve": launches,
+            "device_bytes": info["device_bytes"],
+            "loop_fp64_mg_ms_projected": t_loop, "loop_ms_per_level": per_level,
+            "speedup_vs_loop": t_loop / t_dev,
+            "method": "CG VAR (FP64) + one FP32 MG V(4,4) preconditioner, FP64 coarse CG cap 100; tol 1e-8"}
 
 
 def ctypes_stream(stream):
