@@ -13,6 +13,7 @@
 // The stop test is the reference's: sqrt(r.r) < eps * sqrt(r0.r0) or
 // sqrt(r.r) < eps, checked after the p update; lambda and the p scaling guard
 // their divisors with machine epsilon exactly like cg.hh:99 and :106.
+#include "cg_warp.cuh"
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
 
@@ -21,16 +22,6 @@
 
 namespace hb2
 {
-    template <typename T> struct Eps;
-    template <> struct Eps<double> { static __device__ __forceinline__ double v() { return DBL_EPSILON; } };
-    template <> struct Eps<float> { static __device__ __forceinline__ float v() { return FLT_EPSILON; } };
-
-    template <typename T>
-    __device__ __forceinline__ T guard(T d)
-    {
-        return fabs(d) > Eps<T>::v() ? d : Eps<T>::v();
-    }
-
     // ------------------------------------------------------------------ small
     template <typename T>
     struct SmallMat
@@ -154,38 +145,6 @@ namespace hb2
         }
     }
 
-    // ------------------------------------------------------------------ one warp
-    // Latency-bound coarse solves (the MG coarsest level has 81 unknowns and runs
-    // a hundred iterations per V-cycle): one warp, no block barriers, reductions
-    // by shuffles.  The reference-order dot is one fma chain in lane 0 with the
-    // operands fetched ahead of the chain.
-    template <typename T>
-    __device__ __forceinline__ T warp_dot_exact(const T * a, const T * b, int n)
-    {
-        T s = T(0);
-        if ((threadIdx.x & 31) == 0)
-        {
-            int i = 0;
-            for (; i + 8 <= n; i += 8)
-            {
-                T a0 = a[i], a1 = a[i + 1], a2 = a[i + 2], a3 = a[i + 3], a4 = a[i + 4], a5 = a[i + 5], a6 = a[i + 6],
-                  a7 = a[i + 7];
-                T b0 = b[i], b1 = b[i + 1], b2 = b[i + 2], b3 = b[i + 3], b4 = b[i + 4], b5 = b[i + 5], b6 = b[i + 6],
-                  b7 = b[i + 7];
-                s = Arith<T>::fma(a0, b0, s);
-                s = Arith<T>::fma(a1, b1, s);
-                s = Arith<T>::fma(a2, b2, s);
-                s = Arith<T>::fma(a3, b3, s);
-                s = Arith<T>::fma(a4, b4, s);
-                s = Arith<T>::fma(a5, b5, s);
-                s = Arith<T>::fma(a6, b6, s);
-                s = Arith<T>::fma(a7, b7, s);
-            }
-            for (; i < n; ++i) s = Arith<T>::fma(a[i], b[i], s);
-        }
-        return __shfl_sync(0xffffffffu, s, 0);
-    }
-
     template <typename T>
     __device__ __forceinline__ T warp_dot_tree(const T * a, const T * b, int n)
     {
@@ -265,135 +224,6 @@ namespace hb2
             if (it == max_iters) used = it;
         }
         for (int i = lane; i < n; i += 32) xg[i] = x[i];
-        if (lane == 0)
-        {
-            if (used_out) *used_out = used;
-            if (defect_out) *defect_out = (double)current;
-        }
-    }
-
-    // Register-resident variant for the smallest systems (n <= 32 * RPL, K = 9):
-    // each lane keeps its RPL rows of A and of x, r, p, v in registers; only p
-    // (gathered by the SpMV) and, for the reference-order dots, the dot operands
-    // go through shared memory.
-    // T: arithmetic and matrix type; S: element type of b and x in memory (an
-    // FP32 hierarchy can run its coarsest solve in FP64 on an FP64 copy of the
-    // coarse operator: b is widened on load, x rounded on store).
-    template <typename T, typename S, int RPL>
-    __global__ void __launch_bounds__(32)
-    cg_warp_reg_kernel(EllView<T> Ag, const S * __restrict__ b, S * __restrict__ xg, uint64_t max_iters, double eps_d,
-                       int exact, uint64_t * used_out, double * defect_out, uint64_t vstride, const uint8_t * active)
-    {
-        typedef Arith<T> M;
-        constexpr int K = 9;
-        // batched launches: block j solves the system of vector j (b, x at j * vstride)
-        if (active && ! active[blockIdx.x]) return;
-        b += (uint64_t)blockIdx.x * vstride;
-        xg += (uint64_t)blockIdx.x * vstride;
-        extern __shared__ __align__(16) unsigned char smem_raw[];
-        const int n = (int)Ag.rows, lane = threadIdx.x;
-        T * sp = (T *)smem_raw;   // p (and x for the initial defect)
-        T * sa = sp + n;          // first dot operand (exact mode)
-        T * sb = sa + n;          // second dot operand (exact mode)
-        T av[RPL][K];
-        int ac[RPL][K];
-        T xr[RPL], rr[RPL], pr[RPL], vr[RPL];
-#pragma unroll
-        for (int j = 0; j < RPL; ++j)
-        {
-            const int row = lane + 32 * j;
-            const bool ok = row < n;
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-            {
-                av[j][k] = ok ? Ag.val[(uint64_t)k * Ag.ld + row] : T(0);
-                ac[j][k] = ok ? Ag.col[(uint64_t)k * Ag.ld + row] : -1;
-            }
-            xr[j] = ok ? T(xg[row]) : T(0);
-            if (ok) sp[row] = xr[j];
-        }
-        __syncwarp();
-        auto spmv = [&](T (&out)[RPL]) {
-#pragma unroll
-            for (int j = 0; j < RPL; ++j)
-            {
-                T s = T(0);
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                    if (ac[j][k] >= 0) s = M::add(s, M::mul(av[j][k], sp[ac[j][k]]));
-                out[j] = s;
-            }
-        };
-        // dot of per-lane register vectors a, b over the valid rows
-        auto dot = [&](const T (&a)[RPL], const T (&bb)[RPL]) -> T {
-            if (exact)
-            {
-#pragma unroll
-                for (int j = 0; j < RPL; ++j)
-                {
-                    const int row = lane + 32 * j;
-                    if (row < n) { sa[row] = a[j]; sb[row] = bb[j]; }
-                }
-                __syncwarp();
-                T s = warp_dot_exact(sa, sb, n);
-                __syncwarp();
-                return s;
-            }
-            double s = 0.0;
-#pragma unroll
-            for (int j = 0; j < RPL; ++j)
-                if (lane + 32 * j < n) s = fma((double)a[j], (double)bb[j], s);
-            return (T)warp_sum(s);
-        };
-        T tmp[RPL];
-        spmv(tmp);
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < RPL; ++j)
-        {
-            const int row = lane + 32 * j;
-            rr[j] = row < n ? M::sub(T(b[row]), tmp[j]) : T(0);
-            pr[j] = rr[j];
-            if (row < n) sp[row] = pr[j];
-        }
-        __syncwarp();
-        const T eps = T(eps_d);
-        T alpha = dot(rr, rr);
-        const T initial = sqrt(alpha);
-        T current = initial;
-        uint64_t it = 0, used = 0;
-        while (it < max_iters)
-        {
-            spmv(vr);
-            const T temp = dot(vr, pr);
-            const T lambda = M::div(alpha, guard(temp));
-            const T mlambda = -lambda;
-#pragma unroll
-            for (int j = 0; j < RPL; ++j)
-            {
-                xr[j] = M::add(xr[j], M::mul(lambda, pr[j]));
-                rr[j] = M::add(rr[j], M::mul(mlambda, vr[j]));
-            }
-            const T alpha_old = alpha;
-            alpha = dot(rr, rr);
-            const T talpha = M::div(alpha, guard(alpha_old));
-            __syncwarp();   // every lane is done gathering the old p
-#pragma unroll
-            for (int j = 0; j < RPL; ++j)
-            {
-                const int row = lane + 32 * j;
-                pr[j] = M::add(M::mul(pr[j], talpha), rr[j]);
-                if (row < n) sp[row] = pr[j];
-            }
-            __syncwarp();
-            ++it;
-            current = sqrt(alpha);
-            if (current < M::mul(eps, initial) || current < eps) { used = it; break; }
-            if (it == max_iters) used = it;
-        }
-#pragma unroll
-        for (int j = 0; j < RPL; ++j)
-            if (lane + 32 * j < n) xg[lane + 32 * j] = S(xr[j]);
         if (lane == 0)
         {
             if (used_out) *used_out = used;

@@ -75,11 +75,19 @@ struct hb2_mg_s
     double * r0_dev;         // sqrt(r0.r0)
     uint64_t * iters_dev;    // cycles done
     int sub_top;             // levels 1..sub_top run as cluster kernels (-1: none)
+    int sub_t1;              // of those, levels 1..sub_t1 run in one CTA (fused path)
+    bool sub_fused;          // levels 0..sub_top, coarse CG included, in one launch
     hb2_ell_s * coarse64;    // FP64 copy of the coarsest operator (F32 hierarchies with coarse_fp64)
 };
 
 namespace hb2
 {
+    static uint64_t env_u64(const char * name, uint64_t dflt)
+    {
+        const char * v = getenv(name);
+        return v && *v ? strtoull(v, 0, 10) : dflt;
+    }
+
     static int smooth(hb2_mg_s * mg, MgLevel & L, uint64_t sweeps, cudaStream_t s)
     {
         void * cur = L.x, * nxt = L.tmp;
@@ -121,6 +129,10 @@ namespace hb2
             d[i].tmp = L.tmp;
             d[i].jac = L.jac;
         }
+        if (mg->sub_fused)
+            return launch_subvcycle(mg->dtype, d, mg->sub_top, mg->sub_t1, (int)mg->prm.n_pre_smooth,
+                                    (int)mg->prm.n_post_smooth, mg->lev[0].A, mg->coarse64, mg->prm.max_iters_coarse,
+                                    mg->prm.coarse_eps, mg->prm.coarse_exact, mg->coarse_used_dev, mg->coarse_def_dev, s);
         int st = launch_subcycle(mg->dtype, d, mg->sub_top, (int)mg->prm.n_pre_smooth, (int)mg->prm.n_post_smooth,
                                  true, s);
         if (! st) st = coarse_solve(mg, s);
@@ -319,12 +331,20 @@ namespace hb2
         if (st) return st;
         // the small levels (at most kSubMaxRows rows, above the coarsest) run as
         // cluster kernels unless disabled
+        // (HB2_SUB_MAX_ROWS / HB2_SUB_LOCAL_ROWS override the two row limits;
+        // HB2_SUB_FUSED=1 runs the small levels and the coarse CG as one launch,
+        // measured slower on B200 than down / coarse CG / up as three)
         mg->sub_top = -1;
+        mg->sub_t1 = 0;
+        const uint64_t max_rows = env_u64("HB2_SUB_MAX_ROWS", kSubMaxRows);
+        const uint64_t local_rows = env_u64("HB2_SUB_LOCAL_ROWS", kSubLocalRows);
         if (! mg->prm.no_fused_levels && mg->prm.n_pre_smooth < (1u << 20) && mg->prm.n_post_smooth < (1u << 20))
             for (uint32_t i = 1; i < mg->nlev && i < 10; ++i)
-                if (mg->lev[i].n <= kSubMaxRows) mg->sub_top = (int)i;
+                if (mg->lev[i].n <= max_rows) mg->sub_top = (int)i;
         if (mg->sub_top >= 1)
         {
+            for (int i = 1; i <= mg->sub_top; ++i)
+                if (mg->lev[i].n <= local_rows) mg->sub_t1 = i;
             st = subcycle_prepare();
             if (st) return st;
         }
@@ -338,6 +358,8 @@ namespace hb2
             HB2_CUDA(cudaStreamSynchronize(stream));
         }
         HB2_CUDA(cudaStreamSynchronize(stream));
+        mg->sub_fused = mg->sub_top >= 1 && env_u64("HB2_SUB_FUSED", 0) != 0 &&
+                        subvcycle_supported(mg->lev[0].A, mg->coarse64);
         // prime the coarse kernel's shared-memory attribute outside the capture
         MgLevel & C = mg->lev[0];
         st = launch_cg_small(C.A, C.b, C.x, 0, mg->prm.coarse_eps, mg->prm.coarse_exact, mg->coarse_used_dev,

@@ -18,6 +18,13 @@
 #include "hb2_internal.hh"
 
 #include <cooperative_groups.h>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <type_traits>
+
+#include "cg_warp.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -47,102 +54,205 @@ namespace hb2
         int n_pre, n_post;
     };
 
-    // sum_k A(r, k) * v(col(r, k)), slot order, separately rounded
-    template <typename T, int KT>
+    // sum_k A(r, k) * v(col(r, k)), slot order, separately rounded.  Every
+    // index, value and vector load of the row is issued before the first
+    // product, so a row costs one memory round trip, not K.  L2: vector loads
+    // through L2 (other CTAs of the cluster wrote them); otherwise plain loads,
+    // coherent within the block (block-local phases).
+    template <typename T, int KT, bool L2>
     __device__ __forceinline__ T row_sum(const EllView<T> & A, uint32_t r, const T * v)
     {
         typedef Arith<T> M;
-        T s = T(0);
+        int c[KT];
+        T a[KT], xv[KT];
 #pragma unroll
         for (int k = 0; k < KT; ++k)
         {
-            const int c = __ldg(A.col + (uint64_t)k * A.ld + r);
-            if (c >= 0) s = M::add(s, M::mul(__ldg(A.val + (uint64_t)k * A.ld + r), __ldcg(v + c)));
+            c[k] = __ldg(A.col + (uint64_t)k * A.ld + r);
+            a[k] = __ldg(A.val + (uint64_t)k * A.ld + r);
         }
+#pragma unroll
+        for (int k = 0; k < KT; ++k) xv[k] = c[k] >= 0 ? (L2 ? __ldcg(v + c[k]) : v[c[k]]) : T(0);
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (c[k] >= 0) s = M::add(s, M::mul(a[k], xv[k]));
         return s;
     }
 
-    template <typename T>
+    template <typename T, bool L2 = true>
     __device__ __forceinline__ T row_sum_any(const EllView<T> & A, uint32_t r, const T * v)
     {
-        if (A.K == 9) return row_sum<T, 9>(A, r, v);
-        if (A.K == 4) return row_sum<T, 4>(A, r, v);
+        if (A.K == 9) return row_sum<T, 9, L2>(A, r, v);
+        if (A.K == 4) return row_sum<T, 4, L2>(A, r, v);
         typedef Arith<T> M;
         T s = T(0);
         for (uint32_t k = 0; k < A.K; ++k)
         {
             const int c = __ldg(A.col + (uint64_t)k * A.ld + r);
-            if (c >= 0) s = M::add(s, M::mul(__ldg(A.val + (uint64_t)k * A.ld + r), __ldcg(v + c)));
+            if (c >= 0) s = M::add(s, M::mul(__ldg(A.val + (uint64_t)k * A.ld + r), L2 ? __ldcg(v + c) : v[c]));
         }
         return s;
     }
 
+    // The threads that share the work of one phase: the whole cluster (phases
+    // end with the cluster barrier; vectors are read through L2 because other
+    // CTAs wrote them) or one CTA (block barrier; plain loads, coherent within
+    // the CTA).
+    //
+    // Cluster phases may also use plain loads (PL): the cluster barrier has
+    // acquire semantics, so loads after it observe every store released before
+    // it by the cluster's threads, and plain loads can hit L1 (the nine gathers
+    // of a row share cache lines with the neighbouring rows').
+    template <bool LOCAL, bool PL = false>
+    struct Team
+    {
+        uint32_t tid, nth;
+        static constexpr bool plain = LOCAL || PL;
+        __device__ __forceinline__ void sync() const
+        {
+            if constexpr (LOCAL) __syncthreads();
+            else cg::this_cluster().sync();
+        }
+        template <typename T> __device__ __forceinline__ T ld(const T * p) const
+        {
+            if constexpr (plain) return *p;
+            else return __ldcg(p);
+        }
+    };
+
     // damped Jacobi sweeps with ping-pong (math/ri.hh:110-133), result back in x
-    template <typename T>
-    __device__ void sub_smooth(const SubLevel<T> & L, int sweeps, uint32_t tid, uint32_t nth)
+    template <typename T, bool LOCAL, bool PL>
+    __device__ void sub_smooth(const SubLevel<T> & L, int sweeps, const Team<LOCAL, PL> & tm)
     {
         typedef Arith<T> M;
-        cg::cluster_group cluster = cg::this_cluster();
         T * cur = L.x, * nxt = L.tmp;
         for (int s = 0; s < sweeps; ++s)
         {
-            for (uint32_t r = tid; r < L.n; r += nth)
+            for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
             {
-                const T acc = row_sum_any(L.A, r, cur);
-                nxt[r] = M::add(__ldcg(cur + r), M::mul(__ldg(L.jac + r), M::sub(__ldcg(L.b + r), acc)));
+                const T acc = row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.A, r, cur);
+                nxt[r] = M::add(tm.ld(cur + r), M::mul(__ldg(L.jac + r), M::sub(tm.ld(L.b + r), acc)));
             }
-            cluster.sync();
+            tm.sync();
             T * t = cur;
             cur = nxt;
             nxt = t;
         }
         if (cur != L.x)
         {
-            for (uint32_t r = tid; r < L.n; r += nth) L.x[r] = __ldcg(cur + r);
-            cluster.sync();
+            for (uint32_t r = tm.tid; r < L.n; r += tm.nth) L.x[r] = tm.ld(cur + r);
+            tm.sync();
         }
     }
 
-    template <typename T>
+    // pre-smoothing, defect, restriction + clear of the coarser correction
+    template <typename T, bool LOCAL, bool PL>
+    __device__ void down_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_pre, const Team<LOCAL, PL> & tm)
+    {
+        typedef Arith<T> M;
+        sub_smooth(L, n_pre, tm);
+        for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
+            L.store[r] = M::sub(tm.ld(L.b + r), row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.A, r, L.x));
+        tm.sync();
+        for (uint32_t r = tm.tid; r < C.n; r += tm.nth)
+        {
+            C.b[r] = row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.R, r, L.store);
+            C.x[r] = T(0);
+        }
+        tm.sync();
+    }
+
+    // prolongation + add, post-smoothing
+    template <typename T, bool LOCAL, bool PL>
+    __device__ void up_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_post, const Team<LOCAL, PL> & tm)
+    {
+        typedef Arith<T> M;
+        for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
+            L.x[r] = M::add(tm.ld(L.x + r), row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.P, r, C.x));
+        tm.sync();
+        sub_smooth(L, n_post, tm);
+    }
+
+    template <typename T, bool PL>
     __global__ void __launch_bounds__(1024) mg_sub_down_kernel(const __grid_constant__ SubCycle<T> sc)
     {
-        typedef Arith<T> M;
         cg::cluster_group cluster = cg::this_cluster();
-        const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
-        const uint32_t nth = cluster.num_blocks() * blockDim.x;
-        for (int i = sc.top; i >= 1; --i)
+        const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
+        for (int i = sc.top; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+    }
+
+    template <typename T, bool PL>
+    __global__ void __launch_bounds__(1024) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
+    {
+        cg::cluster_group cluster = cg::this_cluster();
+        const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
+        for (int i = 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
+    }
+
+    // ------------------------------------------------------------------
+    // The whole bottom of the V-cycle in one launch: levels t1+1..top phase by
+    // phase over the cluster; then CTA 0 alone runs levels t1..1 down, the
+    // coarsest CG (its first warp: cg_warp.cuh) and levels 1..t1 up with block
+    // barriers only, while the other CTAs wait at the cluster barrier; then the
+    // cluster runs levels t1+1..top up.  A block barrier costs a small fraction
+    // of a cluster barrier, and the smallest levels have too few rows to keep
+    // more than one CTA busy anyway.
+    template <typename T>
+    struct SubVCycle
+    {
+        SubLevel<T> lev[kSubMaxLevels];
+        int top, t1, n_pre, n_post;
+        EllView<T> C;            // coarsest operator
+        EllView<double> C64;     // its FP64 copy (FP32 hierarchies with an FP64 coarse solve)
+        int mixed, exact;
+        uint64_t max_iters;
+        double eps;
+        uint64_t * used;
+        double * defect;
+    };
+
+    template <typename TA, typename S, typename T>
+    __device__ __forceinline__ void coarse_dispatch(const EllView<TA> & A, const SubVCycle<T> & sc, TA * smem)
+    {
+        const SubLevel<T> & L0 = sc.lev[0];
+        const S * b = (const S *)L0.b;
+        S * x = (S *)L0.x;
+        switch ((L0.n + 31) / 32)
         {
-            const SubLevel<T> & L = sc.lev[i];
-            const SubLevel<T> & C = sc.lev[i - 1];
-            sub_smooth(L, sc.n_pre, tid, nth);
-            for (uint32_t r = tid; r < L.n; r += nth)
-                L.store[r] = M::sub(__ldcg(L.b + r), row_sum_any(L.A, r, L.x));
-            cluster.sync();
-            for (uint32_t r = tid; r < C.n; r += nth)
-            {
-                C.b[r] = row_sum_any(L.R, r, L.store);
-                C.x[r] = T(0);
-            }
-            cluster.sync();
+            case 1: cg_warp_reg<TA, S, 1>(A, b, x, sc.max_iters, sc.eps, sc.exact, sc.used, sc.defect, smem); break;
+            case 2: cg_warp_reg<TA, S, 2>(A, b, x, sc.max_iters, sc.eps, sc.exact, sc.used, sc.defect, smem); break;
+            default: cg_warp_reg<TA, S, 3>(A, b, x, sc.max_iters, sc.eps, sc.exact, sc.used, sc.defect, smem); break;
         }
     }
 
-    template <typename T>
-    __global__ void __launch_bounds__(1024) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
+    constexpr int kSubVThreads = 512;   // 128 registers per thread: the coarse CG stays in registers
+
+    template <typename T, bool PL>
+    __global__ void __launch_bounds__(kSubVThreads, 1) mg_sub_vcycle_kernel(const __grid_constant__ SubVCycle<T> sc)
     {
-        typedef Arith<T> M;
+        __shared__ double cg_smem[3 * 96];
         cg::cluster_group cluster = cg::this_cluster();
-        const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
-        const uint32_t nth = cluster.num_blocks() * blockDim.x;
-        for (int i = 1; i <= sc.top; ++i)
+        const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
+        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+        if (cluster.block_rank() == 0)
         {
-            const SubLevel<T> & L = sc.lev[i];
-            const SubLevel<T> & C = sc.lev[i - 1];
-            for (uint32_t r = tid; r < L.n; r += nth)
-                L.x[r] = M::add(__ldcg(L.x + r), row_sum_any(L.P, r, C.x));
-            cluster.sync();
-            sub_smooth(L, sc.n_post, tid, nth);
+            const Team<true> blk = {threadIdx.x, blockDim.x};
+            for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk);
+            if (threadIdx.x < 32)
+            {
+                if constexpr (std::is_same<T, float>::value)
+                {
+                    if (sc.mixed) coarse_dispatch<double, float>(sc.C64, sc, cg_smem);
+                    else coarse_dispatch<float, float>(sc.C, sc, (float *)cg_smem);
+                }
+                else coarse_dispatch<double, double>(sc.C, sc, cg_smem);
+            }
+            __syncthreads();
+            for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk);
         }
+        cluster.sync();
+        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
     }
 
     template <typename T>
@@ -161,16 +271,29 @@ namespace hb2
         return s;
     }
 
-    static int cluster_width(const void * fn)
+    // HB2_SUB_LDCG=1: cluster phases read vectors with L2-only loads
+    static bool plain_loads()
     {
-        static int width = 0;
-        if (width) return width;
+        static const bool pl = ! (getenv("HB2_SUB_LDCG") && strcmp(getenv("HB2_SUB_LDCG"), "1") == 0);
+        return pl;
+    }
+
+    // widest cluster (16 CTAs of 1024 threads, else 8) that can be resident,
+    // per kernel, computed once outside any stream capture (subcycle_prepare)
+    static int cluster_width(const void * fn, int threads = 1024)
+    {
+        static std::mutex mu;
+        static std::map<const void *, int> widths;
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = widths.find(fn);
+        if (it != widths.end()) return it->second;
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        int width = 1;
         for (int w : {16, 8})
         {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(w);
-            cfg.blockDim = dim3(1024);
+            cfg.blockDim = dim3(threads);
             cudaLaunchAttribute at[1];
             at[0].id = cudaLaunchAttributeClusterDimension;
             at[0].val.clusterDim.x = w;
@@ -182,12 +305,33 @@ namespace hb2
             if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) == cudaSuccess && nclusters > 0)
             {
                 width = w;
-                return width;
+                break;
             }
             cudaGetLastError();
         }
-        width = 1;
+        widths[fn] = width;
         return width;
+    }
+
+    template <typename K, typename P>
+    static int launch_cluster(K kernel, const P & param, int w, cudaStream_t s, const char * what, int threads = 1024)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(w);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = w;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, param);
+        count_launches(1);
+        if (e != cudaSuccess) return cuda_status(e, what);
+        return HB2_OK;
     }
 
     template <typename T>
@@ -198,26 +342,12 @@ namespace hb2
         sc.top = top;
         sc.n_pre = n_pre;
         sc.n_post = n_post;
-        // the cluster width and the non-portable-size attributes were set up
-        // by subcycle_prepare(), outside any stream capture
-        const int w = cluster_width((const void *)mg_sub_down_kernel<double>);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(w);
-        cfg.blockDim = dim3(1024);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = w;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        cudaError_t e = down ? cudaLaunchKernelEx(&cfg, mg_sub_down_kernel<T>, sc)
-                             : cudaLaunchKernelEx(&cfg, mg_sub_up_kernel<T>, sc);
-        count_launches(1);
-        if (e != cudaSuccess) return cuda_status(e, "cluster sub-cycle launch");
-        return HB2_OK;
+        const int w = cluster_width((const void *)mg_sub_down_kernel<T, true>);
+        if (plain_loads())
+            return down ? launch_cluster(mg_sub_down_kernel<T, true>, sc, w, s, "cluster sub-cycle launch (down)")
+                        : launch_cluster(mg_sub_up_kernel<T, true>, sc, w, s, "cluster sub-cycle launch (up)");
+        return down ? launch_cluster(mg_sub_down_kernel<T, false>, sc, w, s, "cluster sub-cycle launch (down)")
+                    : launch_cluster(mg_sub_up_kernel<T, false>, sc, w, s, "cluster sub-cycle launch (up)");
     }
 
     int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int n_pre, int n_post, bool down,
@@ -228,13 +358,66 @@ namespace hb2
                                 : launch_sub_typed<float>(lev, top, n_pre, n_post, down, stream);
     }
 
-    // prime the cluster attributes outside any stream capture
+    bool subvcycle_supported(const hb2_ell_s * coarse, const hb2_ell_s * coarse64)
+    {
+        const hb2_ell_s * C = coarse64 ? coarse64 : coarse;
+        return C->K == 9 && C->rows <= 96 && C->rows > 0;   // up to 3 rows per lane in the coarse CG
+    }
+
+    template <typename T>
+    static int launch_subv_typed(const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post,
+                                 const hb2_ell_s * coarse, const hb2_ell_s * coarse64, uint64_t max_iters, double eps,
+                                 int exact, uint64_t * used, double * defect, cudaStream_t s)
+    {
+        SubVCycle<T> sc;
+        memset(&sc, 0, sizeof(sc));
+        for (int i = 0; i <= top; ++i) sc.lev[i] = sub_level<T>(lev[i]);
+        sc.top = top;
+        sc.t1 = t1;
+        sc.n_pre = n_pre;
+        sc.n_post = n_post;
+        sc.C = coarse->view<T>();
+        sc.mixed = coarse64 != 0;
+        if (coarse64) sc.C64 = coarse64->view<double>();
+        sc.exact = exact;
+        sc.max_iters = max_iters;
+        sc.eps = eps;
+        sc.used = used;
+        sc.defect = defect;
+        const int w = top > t1 ? cluster_width((const void *)mg_sub_vcycle_kernel<T, true>, kSubVThreads) : 1;
+        if (plain_loads())
+            return launch_cluster(mg_sub_vcycle_kernel<T, true>, sc, w, s, "fused small-level V-cycle launch", kSubVThreads);
+        return launch_cluster(mg_sub_vcycle_kernel<T, false>, sc, w, s, "fused small-level V-cycle launch", kSubVThreads);
+    }
+
+    int launch_subvcycle(int dtype, const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post,
+                         const hb2_ell_s * coarse, const hb2_ell_s * coarse64, uint64_t max_iters, double eps, int exact,
+                         uint64_t * used, double * defect, cudaStream_t stream)
+    {
+        if (top < 1 || top >= kSubMaxLevels || t1 < 0 || t1 > top || ! subvcycle_supported(coarse, coarse64))
+            return fail(HB2_ERR_UNSUPPORTED, "fused small-level V-cycle: bad level range or coarse operator");
+        if (coarse64 && dtype != HB2_F32) return fail(HB2_ERR_ARG, "fused small-level V-cycle: FP64 coarse copy of an FP64 level");
+        return dtype == HB2_F64 ? launch_subv_typed<double>(lev, top, t1, n_pre, n_post, coarse, coarse64, max_iters, eps,
+                                                           exact, used, defect, stream)
+                                : launch_subv_typed<float>(lev, top, t1, n_pre, n_post, coarse, coarse64, max_iters, eps,
+                                                          exact, used, defect, stream);
+    }
+
+    // prime the cluster attributes and widths outside any stream capture
     int subcycle_prepare()
     {
-        cluster_width((const void *)mg_sub_down_kernel<double>);
-        cudaFuncSetAttribute((const void *)mg_sub_down_kernel<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cudaFuncSetAttribute((const void *)mg_sub_up_kernel<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cudaFuncSetAttribute((const void *)mg_sub_up_kernel<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        plain_loads();
+        for (bool pl : {false, true})
+        {
+            cluster_width(pl ? (const void *)mg_sub_down_kernel<double, true> : (const void *)mg_sub_down_kernel<double, false>);
+            cluster_width(pl ? (const void *)mg_sub_down_kernel<float, true> : (const void *)mg_sub_down_kernel<float, false>);
+            cluster_width(pl ? (const void *)mg_sub_up_kernel<double, true> : (const void *)mg_sub_up_kernel<double, false>);
+            cluster_width(pl ? (const void *)mg_sub_up_kernel<float, true> : (const void *)mg_sub_up_kernel<float, false>);
+            cluster_width(pl ? (const void *)mg_sub_vcycle_kernel<double, true> : (const void *)mg_sub_vcycle_kernel<double, false>,
+                          kSubVThreads);
+            cluster_width(pl ? (const void *)mg_sub_vcycle_kernel<float, true> : (const void *)mg_sub_vcycle_kernel<float, false>,
+                          kSubVThreads);
+        }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_status(e, "sub-cycle attributes");
         return HB2_OK;
