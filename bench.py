@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     return ap.parse_args()
 
 
@@ -361,6 +362,8 @@ def main():
                                               rank)
     if not args.no_batch:
         line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
+    if not args.no_serving:
+        line["serving"] = serving_loop(rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(L)
     if rank == 0:
@@ -538,6 +541,32 @@ def batched_solves(hb, dev, flush, steps, warmup, rank):
             "loop_fp64_mg_ms_projected": t_loop, "loop_ms_per_level": per_level,
             "speedup_vs_loop": t_loop / t_dev,
             "method": "CG VAR (FP64) + one FP32 MG V(4,4) preconditioner, FP64 coarse CG cap 100; tol 1e-8"}
+
+
+def serving_loop(rank, rates=(100.0, 500.0), duration=5.0):
+    """Config 4, short form: Poisson arrivals for `duration` s per rate, levels log-uniform
+    in 5..11, tolerance 1e-8 / 1e-10 50/50, seeded U[-1,1] RHS; slot pool sized under a
+    120 GB budget.  Latency = host clock from arrival to the solution in pinned host
+    memory.  The FP64 comparison serves the same arrivals one at a time with resident
+    FP64 MG hierarchies.  (python -m honei_b200.serving runs the full 60 s sweep.)"""
+    from honei_b200 import serving
+    pool = serving.RhsPool(seed=rank)
+    srv = serving.PoissonServer(budget_bytes=120e9)
+    serving.run(srv, 200, 1.0, pool, seed=99)
+    out = {"budget_bytes": 120e9, "device_bytes": srv.device_bytes, "slots": srv.slots, "duration_s": duration,
+           "batched_mixed": [], "fp64_sequential": []}
+    for rate in rates:
+        s, _ = serving.run(srv, rate, duration, pool, seed=rank)
+        out["batched_mixed"].append({k: s[k] for k in ("rate_req_s", "finished", "solves_per_s", "p50_ms", "p99_ms",
+                                                         "max_rel_defect_1e-8", "max_rel_defect_1e-10")})
+    del srv
+    seq = serving.FP64SequentialServer()
+    serving.run(seq, 50, 1.0, pool, seed=99)
+    for rate in rates:
+        s, _ = serving.run(seq, rate, duration, pool, seed=rank)
+        out["fp64_sequential"].append({k: s[k] for k in ("rate_req_s", "finished", "solves_per_s", "p50_ms", "p99_ms",
+                                                           "max_rel_defect_1e-8", "max_rel_defect_1e-10")})
+    return out
 
 
 def ctypes_stream(stream):

@@ -7,7 +7,7 @@
 // level >= l) are a prefix 0 .. nv(l)-1 of the numbering.  All systems at level
 // l share one operator, so each stage of the V-cycle -- one Jacobi sweep on
 // level l, one restriction, ... -- is ONE launch over the (row block, vector)
-// grid of every vector that is at that level at that moment, whatever its
+// pairs of every vector that is at that level at that moment, whatever its
 // finest level: the systems whose finest level is l start their cycle there
 // while the larger systems pass through on their way down.  One PCG step of
 // the whole batch is therefore a fixed sequence of launches whose length is set
@@ -18,18 +18,21 @@
 // V-cycle (Jacobi omega, n_pre / n_post sweeps, bilinear transfers) on FP32
 // operators and vectors, with the coarsest-level CG in FP64 arithmetic.
 //
-// Outer kernels walk a work list of (vector, row block) pairs: group g (one
-// finest level) owns blocks block0(g) .. block0(g) + count(g) * gx(g) - 1, so
-// one launch covers every system whatever its size, and each vector's fused
-// dot / norm is reduced over its own row blocks in a fixed order -- a vector's
-// iterates do not depend on which other systems share the batch.
+// Work lists.  Each step starts with a one-block kernel that lists the vectors
+// with work (ascending, so each group's -- each finest level's -- vectors form
+// one segment), and the stop test ends with one that lists the vectors the
+// preconditioner runs for, with the number of them present on each level (a
+// prefix of the list).  Every other kernel of the step is a persistent grid
+// walking the (vector, row block) items of a list, so a step costs what its
+// live vectors need, not what the batch could hold.  Each vector's fused dot /
+// norm is reduced over its own row blocks in a fixed order: a vector's iterates
+// do not depend on which other systems share the batch or when they started.
 //
 // Per-vector state machine: kNew (start requested) -> first step computes
 // r = b - A x and ||r0||; kRun -> each step updates x, r and tests
-// ||r|| < eps ||r0|| or ||r|| < eps or max_iters; then kDone.  Vectors that are
-// idle or done are skipped by every launch (their blocks exit at once).  New
-// systems can be started between steps while others are in flight: that is how
-// the serving loop interleaves requests.
+// ||r|| < eps ||r0|| or ||r|| < eps or max_iters; then kDone.  New systems can
+// be started between steps while others are in flight: that is how the
+// serving loop interleaves requests.
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
 
@@ -53,7 +56,22 @@ namespace hb2
     constexpr int kOuterThreads = 256;
     constexpr int kOuterRows = 2;   // rows per thread: one 128-bit load of FP64 values per slot
 
-    // per-vector device scalars
+    constexpr int kMaxLevels = 16;
+
+    // Work lists of one step, built on the device (one block): the ascending
+    // list of vectors with work, with each group's segment of it (a group's
+    // vectors are consecutive, so its listed vectors are too) and the first
+    // work item (vector x row block) of each group; for the V-cycle, the number
+    // of listed vectors present on each level (a prefix of the list).
+    struct Plan
+    {
+        uint32_t live_start[kMaxGroups], live_n[kMaxGroups], live_item0[kMaxGroups + 1];
+        uint32_t prec_start[kMaxGroups], prec_n[kMaxGroups], prec_item0[kMaxGroups + 1];
+        uint32_t vcount[kMaxLevels];
+        uint32_t nactive;
+    };
+
+    // per-vector device scalars and the work lists
     struct SlotScalars
     {
         double * red_a;     // phase A: ||r0||^2 (kNew) or v.p (kRun)
@@ -68,7 +86,9 @@ namespace hb2
         uint8_t * state;
         uint8_t * fresh;    // first preconditioner application of this vector
         uint8_t * prec;     // preconditioner runs for this vector in this step
-        uint32_t * nactive;
+        uint32_t * live;    // list: vectors in kNew / kRun at the start of the step
+        uint32_t * plist;   // list: vectors the preconditioner runs for
+        Plan * plan;
         uint64_t * steps;
     };
 
@@ -77,7 +97,6 @@ namespace hb2
         EllView<double> A;            // FP64 operator of the finest level (plain layout)
         uint64_t n, vs;               // rows, stride of the FP64 vectors
         uint64_t vs32;                // stride of the level's FP32 vectors
-        uint64_t block0;              // first block of the group in the work list
         uint32_t first, count;        // vector range
         uint32_t gx;                  // row blocks per vector
         double * x, * b, * r, * p, * v;   // count vectors each, index j - first
@@ -90,24 +109,14 @@ namespace hb2
     {
         OuterGroup g[kMaxGroups];
         int ngroups;
+        uint32_t nv[kMaxLevels];      // vectors present on each level (index level - coarse)
+        int nlev;
     };
 
     __device__ __forceinline__ double guard_signed(double d)
     {
         // math/cg.hh:173 and :203: |d| > eps ? d : eps * sign(d)
         return fabs(d) > DBL_EPSILON ? d : __dmul_rn(DBL_EPSILON, __ddiv_rn(d, fabs(d)));
-    }
-
-    // block -> (group, vector, row block)
-    __device__ __forceinline__ const OuterGroup & locate(const OuterPlan & P, uint32_t & lj, uint32_t & blk)
-    {
-        int g = 0;
-        while (g + 1 < P.ngroups && (uint64_t)blockIdx.x >= P.g[g + 1].block0) ++g;
-        const OuterGroup & G = P.g[g];
-        const uint64_t local = (uint64_t)blockIdx.x - G.block0;
-        lj = (uint32_t)(local / G.gx);
-        blk = (uint32_t)(local % G.gx);
-        return G;
     }
 
     // acc[i] = sum_k A(r0 + i, k) * x(col), slot order, separately rounded
@@ -119,10 +128,10 @@ namespace hb2
         acc[0] = acc[1] = 0.0;
         if (r0 >= A.rows) return;
         const int K = KT > 0 ? KT : (int)A.K;
-        double2 v[KT > 0 ? KT : 1];
-        int2 c[KT > 0 ? KT : 1];
         if constexpr (KT > 0)
         {
+            double2 v[KT];
+            int2 c[KT];
 #pragma unroll
             for (int k = 0; k < KT; ++k)
             {
@@ -160,78 +169,177 @@ namespace hb2
             on_total();
     }
 
+    // Persistent walk over the work items (vector x row block) of one list:
+    // body(G, j, lj, blk) for every item, the items of one block in turn.
+    template <typename F>
+    __device__ __forceinline__ void walk(const OuterPlan & P, const uint32_t * list, const uint32_t * start,
+                                         const uint32_t * item0, F && body)
+    {
+        __shared__ uint32_t s_item0[kMaxGroups + 1], s_start[kMaxGroups];
+        if (threadIdx.x <= (unsigned)P.ngroups) s_item0[threadIdx.x] = item0[threadIdx.x];
+        if (threadIdx.x < (unsigned)P.ngroups) s_start[threadIdx.x] = start[threadIdx.x];
+        __syncthreads();
+        const uint32_t total = s_item0[P.ngroups];
+        for (uint32_t item = blockIdx.x; item < total; item += gridDim.x)
+        {
+            int g = 0;
+            while (g + 1 < P.ngroups && item >= s_item0[g + 1]) ++g;
+            const OuterGroup & G = P.g[g];
+            const uint32_t local = item - s_item0[g];
+            const uint32_t j = list[s_start[g] + local / G.gx];
+            body(G, j, j - G.first, local % G.gx);
+        }
+    }
+
     // Phase A.  kNew: r = b - A x (math/cg.hh:161), ||r||^2; kRun: v = A p,
     // v.p (cg.hh:174-175).  Either way the inner rhs of the finest level gets
     // (float) r and the inner correction 0, ready for the preconditioner.
     template <int KT>
     __global__ void __launch_bounds__(kOuterThreads) bpcg_phase_a_kernel(const __grid_constant__ OuterPlan P, SlotScalars S)
     {
-        uint32_t lj, blk;
-        const OuterGroup & G = locate(P, lj, blk);
-        const uint32_t j = G.first + lj;
-        const uint8_t st = S.state[j];
-        if (st != kNew && st != kRun) return;
-        const bool init = st == kNew;
-        const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
-        const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
-        double acc[kOuterRows];
-        rows_product<KT>(G.A, r0, (init ? G.x : G.p) + o, acc);
-        double part = 0.0;
+        walk(P, S.live, S.plan->live_start, S.plan->live_item0, [&](const OuterGroup & G, uint32_t j, uint32_t lj, uint32_t blk) {
+            const bool init = S.state[j] == kNew;
+            const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
+            const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
+            double acc[kOuterRows];
+            rows_product<KT>(G.A, r0, (init ? G.x : G.p) + o, acc);
+            double part = 0.0;
 #pragma unroll
-        for (int i = 0; i < kOuterRows; ++i)
-        {
-            const uint64_t row = r0 + i;
-            if (row >= G.n) break;
-            if (init)
+            for (int i = 0; i < kOuterRows; ++i)
             {
-                const double d = __dsub_rn(G.b[o + row], acc[i]);
-                G.r[o + row] = d;
-                G.b32[o32 + row] = __double2float_rn(d);
-                G.x32[o32 + row] = 0.f;
-                part = fma(d, d, part);
+                const uint64_t row = r0 + i;
+                if (row >= G.n) break;
+                if (init)
+                {
+                    const double d = __dsub_rn(G.b[o + row], acc[i]);
+                    G.r[o + row] = d;
+                    G.b32[o32 + row] = __double2float_rn(d);
+                    G.x32[o32 + row] = 0.f;
+                    part = fma(d, d, part);
+                }
+                else
+                {
+                    G.v[o + row] = acc[i];
+                    part = fma(acc[i], G.p[o + row], part);
+                }
             }
-            else
-            {
-                G.v[o + row] = acc[i];
-                part = fma(acc[i], G.p[o + row], part);
-            }
-        }
-        finish(G, lj, blk, part, S.red_a + j, [] {});
+            finish(G, lj, blk, part, S.red_a + j, [] {});
+        });
     }
 
     // kRun: lambda = alpha_new / temp; x += lambda p; r -= lambda v; ||r||^2
     // (math/cg.hh:173-183); the inner rhs gets (float) r.
     __global__ void __launch_bounds__(kOuterThreads) bpcg_update_kernel(const __grid_constant__ OuterPlan P, SlotScalars S)
     {
-        uint32_t lj, blk;
-        const OuterGroup & G = locate(P, lj, blk);
-        const uint32_t j = G.first + lj;
-        if (S.state[j] != kRun) return;
-        const double lambda = __ddiv_rn(S.an[j], guard_signed(S.red_a[j]));
-        const double mlambda = -lambda;
-        const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
-        const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
-        double part = 0.0;
+        walk(P, S.live, S.plan->live_start, S.plan->live_item0, [&](const OuterGroup & G, uint32_t j, uint32_t lj, uint32_t blk) {
+            if (S.state[j] != kRun) return;
+            const double lambda = __ddiv_rn(S.an[j], guard_signed(S.red_a[j]));
+            const double mlambda = -lambda;
+            const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
+            const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
+            double part = 0.0;
 #pragma unroll
-        for (int i = 0; i < kOuterRows; ++i)
-        {
-            const uint64_t row = r0 + i;
-            if (row >= G.n) break;
-            G.x[o + row] = __dadd_rn(G.x[o + row], __dmul_rn(lambda, G.p[o + row]));
-            const double rr = __dadd_rn(G.r[o + row], __dmul_rn(mlambda, G.v[o + row]));
-            G.r[o + row] = rr;
-            G.b32[o32 + row] = __double2float_rn(rr);
-            G.x32[o32 + row] = 0.f;
-            part = fma(rr, rr, part);
-        }
-        finish(G, lj, blk, part, S.red_u + j, [] {});
+            for (int i = 0; i < kOuterRows; ++i)
+            {
+                const uint64_t row = r0 + i;
+                if (row >= G.n) break;
+                G.x[o + row] = __dadd_rn(G.x[o + row], __dmul_rn(lambda, G.p[o + row]));
+                const double rr = __dadd_rn(G.r[o + row], __dmul_rn(mlambda, G.v[o + row]));
+                G.r[o + row] = rr;
+                G.b32[o32 + row] = __double2float_rn(rr);
+                G.x32[o32 + row] = 0.f;
+                part = fma(rr, rr, part);
+            }
+            finish(G, lj, blk, part, S.red_u + j, [] {});
+        });
     }
 
-    // Stop tests (math/cg.hh:185-200) and the preconditioner mask of this step.
-    __global__ void __launch_bounds__(1024) bpcg_decide_kernel(SlotScalars S, uint32_t nvec, uint64_t max_iters)
+    // one block: ascending list of the j < n with flag(j); returns the count
+    template <typename F>
+    __device__ uint32_t block_compact(uint32_t n, F && flag, uint32_t * list)
     {
-        __shared__ double scratch[32];
-        double count = 0.0;
+        __shared__ uint32_t wsum[32];
+        __shared__ uint32_t total;
+        const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+        const uint32_t lo = min(n, threadIdx.x * per), hi = min(n, lo + per);
+        uint32_t c = 0;
+        for (uint32_t j = lo; j < hi; ++j) c += flag(j) ? 1u : 0u;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0)
+        {
+            const int nw = (blockDim.x + 31) >> 5;
+            uint32_t w = lane < nw ? wsum[lane] : 0u, wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            if (lane < nw) wsum[lane] = wi - w;   // exclusive prefix of the warps
+            if (lane == 31) total = wi;
+        }
+        __syncthreads();
+        uint32_t pos = wsum[warp] + incl - c;
+        for (uint32_t j = lo; j < hi; ++j)
+            if (flag(j)) list[pos++] = j;
+        __syncthreads();
+        return total;
+    }
+
+    __device__ __forceinline__ uint32_t lower_bound(const uint32_t * list, uint32_t n, uint32_t v)
+    {
+        uint32_t lo = 0, hi = n;
+        while (lo < hi)
+        {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (list[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    }
+
+    // group segments and item offsets of a list
+    __device__ void segments(const OuterPlan & P, const uint32_t * list, uint32_t n, uint32_t * start, uint32_t * cnt,
+                             uint32_t * item0)
+    {
+        if (threadIdx.x == 0)
+        {
+            uint32_t items = 0;
+            for (int g = 0; g < P.ngroups; ++g)
+            {
+                const uint32_t a = lower_bound(list, n, P.g[g].first);
+                const uint32_t b = lower_bound(list, n, P.g[g].first + P.g[g].count);
+                start[g] = a;
+                cnt[g] = b - a;
+                item0[g] = items;
+                items += (b - a) * P.g[g].gx;
+            }
+            item0[P.ngroups] = items;
+        }
+        __syncthreads();
+    }
+
+    // start of a step: the vectors with work (kNew, kRun)
+    __global__ void __launch_bounds__(1024) bpcg_plan_kernel(const __grid_constant__ OuterPlan P, SlotScalars S, uint32_t nvec)
+    {
+        const uint32_t n = block_compact(nvec, [&](uint32_t j) { const uint8_t st = S.state[j]; return st == kNew || st == kRun; },
+                                         S.live);
+        segments(P, S.live, n, S.plan->live_start, S.plan->live_n, S.plan->live_item0);
+    }
+
+    // Stop tests (math/cg.hh:185-200), then the preconditioner's work list.
+    __global__ void __launch_bounds__(1024) bpcg_decide_kernel(const __grid_constant__ OuterPlan P, SlotScalars S,
+                                                               uint32_t nvec, uint64_t max_iters)
+    {
         for (uint32_t j = threadIdx.x; j < nvec; j += blockDim.x)
         {
             const uint8_t st = S.state[j];
@@ -267,56 +375,54 @@ namespace hb2
                 }
             }
             S.prec[j] = prec;
-            count += prec;
         }
-        count = block_sum(count, scratch);
-        if (threadIdx.x == 0) *S.nactive = (uint32_t)count;
+        __syncthreads();
+        const uint32_t n = block_compact(nvec, [&](uint32_t j) { return S.prec[j] != 0; }, S.plist);
+        segments(P, S.plist, n, S.plan->prec_start, S.plan->prec_n, S.plan->prec_item0);
+        if (threadIdx.x < (unsigned)P.nlev) S.plan->vcount[threadIdx.x] = lower_bound(S.plist, n, P.nv[threadIdx.x]);
+        if (threadIdx.x == 0) S.plan->nactive = n;
     }
 
     // alpha_new = r.z with z = (double) inner correction (cg.hh:202-204)
     __global__ void __launch_bounds__(kOuterThreads) bpcg_dot_z_kernel(const __grid_constant__ OuterPlan P, SlotScalars S)
     {
-        uint32_t lj, blk;
-        const OuterGroup & G = locate(P, lj, blk);
-        const uint32_t j = G.first + lj;
-        if (! S.prec[j]) return;
-        const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
-        const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
-        double part = 0.0;
+        walk(P, S.plist, S.plan->prec_start, S.plan->prec_item0, [&](const OuterGroup & G, uint32_t j, uint32_t lj, uint32_t blk) {
+            const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
+            const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
+            double part = 0.0;
 #pragma unroll
-        for (int i = 0; i < kOuterRows; ++i)
-        {
-            const uint64_t row = r0 + i;
-            if (row >= G.n) break;
-            part = fma(G.r[o + row], (double)G.x32[o32 + row], part);
-        }
-        finish(G, lj, blk, part, S.red_z + j, [&] {
-            const double an_new = S.red_z[j];
-            const double an_old = S.an[j];
-            S.tco[j] = S.fresh[j] ? 0.0 : __ddiv_rn(an_new, guard_signed(an_old));
-            S.an[j] = an_new;
+            for (int i = 0; i < kOuterRows; ++i)
+            {
+                const uint64_t row = r0 + i;
+                if (row >= G.n) break;
+                part = fma(G.r[o + row], (double)G.x32[o32 + row], part);
+            }
+            finish(G, lj, blk, part, S.red_z + j, [&] {
+                const double an_new = S.red_z[j];
+                const double an_old = S.an[j];
+                S.tco[j] = S.fresh[j] ? 0.0 : __ddiv_rn(an_new, guard_signed(an_old));
+                S.an[j] = an_new;
+            });
         });
     }
 
     // p = z (first application, cg.hh:163) or p = talpha p + z (cg.hh:205-207)
     __global__ void __launch_bounds__(kOuterThreads) bpcg_p_kernel(const __grid_constant__ OuterPlan P, SlotScalars S)
     {
-        uint32_t lj, blk;
-        const OuterGroup & G = locate(P, lj, blk);
-        const uint32_t j = G.first + lj;
-        if (! S.prec[j]) return;
-        const bool fresh = S.fresh[j] != 0;
-        const double t = S.tco[j];
-        const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
-        const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
+        walk(P, S.plist, S.plan->prec_start, S.plan->prec_item0, [&](const OuterGroup & G, uint32_t j, uint32_t lj, uint32_t blk) {
+            const bool fresh = S.fresh[j] != 0;
+            const double t = S.tco[j];
+            const uint64_t o = (uint64_t)lj * G.vs, o32 = (uint64_t)j * G.vs32;
+            const uint64_t r0 = ((uint64_t)blk * kOuterThreads + threadIdx.x) * kOuterRows;
 #pragma unroll
-        for (int i = 0; i < kOuterRows; ++i)
-        {
-            const uint64_t row = r0 + i;
-            if (row >= G.n) break;
-            const double z = (double)G.x32[o32 + row];
-            G.p[o + row] = fresh ? z : __dadd_rn(__dmul_rn(G.p[o + row], t), z);
-        }
+            for (int i = 0; i < kOuterRows; ++i)
+            {
+                const uint64_t row = r0 + i;
+                if (row >= G.n) break;
+                const double z = (double)G.x32[o32 + row];
+                G.p[o + row] = fresh ? z : __dadd_rn(__dmul_rn(G.p[o + row], t), z);
+            }
+        });
     }
 
     __global__ void bpcg_start_kernel(SlotScalars S, uint32_t first, uint32_t count, double eps)
@@ -334,12 +440,12 @@ namespace hb2
         cudaGraphSetConditional(h, 1u);
     }
 
-    __global__ void bpcg_loop_decide_kernel(const uint32_t * nactive, uint64_t * steps, uint64_t max_steps,
+    __global__ void bpcg_loop_decide_kernel(const Plan * plan, uint64_t * steps, uint64_t max_steps,
                                             cudaGraphConditionalHandle h)
     {
         const uint64_t s = *steps + 1;
         *steps = s;
-        cudaGraphSetConditional(h, (*nactive > 0 && s < max_steps) ? 1u : 0u);
+        cudaGraphSetConditional(h, (plan->nactive > 0 && s < max_steps) ? 1u : 0u);
     }
 
     __global__ void bpcg_count_step_kernel(uint64_t * steps) { *steps += 1; }
@@ -375,7 +481,7 @@ struct hb2_batch_s
     std::vector<hb2::BGroup> grp;
     hb2_ell coarse64 = 0;
     hb2::OuterPlan plan;
-    uint64_t outer_blocks = 0;
+    uint64_t outer_items = 0;           // largest number of outer work items of a step
     bool outer_k9 = true;
     hb2::SlotScalars S;
     void * block = 0;                   // every device array of the batch
@@ -397,9 +503,10 @@ namespace hb2
     static uint64_t round64(uint64_t n) { return std::max<uint64_t>(64, (n + 63) / 64 * 64); }
     static uint64_t q1_rows(unsigned level) { const uint64_t m = (1ull << level) + 1; return m * m; }
 
+    // outer kernels: a persistent grid (8 blocks of 256 threads per SM) over the work list
     static int outer_launch(hb2_batch_s * B, int which, cudaStream_t s)
     {
-        const dim3 grid((unsigned)B->outer_blocks);
+        const dim3 grid((unsigned)std::min<uint64_t>(B->outer_items, list_grid_cap()));
         switch (which)
         {
             case 0:
@@ -420,7 +527,8 @@ namespace hb2
         Batch bt;
         bt.nvec = L.nv;
         bt.vstride = L.vs;
-        bt.active = B->S.prec;
+        bt.list = B->S.plist;
+        bt.count = &B->S.plan->vcount[L.level - B->coarse_level];
         float * cur = L.x, * nxt = L.tmp;
         for (uint64_t k = 0; k < sweeps; ++k)
         {
@@ -445,7 +553,8 @@ namespace hb2
             Batch bt;
             bt.nvec = L.nv;
             bt.vstride = L.vs;
-            bt.active = B->S.prec;
+            bt.list = B->S.plist;
+            bt.count = &B->S.plan->vcount[i];
             if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, 0, s, 0, &bt);
             Batch br = bt;
             br.vstride = C.vs;
@@ -455,8 +564,8 @@ namespace hb2
             if (st) return st;
         }
         BLevel & C0 = B->lev[0];
-        int st = launch_cg_warp_batched(B->coarse64, HB2_F32, C0.b, C0.x, C0.nv, C0.vs, B->S.prec,
-                                        B->prm.max_iters_coarse, B->prm.coarse_eps, s);
+        int st = launch_cg_warp_batched(B->coarse64, HB2_F32, C0.b, C0.x, C0.nv, C0.vs, 0,
+                                        B->prm.max_iters_coarse, B->prm.coarse_eps, s, B->S.plist, &B->S.plan->vcount[0]);
         if (st) return st;
         for (int i = 1; i <= top; ++i)
         {
@@ -466,7 +575,8 @@ namespace hb2
             bp.nvec = L.nv;
             bp.vstride = L.vs;
             bp.xstride = C.vs;
-            bp.active = B->S.prec;
+            bp.list = B->S.plist;
+            bp.count = &B->S.plan->vcount[i];
             st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, 0, s, 0, &bp);
             if (! st) st = b_smooth(B, L, B->prm.n_post_smooth, s);
             if (st) return st;
@@ -476,11 +586,14 @@ namespace hb2
 
     static int record_step(hb2_batch_s * B, cudaStream_t s)
     {
+        bpcg_plan_kernel<<<1, 1024, 0, s>>>(B->plan, B->S, B->nvec);
+        count_launches(1);
+        HB2_LAUNCH_CHECK("bpcg_plan_kernel");
         int st = outer_launch(B, 0, s);
         if (! st) st = outer_launch(B, 1, s);
         if (! st)
         {
-            bpcg_decide_kernel<<<1, 1024, 0, s>>>(B->S, B->nvec, B->prm.max_iters);
+            bpcg_decide_kernel<<<1, 1024, 0, s>>>(B->plan, B->S, B->nvec, B->prm.max_iters);
             count_launches(1);
             HB2_LAUNCH_CHECK("bpcg_decide_kernel");
         }
@@ -559,7 +672,7 @@ namespace hb2
         int st = record_step(B, B->cap2);
         if (! st)
         {
-            bpcg_loop_decide_kernel<<<1, 1, 0, B->cap2>>>(B->S.nactive, B->S.steps, B->prm.max_iters + 2, h);
+            bpcg_loop_decide_kernel<<<1, 1, 0, B->cap2>>>(B->S.plan, B->S.steps, B->prm.max_iters + 2, h);
             e = cudaGetLastError();
             if (e != cudaSuccess) st = cuda_status(e, "bpcg_loop_decide_kernel");
         }
@@ -700,7 +813,7 @@ namespace hb2
             go[i * 8 + 7] = take((size_t)g.count * (ngr + 1) * sizeof(unsigned));
         }
         const size_t nv = B->nvec;
-        const size_t so = take(nv * sizeof(double) * 8 + nv * sizeof(uint32_t) + nv * 3 + 64);
+        const size_t so = take(nv * sizeof(double) * 8 + nv * sizeof(uint32_t) * 3 + nv * 3 + sizeof(Plan) + 256);
         cudaError_t e = cudaMalloc(&B->block, total);
         if (e != cudaSuccess) return cuda_status(e, "hb2_batch_create_q1: device memory");
         B->bytes = total;
@@ -727,8 +840,10 @@ namespace hb2
         B->S.tco = (double *)sp; sp += nv * 8;
         B->S.eps = (double *)sp; sp += nv * 8;
         B->S.steps = (uint64_t *)sp; sp += 8;
+        B->S.plan = (Plan *)sp; sp += (sizeof(Plan) + 15) / 16 * 16;
         B->S.iters = (uint32_t *)sp; sp += nv * 4;
-        B->S.nactive = (uint32_t *)sp; sp += 4;
+        B->S.live = (uint32_t *)sp; sp += nv * 4;
+        B->S.plist = (uint32_t *)sp; sp += nv * 4;
         B->S.state = (uint8_t *)sp; sp += nv;
         B->S.fresh = (uint8_t *)sp; sp += nv;
         B->S.prec = (uint8_t *)sp;
@@ -754,7 +869,6 @@ namespace hb2
             o.vs32 = L.vs;
             o.b32 = L.b;
             o.x32 = L.x;
-            o.block0 = blocks;
             o.first = g.first;
             o.count = g.count;
             o.gx = g.gx;
@@ -769,7 +883,9 @@ namespace hb2
             blocks += (uint64_t)g.count * g.gx;
         }
         if (blocks > 0x7fffffffull) return fail(HB2_ERR_UNSUPPORTED, "hb2_batch_create_q1: work list too long");
-        B->outer_blocks = blocks;
+        B->outer_items = blocks;
+        for (size_t i = 0; i < B->lev.size(); ++i) B->plan.nv[i] = B->lev[i].nv;
+        B->plan.nlev = (int)B->lev.size();
         // pinned host mirror
         const size_t hb = nv * (1 + 4 + 8 + 8) + 64;
         HB2_CUDA(cudaMallocHost(&B->h_block, hb));

@@ -17,6 +17,7 @@
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
 
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 
@@ -234,7 +235,8 @@ namespace hb2
     template <typename T, typename S>
     static bool launch_warp_reg(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
                                 uint64_t * used_dev, double * defect_dev, cudaStream_t stream, uint32_t nvec = 1,
-                                uint64_t vstride = 0, const uint8_t * active = nullptr)
+                                uint64_t vstride = 0, const uint8_t * active = nullptr,
+                                const uint32_t * list = nullptr, const uint32_t * count = nullptr)
     {
         if (A->K != 9 || A->rows > 128) return false;
         const int rpl = (int)((A->rows + 31) / 32);
@@ -242,12 +244,13 @@ namespace hb2
         EllView<T> v = A->view<T>();
         const S * bp = (const S *)b;
         S * xp = (S *)x;
+        const unsigned grid = list ? (unsigned)std::min<uint64_t>(nvec, list_grid_cap()) : nvec;
         switch (rpl)
         {
-            case 1: cg_warp_reg_kernel<T, S, 1><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
-            case 2: cg_warp_reg_kernel<T, S, 2><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
-            case 3: cg_warp_reg_kernel<T, S, 3><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
-            default: cg_warp_reg_kernel<T, S, 4><<<nvec, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active); break;
+            case 1: cg_warp_reg_kernel<T, S, 1><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            case 2: cg_warp_reg_kernel<T, S, 2><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            case 3: cg_warp_reg_kernel<T, S, 3><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            default: cg_warp_reg_kernel<T, S, 4><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
         }
         return true;
     }
@@ -256,16 +259,16 @@ namespace hb2
     // arithmetic on FP32 vectors (A64 FP64) or in the operator's own type
     int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
                                uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
-                               cudaStream_t stream)
+                               cudaStream_t stream, const uint32_t * list, const uint32_t * count)
     {
         if (nvec == 0) return HB2_OK;
         bool ok;
         if (A->dtype == HB2_F64 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
         else if (A->dtype == HB2_F64 && vec_dtype == HB2_F64)
-            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
         else if (A->dtype == HB2_F32 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active);
+            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
         else return fail(HB2_ERR_ARG, "batched coarse CG: unsupported element types");
         if (! ok) return fail(HB2_ERR_UNSUPPORTED, "batched coarse CG: the coarsest level needs <= 128 rows and 9 slots");
         count_launches(1);

@@ -184,11 +184,24 @@ namespace hb2
     template <typename T, typename S, int RPL>
     __global__ void __launch_bounds__(32)
     cg_warp_reg_kernel(EllView<T> Ag, const S * __restrict__ b, S * __restrict__ xg, uint64_t max_iters, double eps_d,
-                       int exact, uint64_t * used_out, double * defect_out, uint64_t vstride, const uint8_t * active)
+                       int exact, uint64_t * used_out, double * defect_out, uint64_t vstride, const uint8_t * active,
+                       const uint32_t * list, const uint32_t * count)
     {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        if (list)
+        {
+            // work list: the systems of vectors list[0 .. *count - 1], one per warp in turn
+            const uint32_t n = *count;
+            for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
+            {
+                const uint64_t o = (uint64_t)list[i] * vstride;
+                cg_warp_reg<T, S, RPL>(Ag, b + o, xg + o, max_iters, eps_d, exact, used_out, defect_out, (T *)smem_raw);
+                __syncwarp();
+            }
+            return;
+        }
         // batched launches: block j solves the system of vector j (b, x at j * vstride)
         if (active && ! active[blockIdx.x]) return;
-        extern __shared__ __align__(16) unsigned char smem_raw[];
         cg_warp_reg<T, S, RPL>(Ag, b + (uint64_t)blockIdx.x * vstride, xg + (uint64_t)blockIdx.x * vstride, max_iters,
                                eps_d, exact, used_out, defect_out, (T *)smem_raw);
     }

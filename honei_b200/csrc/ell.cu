@@ -20,6 +20,7 @@
 #include "hb2_internal.hh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 namespace hb2
@@ -59,22 +60,29 @@ namespace hb2
     // One thread: R consecutive rows; KT = compile-time slot count (0: runtime).
     template <typename T, int KT, int MODE>
     __global__ void __launch_bounds__(kEllThreads)
-    ell_kernel(EllView<T> A, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ aux,
-               const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt,
+    ell_kernel(EllView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
+               const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
                int flags, Batch bt)
     {
         constexpr int R = RowsPerThread<T>::value;
         typedef Arith<T> M;
-        if (bt.active && ! bt.active[blockIdx.y]) return;
+        // work items: (vector j, row block) -- the launch grid (blockIdx.x, blockIdx.y),
+        // or, with a device work list, items 0 .. count * gx - 1 walked by a
+        // persistent grid (vector list[item / gx], row block item % gx)
+        const bool listed = bt.list != nullptr;
+        const uint32_t total = listed ? *bt.count * bt.gx : 1;
+        for (uint32_t item = listed ? blockIdx.x : 0; item < total; item += listed ? gridDim.x : 1)
         {
-            const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
-            x += (uint64_t)blockIdx.y * (bt.xstride ? bt.xstride : bt.vstride);
-            y += vo;
-            if (aux) aux += vo;
-            if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;
-            if (red) red += blockIdx.y;   // grid_sum_finish offsets its partials / counters itself
-        }
-        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x;
+        const uint32_t j = listed ? bt.list[item / bt.gx] : blockIdx.y;
+        if (! listed && bt.active && ! bt.active[j]) return;
+        const uint64_t vo = (uint64_t)j * bt.vstride;
+        const T * __restrict__ x = x_ + (uint64_t)j * (bt.xstride ? bt.xstride : bt.vstride);
+        T * __restrict__ y = y_ + vo;
+        const T * __restrict__ aux = aux_ ? aux_ + vo : aux_;
+        T * __restrict__ zero = zero_ ? zero_ + (uint64_t)j * bt.zstride : zero_;
+        double * red = red_ ? red_ + j : red_;   // grid_sum_finish offsets its partials / counters itself
+        const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
+        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
         const bool keep = (flags & kKeepL2) != 0;
         const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
         const int K = KT > 0 ? KT : (int)A.K;
@@ -141,6 +149,7 @@ namespace hb2
             double s = block_sum(part, scratch);
             grid_sum_finish(s, rs, red, want_sqrt, scratch);
         }
+        }
     }
 
     template <typename T, int MODE>
@@ -178,11 +187,26 @@ namespace hb2
         }
     }
 
+    // blocks of a work-list launch: at most 32 per SM, or HB2_LIST_GRID (0: one
+    // block per possible work item).  Measured on the 512-system batch: 8 per
+    // SM (one resident wave, each block looping over its items) is 15 % slower
+    // than one block per item, 16 per SM within 2 %; the cap keeps a mostly idle
+    // batch from paying for hundreds of thousands of empty blocks.
+    uint64_t list_grid_cap()
+    {
+        static const uint64_t cap = [] {
+            const char * v = getenv("HB2_LIST_GRID");
+            const uint64_t c = v && *v ? strtoull(v, 0, 10) : (uint64_t)num_sms() * 32;
+            return c ? c : ~0ull;
+        }();
+        return cap;
+    }
+
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
                    void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags,
                    const Batch * batch)
     {
-        const Batch b = batch ? *batch : Batch();
+        Batch b = batch ? *batch : Batch();
         if (A->rows == 0)
         {
             // empty matrix: defined results without a launch
@@ -192,7 +216,14 @@ namespace hb2
         const int R = A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value;
         const unsigned gx = A->code ? compact_grid(A, red != 0) : ceil_div(A->rows, (uint64_t)kEllThreads * R);
         if (b.nvec == 0 || b.nvec > 65535) return fail(HB2_ERR_ARG, "ELL batch: 1..65535 vectors");
-        const dim3 grid(gx, b.nvec);
+        dim3 grid(gx, b.nvec);
+        if (b.list)
+        {
+            // persistent grid over the work list: at most 8 blocks per SM
+            if (red || ! b.count) return fail(HB2_ERR_ARG, "ELL work list: no fused reduction, count required");
+            b.gx = gx;
+            grid = dim3((unsigned)std::min<uint64_t>((uint64_t)gx * b.nvec, list_grid_cap()), 1);
+        }
         ReduceSlot rs;
         rs.partials = 0;
         rs.gpart = 0;

@@ -143,26 +143,33 @@ namespace hb2
 
     template <typename T, int KT, int MODE, int R>
     __global__ void __launch_bounds__(kEllThreads)
-    ell_compact_kernel(EllCompactView<T> A, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ aux,
-                       const T * __restrict__ aux2, T * __restrict__ zero, ReduceSlot rs, double * red, int want_sqrt,
+    ell_compact_kernel(EllCompactView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
+                       const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
                        int flags, Batch bt)
     {
         typedef Arith<T> M;
         typedef typename CodeWord<R>::C CW;
         typedef typename CodeWord<R>::D DW;
-        if (bt.active && ! bt.active[blockIdx.y]) return;
-        {
-            const uint64_t vo = (uint64_t)blockIdx.y * bt.vstride;
-            x += (uint64_t)blockIdx.y * (bt.xstride ? bt.xstride : bt.vstride);
-            y += vo;
-            if (aux) aux += vo;
-            if (zero) zero += (uint64_t)blockIdx.y * bt.zstride;
-            if (red) red += blockIdx.y;   // grid_sum_finish offsets its partials / counters itself
-        }
         __shared__ T table[256];
         for (uint32_t i = threadIdx.x; i < A.ntable; i += blockDim.x) table[i] = A.table[i];
         __syncthreads();
-        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x;
+        // work items: (vector j, row block) -- the launch grid (blockIdx.x, blockIdx.y),
+        // or, with a device work list, items 0 .. count * gx - 1 walked by a
+        // persistent grid (vector list[item / gx], row block item % gx)
+        const bool listed = bt.list != nullptr;
+        const uint32_t total = listed ? *bt.count * bt.gx : 1;
+        for (uint32_t item = listed ? blockIdx.x : 0; item < total; item += listed ? gridDim.x : 1)
+        {
+        const uint32_t j = listed ? bt.list[item / bt.gx] : blockIdx.y;
+        if (! listed && bt.active && ! bt.active[j]) return;
+        const uint64_t vo = (uint64_t)j * bt.vstride;
+        const T * __restrict__ x = x_ + (uint64_t)j * (bt.xstride ? bt.xstride : bt.vstride);
+        T * __restrict__ y = y_ + vo;
+        const T * __restrict__ aux = aux_ ? aux_ + vo : aux_;
+        T * __restrict__ zero = zero_ ? zero_ + (uint64_t)j * bt.zstride : zero_;
+        double * red = red_ ? red_ + j : red_;   // grid_sum_finish offsets its partials / counters itself
+        const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
+        const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
         const bool keep = (flags & kKeepL2) != 0;
         const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
         const int K = KT > 0 ? KT : (int)A.K;
@@ -236,6 +243,7 @@ namespace hb2
             __shared__ double scratch[32];
             double s = block_sum(part, scratch);
             grid_sum_finish(s, rs, red, want_sqrt, scratch);
+        }
         }
     }
 

@@ -105,7 +105,9 @@ namespace hb2
     // -- xstride 0 means vstride; a rectangular transfer matrix reads and
     // writes vectors of two levels --, of zero at j * zstride, of red at j);
     // the matrix and aux2 (the Jacobi vector) are shared; a vector whose
-    // active[j] is 0 is skipped entirely.
+    // active[j] is 0 is skipped entirely.  With a work list (list, count on the
+    // device) the vectors are list[0 .. *count - 1] instead, walked by a
+    // persistent grid, so idle vectors cost no blocks (no fused reduction).
     struct Batch
     {
         uint32_t nvec = 1;
@@ -113,6 +115,9 @@ namespace hb2
         uint64_t xstride = 0;
         uint64_t zstride = 0;          // element offset between the `zero` vectors
         const uint8_t * active = nullptr;
+        const uint32_t * list = nullptr;
+        const uint32_t * count = nullptr;
+        uint32_t gx = 0;               // row blocks per vector (set by launch_ell)
     };
 
     // Launch one ELL kernel on `stream`.  aux: rhs / b; aux2: Jacobi P; zero:
@@ -122,6 +127,8 @@ namespace hb2
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
                    void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream,
                    int flags = 0, const Batch * batch = nullptr);
+
+    uint64_t list_grid_cap();
 
     // compressed ELL layout (ell_compact.cu)
     int ell_build_compact(hb2_ell_s * A, cudaStream_t stream);
@@ -174,5 +181,5 @@ namespace hb2
                               int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
     int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
                                uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
-                               cudaStream_t stream);
+                               cudaStream_t stream, const uint32_t * list = nullptr, const uint32_t * count = nullptr);
 }
