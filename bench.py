@@ -52,33 +52,55 @@ def parse():
     return ap.parse_args()
 
 
-def mg_solve_bytes(level: int, cycles: int, min_level: int = MIN_LEVEL, n_pre: int = 4, n_post: int = 4,
-                   s: int = 8, si: int = 4, s_mat: int = 8) -> int:
+def mg_solve_bytes(level: int, cycles: int, row_bytes, min_level: int = MIN_LEVEL, n_pre: int = 4, n_post: int = 4,
+                   s: int = 8) -> int:
     """Algorithmic HBM bytes of one MG solve (each vector / matrix entry touched once per pass).
 
-    Jacobi sweep 9(m)+4s per row; defect 9(m)+3s; restriction R (coarse rows,
-    <=9 slots) 9(m)+2s per coarse row + the fine input; prolongation-add P (fine
-    rows, 4 slots) 4(m)+2s per fine row + the coarse input; convergence defect once
-    per cycle plus the initial one; the coarse solve is counted once (it runs in
-    registers).  m = bytes per stored matrix slot: s_mat + si (plain: value +
-    int32 column = 12 in FP64; compressed: 1-byte code + 2-byte offset = 3)."""
+    row_bytes(l, which) = matrix bytes per row of the layout the level-l operator
+    ("A"), its restriction ("R", rows = level l-1) or prolongation ("P") runs on
+    (plain FP64: 9 x 12 = 108; compressed: 3 per slot; row patterns: 1).
+    Jacobi sweep rb + 4s per row; defect rb + 3s; restriction rb(R) + 2s per
+    coarse row + the fine input; prolongation-add rb(P) + 2s per fine row + the
+    coarse input; convergence defect once per cycle plus the initial one; the
+    coarse solve is counted once (it runs in registers)."""
     total = 0
-    si = s_mat + si - s           # so that (s + si) below is the slot size
     for l in range(min_level + 1, level + 1):
         nf = ((1 << l) + 1) ** 2
         nc = ((1 << (l - 1)) + 1) ** 2
-        total += (n_pre + n_post) * nf * (9 * (s + si) + 4 * s)
-        total += nf * (9 * (s + si) + 3 * s)
-        total += nc * (9 * (s + si) + 2 * s) + nf * s
-        total += nf * (4 * (s + si) + 2 * s) + nc * s
+        total += (n_pre + n_post) * nf * (row_bytes(l, "A") + 4 * s)
+        total += nf * (row_bytes(l, "A") + 3 * s)
+        total += nc * (row_bytes(l, "R") + 2 * s) + nf * s
+        total += nf * (row_bytes(l, "P") + 2 * s) + nc * s
     n0 = ((1 << min_level) + 1) ** 2
-    total += n0 * (9 * (s + si) + 2 * s)
+    total += n0 * (row_bytes(min_level, "A") + 2 * s)
     nF = ((1 << level) + 1) ** 2
-    total += nF * (9 * (s + si) + 3 * s)      # convergence defect + norm
-    return cycles * total + nF * (9 * (s + si) + 3 * s)
+    total += nF * (row_bytes(level, "A") + 3 * s)      # convergence defect + norm
+    return cycles * total + nF * (row_bytes(level, "A") + 3 * s)
+
+
+def layout_row_bytes(hb, dtype, levels):
+    """row_bytes(l, which) for mg_solve_bytes, from matrices of the same shapes as the
+    hierarchy's (the layout choice is made once per shape and process)."""
+    import torch
+    table = {}
+    for l in levels:
+        table[(l, "A")] = hb.SparseMatrixELL.poisson_q1(l, dtype).layout()[2]
+        if l > min(levels):
+            P, R = hb.SparseMatrixELL.transfer(l, dtype)
+            table[(l, "P")], table[(l, "R")] = P.layout()[2], R.layout()[2]
+    return lambda l, which: table[(l, which)]
 
 
 JACOBI_BYTES_PER_ROW = 9 * (8 + 4) + 4 * 8     # FP64 values, int32 columns: 140 B
+KERNEL_OF_LAYOUT = {0: "ell_kernel", 1: "ell_compact_kernel", 2: "ell_pattern_kernel"}
+
+
+def layout_text(kind, table_size, bytes_per_row):
+    if kind == 2:
+        return "row patterns: 1-byte pattern id per row (%d patterns), %d B/row" % (table_size, bytes_per_row)
+    if kind == 1:
+        return "1-byte value codes (table of %d) + int16 column offsets, %d B/row" % (table_size, bytes_per_row)
+    return "FP64 values + int32 columns, %d B/row" % bytes_per_row
 
 
 class Clocks:
@@ -328,14 +350,14 @@ def main():
             kms.append(k0.elapsed_time(k1))
         xa, xb = xb, xa
     k_ms = statistics.mean(kms)
-    compact, table_size, slot_bytes = A.layout()
-    k_bytes = (9 * slot_bytes + 4 * 8) * n
+    kind, table_size, row_bytes = A.layout()
+    k_bytes = (row_bytes + 4 * 8) * n
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
     peaks = load_peaks()
     traffic = load_traffic()
 
-    solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)), si=4 if not compact else 0,
-                                 s_mat=8 if not compact else 3)
+    solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)),
+                                 layout_row_bytes(hb, torch.float64, range(MIN_LEVEL, L + 1)))
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean_ms_max, "higher_is_better": True, "scaling": "weak",
@@ -346,9 +368,8 @@ def main():
         "cycles": int(statistics.median(cycles)), "relres": relres,
         "wall_ms_per_step_incl_flush": 1000 * t_wall / args.steps,
         "roofline": {"bound": "hbm", "kernel": "%s<double,9,kJacobi> (fused Jacobi sweep, level %d)" % (
-                         "ell_compact_kernel" if compact else "ell_kernel", L),
-                     "layout": "%d-byte value codes (table of %d) + int16 column offsets, %d B/row" % (1, table_size,
-                                9 * slot_bytes + 32) if compact else "FP64 values + int32 columns, 140 B/row",
+                         KERNEL_OF_LAYOUT[kind], L),
+                     "layout": layout_text(kind, table_size, row_bytes + 32),
                      "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
                      "peak_source": peaks[1], "traffic": traffic, "algorithmic_bytes": k_bytes,
                      "launch_us": 1000 * k_ms},

@@ -202,6 +202,16 @@ namespace hb2
         return cap;
     }
 
+    uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)
+    {
+        const int cls = reducing ? 1 : 0;
+        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * A->rpt[cls];
+        if (A->layout[cls] == kLayoutCompact) return (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt);
+        return (uint64_t)kEllThreads * (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
+    }
+
+    unsigned ell_grid(const hb2_ell_s * A, bool reducing) { return ceil_div(A->rows, ell_rows_per_block(A, reducing)); }
+
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
                    void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags,
                    const Batch * batch)
@@ -213,8 +223,7 @@ namespace hb2
             if (red) HB2_CUDA(cudaMemsetAsync(red, 0, sizeof(double), stream));
             return HB2_OK;
         }
-        const int R = A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value;
-        const unsigned gx = A->code ? compact_grid(A, red != 0) : ceil_div(A->rows, (uint64_t)kEllThreads * R);
+        const unsigned gx = ell_grid(A, red != 0);
         if (b.nvec == 0 || b.nvec > 65535) return fail(HB2_ERR_ARG, "ELL batch: 1..65535 vectors");
         dim3 grid(gx, b.nvec);
         if (b.list)
@@ -238,7 +247,11 @@ namespace hb2
                 return fail(HB2_ERR_UNSUPPORTED, "matrix / batch too large for the reduction workspace");
             rs = ws->slot();
         }
-        if (A->code) launch_ell_compact(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+        const int cls = red != 0;
+        if (A->layout[cls] == kLayoutPattern)
+            launch_ell_pattern(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, A->rpt[cls]);
+        else if (A->layout[cls] == kLayoutCompact)
+            launch_ell_compact(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
         else if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
         else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
         count_launches(1);
@@ -614,6 +627,7 @@ extern "C" int hb2_ell_destroy(hb2_ell A)
     cudaFree(A->val);
     cudaFree(A->col);
     ell_free_compact(A);
+    ell_free_pattern(A);
     delete A;
     return HB2_OK;
 }
@@ -627,16 +641,17 @@ extern "C" int hb2_ell_info(hb2_ell A, uint64_t * rows, uint64_t * cols, uint64_
     if (stride) *stride = A->ref_stride;
     if (K) *K = A->ref_K;
     if (threads) *threads = A->ref_T;
-    if (device_bytes) *device_bytes = A->bytes + A->compact_bytes;
+    if (device_bytes) *device_bytes = A->bytes + A->compact_bytes + A->pattern_bytes;
     return HB2_OK;
 }
 
-extern "C" int hb2_ell_layout(hb2_ell A, int * compact, uint32_t * table_size, uint32_t * slot_bytes)
+extern "C" int hb2_ell_layout(hb2_ell A, int * layout, uint32_t * table_size, uint32_t * row_bytes)
 {
     if (! A) return fail(HB2_ERR_ARG, "hb2_ell_layout: null matrix");
-    if (compact) *compact = A->code ? 1 : 0;
-    if (table_size) *table_size = A->ntable;
-    if (slot_bytes) *slot_bytes = A->code ? 3u : (uint32_t)(dtype_size(A->dtype) + 4);
+    const int l = A->layout[0];
+    if (layout) *layout = l;
+    if (table_size) *table_size = l == kLayoutPattern ? A->npat : (l == kLayoutCompact ? A->ntable : 0u);
+    if (row_bytes) *row_bytes = l == kLayoutPattern ? 1u : A->K * (l == kLayoutCompact ? 3u : (uint32_t)(dtype_size(A->dtype) + 4));
     return HB2_OK;
 }
 

@@ -47,16 +47,21 @@ namespace hb2
         return rows == cols ? (int64_t)r : (int64_t)((r * cols) / rows);
     }
 
+    // one insert per distinct value of a warp: matrices with few values would
+    // otherwise send every slot's atomic to the same few addresses
     template <typename T>
     __global__ void dict_insert_kernel(const T * __restrict__ val, const int32_t * __restrict__ col, uint64_t n,
                                        unsigned long long * keys, int * flag)
     {
         const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride)
         {
-            if (col[i] < 0) continue;
-            const unsigned long long k = key_of(val[i]);
-            if (k == kEmptyKey) { atomicExch(flag, 3); continue; }
+            const uint64_t i = base + threadIdx.x;
+            const bool live = i < n && col[i] >= 0;
+            const unsigned long long k = live ? key_of(val[i]) : kEmptyKey;
+            if (live && k == kEmptyKey) atomicExch(flag, 3);
+            const unsigned peers = __match_any_sync(0xffffffffu, k);
+            if (k == kEmptyKey || (threadIdx.x & 31) != (unsigned)(__ffs(peers) - 1)) continue;
             uint32_t h = dict_hash(k);
             bool placed = false;
             for (uint32_t p = 0; p < kDictSlots; ++p)
@@ -390,11 +395,13 @@ namespace hb2
         return st;
     }
 
-    // Autotuner: time y = A x and the defect with its fused norm, with the plain
-    // layout and with the compressed layout at 2, 4 and 8 rows per thread (three
-    // timed launches each, after one warm-up), and keep the fastest for each of
-    // the two kernel classes; the compressed arrays are freed when the plain
-    // layout wins both.  Runs once per matrix, at creation, on `stream`.
+    // Autotuner: time y = A x and the defect with its fused norm on every layout
+    // the matrix admits -- plain; compressed with 2, 4 or 8 rows per thread;
+    // row patterns with 1, 2 or 4 rows per thread -- (three timed launches
+    // each, after one warm-up) and keep the fastest for each of the two kernel
+    // classes; the arrays of a layout neither class uses are freed.  Runs once
+    // per matrix shape and process, at creation, on `stream`.
+    //
     // The decision is kept per (device, element type, shape, slots, table size)
     // for the life of the process: matrices of one shape always run the same
     // launch shape, so a reduction over them sums in the same order whichever
@@ -403,40 +410,46 @@ namespace hb2
     {
         int device, dtype;
         uint64_t rows, cols;
-        uint32_t K, ntable;
+        uint32_t K, ntable, npat;
         bool operator<(const TuneKey & o) const
         {
-            return std::tie(device, dtype, rows, cols, K, ntable) < std::tie(o.device, o.dtype, o.rows, o.cols, o.K, o.ntable);
+            return std::tie(device, dtype, rows, cols, K, ntable, npat) <
+                   std::tie(o.device, o.dtype, o.rows, o.cols, o.K, o.ntable, o.npat);
         }
     };
-    static std::mutex g_tune_mutex;
-    static std::map<TuneKey, std::pair<int, int>> g_tune;
-
-    static void apply_decision(hb2_ell_s * A, int plain_v, int red_v)
+    struct Choice
     {
-        if (plain_v == 0 && red_v == 0)
+        int layout[2], rpt[2];
+    };
+    static std::mutex g_tune_mutex;
+    static std::map<TuneKey, Choice> g_tune;
+
+    static void apply_choice(hb2_ell_s * A, const Choice & c)
+    {
+        for (int cls = 0; cls < 2; ++cls)
+        {
+            A->layout[cls] = c.layout[cls];
+            A->rpt[cls] = c.rpt[cls];
+        }
+        if (c.layout[0] == kLayoutCompact) A->compact_rpt = c.rpt[0];
+        if (c.layout[1] == kLayoutCompact) A->compact_rpt_red = c.rpt[1];
+        if (c.layout[0] != kLayoutCompact && c.layout[1] != kLayoutCompact)
         {
             ell_free_compact(A);
             A->compact_bytes = 0;
         }
-        else
-        {
-            // one layout serves both classes: if only one class prefers plain,
-            // the compressed kernel runs at that class's fastest compressed shape
-            A->compact_rpt = plain_v ? plain_v : (red_v ? red_v : 2);
-            A->compact_rpt_red = red_v ? red_v : A->compact_rpt;
-        }
+        if (c.layout[0] != kLayoutPattern && c.layout[1] != kLayoutPattern) ell_free_pattern(A);
     }
 
     static int autotune(hb2_ell_s * A, cudaStream_t s)
     {
-        const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable};
+        const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable, A->npat};
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
             auto it = g_tune.find(key);
             if (it != g_tune.end())
             {
-                apply_decision(A, it->second.first, it->second.second);
+                apply_choice(A, it->second);
                 return HB2_OK;
             }
         }
@@ -454,15 +467,21 @@ namespace hb2
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        uint8_t * code = A->code;
-        const int variants[4] = {0, 2, 4, 8};   // 0: plain layout
+        std::vector<std::pair<int, int>> variants = {{kLayoutPlain, 0}, {kLayoutCompact, 2}, {kLayoutCompact, 4},
+                                                     {kLayoutCompact, 8}};
+        if (A->pat)
+            for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         float best[2] = {1e30f, 1e30f};
-        int best_v[2] = {0, 0};
+        Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}};
         for (int cls = 0; cls < (square ? 2 : 1); ++cls)
-            for (int v : variants)
+            for (const auto & v : variants)
             {
-                A->code = v ? code : 0;
-                A->compact_rpt = A->compact_rpt_red = v ? v : 8;
+                A->layout[cls] = v.first;
+                A->rpt[cls] = v.second;
+                if (v.first == kLayoutCompact) (cls ? A->compact_rpt_red : A->compact_rpt) = v.second;
+                // a fused reduction needs one partial per row block: shapes beyond
+                // the workspace are not candidates
+                if (cls == 1 && (uint64_t)ell_grid(A, true) > ws->max_blocks) continue;
                 float total = 0.f;
                 for (int rep = 0; rep < 4; ++rep)
                 {
@@ -477,20 +496,28 @@ namespace hb2
                     if (rep > 0) total += ms;
                 }
                 if (st) break;
-                if (total < best[cls]) { best[cls] = total; best_v[cls] = v; }
+                if (total < best[cls])
+                {
+                    best[cls] = total;
+                    c.layout[cls] = v.first;
+                    c.rpt[cls] = v.second;
+                }
             }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaStreamSynchronize(s);
         cudaFree(buf);
-        A->code = code;
         if (st) return st;
-        if (! square) best_v[1] = best_v[0];
+        if (! square)
+        {
+            c.layout[1] = c.layout[0];
+            c.rpt[1] = c.rpt[0];
+        }
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
-            g_tune[key] = std::make_pair(best_v[0], best_v[1]);
+            g_tune[key] = c;
         }
-        apply_decision(A, best_v[0], best_v[1]);
+        apply_choice(A, c);
         HB2_LAUNCH_CHECK("ELL layout autotuning");
         return HB2_OK;
     }
@@ -500,13 +527,29 @@ namespace hb2
         if (! compact_enabled() || A->rows < kCompactMinRows) return HB2_OK;
         int st = A->dtype == HB2_F64 ? build_compact_typed<double>(A, stream) : build_compact_typed<float>(A, stream);
         if (st || ! A->code) return st;
+        st = ell_build_pattern(A, stream);
+        if (st) return st;
         const char * v = getenv("HB2_ELL_COMPACT");
-        if (v && strncmp(v, "force", 5) == 0)
+        if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0))
         {
             // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
-            // rows per thread, no autotuning
-            const int r = atoi(v + 5);
-            A->compact_rpt = A->compact_rpt_red = (r == 4 || r == 8) ? r : 2;
+            // rows per thread; pattern[1|2|4]: the row-pattern layout (square
+            // matrices that admit it; the others compressed, 2 rows per thread);
+            // no autotuning
+            Choice c;
+            if (v[0] == 'p' && A->pat)
+            {
+                const int r = atoi(v + 7);
+                c.layout[0] = c.layout[1] = kLayoutPattern;
+                c.rpt[0] = c.rpt[1] = (r == 2 || r == 4) ? r : 1;
+            }
+            else
+            {
+                const int r = v[0] == 'f' ? atoi(v + 5) : 2;
+                c.layout[0] = c.layout[1] = kLayoutCompact;
+                c.rpt[0] = c.rpt[1] = (r == 4 || r == 8) ? r : 2;
+            }
+            apply_choice(A, c);
             return HB2_OK;
         }
         return autotune(A, stream);

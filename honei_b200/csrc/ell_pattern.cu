@@ -1,0 +1,364 @@
+// Row-pattern device layout for square SparseMatrixELL matrices.
+//
+// Stencil and FEM operators on structured grids repeat a handful of rows: every
+// interior row of the Q1 Poisson matrix has the same nine (value, column - row)
+// pairs, every Dirichlet row the same single one.  When a square matrix has at
+// most kPatMax distinct rows in that sense (its compressed layout -- value codes
+// and 16-bit column offsets, ell_compact.cu -- exists and repeats), each row is
+// stored as a one-byte pattern id and the pattern table (K (value, offset)
+// entries per pattern) lives in shared memory: 1 byte per row instead of 3 per
+// slot.  A warp computes 32 consecutive rows per step (one per lane, R steps per
+// thread), so every pattern, vector and gather load is coalesced, and the
+// kernel forms exactly the products and slot-ordered sums of the plain layout:
+// results are bit-identical.  Creation: each row's (code, offset) signature is
+// hashed, distinct hashes are collected in a small device hash set, every row
+// is verified against its pattern's representative row (a hash collision
+// abandons the layout), and the autotuner (ell_compact.cu) then decides per
+// kernel class whether this layout is the fastest.
+#include "hb2_common.cuh"
+#include "hb2_internal.hh"
+
+#include <climits>
+#include <cstring>
+#include <vector>
+
+namespace hb2
+{
+    constexpr uint32_t kPatSlots = 1024;                  // hash set
+    constexpr unsigned long long kPatEmptyKey = ~0ull;
+    constexpr int32_t kPatEmpty = INT_MIN;
+
+    template <typename T>
+    struct PatEnt
+    {
+        T val;
+        int32_t off;      // column - row, kPatEmpty past the row's length
+    };
+
+    template <typename T>
+    struct EllPatternView
+    {
+        const uint8_t * pat;
+        const PatEnt<T> * tab;   // npat * K entries
+        uint64_t rows;
+        uint32_t K, npat;
+    };
+
+    __device__ __forceinline__ unsigned long long row_signature(const uint8_t * code, const int16_t * delta, uint64_t ld,
+                                                                uint32_t K, uint64_t r)
+    {
+        unsigned long long h = 0xcbf29ce484222325ull;
+        for (uint32_t k = 0; k < K; ++k)
+        {
+            const uint32_t w = (uint32_t)code[(uint64_t)k * ld + r] | ((uint32_t)(uint16_t)delta[(uint64_t)k * ld + r] << 8);
+            h = (h ^ w) * 0x100000001b3ull;
+            h ^= h >> 29;
+        }
+        return h == kPatEmptyKey ? h - 1 : h;
+    }
+
+    __device__ __forceinline__ uint32_t pat_hash(unsigned long long k)
+    {
+        k ^= k >> 31;
+        k *= 0x9e3779b97f4a7c15ull;
+        return (uint32_t)(k >> 40) & (kPatSlots - 1);
+    }
+
+    // signatures into the hash set; one insert per distinct signature of a warp
+    __global__ void pat_insert_kernel(const uint8_t * code, const int16_t * delta, uint64_t ld, uint32_t K,
+                                      uint64_t rows, unsigned long long * sig, unsigned long long * keys,
+                                      unsigned * nkeys, int * flag)
+    {
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < rows; base += stride)
+        {
+            const uint64_t r = base + threadIdx.x;
+            const bool ok = r < rows;
+            const unsigned long long h = ok ? row_signature(code, delta, ld, K, r) : kPatEmptyKey;
+            if (ok) sig[r] = h;
+            const unsigned peers = __match_any_sync(0xffffffffu, h);
+            if (! ok || (threadIdx.x & 31) != (unsigned)(__ffs(peers) - 1)) continue;
+            uint32_t s = pat_hash(h);
+            bool placed = false;
+            for (uint32_t p = 0; p < kPatSlots; ++p)
+            {
+                const unsigned long long prev = atomicCAS(keys + s, kPatEmptyKey, h);
+                if (prev == kPatEmptyKey) { atomicAdd(nkeys, 1u); placed = true; break; }
+                if (prev == h) { placed = true; break; }
+                s = (s + 1) & (kPatSlots - 1);
+            }
+            if (! placed) atomicExch(flag, 1);
+        }
+    }
+
+    // pattern id per row, and the smallest row of each pattern (its representative)
+    __global__ void pat_encode_kernel(const unsigned long long * sig, uint64_t rows, const unsigned long long * keys,
+                                      const uint8_t * id_of_slot, uint8_t * pat, unsigned * rep, int * flag)
+    {
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += stride)
+        {
+            const unsigned long long h = sig[r];
+            uint32_t s = pat_hash(h), p = 0;
+            while (keys[s] != h && p < kPatSlots) { s = (s + 1) & (kPatSlots - 1); ++p; }
+            if (p == kPatSlots) { atomicExch(flag, 2); continue; }
+            const uint8_t id = id_of_slot[s];
+            pat[r] = id;
+            atomicMin(rep + id, (unsigned)r);
+        }
+    }
+
+    // every row equals its pattern's representative row, slot by slot
+    __global__ void pat_verify_kernel(const uint8_t * code, const int16_t * delta, uint64_t ld, uint32_t K, uint64_t rows,
+                                      const uint8_t * pat, const unsigned * rep, int * flag)
+    {
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += stride)
+        {
+            const uint64_t q = rep[pat[r]];
+            for (uint32_t k = 0; k < K; ++k)
+                if (code[(uint64_t)k * ld + r] != code[(uint64_t)k * ld + q] || delta[(uint64_t)k * ld + r] != delta[(uint64_t)k * ld + q])
+                {
+                    atomicExch(flag, 3);
+                    break;
+                }
+        }
+    }
+
+    // ------------------------------------------------------------------ kernel
+    // One warp: 32 consecutive rows per step, R steps (rows w*32R + i*32 + lane).
+    template <typename T, int KT, int MODE, int R>
+    __global__ void __launch_bounds__(kEllThreads)
+    ell_pattern_kernel(EllPatternView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
+                       const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
+                       int flags, Batch bt)
+    {
+        typedef Arith<T> M;
+        __shared__ PatEnt<T> tab[kPatMax * kPatMaxK];
+        const int K = KT > 0 ? KT : (int)A.K;
+        for (uint32_t i = threadIdx.x; i < A.npat * (uint32_t)K; i += blockDim.x) tab[i] = A.tab[i];
+        __syncthreads();
+        const bool listed = bt.list != nullptr;
+        const uint32_t total = listed ? *bt.count * bt.gx : 1;
+        for (uint32_t item = listed ? blockIdx.x : 0; item < total; item += listed ? gridDim.x : 1)
+        {
+            const uint32_t j = listed ? bt.list[item / bt.gx] : blockIdx.y;
+            if (! listed && bt.active && ! bt.active[j]) return;
+            const uint64_t vo = (uint64_t)j * bt.vstride;
+            const T * __restrict__ x = x_ + (uint64_t)j * (bt.xstride ? bt.xstride : bt.vstride);
+            T * __restrict__ y = y_ + vo;
+            const T * __restrict__ aux = aux_ ? aux_ + vo : aux_;
+            T * __restrict__ zero = zero_ ? zero_ + (uint64_t)j * bt.zstride : zero_;
+            double * red = red_ ? red_ + j : red_;
+            const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
+            const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
+            const uint64_t r0 = blk * (uint64_t)kEllThreads * R + (uint64_t)(threadIdx.x >> 5) * 32 * R + (threadIdx.x & 31);
+            // every load that does not depend on the pattern is issued first
+            uint32_t p[R];
+            T acc[R], ea[R], ep[R], ex[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+            {
+                const uint64_t r = r0 + 32 * i;
+                const bool ok = r < A.rows;
+                p[i] = ok ? (uint32_t)__ldcs(A.pat + r) : 0u;
+                acc[i] = T(0);
+                if (MODE == kDefect || MODE == kJacobi) ea[i] = ok ? aux[r] : T(0);
+                if (MODE == kJacobi) { ep[i] = ok ? aux2[r] : T(0); ex[i] = ok ? x[r] : T(0); }
+                if (MODE == kDot) ex[i] = ok ? x[r] : T(0);
+                if (MODE == kAdd) ex[i] = ok ? y[r] : T(0);
+            }
+#pragma unroll
+            for (int k = 0; k < (KT > 0 ? KT : kPatMaxK); ++k)
+            {
+                if (KT == 0 && k >= K) break;
+#pragma unroll
+                for (int i = 0; i < R; ++i)
+                {
+                    const uint64_t r = r0 + 32 * i;
+                    const PatEnt<T> e = tab[p[i] * (uint32_t)K + k];
+                    if (r < A.rows && e.off != kPatEmpty)
+                        acc[i] = M::add(acc[i], M::mul(e.val, __ldg(x + (uint32_t)((int32_t)r + e.off))));
+                }
+            }
+            double part = 0.0;
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+            {
+                const uint64_t r = r0 + 32 * i;
+                if (r >= A.rows) continue;
+                if (MODE == kPlain) y[r] = acc[i];
+                else if (MODE == kDefect)
+                {
+                    const T d = M::sub(ea[i], acc[i]);
+                    y[r] = d;
+                    part = fma((double)d, (double)d, part);
+                }
+                else if (MODE == kDot)
+                {
+                    y[r] = acc[i];
+                    part = fma((double)acc[i], (double)ex[i], part);
+                }
+                else if (MODE == kAdd) y[r] = M::add(ex[i], acc[i]);
+                else if (MODE == kJacobi) y[r] = M::add(ex[i], M::mul(ep[i], M::sub(ea[i], acc[i])));
+                else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
+            }
+            if ((MODE == kDefect || MODE == kDot) && red != 0)
+            {
+                __shared__ double scratch[32];
+                const double s = block_sum(part, scratch);
+                grid_sum_finish(s, rs, red, want_sqrt, scratch);
+            }
+        }
+    }
+
+    template <typename T, int MODE>
+    static void pattern_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
+                             void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
+                             int flags, Batch b, int R)
+    {
+        EllPatternView<T> v;
+        v.pat = A->pat;
+        v.tab = (const PatEnt<T> *)A->ptab;
+        v.rows = A->rows;
+        v.K = A->K;
+        v.npat = A->npat;
+#define HB2_PAT_LAUNCH(KT_, R_)                                                                              \
+        ell_pattern_kernel<T, KT_, MODE, R_><<<grid, kEllThreads, 0, s>>>(v, (const T *)x, (T *)y, (const T *)aux, \
+            (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags, b)
+        if (A->K == 9) { if (R == 1) HB2_PAT_LAUNCH(9, 1); else if (R == 2) HB2_PAT_LAUNCH(9, 2); else HB2_PAT_LAUNCH(9, 4); }
+        else { if (R == 1) HB2_PAT_LAUNCH(0, 1); else if (R == 2) HB2_PAT_LAUNCH(0, 2); else HB2_PAT_LAUNCH(0, 4); }
+#undef HB2_PAT_LAUNCH
+    }
+
+    template <typename T>
+    static void pattern_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                              const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                              cudaStream_t s, int f, Batch b, int R)
+    {
+        switch (mode)
+        {
+            case kPlain: pattern_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kDefect: pattern_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kDot: pattern_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kAdd: pattern_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kJacobi: pattern_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kRestrict: pattern_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+        }
+    }
+
+    void launch_ell_pattern(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                            const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                            cudaStream_t stream, int flags, Batch b, int R)
+    {
+        if (A->dtype == HB2_F64) pattern_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R);
+        else pattern_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R);
+    }
+
+    // ------------------------------------------------------------------ build
+    template <typename T>
+    static int build_pattern_typed(hb2_ell_s * A, cudaStream_t s)
+    {
+        const uint64_t rows = A->rows;
+        unsigned long long * sig = 0, * keys = 0;
+        unsigned * nkeys = 0, * rep = 0;
+        int * flag = 0;
+        uint8_t * ids = 0, * pcode = 0;
+        int16_t * pdelta = 0;
+        void * tmp = 0;
+        // one temporary block: signatures | hash set | counters | representatives | id map
+        const size_t bytes = rows * 8 + kPatSlots * 8 + 64 + kPatMax * 4 + kPatSlots + 256;
+        HB2_CUDA(cudaMalloc(&tmp, bytes));
+        char * p = (char *)tmp;
+        sig = (unsigned long long *)p; p += rows * 8;
+        keys = (unsigned long long *)p; p += kPatSlots * 8;
+        nkeys = (unsigned *)p; flag = (int *)(p + 4); p += 64;
+        rep = (unsigned *)p; p += kPatMax * 4;
+        ids = (uint8_t *)p;
+        cudaError_t e = cudaMemsetAsync(keys, 0xFF, kPatSlots * 8, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(nkeys, 0, 64, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(rep, 0xFF, kPatMax * 4, s);
+        const unsigned grid = (unsigned)std::min<uint64_t>(4096, (rows + 255) / 256);
+        if (e == cudaSuccess)
+        {
+            pat_insert_kernel<<<grid, 256, 0, s>>>(A->code, A->delta, A->ld, A->K, rows, sig, keys, nkeys, flag);
+            count_launches(1);
+            e = cudaGetLastError();
+        }
+        std::vector<unsigned long long> hk(kPatSlots);
+        unsigned hn[2] = {0, 0};
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hk.data(), keys, kPatSlots * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hn, nkeys, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        bool ok = e == cudaSuccess && hn[1] == 0 && hn[0] >= 1 && hn[0] <= (unsigned)kPatMax;
+        std::vector<uint8_t> id_of_slot(kPatSlots, 0);
+        uint32_t np = 0;
+        if (ok)
+        {
+            for (uint32_t h = 0; h < kPatSlots; ++h)
+                if (hk[h] != kPatEmptyKey) id_of_slot[h] = (uint8_t)np++;
+            e = cudaMemcpyAsync(ids, id_of_slot.data(), kPatSlots, cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaMalloc(&A->pat, std::max<uint64_t>(rows, 16));
+            if (e == cudaSuccess)
+            {
+                pat_encode_kernel<<<grid, 256, 0, s>>>(sig, rows, keys, ids, A->pat, rep, flag);
+                pat_verify_kernel<<<grid, 256, 0, s>>>(A->code, A->delta, A->ld, A->K, rows, A->pat, rep, flag);
+                count_launches(2);
+                e = cudaGetLastError();
+            }
+            std::vector<unsigned> hrep(np);
+            int hflag = 0;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hrep.data(), rep, np * 4, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            ok = e == cudaSuccess && hflag == 0;
+            if (ok)
+            {
+                // the pattern table from the representative rows
+                std::vector<T> vtab(A->ntable);
+                e = cudaMemcpy(vtab.data(), A->table, A->ntable * sizeof(T), cudaMemcpyDeviceToHost);
+                std::vector<PatEnt<T>> tab((size_t)np * A->K);
+                for (uint32_t q = 0; q < np && e == cudaSuccess; ++q)
+                    for (uint32_t k = 0; k < A->K && e == cudaSuccess; ++k)
+                    {
+                        uint8_t c = 0;
+                        int16_t d = 0;
+                        e = cudaMemcpy(&c, A->code + (uint64_t)k * A->ld + hrep[q], 1, cudaMemcpyDeviceToHost);
+                        if (e == cudaSuccess) e = cudaMemcpy(&d, A->delta + (uint64_t)k * A->ld + hrep[q], 2, cudaMemcpyDeviceToHost);
+                        PatEnt<T> & t = tab[(size_t)q * A->K + k];
+                        t.val = vtab.empty() ? T(0) : vtab[c];
+                        t.off = d == (int16_t)-32768 ? kPatEmpty : (int32_t)d;
+                    }
+                if (e == cudaSuccess) e = cudaMalloc(&A->ptab, tab.size() * sizeof(PatEnt<T>));
+                if (e == cudaSuccess) e = cudaMemcpy(A->ptab, tab.data(), tab.size() * sizeof(PatEnt<T>), cudaMemcpyHostToDevice);
+                ok = e == cudaSuccess;
+                A->npat = np;
+            }
+        }
+        cudaFree(tmp);
+        if (! ok)
+        {
+            ell_free_pattern(A);
+            cudaGetLastError();
+            return e == cudaSuccess ? HB2_OK : cuda_status(e, "ELL row patterns");
+        }
+        A->pattern_bytes = rows + (uint64_t)np * A->K * sizeof(PatEnt<T>);
+        return HB2_OK;
+    }
+
+    int ell_build_pattern(hb2_ell_s * A, cudaStream_t stream)
+    {
+        if (! A->code || A->rows != A->cols || A->rows == 0 || A->K > (uint32_t)kPatMaxK) return HB2_OK;
+        return A->dtype == HB2_F64 ? build_pattern_typed<double>(A, stream) : build_pattern_typed<float>(A, stream);
+    }
+
+    void ell_free_pattern(hb2_ell_s * A)
+    {
+        cudaFree(A->pat);
+        cudaFree(A->ptab);
+        A->pat = 0;
+        A->ptab = 0;
+        A->npat = 0;
+        A->pattern_bytes = 0;
+    }
+}

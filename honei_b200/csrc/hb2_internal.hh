@@ -57,6 +57,17 @@ struct hb2_ell_s
     uint64_t compact_bytes = 0;
     int compact_rpt = 2;       // rows per thread of the compressed kernel (autotuned)
     int compact_rpt_red = 2;   // the same for the modes with a fused reduction
+    // optional row-pattern layout (ell_pattern.cu, square matrices): 1-byte
+    // pattern id per row, npat * K (value, column offset) table entries
+    uint8_t * pat = nullptr;
+    void * ptab = nullptr;
+    uint32_t npat = 0;
+    uint64_t pattern_bytes = 0;
+    // layout each kernel class runs on (index 0: no fused reduction, 1: fused
+    // reduction): hb2::kLayoutPlain / kLayoutCompact / kLayoutPattern, and
+    // its rows per thread
+    int layout[2] = {0, 0};
+    int rpt[2] = {2, 2};
 
     template <typename T> hb2::EllView<T> view() const
     {
@@ -129,6 +140,26 @@ namespace hb2
                    int flags = 0, const Batch * batch = nullptr);
 
     uint64_t list_grid_cap();
+
+    enum LayoutKind
+    {
+        kLayoutPlain = 0,
+        kLayoutCompact = 1,
+        kLayoutPattern = 2
+    };
+    constexpr int kPatMax = 32;     // patterns per matrix
+    constexpr int kPatMaxK = 16;    // slots per row of the pattern layout
+
+    // row blocks of one launch on A for the kernel class (reducing or not)
+    unsigned ell_grid(const hb2_ell_s * A, bool reducing);
+    uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing);
+
+    // row-pattern layout (ell_pattern.cu)
+    int ell_build_pattern(hb2_ell_s * A, cudaStream_t stream);
+    void ell_free_pattern(hb2_ell_s * A);
+    void launch_ell_pattern(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                            const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                            cudaStream_t stream, int flags, Batch b, int R);
 
     // compressed ELL layout (ell_compact.cu)
     int ell_build_compact(hb2_ell_s * A, cudaStream_t stream);

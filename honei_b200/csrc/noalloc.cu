@@ -12,9 +12,11 @@
 // Limits and sharing:
 //  * the scratch holds kNoAllocMaxBlocks block partials, so the matrix may have
 //    at most kNoAllocMaxBlocks * 512 rows in FP64 (8,388,608) and
-//    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216); larger matrices are
+//    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216), and at most
+//    kNoAllocMaxBlocks row blocks in the layout it runs on (the row-pattern
+//    layout at one row per thread: 4,194,304 rows); larger matrices are
 //    rejected with HB2_ERR_UNSUPPORTED before anything is launched;
-//  * every GPU that loads the library holds the array (about 136 KiB) until the
+//  * every GPU that loads the library holds the array (about 134 KiB) until the
 //    process exits;
 //  * all calls on a device share the one array: calls whose kernels overlap on
 //    the GPU (different streams without ordering between them) race on it and
@@ -69,10 +71,12 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
     if (! A || ! norm2_dev) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null matrix or norm output");
     if (A->rows != A->cols) return fail(HB2_ERR_SIZE, "hb2_defect_ell_noalloc: VectorSizeDoesNotMatch (rhs vs columns)");
     if (A->rows > 0 && (! rhs || ! x || ! r)) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null vector");
+    // at most max_rows rows (512 per scratch partial in FP64, 1024 in FP32), and
+    // the row blocks of the layout the matrix runs on must fit the scratch
     const uint64_t rows_per_block = (uint64_t)kEllThreads *
                                     (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
     const uint64_t max_rows = (uint64_t)kNoAllocMaxBlocks * rows_per_block;
-    if (A->rows > max_rows)
+    if (A->rows > max_rows || ell_grid(A, true) > kNoAllocMaxBlocks)
         return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: " + std::to_string(A->rows) +
                     " rows exceed the static scratch limit of " + std::to_string(max_rows) +
                     " rows for this element type; use hb2_defect_ell");

@@ -55,7 +55,7 @@ def main(argv=None) -> int:
         return DenseVector(torch.from_numpy(uniform(m, seed, dtype=npdt)).to(dev))
 
     A = SparseMatrixELL.poisson_q1(L, dt)
-    sb = A.layout()[2]              # bytes per stored slot of the layout in use
+    rb = A.layout()[2]              # matrix bytes per row of the layout in use
     x, b, y, y2 = vec(n, 1), vec(n, 2), vec(n, 3), vec(n, 4)
     _lib.call("hb2_product_ell", A.handle, x.ptr, b.ptr, stream)        # b = A x (setup)
     P = DenseVector(n, dtype=dt)
@@ -63,10 +63,10 @@ def main(argv=None) -> int:
     nrm = torch.zeros(1, dtype=torch.float64, device=dev)
     kernels = {
         "jacobi": (lambda: _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, b.ptr, x.ptr, y.ptr, stream),
-                   n * (9 * sb + 4 * s)),
-        "spmv": (lambda: _lib.call("hb2_product_ell", A.handle, x.ptr, y.ptr, stream), n * (9 * sb + 2 * s)),
+                   n * (rb + 4 * s)),
+        "spmv": (lambda: _lib.call("hb2_product_ell", A.handle, x.ptr, y.ptr, stream), n * (rb + 2 * s)),
         "defect": (lambda: _lib.call("hb2_defect_ell", A.handle, b.ptr, x.ptr, y.ptr,
-                                     ctypes.c_void_p(nrm.data_ptr()), stream), n * (9 * sb + 3 * s)),
+                                     ctypes.c_void_p(nrm.data_ptr()), stream), n * (rb + 3 * s)),
     }
     if a.kernel in ("all", "q1"):
         Q = BandedMatrixQx.poisson_q1(L, dt)
@@ -74,11 +74,11 @@ def main(argv=None) -> int:
     if a.kernel in ("all", "restrict", "prolong"):
         Pm, Rm = SparseMatrixELL.transfer(L, dt)
         c = vec(nc, 5)
-        sbr, sbp = Rm.layout()[2], Pm.layout()[2]
+        rbr, rbp = Rm.layout()[2], Pm.layout()[2]
         kernels["restrict"] = (lambda: _lib.call("hb2_product_ell", Rm.handle, x.ptr, c.ptr, stream),
-                               nc * (9 * sbr + s) + n * s)
+                               nc * (rbr + s) + n * s)
         kernels["prolong"] = (lambda: _lib.call("hb2_product_add_ell", Pm.handle, c.ptr, y2.ptr, stream),
-                              n * (4 * sbp + 2 * s) + nc * s)
+                              n * (rbp + 2 * s) + nc * s)
     names = list(kernels) if a.kernel == "all" else [a.kernel]
     peak = peak_gbs()
     for name in names:
@@ -95,7 +95,7 @@ def main(argv=None) -> int:
                 times.append(e0.elapsed_time(e1))
         ms = statistics.mean(times)
         gbs = nbytes / (ms * 1e-3) / 1e9
-        print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "layout_slot_bytes": sb,
+        print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "layout": A.layout()[0], "matrix_bytes_per_row": rb,
                           "launch_us": 1000 * ms,
                           "algorithmic_bytes": nbytes, "gbs": gbs, "frac_of_measured_peak": gbs / peak}),
               flush=True)

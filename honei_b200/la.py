@@ -148,10 +148,12 @@ class SparseMatrixELL:
         return self._cols
 
     def layout(self):
-        """(compact, table_size, bytes_per_slot) of the device layout in use."""
-        c, t, sb = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_uint32()
-        call("hb2_ell_layout", self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(sb))
-        return bool(c.value), t.value, sb.value
+        """(kind, table_size, matrix_bytes_per_row) of the device layout the
+        matrix-vector kernels run on; kind 0 plain, 1 compressed (value codes +
+        16-bit offsets), 2 row patterns."""
+        c, t, rb = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_uint32()
+        call("hb2_ell_layout", self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(rb))
+        return c.value, t.value, rb.value
 
     def stride(self) -> int:
         return self._stride

@@ -98,11 +98,16 @@ HB2_API int hb2_ell_destroy(hb2_ell A);
 /* rows, cols, reference stride / num_cols_per_row / threads, device bytes */
 HB2_API int hb2_ell_info(hb2_ell A, uint64_t *rows, uint64_t *cols, uint64_t *stride, uint64_t *num_cols_per_row,
                  uint64_t *threads, uint64_t *device_bytes);
-/* Device layout in use: *compact = 1 when slots are stored as 1-byte value codes
- * (a per-matrix table of *table_size distinct values) plus 16-bit column offsets,
- * 0 for plain values + int32 columns; *slot_bytes = bytes per stored slot.
+/* Device layout the matrix-vector kernels (no fused reduction) run on, chosen by
+ * timing at creation among the lossless layouts the matrix admits:
+ *   *layout = 0  plain: values + int32 columns (*table_size = 0);
+ *             1  compressed: 1-byte value codes into a table of *table_size
+ *                distinct values + 16-bit column offsets from the row;
+ *             2  row patterns (square matrices): a 1-byte pattern id per row into
+ *                a table of *table_size patterns of (value, column - row) slots.
+ * *row_bytes = matrix bytes read per row.  Every layout gives the same bits.
  * No counterpart in the reference (its device copy is the raw arrays). */
-HB2_API int hb2_ell_layout(hb2_ell A, int *compact, uint32_t *table_size, uint32_t *slot_bytes);
+HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_t *row_bytes);
 /* Download the matrix in the reference layout (host arrays of K*stride, K*stride
  * and rows elements); Arl as the reference computes it. */
 HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);
@@ -129,9 +134,11 @@ HB2_API int hb2_defect_ell(hb2_ell A, const void *rhs, const void *x, void *r, d
  * latency-critical loop where a cudaMalloc would stall the device):
  * hb2_defect_ell's reduction workspace is cudaMalloc'd on first use of a stream,
  * this variant keeps the reduction scratch in a fixed file-scope device array
- * (about 128 KiB per GPU that loads the library, held until exit).  norm2_dev
- * is required.  Limit: at most 8,388,608 rows in F64 and 16,777,216 in F32;
- * larger matrices return HB2_ERR_UNSUPPORTED before any launch.  All calls on a
+ * (about 134 KiB per GPU that loads the library, held until exit).  norm2_dev
+ * is required.  Limit: at most 8,388,608 rows in F64 and 16,777,216 in F32,
+ * and at most 16,384 row blocks in the device layout the matrix runs on (the
+ * row-pattern layout at one row per thread: 4,194,304 rows); larger matrices
+ * return HB2_ERR_UNSUPPORTED before any launch.  All calls on a
  * device share the array, so calls that overlap on the GPU race; calls ordered on
  * one stream are safe.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) and caches it: make it before any stream capture. */

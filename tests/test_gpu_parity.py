@@ -429,22 +429,28 @@ def test_ir_mixed_fp64_coarse(oracle):
     assert it <= 6
 
 
-@pytest.mark.parametrize("rpt", [2, 4, 8])
+@pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
-def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, rpt):
-    """Value-dictionary + 16-bit offset layout: same bits as the plain layout (and the oracle)
-    for every ELL kernel mode, square and rectangular."""
+def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
+    """Value-dictionary + 16-bit offset layout (forceR) and row-pattern layout (patternR,
+    square matrices; the rectangular transfers stay compressed): same bits as the plain
+    layout (and the oracle) for every ELL kernel mode, square and rectangular."""
     from honei_b200 import _lib
     npdt = np.float64 if dt == torch.float64 else np.float32
     L = 9
-    monkeypatch.setenv("HB2_ELL_COMPACT", f"force{rpt}")   # compressed layout, no autotuning
+    monkeypatch.setenv("HB2_ELL_COMPACT", layout)   # that layout, no autotuning
     A = SparseMatrixELL.poisson_q1(L, dt)
     P, R = SparseMatrixELL.transfer(L, dt)
-    assert A.layout()[0] and A.layout()[1] == 3 and P.layout()[0] and R.layout()[0]
+    if layout.startswith("pattern"):
+        # two row patterns: interior stencil, Dirichlet identity row; 1 matrix byte per row
+        assert A.layout() == (2, 2, 1)
+    else:
+        assert A.layout() == (1, 3, 27)
+    assert P.layout()[0] == 1 and R.layout()[0] == 1
     monkeypatch.setenv("HB2_ELL_COMPACT", "0")
     A0 = SparseMatrixELL.poisson_q1(L, dt)
     P0, R0 = SparseMatrixELL.transfer(L, dt)
-    assert not A0.layout()[0] and not P0.layout()[0]
+    assert A0.layout()[0] == 0 and P0.layout()[0] == 0
     n, nc = A.rows(), R.rows()
     x, b = oracle.uniform(n, 3, npdt), oracle.uniform(n, 4, npdt)
     c = oracle.uniform(nc, 5, npdt)
@@ -476,7 +482,7 @@ def test_compressed_layout_falls_back_when_not_eligible(oracle):
     Ax[Ax != 0] = oracle.uniform(int((Ax != 0).sum()), 77) + 2.0   # many distinct values
     Arl = ref.Arl
     A = SparseMatrixELL.from_arrays(ref.rows, ref.cols, ref.stride, ref.K, ref.Aj, Ax, Arl)
-    assert not A.layout()[0]
+    assert A.layout()[0] == 0
     ref2 = oracle.Ell(ref.rows, ref.cols, ref.stride, ref.K, 1, ref.Aj, Ax, Arl)
     x = oracle.uniform(ref.cols, 1)
     y = dvec(np.zeros(ref.rows))
