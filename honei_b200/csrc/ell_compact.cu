@@ -15,6 +15,7 @@
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
 
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -424,6 +425,43 @@ namespace hb2
     static std::mutex g_tune_mutex;
     static std::map<TuneKey, Choice> g_tune;
 
+    // HB2_TUNE_FILE=<path>: decisions are read from the file when it exists and
+    // every new decision is appended to it, so a later process (a profiler
+    // run, whose replays would distort the timings) makes the same choices.
+    // Called with g_tune_mutex held.
+    static void tune_file_load()
+    {
+        static bool loaded = false;
+        if (loaded) return;
+        loaded = true;
+        const char * path = getenv("HB2_TUNE_FILE");
+        if (! path || ! *path) return;
+        FILE * f = fopen(path, "r");
+        if (! f) return;
+        TuneKey k;
+        Choice c;
+        unsigned long long rows, cols;
+        while (fscanf(f, "%d %d %llu %llu %u %u %u %d %d %d %d", &k.device, &k.dtype, &rows, &cols, &k.K, &k.ntable,
+                      &k.npat, &c.layout[0], &c.rpt[0], &c.layout[1], &c.rpt[1]) == 11)
+        {
+            k.rows = rows;
+            k.cols = cols;
+            g_tune[k] = c;
+        }
+        fclose(f);
+    }
+
+    static void tune_file_append(const TuneKey & k, const Choice & c)
+    {
+        const char * path = getenv("HB2_TUNE_FILE");
+        if (! path || ! *path) return;
+        FILE * f = fopen(path, "a");
+        if (! f) return;
+        fprintf(f, "%d %d %llu %llu %u %u %u %d %d %d %d\n", k.device, k.dtype, (unsigned long long)k.rows,
+                (unsigned long long)k.cols, k.K, k.ntable, k.npat, c.layout[0], c.rpt[0], c.layout[1], c.rpt[1]);
+        fclose(f);
+    }
+
     static void apply_choice(hb2_ell_s * A, const Choice & c)
     {
         for (int cls = 0; cls < 2; ++cls)
@@ -446,6 +484,7 @@ namespace hb2
         const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable, A->npat};
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
+            tune_file_load();
             auto it = g_tune.find(key);
             if (it != g_tune.end())
             {
@@ -516,6 +555,7 @@ namespace hb2
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
             g_tune[key] = c;
+            tune_file_append(key, c);
         }
         apply_choice(A, c);
         HB2_LAUNCH_CHECK("ELL layout autotuning");

@@ -96,15 +96,25 @@ namespace hb2
                                       const uint8_t * id_of_slot, uint8_t * pat, unsigned * rep, int * flag)
     {
         const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-        for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += stride)
+        for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < rows; base += stride)
         {
-            const unsigned long long h = sig[r];
-            uint32_t s = pat_hash(h), p = 0;
-            while (keys[s] != h && p < kPatSlots) { s = (s + 1) & (kPatSlots - 1); ++p; }
-            if (p == kPatSlots) { atomicExch(flag, 2); continue; }
-            const uint8_t id = id_of_slot[s];
-            pat[r] = id;
-            atomicMin(rep + id, (unsigned)r);
+            const uint64_t r = base + threadIdx.x;
+            int id = -1;
+            if (r < rows)
+            {
+                const unsigned long long h = sig[r];
+                uint32_t s = pat_hash(h), p = 0;
+                while (keys[s] != h && p < kPatSlots) { s = (s + 1) & (kPatSlots - 1); ++p; }
+                if (p == kPatSlots) atomicExch(flag, 2);
+                else
+                {
+                    id = id_of_slot[s];
+                    pat[r] = (uint8_t)id;
+                }
+            }
+            // the lowest lane of each id in the warp holds the warp's smallest row of it
+            const unsigned peers = __match_any_sync(0xffffffffu, id);
+            if (id >= 0 && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicMin(rep + id, (unsigned)r);
         }
     }
 
