@@ -191,12 +191,12 @@ namespace hb2
         const void * jac;
     };
     constexpr uint64_t kSubMaxRows = 20000;
-    int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int n_pre, int n_post, bool down,
+    int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post, bool down,
                         cudaStream_t stream);
     int subcycle_prepare();
     // the whole bottom of the cycle (levels 0..top, coarsest CG included) in one
     // launch; levels 1..t1 run in one CTA (subcycle.cu)
-    constexpr uint64_t kSubLocalRows = 4500;
+    constexpr uint64_t kSubLocalRows = 1100;
     bool subvcycle_supported(const hb2_ell_s * coarse, const hb2_ell_s * coarse64);
     int launch_subvcycle(int dtype, const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post,
                          const hb2_ell_s * coarse, const hb2_ell_s * coarse64, uint64_t max_iters, double eps, int exact,

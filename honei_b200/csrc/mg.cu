@@ -75,7 +75,7 @@ struct hb2_mg_s
     double * r0_dev;         // sqrt(r0.r0)
     uint64_t * iters_dev;    // cycles done
     int sub_top;             // levels 1..sub_top run as cluster kernels (-1: none)
-    int sub_t1;              // of those, levels 1..sub_t1 run in one CTA (fused path)
+    int sub_t1;              // of those, levels 1..sub_t1 run in one CTA
     bool sub_fused;          // levels 0..sub_top, coarse CG included, in one launch
     hb2_ell_s * coarse64;    // FP64 copy of the coarsest operator (F32 hierarchies with coarse_fp64)
 };
@@ -133,10 +133,10 @@ namespace hb2
             return launch_subvcycle(mg->dtype, d, mg->sub_top, mg->sub_t1, (int)mg->prm.n_pre_smooth,
                                     (int)mg->prm.n_post_smooth, mg->lev[0].A, mg->coarse64, mg->prm.max_iters_coarse,
                                     mg->prm.coarse_eps, mg->prm.coarse_exact, mg->coarse_used_dev, mg->coarse_def_dev, s);
-        int st = launch_subcycle(mg->dtype, d, mg->sub_top, (int)mg->prm.n_pre_smooth, (int)mg->prm.n_post_smooth,
-                                 true, s);
+        int st = launch_subcycle(mg->dtype, d, mg->sub_top, mg->sub_t1, (int)mg->prm.n_pre_smooth,
+                                 (int)mg->prm.n_post_smooth, true, s);
         if (! st) st = coarse_solve(mg, s);
-        if (! st) st = launch_subcycle(mg->dtype, d, mg->sub_top, (int)mg->prm.n_pre_smooth,
+        if (! st) st = launch_subcycle(mg->dtype, d, mg->sub_top, mg->sub_t1, (int)mg->prm.n_pre_smooth,
                                        (int)mg->prm.n_post_smooth, false, s);
         return st;
     }

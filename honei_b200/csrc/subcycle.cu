@@ -51,6 +51,7 @@ namespace hb2
     {
         SubLevel<T> lev[kSubMaxLevels];   // lev[0]: coarsest
         int top;                          // highest level index handled here
+        int t1;                           // levels 1..t1 run in CTA 0 alone (block barriers)
         int n_pre, n_post;
     };
 
@@ -174,20 +175,36 @@ namespace hb2
         sub_smooth(L, n_post, tm);
     }
 
+    // down: levels top..t1+1 over the cluster, then levels t1..1 in CTA 0 alone
+    // (the smallest levels have too few rows to need more than one CTA, and a
+    // block barrier is far cheaper than a cluster barrier)
     template <typename T, bool PL>
     __global__ void __launch_bounds__(1024) mg_sub_down_kernel(const __grid_constant__ SubCycle<T> sc)
     {
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
-        for (int i = sc.top; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+        if (sc.t1 < 1 || cluster.block_rank() != 0) return;
+        const Team<true> blk = {threadIdx.x, blockDim.x};
+        for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk);
     }
 
+    // up: levels 1..t1 in CTA 0 alone, then t1+1..top over the cluster
     template <typename T, bool PL>
     __global__ void __launch_bounds__(1024) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
     {
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
-        for (int i = 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
+        if (sc.t1 >= 1)
+        {
+            if (cluster.block_rank() == 0)
+            {
+                const Team<true> blk = {threadIdx.x, blockDim.x};
+                for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk);
+            }
+            cluster.sync();
+        }
+        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
     }
 
     // ------------------------------------------------------------------
@@ -289,8 +306,12 @@ namespace hb2
         if (it != widths.end()) return it->second;
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         int width = 1;
-        for (int w : {16, 8})
+        // HB2_SUB_CLUSTER=<w> caps the width (16, 8, 4, 2)
+        const char * cap = getenv("HB2_SUB_CLUSTER");
+        const int wmax = cap && *cap ? atoi(cap) : 16;
+        for (int w : {16, 8, 4, 2})
         {
+            if (w > wmax) continue;
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(w);
             cfg.blockDim = dim3(threads);
@@ -335,11 +356,13 @@ namespace hb2
     }
 
     template <typename T>
-    static int launch_sub_typed(const SubLevelDesc * lev, int top, int n_pre, int n_post, bool down, cudaStream_t s)
+    static int launch_sub_typed(const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post, bool down,
+                                cudaStream_t s)
     {
         SubCycle<T> sc;
         for (int i = 0; i <= top; ++i) sc.lev[i] = sub_level<T>(lev[i]);
         sc.top = top;
+        sc.t1 = t1;
         sc.n_pre = n_pre;
         sc.n_post = n_post;
         const int w = cluster_width((const void *)mg_sub_down_kernel<T, true>);
@@ -350,12 +373,12 @@ namespace hb2
                     : launch_cluster(mg_sub_up_kernel<T, false>, sc, w, s, "cluster sub-cycle launch (up)");
     }
 
-    int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int n_pre, int n_post, bool down,
+    int launch_subcycle(int dtype, const SubLevelDesc * lev, int top, int t1, int n_pre, int n_post, bool down,
                         cudaStream_t stream)
     {
-        if (top < 1 || top >= kSubMaxLevels) return fail(HB2_ERR_UNSUPPORTED, "sub-cycle: bad level range");
-        return dtype == HB2_F64 ? launch_sub_typed<double>(lev, top, n_pre, n_post, down, stream)
-                                : launch_sub_typed<float>(lev, top, n_pre, n_post, down, stream);
+        if (top < 1 || top >= kSubMaxLevels || t1 < 0 || t1 > top) return fail(HB2_ERR_UNSUPPORTED, "sub-cycle: bad level range");
+        return dtype == HB2_F64 ? launch_sub_typed<double>(lev, top, t1, n_pre, n_post, down, stream)
+                                : launch_sub_typed<float>(lev, top, t1, n_pre, n_post, down, stream);
     }
 
     bool subvcycle_supported(const hb2_ell_s * coarse, const hb2_ell_s * coarse64)
