@@ -176,6 +176,7 @@ namespace hb2
                                          const uint32_t * item0, F && body)
     {
         __shared__ uint32_t s_item0[kMaxGroups + 1], s_start[kMaxGroups];
+        pdl_entry();
         if (threadIdx.x <= (unsigned)P.ngroups) s_item0[threadIdx.x] = item0[threadIdx.x];
         if (threadIdx.x < (unsigned)P.ngroups) s_start[threadIdx.x] = start[threadIdx.x];
         __syncthreads();
@@ -331,6 +332,7 @@ namespace hb2
     // start of a step: the vectors with work (kNew, kRun)
     __global__ void __launch_bounds__(1024) bpcg_plan_kernel(const __grid_constant__ OuterPlan P, SlotScalars S, uint32_t nvec)
     {
+        pdl_entry();
         const uint32_t n = block_compact(nvec, [&](uint32_t j) { const uint8_t st = S.state[j]; return st == kNew || st == kRun; },
                                          S.live);
         segments(P, S.live, n, S.plan->live_start, S.plan->live_n, S.plan->live_item0);
@@ -340,6 +342,7 @@ namespace hb2
     __global__ void __launch_bounds__(1024) bpcg_decide_kernel(const __grid_constant__ OuterPlan P, SlotScalars S,
                                                                uint32_t nvec, uint64_t max_iters)
     {
+        pdl_entry();
         for (uint32_t j = threadIdx.x; j < nvec; j += blockDim.x)
         {
             const uint8_t st = S.state[j];
@@ -443,6 +446,7 @@ namespace hb2
     __global__ void bpcg_loop_decide_kernel(const Plan * plan, uint64_t * steps, uint64_t max_steps,
                                             cudaGraphConditionalHandle h)
     {
+        pdl_entry();
         const uint64_t s = *steps + 1;
         *steps = s;
         cudaGraphSetConditional(h, (plan->nactive > 0 && s < max_steps) ? 1u : 0u);
@@ -510,12 +514,12 @@ namespace hb2
         switch (which)
         {
             case 0:
-                if (B->outer_k9) bpcg_phase_a_kernel<9><<<grid, kOuterThreads, 0, s>>>(B->plan, B->S);
-                else bpcg_phase_a_kernel<0><<<grid, kOuterThreads, 0, s>>>(B->plan, B->S);
+                if (B->outer_k9) launch_pdl(bpcg_phase_a_kernel<9>, grid, dim3(kOuterThreads), 0, s, B->plan, B->S);
+                else launch_pdl(bpcg_phase_a_kernel<0>, grid, dim3(kOuterThreads), 0, s, B->plan, B->S);
                 break;
-            case 1: bpcg_update_kernel<<<grid, kOuterThreads, 0, s>>>(B->plan, B->S); break;
-            case 2: bpcg_dot_z_kernel<<<grid, kOuterThreads, 0, s>>>(B->plan, B->S); break;
-            default: bpcg_p_kernel<<<grid, kOuterThreads, 0, s>>>(B->plan, B->S); break;
+            case 1: launch_pdl(bpcg_update_kernel, grid, dim3(kOuterThreads), 0, s, B->plan, B->S); break;
+            case 2: launch_pdl(bpcg_dot_z_kernel, grid, dim3(kOuterThreads), 0, s, B->plan, B->S); break;
+            default: launch_pdl(bpcg_p_kernel, grid, dim3(kOuterThreads), 0, s, B->plan, B->S); break;
         }
         count_launches(1);
         HB2_LAUNCH_CHECK("batched PCG outer kernel");
@@ -586,14 +590,14 @@ namespace hb2
 
     static int record_step(hb2_batch_s * B, cudaStream_t s)
     {
-        bpcg_plan_kernel<<<1, 1024, 0, s>>>(B->plan, B->S, B->nvec);
+        launch_pdl(bpcg_plan_kernel, dim3(1), dim3(1024), 0, s, B->plan, B->S, B->nvec);
         count_launches(1);
         HB2_LAUNCH_CHECK("bpcg_plan_kernel");
         int st = outer_launch(B, 0, s);
         if (! st) st = outer_launch(B, 1, s);
         if (! st)
         {
-            bpcg_decide_kernel<<<1, 1024, 0, s>>>(B->plan, B->S, B->nvec, B->prm.max_iters);
+            launch_pdl(bpcg_decide_kernel, dim3(1), dim3(1024), 0, s, B->plan, B->S, B->nvec, B->prm.max_iters);
             count_launches(1);
             HB2_LAUNCH_CHECK("bpcg_decide_kernel");
         }
@@ -672,7 +676,7 @@ namespace hb2
         int st = record_step(B, B->cap2);
         if (! st)
         {
-            bpcg_loop_decide_kernel<<<1, 1, 0, B->cap2>>>(B->S.plan, B->S.steps, B->prm.max_iters + 2, h);
+            launch_pdl(bpcg_loop_decide_kernel, dim3(1), dim3(1), 0, B->cap2, B->S.plan, B->S.steps, B->prm.max_iters + 2, h);
             e = cudaGetLastError();
             if (e != cudaSuccess) st = cuda_status(e, "bpcg_loop_decide_kernel");
         }

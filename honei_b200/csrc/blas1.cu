@@ -21,6 +21,7 @@ namespace hb2
                                  uint64_t n)
     {
         typedef Arith<T> M;
+        pdl_entry();
         const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         {
@@ -49,9 +50,9 @@ namespace hb2
         if (! out) return fail(HB2_ERR_ARG, "BLAS-1: null output vector");
         unsigned grid = stream_grid(n);
         if (dt == HB2_F64)
-            blas1_kernel<double, OP><<<grid, 256, 0, st>>>((double *)out, (const double *)a, (const double *)b, s, n);
+            launch_pdl(blas1_kernel<double, OP>, grid, dim3(256), 0, st, (double *)out, (const double *)a, (const double *)b, s, n);
         else
-            blas1_kernel<float, OP><<<grid, 256, 0, st>>>((float *)out, (const float *)a, (const float *)b, (float)s, n);
+            launch_pdl(blas1_kernel<float, OP>, grid, dim3(256), 0, st, (float *)out, (const float *)a, (const float *)b, (float)s, n);
         count_launches(1);
         HB2_LAUNCH_CHECK("BLAS-1 launch");
         return HB2_OK;

@@ -247,10 +247,10 @@ namespace hb2
         const unsigned grid = list ? (unsigned)std::min<uint64_t>(nvec, list_grid_cap()) : nvec;
         switch (rpl)
         {
-            case 1: cg_warp_reg_kernel<T, S, 1><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
-            case 2: cg_warp_reg_kernel<T, S, 2><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
-            case 3: cg_warp_reg_kernel<T, S, 3><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
-            default: cg_warp_reg_kernel<T, S, 4><<<grid, 32, smem, stream>>>(v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            case 1: launch_pdl(cg_warp_reg_kernel<T, S, 1>, dim3(grid), dim3(32), smem, stream, v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            case 2: launch_pdl(cg_warp_reg_kernel<T, S, 2>, dim3(grid), dim3(32), smem, stream, v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            case 3: launch_pdl(cg_warp_reg_kernel<T, S, 3>, dim3(grid), dim3(32), smem, stream, v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
+            default: launch_pdl(cg_warp_reg_kernel<T, S, 4>, dim3(grid), dim3(32), smem, stream, v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
         }
         return true;
     }

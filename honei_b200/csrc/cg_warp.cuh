@@ -188,6 +188,7 @@ namespace hb2
                        const uint32_t * list, const uint32_t * count)
     {
         extern __shared__ __align__(16) unsigned char smem_raw[];
+        pdl_entry();
         if (list)
         {
             // work list: the systems of vectors list[0 .. *count - 1], one per warp in turn

@@ -66,6 +66,7 @@ namespace hb2
     {
         constexpr int R = RowsPerThread<T>::value;
         typedef Arith<T> M;
+        pdl_entry();
         // work items: (vector j, row block) -- the launch grid (blockIdx.x, blockIdx.y),
         // or, with a device work list, items 0 .. count * gx - 1 walked by a
         // persistent grid (vector list[item / gx], row block item % gx)
@@ -161,14 +162,14 @@ namespace hb2
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         if (A->K == 9)
-            ell_kernel<T, 9, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags, b);
+            launch_pdl(ell_kernel<T, 9, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+                       (T *)zero, rs, red, want_sqrt, flags, b);
         else if (A->K == 4)
-            ell_kernel<T, 4, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags, b);
+            launch_pdl(ell_kernel<T, 4, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+                       (T *)zero, rs, red, want_sqrt, flags, b);
         else
-            ell_kernel<T, 0, MODE><<<grid, kEllThreads, 0, s>>>(v, xp, yp, (const T *)aux, (const T *)aux2,
-                                                                (T *)zero, rs, red, want_sqrt, flags, b);
+            launch_pdl(ell_kernel<T, 0, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+                       (T *)zero, rs, red, want_sqrt, flags, b);
     }
 
     template <typename T>

@@ -159,6 +159,7 @@ namespace hb2
         __shared__ T table[256];
         for (uint32_t i = threadIdx.x; i < A.ntable; i += blockDim.x) table[i] = A.table[i];
         __syncthreads();
+        pdl_entry();   // the value table is constant: loaded before the wait
         // work items: (vector j, row block) -- the launch grid (blockIdx.x, blockIdx.y),
         // or, with a device work list, items 0 .. count * gx - 1 walked by a
         // persistent grid (vector list[item / gx], row block item % gx)
@@ -273,8 +274,8 @@ namespace hb2
         const T * a2 = (const T *)aux2;
         T * zp = (T *)zero;
 #define HB2_COMPACT_LAUNCH(KT_, R_)                                                                          \
-        ell_compact_kernel<T, KT_, MODE, R_><<<grid, kEllThreads, 0, s>>>(v, xp, yp, ap, a2, zp, rs, red,      \
-                                                                          want_sqrt, flags, b)
+        launch_pdl(ell_compact_kernel<T, KT_, MODE, R_>, grid, dim3(kEllThreads), 0, s, v, xp, yp, ap, a2, zp, rs, \
+                   red, want_sqrt, flags, b)
         const int R = red ? A->compact_rpt_red : A->compact_rpt;
         if (A->K == 9) { if (R == 2) HB2_COMPACT_LAUNCH(9, 2); else if (R == 4) HB2_COMPACT_LAUNCH(9, 4); else HB2_COMPACT_LAUNCH(9, 8); }
         else if (A->K == 4) { if (R == 2) HB2_COMPACT_LAUNCH(4, 2); else if (R == 4) HB2_COMPACT_LAUNCH(4, 4); else HB2_COMPACT_LAUNCH(4, 8); }

@@ -53,6 +53,20 @@ namespace hb2
     };
 
     // ------------------------------------------------------------------
+    // Programmatic dependent launch.  A kernel launched with
+    // cudaLaunchAttributeProgrammaticStreamSerialization (launch_pdl) may be
+    // scheduled while its predecessor in the stream is still finishing; it
+    // waits here until the predecessor has completed and its writes are
+    // visible, then lets its own successor start launching.  Without the
+    // attribute both instructions return at once.  Every kernel launched with
+    // the attribute calls this before it reads anything a predecessor wrote.
+    __device__ __forceinline__ void pdl_entry()
+    {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
+
+    // ------------------------------------------------------------------
     // Deterministic reductions.  A block reduces its threads' partials with a
     // fixed shuffle tree, writes one partial per block, and the last block to
     // finish (ticket counter) reduces the partials in a fixed order.  The result

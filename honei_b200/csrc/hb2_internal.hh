@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "hb2_common.cuh"
 
 namespace hb2
@@ -13,6 +15,27 @@ namespace hb2
     // FP64, two rows; four rows for FP32).
     constexpr int kEllThreads = 256;
     constexpr uint32_t kMaxReduceBlocks = 1u << 16;
+
+    // Launch with programmatic dependent launch (pdl_entry in the kernel) when
+    // HB2_PDL=1: the kernel's blocks may start while the stream's previous
+    // kernel finishes (a chain of small kernels, a V-cycle's small levels).
+    bool pdl_enabled();
+    template <typename... KArgs, typename... Args>
+    inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  Args &&... args)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl_enabled() ? 1 : 0;
+        return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    }
 
     void count_launches(uint64_t n);
     void set_launch_count(uint64_t n);   // undo the counting of captured (not launched) kernels
@@ -61,6 +84,7 @@ struct hb2_ell_s
     // pattern id per row, npat * K (value, column offset) table entries
     uint8_t * pat = nullptr;
     void * ptab = nullptr;
+    void * ptab_host = nullptr;   // host copy of the table (launch parameters)
     uint32_t npat = 0;
     uint64_t pattern_bytes = 0;
     // layout each kernel class runs on (index 0: no fused reduction, 1: fused

@@ -179,6 +179,7 @@ namespace hb2
     __global__ void mg_loop_decide_kernel(const double * norm, const double * r0, uint64_t * iters, uint64_t max_iters,
                                           double eps, cudaGraphConditionalHandle h)
     {
+        pdl_entry();
         const uint64_t it = *iters + 1;
         *iters = it;
         const double rc = *norm;
@@ -233,8 +234,8 @@ namespace hb2
         if (! st) st = finest_norm(mg, mg->cap2);
         if (! st)
         {
-            mg_loop_decide_kernel<<<1, 1, 0, mg->cap2>>>(mg->norm_dev, mg->r0_dev, mg->iters_dev, mg->prm.max_iters,
-                                                          mg->prm.eps_relative, h);
+            launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap2, mg->norm_dev, mg->r0_dev, mg->iters_dev,
+                       mg->prm.max_iters, mg->prm.eps_relative, h);
             count_launches(1);
             e = cudaGetLastError();
             if (e != cudaSuccess) return capture_error(e, "decide kernel", mg);

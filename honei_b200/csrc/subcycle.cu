@@ -181,6 +181,7 @@ namespace hb2
     template <typename T, bool PL>
     __global__ void __launch_bounds__(1024) mg_sub_down_kernel(const __grid_constant__ SubCycle<T> sc)
     {
+        pdl_entry();
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
         for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
@@ -193,6 +194,7 @@ namespace hb2
     template <typename T, bool PL>
     __global__ void __launch_bounds__(1024) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
     {
+        pdl_entry();
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
         if (sc.t1 >= 1)
@@ -248,6 +250,7 @@ namespace hb2
     template <typename T, bool PL>
     __global__ void __launch_bounds__(kSubVThreads, 1) mg_sub_vcycle_kernel(const __grid_constant__ SubVCycle<T> sc)
     {
+        pdl_entry();
         __shared__ double cg_smem[3 * 96];
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
@@ -342,13 +345,15 @@ namespace hb2
         cfg.blockDim = dim3(threads);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = s;
-        cudaLaunchAttribute at[1];
+        cudaLaunchAttribute at[2];
         at[0].id = cudaLaunchAttributeClusterDimension;
         at[0].val.clusterDim.x = w;
         at[0].val.clusterDim.y = 1;
         at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = pdl_enabled() ? 2 : 1;
         cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, param);
         count_launches(1);
         if (e != cudaSuccess) return cuda_status(e, what);
