@@ -491,9 +491,13 @@ struct hb2_batch_s
     void * block = 0;                   // every device array of the batch
     uint64_t bytes = 0;
     cudaStream_t cap = 0, cap2 = 0;
-    cudaGraph_t step_graph = 0, solve_graph = 0;
-    cudaGraphExec_t step_exec = 0, solve_exec = 0;
+    cudaGraph_t step_graph = 0, solve_graph = 0, light_graph = 0;
+    cudaGraphExec_t step_exec = 0, solve_exec = 0, light_exec = 0;
     uint64_t step_kernels = 0;
+    uint64_t grid_cap = 0;              // blocks of the work-list launches being recorded (0: default)
+    uint64_t light_rows = 0;            // live rows up to which hb2_batch_step uses the light graph
+    uint64_t started_rows = 0;          // rows of the vectors started since the last step
+    std::vector<uint64_t> vec_rows;     // finest-level rows of each vector
     // pinned host mirror of the per-vector results
     uint8_t * h_state = 0;
     uint32_t * h_iters = 0;
@@ -510,7 +514,7 @@ namespace hb2
     // outer kernels: a persistent grid (8 blocks of 256 threads per SM) over the work list
     static int outer_launch(hb2_batch_s * B, int which, cudaStream_t s)
     {
-        const dim3 grid((unsigned)std::min<uint64_t>(B->outer_items, list_grid_cap()));
+        const dim3 grid((unsigned)std::min<uint64_t>(B->outer_items, B->grid_cap ? B->grid_cap : list_grid_cap()));
         switch (which)
         {
             case 0:
@@ -533,6 +537,7 @@ namespace hb2
         bt.vstride = L.vs;
         bt.list = B->S.plist;
         bt.count = &B->S.plan->vcount[L.level - B->coarse_level];
+        bt.cap = B->grid_cap;
         float * cur = L.x, * nxt = L.tmp;
         for (uint64_t k = 0; k < sweeps; ++k)
         {
@@ -559,6 +564,7 @@ namespace hb2
             bt.vstride = L.vs;
             bt.list = B->S.plist;
             bt.count = &B->S.plan->vcount[i];
+            bt.cap = B->grid_cap;
             if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, 0, s, 0, &bt);
             Batch br = bt;
             br.vstride = C.vs;
@@ -569,7 +575,7 @@ namespace hb2
         }
         BLevel & C0 = B->lev[0];
         int st = launch_cg_warp_batched(B->coarse64, HB2_F32, C0.b, C0.x, C0.nv, C0.vs, 0,
-                                        B->prm.max_iters_coarse, B->prm.coarse_eps, s, B->S.plist, &B->S.plan->vcount[0]);
+                                        B->prm.max_iters_coarse, B->prm.coarse_eps, s, B->S.plist, &B->S.plan->vcount[0], B->grid_cap);
         if (st) return st;
         for (int i = 1; i <= top; ++i)
         {
@@ -581,6 +587,7 @@ namespace hb2
             bp.xstride = C.vs;
             bp.list = B->S.plist;
             bp.count = &B->S.plan->vcount[i];
+            bp.cap = B->grid_cap;
             st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, 0, s, 0, &bp);
             if (! st) st = b_smooth(B, L, B->prm.n_post_smooth, s);
             if (st) return st;
@@ -616,8 +623,12 @@ namespace hb2
         return HB2_OK;
     }
 
-    static int build_step_graph(hb2_batch_s * B)
+    // The step graph with the work-list launches capped at `cap` blocks (0: the
+    // default, 32 per SM).  A light copy with 2 blocks per SM serves steps with
+    // few live vectors, where the full cap would mostly launch empty blocks.
+    static int build_step_graph(hb2_batch_s * B, uint64_t cap, cudaGraph_t * graph_out, cudaGraphExec_t * exec_out)
     {
+        B->grid_cap = cap;
         const uint64_t before = hb2_launch_count();
         HB2_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
         int st = record_step(B, B->cap);
@@ -630,10 +641,11 @@ namespace hb2
         const int st2 = end_capture(B->cap, &g);
         B->step_kernels = hb2_launch_count() - before;
         set_launch_count(before);
+        B->grid_cap = 0;
         if (st) { if (g) cudaGraphDestroy(g); return st; }
         if (st2) return st2;
-        B->step_graph = g;
-        HB2_CUDA(cudaGraphInstantiate(&B->step_exec, g, 0));
+        *graph_out = g;
+        HB2_CUDA(cudaGraphInstantiate(exec_out, g, 0));
         return HB2_OK;
     }
 
@@ -903,7 +915,14 @@ namespace hb2
         HB2_CUDA(cudaStreamSynchronize(stream));
         HB2_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
         HB2_CUDA(cudaStreamCreateWithFlags(&B->cap2, cudaStreamNonBlocking));
-        st = build_step_graph(B);
+        st = build_step_graph(B, 0, &B->step_graph, &B->step_exec);
+        if (! st) st = build_step_graph(B, (uint64_t)num_sms() * 2, &B->light_graph, &B->light_exec);
+        // the light graph (2 blocks per SM) serves up to about two row blocks of
+        // work per block: ~150k live rows (a few systems of level 8 and below)
+        B->light_rows = (uint64_t)num_sms() * 2 * kEllThreads * 2;
+        B->vec_rows.assign(B->nvec, 0);
+        for (uint32_t s = 0; s < B->nsys; ++s)
+            for (uint32_t k = 0; k < B->sys_nrhs[s]; ++k) B->vec_rows[B->sys_first[s] + k] = q1_rows(B->sys_level[s]);
         if (! st) st = build_solve_graph(B);
         return st;
     }
@@ -955,6 +974,8 @@ extern "C" int hb2_batch_destroy(hb2_batch B)
     if (! B) return HB2_OK;
     if (B->step_exec) cudaGraphExecDestroy(B->step_exec);
     if (B->step_graph) cudaGraphDestroy(B->step_graph);
+    if (B->light_exec) cudaGraphExecDestroy(B->light_exec);
+    if (B->light_graph) cudaGraphDestroy(B->light_graph);
     if (B->solve_exec) cudaGraphExecDestroy(B->solve_exec);
     if (B->solve_graph) cudaGraphDestroy(B->solve_graph);
     if (B->cap) cudaStreamDestroy(B->cap);
@@ -1001,17 +1022,25 @@ extern "C" int hb2_batch_start(hb2_batch B, uint32_t system, double eps_relative
     if (zero_guess)
         HB2_CUDA(cudaMemsetAsync(g->x + (uint64_t)(B->sys_first[system] - g->first) * g->vs, 0,
                                  (size_t)B->sys_nrhs[system] * g->vs * sizeof(double), stream));
+    B->started_rows += (uint64_t)B->sys_nrhs[system] * q1_rows(B->sys_level[system]);
     return start_range(B, B->sys_first[system], B->sys_nrhs[system], eps_relative, stream);
 }
 
 extern "C" int hb2_batch_step(hb2_batch B, uint32_t steps, uint8_t * done, cudaStream_t stream)
 {
     if (! B) return fail(HB2_ERR_ARG, "hb2_batch_step: null handle");
+    // little work in flight (rows of the live vectors as of the last step, plus
+    // those started since): the light graph
+    uint64_t rows = B->started_rows;
+    for (uint32_t j = 0; j < B->nvec; ++j)
+        if (B->h_state[j] == kNew || B->h_state[j] == kRun) rows += B->vec_rows[j];
+    cudaGraphExec_t exec = rows <= B->light_rows ? B->light_exec : B->step_exec;
     for (uint32_t i = 0; i < steps; ++i)
     {
-        HB2_CUDA(cudaGraphLaunch(B->step_exec, stream));
+        HB2_CUDA(cudaGraphLaunch(exec, stream));
         count_launches(B->step_kernels);
     }
+    B->started_rows = 0;
     int st = mirror(B, stream);
     if (st) return st;
     HB2_CUDA(cudaStreamSynchronize(stream));

@@ -236,7 +236,7 @@ namespace hb2
     static bool launch_warp_reg(const hb2_ell_s * A, const void * b, void * x, uint64_t max_iters, double eps, int exact,
                                 uint64_t * used_dev, double * defect_dev, cudaStream_t stream, uint32_t nvec = 1,
                                 uint64_t vstride = 0, const uint8_t * active = nullptr,
-                                const uint32_t * list = nullptr, const uint32_t * count = nullptr)
+                                const uint32_t * list = nullptr, const uint32_t * count = nullptr, uint64_t cap = 0)
     {
         if (A->K != 9 || A->rows > 128) return false;
         const int rpl = (int)((A->rows + 31) / 32);
@@ -244,7 +244,7 @@ namespace hb2
         EllView<T> v = A->view<T>();
         const S * bp = (const S *)b;
         S * xp = (S *)x;
-        const unsigned grid = list ? (unsigned)std::min<uint64_t>(nvec, list_grid_cap()) : nvec;
+        const unsigned grid = list ? (unsigned)std::min<uint64_t>(nvec, cap ? cap : list_grid_cap()) : nvec;
         switch (rpl)
         {
             case 1: launch_pdl(cg_warp_reg_kernel<T, S, 1>, dim3(grid), dim3(32), smem, stream, v, bp, xp, max_iters, eps, exact, used_dev, defect_dev, vstride, active, list, count); break;
@@ -259,16 +259,16 @@ namespace hb2
     // arithmetic on FP32 vectors (A64 FP64) or in the operator's own type
     int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
                                uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
-                               cudaStream_t stream, const uint32_t * list, const uint32_t * count)
+                               cudaStream_t stream, const uint32_t * list, const uint32_t * count, uint64_t cap)
     {
         if (nvec == 0) return HB2_OK;
         bool ok;
         if (A->dtype == HB2_F64 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
+            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else if (A->dtype == HB2_F64 && vec_dtype == HB2_F64)
-            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
+            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else if (A->dtype == HB2_F32 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count);
+            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else return fail(HB2_ERR_ARG, "batched coarse CG: unsupported element types");
         if (! ok) return fail(HB2_ERR_UNSUPPORTED, "batched coarse CG: the coarsest level needs <= 128 rows and 9 slots");
         count_launches(1);

@@ -232,7 +232,7 @@ namespace hb2
             // persistent grid over the work list: at most 8 blocks per SM
             if (red || ! b.count) return fail(HB2_ERR_ARG, "ELL work list: no fused reduction, count required");
             b.gx = gx;
-            grid = dim3((unsigned)std::min<uint64_t>((uint64_t)gx * b.nvec, list_grid_cap()), 1);
+            grid = dim3((unsigned)std::min<uint64_t>((uint64_t)gx * b.nvec, b.cap ? b.cap : list_grid_cap()), 1);
         }
         ReduceSlot rs;
         rs.partials = 0;

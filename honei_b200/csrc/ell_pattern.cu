@@ -45,18 +45,6 @@ namespace hb2
         uint32_t K, npat;
     };
 
-    // Small pattern tables (npat * K <= kPatParam entries, the Q1 operator's is
-    // 18) travel in the kernel's parameter space: warp-uniform lookups are then
-    // served by the constant cache instead of the L1 / shared-memory pipe the
-    // gathers already saturate.
-    constexpr int kPatParam = 64;
-    template <typename T>
-    struct PatParam
-    {
-        PatEnt<T> e[kPatParam];
-        int use;
-    };
-
     __device__ __forceinline__ unsigned long long row_signature(const uint8_t * code, const int16_t * delta, uint64_t ld,
                                                                 uint32_t K, uint64_t r)
     {
@@ -154,13 +142,12 @@ namespace hb2
     __global__ void __launch_bounds__(kEllThreads)
     ell_pattern_kernel(EllPatternView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
                        const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
-                       int flags, Batch bt, const __grid_constant__ PatParam<T> pp)
+                       int flags, Batch bt)
     {
         typedef Arith<T> M;
         __shared__ PatEnt<T> tab[kPatMax * kPatMaxK];
         const int K = KT > 0 ? KT : (int)A.K;
-        if (! pp.use)
-            for (uint32_t i = threadIdx.x; i < A.npat * (uint32_t)K; i += blockDim.x) tab[i] = A.tab[i];
+        for (uint32_t i = threadIdx.x; i < A.npat * (uint32_t)K; i += blockDim.x) tab[i] = A.tab[i];
         __syncthreads();
         pdl_entry();   // the pattern table is constant: loaded before the wait
         const bool listed = bt.list != nullptr;
@@ -201,7 +188,7 @@ namespace hb2
                 for (int i = 0; i < R; ++i)
                 {
                     const uint64_t r = r0 + 32 * i;
-                    const PatEnt<T> e = pp.use ? pp.e[p[i] * (uint32_t)K + k] : tab[p[i] * (uint32_t)K + k];
+                    const PatEnt<T> e = tab[p[i] * (uint32_t)K + k];
                     if (r < A.rows && e.off != kPatEmpty)
                         acc[i] = M::add(acc[i], M::mul(e.val, __ldg(x + (uint32_t)((int32_t)r + e.off))));
                 }
@@ -237,13 +224,6 @@ namespace hb2
         }
     }
 
-    // HB2_PAT_PARAM=0 keeps the table in shared memory
-    static bool param_table_enabled()
-    {
-        static const bool on = ! (getenv("HB2_PAT_PARAM") && strcmp(getenv("HB2_PAT_PARAM"), "0") == 0);
-        return on;
-    }
-
     template <typename T, int MODE>
     static void pattern_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
                              void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
@@ -255,12 +235,9 @@ namespace hb2
         v.rows = A->rows;
         v.K = A->K;
         v.npat = A->npat;
-        PatParam<T> pp;
-        pp.use = A->ptab_host && A->npat * A->K <= (uint32_t)kPatParam && param_table_enabled();
-        if (pp.use) memcpy(pp.e, A->ptab_host, A->npat * A->K * sizeof(PatEnt<T>));
 #define HB2_PAT_LAUNCH(KT_, R_)                                                                              \
         launch_pdl(ell_pattern_kernel<T, KT_, MODE, R_>, grid, dim3(kEllThreads), 0, s, v, (const T *)x, (T *)y, \
-                   (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags, b, pp)
+                   (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags, b)
         if (A->K == 9) { if (R == 1) HB2_PAT_LAUNCH(9, 1); else if (R == 2) HB2_PAT_LAUNCH(9, 2); else HB2_PAT_LAUNCH(9, 4); }
         else { if (R == 1) HB2_PAT_LAUNCH(0, 1); else if (R == 2) HB2_PAT_LAUNCH(0, 2); else HB2_PAT_LAUNCH(0, 4); }
 #undef HB2_PAT_LAUNCH
@@ -366,11 +343,6 @@ namespace hb2
                     }
                 if (e == cudaSuccess) e = cudaMalloc(&A->ptab, tab.size() * sizeof(PatEnt<T>));
                 if (e == cudaSuccess) e = cudaMemcpy(A->ptab, tab.data(), tab.size() * sizeof(PatEnt<T>), cudaMemcpyHostToDevice);
-                if (e == cudaSuccess)
-                {
-                    A->ptab_host = malloc(tab.size() * sizeof(PatEnt<T>));
-                    if (A->ptab_host) memcpy(A->ptab_host, tab.data(), tab.size() * sizeof(PatEnt<T>));
-                }
                 ok = e == cudaSuccess;
                 A->npat = np;
             }
@@ -396,8 +368,6 @@ namespace hb2
     {
         cudaFree(A->pat);
         cudaFree(A->ptab);
-        free(A->ptab_host);
-        A->ptab_host = 0;
         A->pat = 0;
         A->ptab = 0;
         A->npat = 0;

@@ -84,7 +84,6 @@ struct hb2_ell_s
     // pattern id per row, npat * K (value, column offset) table entries
     uint8_t * pat = nullptr;
     void * ptab = nullptr;
-    void * ptab_host = nullptr;   // host copy of the table (launch parameters)
     uint32_t npat = 0;
     uint64_t pattern_bytes = 0;
     // layout each kernel class runs on (index 0: no fused reduction, 1: fused
@@ -153,6 +152,7 @@ namespace hb2
         const uint32_t * list = nullptr;
         const uint32_t * count = nullptr;
         uint32_t gx = 0;               // row blocks per vector (set by launch_ell)
+        uint64_t cap = 0;              // blocks of a work-list launch (0: list_grid_cap())
     };
 
     // Launch one ELL kernel on `stream`.  aux: rhs / b; aux2: Jacobi P; zero:
@@ -236,5 +236,6 @@ namespace hb2
                               int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream);
     int launch_cg_warp_batched(const hb2_ell_s * A, int vec_dtype, const void * b, void * x, uint32_t nvec,
                                uint64_t vstride, const uint8_t * active, uint64_t max_iters, double eps,
-                               cudaStream_t stream, const uint32_t * list = nullptr, const uint32_t * count = nullptr);
+                               cudaStream_t stream, const uint32_t * list = nullptr, const uint32_t * count = nullptr,
+                               uint64_t cap = 0);
 }

@@ -107,7 +107,12 @@ def default_slots(budget_bytes, levels=LEVELS, base=32, coarse_level=3):
 
 
 class PoissonServer:
-    def __init__(self, slots=None, budget_bytes=120e9, coarse_level=3, params=None, stream=None):
+    """keep_results: hand each finished request a host copy of its solution (req.x);
+    otherwise the solution is copied to the slot's pinned host buffer and left there
+    until the slot's next request (a long run at a high rate would fill host memory)."""
+
+    def __init__(self, slots=None, budget_bytes=120e9, coarse_level=3, params=None, stream=None, keep_results=False):
+        self.keep_results = keep_results
         self.slots = slots or default_slots(budget_bytes, coarse_level=coarse_level)
         self.levels = sorted(self.slots)
         estimate = sum(slot_bytes(L, coarse_level) * k for L, k in self.slots.items())
@@ -162,7 +167,7 @@ class PoissonServer:
             torch.cuda.current_stream().synchronize()
             now = clock()
             for slot, req in finished:
-                req.x = self.out[slot].clone()
+                req.x = self.out[slot].clone() if self.keep_results else None
                 req.done = now
                 self.free[req.level].append(slot)
         return [req for _, req in finished]
@@ -172,7 +177,8 @@ class FP64SequentialServer:
     """Resident FP64 MG hierarchies per level (levels 3..L, V(4,4), coarse CG cap 100);
     requests solved one at a time in arrival order."""
 
-    def __init__(self, levels=LEVELS, coarse_level=3):
+    def __init__(self, levels=LEVELS, coarse_level=3, keep_results=False):
+        self.keep_results = keep_results
         self.data = {}
         self.vec = {}
         for L in levels:
@@ -203,7 +209,7 @@ class FP64SequentialServer:
         torch.cuda.current_stream().synchronize()
         req.iters = data.used_iters
         req.rel_defect = data.rnorm_final / data.rnorm_initial
-        req.x = out.reshape(1, -1).clone()
+        req.x = out.reshape(1, -1).clone() if self.keep_results else None
         req.done = clock()
         return [req]
 

@@ -40,12 +40,12 @@ def serve(server, batches):
 def test_results_are_the_same_alone_and_in_the_mix(oracle):
     mix = [[make(0, 7, 1e-10), make(1, 5, 1e-8)], [make(2, 6, 1e-8)], [], [make(3, 5, 1e-10), make(4, 7, 1e-8)],
            [make(5, 6, 1e-10), make(6, 5, 1e-8), make(7, 5, 1e-8)]]   # 3 level-5 slots: one waits in the queue
-    server = serving.PoissonServer(slots=SLOTS, budget_bytes=4e9)
+    server = serving.PoissonServer(slots=SLOTS, budget_bytes=4e9, keep_results=True)
     got = serve(server, mix)
     assert sorted(got) == list(range(8))
     for reqs in mix:
         for r in reqs:
-            alone = serve(serving.PoissonServer(slots=SLOTS, budget_bytes=4e9), [[make(r.rid, r.level, r.tol)]])
+            alone = serve(serving.PoissonServer(slots=SLOTS, budget_bytes=4e9, keep_results=True), [[make(r.rid, r.level, r.tol)]])
             a, m = alone[r.rid], got[r.rid]
             assert np.array_equal(a.x.numpy().view(np.uint64), m.x.numpy().view(np.uint64)), r.rid
             assert a.iters == m.iters
@@ -57,14 +57,14 @@ def test_results_are_the_same_alone_and_in_the_mix(oracle):
 
 
 def test_admission_respects_the_device_memory_budget():
-    server = serving.PoissonServer(slots=SLOTS, budget_bytes=4e9)
+    server = serving.PoissonServer(slots=SLOTS, budget_bytes=4e9, keep_results=True)
     assert server.device_bytes <= 4e9
     with pytest.raises(MemoryError):
         serving.PoissonServer(slots={7: 64}, budget_bytes=50e6)
 
 
 def test_queue_waits_for_a_free_slot():
-    server = serving.PoissonServer(slots={5: 1}, budget_bytes=1e9)
+    server = serving.PoissonServer(slots={5: 1}, budget_bytes=1e9, keep_results=True)
     reqs = [make(i, 5, 1e-8) for i in range(3)]
     got = serve(server, [reqs])
     # one slot: requests finish strictly one after another, in arrival order
