@@ -629,6 +629,8 @@ extern "C" int hb2_ell_destroy(hb2_ell A)
     cudaFree(A->col);
     ell_free_compact(A);
     ell_free_pattern(A);
+    cudaFree(A->spat);
+    cudaFree(A->sptab);
     delete A;
     return HB2_OK;
 }

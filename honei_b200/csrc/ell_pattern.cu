@@ -27,14 +27,6 @@ namespace hb2
 {
     constexpr uint32_t kPatSlots = 1024;                  // hash set
     constexpr unsigned long long kPatEmptyKey = ~0ull;
-    constexpr int32_t kPatEmpty = INT_MIN;
-
-    template <typename T>
-    struct PatEnt
-    {
-        T val;
-        int32_t off;      // column - row, kPatEmpty past the row's length
-    };
 
     template <typename T>
     struct EllPatternView
@@ -362,6 +354,61 @@ namespace hb2
     {
         if (! A->code || A->rows != A->cols || A->rows == 0 || A->K > (uint32_t)kPatMaxK) return HB2_OK;
         return A->dtype == HB2_F64 ? build_pattern_typed<double>(A, stream) : build_pattern_typed<float>(A, stream);
+    }
+
+    // Host-side row patterns of a small square matrix (K <= 9 slots, at most
+    // kSubPatMax distinct rows): the fused small-level kernels keep the table in
+    // shared memory and each row's pattern id in shared memory, so a row's
+    // product needs one memory round trip (the gathers), not two.
+    template <typename T>
+    static int small_patterns_typed(hb2_ell_s * A)
+    {
+        const uint64_t n = A->rows, ld = A->ld;
+        const uint32_t K = A->K;
+        std::vector<T> val((size_t)K * ld);
+        std::vector<int32_t> col((size_t)K * ld);
+        HB2_CUDA(cudaMemcpy(val.data(), A->val, val.size() * sizeof(T), cudaMemcpyDeviceToHost));
+        HB2_CUDA(cudaMemcpy(col.data(), A->col, col.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        std::vector<PatEnt<T>> tab;
+        std::vector<uint8_t> pat(n);
+        std::vector<PatEnt<T>> row(K);
+        for (uint64_t r = 0; r < n; ++r)
+        {
+            for (uint32_t k = 0; k < K; ++k)
+            {
+                const int32_t c = col[(size_t)k * ld + r];
+                row[k].val = c >= 0 ? val[(size_t)k * ld + r] : T(0);
+                row[k].off = c >= 0 ? (int32_t)(c - (int64_t)r) : kPatEmpty;
+            }
+            uint32_t q = 0;
+            const uint32_t np = (uint32_t)(tab.size() / K);
+            for (; q < np; ++q)
+            {
+                bool same = true;
+                for (uint32_t k = 0; k < K && same; ++k)
+                    same = tab[(size_t)q * K + k].off == row[k].off &&
+                           memcmp(&tab[(size_t)q * K + k].val, &row[k].val, sizeof(T)) == 0;
+                if (same) break;
+            }
+            if (q == np)
+            {
+                if (np == (uint32_t)kSubPatMax) return HB2_OK;   // too many distinct rows: none
+                tab.insert(tab.end(), row.begin(), row.end());
+            }
+            pat[r] = (uint8_t)q;
+        }
+        HB2_CUDA(cudaMalloc(&A->spat, std::max<uint64_t>(n, 16)));
+        HB2_CUDA(cudaMemcpy(A->spat, pat.data(), n, cudaMemcpyHostToDevice));
+        HB2_CUDA(cudaMalloc(&A->sptab, tab.size() * sizeof(PatEnt<T>)));
+        HB2_CUDA(cudaMemcpy(A->sptab, tab.data(), tab.size() * sizeof(PatEnt<T>), cudaMemcpyHostToDevice));
+        A->snpat = (uint32_t)(tab.size() / K);
+        return HB2_OK;
+    }
+
+    int ell_small_patterns(hb2_ell_s * A)
+    {
+        if (A->spat || A->rows != A->cols || A->rows == 0 || A->K != 9 || A->rows > (1u << 20)) return HB2_OK;
+        return A->dtype == HB2_F64 ? small_patterns_typed<double>(A) : small_patterns_typed<float>(A);
     }
 
     void ell_free_pattern(hb2_ell_s * A)

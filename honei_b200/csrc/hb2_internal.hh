@@ -86,6 +86,11 @@ struct hb2_ell_s
     void * ptab = nullptr;
     uint32_t npat = 0;
     uint64_t pattern_bytes = 0;
+    // row patterns of a small square matrix for the fused small-level kernels
+    // (subcycle.cu), built on the host when the matrix joins a hierarchy
+    uint8_t * spat = nullptr;
+    void * sptab = nullptr;     // snpat * K hb2::PatEnt<T>
+    uint32_t snpat = 0;
     // layout each kernel class runs on (index 0: no fused reduction, 1: fused
     // reduction): hb2::kLayoutPlain / kLayoutCompact / kLayoutPattern, and
     // its rows per thread
@@ -164,6 +169,17 @@ namespace hb2
                    int flags = 0, const Batch * batch = nullptr);
 
     uint64_t list_grid_cap();
+
+    // one slot of a row pattern: value and column - row (kPatEmpty past the row)
+    template <typename T>
+    struct PatEnt
+    {
+        T val;
+        int32_t off;
+    };
+    constexpr int32_t kPatEmpty = (-2147483647 - 1);
+    constexpr int kSubPatMax = 8;    // patterns of a small-level operator in the fused kernels
+    int ell_small_patterns(hb2_ell_s * A);
 
     enum LayoutKind
     {

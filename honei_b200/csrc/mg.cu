@@ -345,7 +345,11 @@ namespace hb2
         if (mg->sub_top >= 1)
         {
             for (int i = 1; i <= mg->sub_top; ++i)
+            {
                 if (mg->lev[i].n <= local_rows) mg->sub_t1 = i;
+                st = ell_small_patterns(mg->lev[i].A);
+                if (st) return st;
+            }
             st = subcycle_prepare();
             if (st) return st;
         }

@@ -42,9 +42,15 @@ namespace hb2
         T * tmp;
         const T * jac;
         uint32_t n;
+        // row patterns of A (host-built, ell_small_patterns): a row's product
+        // then reads its nine (value, offset) pairs from shared memory
+        const uint8_t * pat;
+        const PatEnt<T> * ptab;
+        uint32_t npat;
     };
 
     constexpr int kSubMaxLevels = 10;
+    constexpr int kSubRowsPerThread = 3;   // kSubMaxRows / (8 CTAs x 1024 threads), rounded up
 
     template <typename T>
     struct SubCycle
@@ -96,6 +102,48 @@ namespace hb2
         return s;
     }
 
+    // the same product from a row pattern: (value, offset) pairs from shared
+    // memory, every vector load issued before the first product
+    template <typename T, bool L2>
+    __device__ __forceinline__ T row_sum_pat(const PatEnt<T> * e, uint32_t r, const T * v)
+    {
+        typedef Arith<T> M;
+        T a[9], xv[9];
+        int32_t off[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            off[k] = e[k].off;
+            a[k] = e[k].val;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            xv[k] = off[k] != kPatEmpty ? (L2 ? __ldcg(v + (uint32_t)((int32_t)r + off[k])) : v[(uint32_t)((int32_t)r + off[k])]) : T(0);
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            if (off[k] != kPatEmpty) s = M::add(s, M::mul(a[k], xv[k]));
+        return s;
+    }
+
+    // Shared-memory copies of a level's pattern table and of the pattern ids
+    // of the rows this thread owns (row tid + j * nth in slot j); ids null:
+    // read the id from global memory.
+    template <typename T>
+    struct SubPat
+    {
+        const PatEnt<T> * tab;
+        const uint8_t * ids;
+    };
+
+    template <typename T, bool L2>
+    __device__ __forceinline__ T row_A(const SubLevel<T> & L, const SubPat<T> & sp, uint32_t r, uint32_t j, const T * v)
+    {
+        if (! sp.tab) return row_sum_any<T, L2>(L.A, r, v);
+        const uint32_t p = sp.ids ? sp.ids[j * 1024 + threadIdx.x] : __ldg(L.pat + r);
+        return row_sum_pat<T, L2>(sp.tab + p * 9, r, v);
+    }
+
     // The threads that share the work of one phase: the whole cluster (phases
     // end with the cluster barrier; vectors are read through L2 because other
     // CTAs wrote them) or one CTA (block barrier; plain loads, coherent within
@@ -124,15 +172,16 @@ namespace hb2
 
     // damped Jacobi sweeps with ping-pong (math/ri.hh:110-133), result back in x
     template <typename T, bool LOCAL, bool PL>
-    __device__ void sub_smooth(const SubLevel<T> & L, int sweeps, const Team<LOCAL, PL> & tm)
+    __device__ void sub_smooth(const SubLevel<T> & L, int sweeps, const Team<LOCAL, PL> & tm, const SubPat<T> & sp)
     {
         typedef Arith<T> M;
         T * cur = L.x, * nxt = L.tmp;
         for (int s = 0; s < sweeps; ++s)
         {
-            for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
+            uint32_t j = 0;
+            for (uint32_t r = tm.tid; r < L.n; r += tm.nth, ++j)
             {
-                const T acc = row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.A, r, cur);
+                const T acc = row_A<T, ! Team<LOCAL, PL>::plain>(L, sp, r, j, cur);
                 nxt[r] = M::add(tm.ld(cur + r), M::mul(__ldg(L.jac + r), M::sub(tm.ld(L.b + r), acc)));
             }
             tm.sync();
@@ -149,12 +198,14 @@ namespace hb2
 
     // pre-smoothing, defect, restriction + clear of the coarser correction
     template <typename T, bool LOCAL, bool PL>
-    __device__ void down_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_pre, const Team<LOCAL, PL> & tm)
+    __device__ void down_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_pre, const Team<LOCAL, PL> & tm,
+                               const SubPat<T> & sp)
     {
         typedef Arith<T> M;
-        sub_smooth(L, n_pre, tm);
-        for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
-            L.store[r] = M::sub(tm.ld(L.b + r), row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.A, r, L.x));
+        sub_smooth(L, n_pre, tm, sp);
+        uint32_t j = 0;
+        for (uint32_t r = tm.tid; r < L.n; r += tm.nth, ++j)
+            L.store[r] = M::sub(tm.ld(L.b + r), row_A<T, ! Team<LOCAL, PL>::plain>(L, sp, r, j, L.x));
         tm.sync();
         for (uint32_t r = tm.tid; r < C.n; r += tm.nth)
         {
@@ -166,47 +217,89 @@ namespace hb2
 
     // prolongation + add, post-smoothing
     template <typename T, bool LOCAL, bool PL>
-    __device__ void up_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_post, const Team<LOCAL, PL> & tm)
+    __device__ void up_level(const SubLevel<T> & L, const SubLevel<T> & C, int n_post, const Team<LOCAL, PL> & tm,
+                             const SubPat<T> & sp)
     {
         typedef Arith<T> M;
         for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
             L.x[r] = M::add(tm.ld(L.x + r), row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.P, r, C.x));
         tm.sync();
-        sub_smooth(L, n_post, tm);
+        sub_smooth(L, n_post, tm, sp);
+    }
+
+    // Shared memory of the split kernels: the pattern tables of every level and,
+    // for the levels that run over the whole cluster, the pattern ids of the
+    // rows each thread owns.  Loaded once per launch (the data are constant).
+    template <typename T>
+    struct SubShared
+    {
+        PatEnt<T> tab[kSubMaxLevels][kSubPatMax * 9];
+        uint8_t ids[kSubMaxLevels][kSubRowsPerThread * 1024];
+    };
+
+    template <typename T>
+    __device__ void sub_load_patterns(const SubCycle<T> & sc, SubShared<T> & sh, uint32_t tid, uint32_t nth)
+    {
+        for (int i = 1; i <= sc.top; ++i)
+        {
+            const SubLevel<T> & L = sc.lev[i];
+            if (! L.ptab) continue;
+            for (uint32_t e = threadIdx.x; e < L.npat * 9; e += blockDim.x) sh.tab[i][e] = L.ptab[e];
+            if (i > sc.t1)
+            {
+                uint32_t j = 0;
+                for (uint32_t r = tid; j < (uint32_t)kSubRowsPerThread; r += nth, ++j)
+                    sh.ids[i][j * 1024 + threadIdx.x] = r < L.n ? __ldg(L.pat + r) : (uint8_t)0;
+            }
+        }
+        __syncthreads();
+    }
+
+    template <typename T>
+    __device__ __forceinline__ SubPat<T> sub_pat(const SubCycle<T> & sc, const SubShared<T> & sh, int i, bool cluster_wide)
+    {
+        SubPat<T> p;
+        p.tab = sc.lev[i].ptab ? sh.tab[i] : nullptr;
+        p.ids = cluster_wide ? sh.ids[i] : nullptr;
+        return p;
     }
 
     // down: levels top..t1+1 over the cluster, then levels t1..1 in CTA 0 alone
     // (the smallest levels have too few rows to need more than one CTA, and a
     // block barrier is far cheaper than a cluster barrier)
     template <typename T, bool PL>
-    __global__ void __launch_bounds__(1024) mg_sub_down_kernel(const __grid_constant__ SubCycle<T> sc)
+    __global__ void __launch_bounds__(1024, 1) mg_sub_down_kernel(const __grid_constant__ SubCycle<T> sc)
     {
+        __shared__ SubShared<T> sh;
         pdl_entry();
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
-        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+        sub_load_patterns(sc, sh, all.tid, all.nth);
+        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all, sub_pat(sc, sh, i, true));
         if (sc.t1 < 1 || cluster.block_rank() != 0) return;
         const Team<true> blk = {threadIdx.x, blockDim.x};
-        for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk);
+        for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk, sub_pat(sc, sh, i, false));
     }
 
     // up: levels 1..t1 in CTA 0 alone, then t1+1..top over the cluster
     template <typename T, bool PL>
-    __global__ void __launch_bounds__(1024) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
+    __global__ void __launch_bounds__(1024, 1) mg_sub_up_kernel(const __grid_constant__ SubCycle<T> sc)
     {
+        __shared__ SubShared<T> sh;
         pdl_entry();
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
+        sub_load_patterns(sc, sh, all.tid, all.nth);
         if (sc.t1 >= 1)
         {
             if (cluster.block_rank() == 0)
             {
                 const Team<true> blk = {threadIdx.x, blockDim.x};
-                for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk);
+                for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk, sub_pat(sc, sh, i, false));
             }
             cluster.sync();
         }
-        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
+        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all, sub_pat(sc, sh, i, true));
     }
 
     // ------------------------------------------------------------------
@@ -254,11 +347,12 @@ namespace hb2
         __shared__ double cg_smem[3 * 96];
         cg::cluster_group cluster = cg::this_cluster();
         const Team<false, PL> all = {cluster.block_rank() * blockDim.x + threadIdx.x, cluster.num_blocks() * blockDim.x};
-        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all);
+        const SubPat<T> none = {nullptr, nullptr};
+        for (int i = sc.top; i > sc.t1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, all, none);
         if (cluster.block_rank() == 0)
         {
             const Team<true> blk = {threadIdx.x, blockDim.x};
-            for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk);
+            for (int i = sc.t1; i >= 1; --i) down_level(sc.lev[i], sc.lev[i - 1], sc.n_pre, blk, none);
             if (threadIdx.x < 32)
             {
                 if constexpr (std::is_same<T, float>::value)
@@ -269,10 +363,17 @@ namespace hb2
                 else coarse_dispatch<double, double>(sc.C, sc, cg_smem);
             }
             __syncthreads();
-            for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk);
+            for (int i = 1; i <= sc.t1; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, blk, none);
         }
         cluster.sync();
-        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all);
+        for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all, none);
+    }
+
+    // HB2_SUB_PATTERNS=0: the fused small levels read the plain ELL arrays
+    static bool sub_patterns_enabled()
+    {
+        static const bool on = ! (getenv("HB2_SUB_PATTERNS") && strcmp(getenv("HB2_SUB_PATTERNS"), "0") == 0);
+        return on;
     }
 
     template <typename T>
@@ -288,6 +389,10 @@ namespace hb2
         s.tmp = (T *)d.tmp;
         s.jac = (const T *)d.jac;
         s.n = (uint32_t)d.A->rows;
+        const bool pat = d.A->sptab && d.A->snpat > 0 && d.A->snpat <= (uint32_t)kSubPatMax && sub_patterns_enabled();
+        s.pat = pat ? d.A->spat : nullptr;
+        s.ptab = pat ? (const PatEnt<T> *)d.A->sptab : nullptr;
+        s.npat = pat ? d.A->snpat : 0;
         return s;
     }
 
