@@ -78,6 +78,7 @@ struct hb2_mg_s
     int sub_t1;              // of those, levels 1..sub_t1 run in one CTA
     bool sub_fused;          // levels 0..sub_top, coarse CG included, in one launch
     hb2_ell_s * coarse64;    // FP64 copy of the coarsest operator (F32 hierarchies with coarse_fp64)
+    double * ir_r;           // outer FP64 defect of hb2_ir_solve (allocated on first use, kept)
 };
 
 namespace hb2
@@ -540,6 +541,7 @@ extern "C" int hb2_mg_destroy(hb2_mg mg)
     if (mg->cap) cudaStreamDestroy(mg->cap);
     if (mg->cap2) cudaStreamDestroy(mg->cap2);
     if (mg->coarse64) hb2_ell_destroy(mg->coarse64);
+    if (mg->ir_r) cudaFree(mg->ir_r);
     if (mg->vec_block) cudaFree(mg->vec_block);
     workspace_destroy(mg->ws);
     if (mg->owns_matrices)
@@ -588,8 +590,8 @@ extern "C" int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void * b, void * x, d
     Workspace * ws = 0;
     int st = stream_workspace(stream, &ws);
     if (st) return st;
-    void * r = 0;
-    HB2_CUDA(cudaMallocAsync(&r, A->rows * 8 + 16, stream));
+    if (! inner->ir_r) HB2_CUDA(cudaMalloc(&inner->ir_r, A->rows * 8 + 16));
+    void * r = inner->ir_r;
     double r0 = 1e16, rc = 1e16;
     uint64_t used = 0, inner_total = 0;
     for (uint64_t i = 0; i < max_iters && ! st; ++i)
@@ -617,7 +619,6 @@ extern "C" int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void * b, void * x, d
         inner_total += (uint64_t)ist[0];
         if (! st) st = launch_add_converted(x, inner->dtype, F.x, F.n, stream);
     }
-    cudaFreeAsync(r, stream);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (! st && e != cudaSuccess) st = cuda_status(e, "hb2_ir_solve");
     if (stats)
