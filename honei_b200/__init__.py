@@ -5,6 +5,7 @@ include/honei_b200.h (libhonei_b200.so).  There is no CPU fallback: the first
 operator call without the built library raises ImportError.
 """
 from ._lib import DeviceTimeout, HoneiError, NotFinite, VectorSizeDoesNotMatch, launch_count
+from .io import MatrixIO, VectorIO, io_formats
 from .la import (BandedMatrixQx, Defect, DenseVector, Difference, DotProduct, ElementProduct, Norm, Product, Scale,
                  ScaledSum, SparseMatrixELL, Sum, convert, copy, fill, tags)
 from .solvers import (BatchedPoissonSolver, CGSolver, IRSolver, MGData, MGSolver, Prolongation, Restriction,
@@ -12,7 +13,7 @@ from .solvers import (BatchedPoissonSolver, CGSolver, IRSolver, MGData, MGSolver
 
 __all__ = [
     "BandedMatrixQx", "BatchedPoissonSolver", "CGSolver", "Defect", "DenseVector", "DeviceTimeout", "Difference", "DotProduct",
-    "ElementProduct", "HoneiError", "IRSolver", "MGData", "MGSolver", "Norm", "NotFinite", "Product",
+    "ElementProduct", "HoneiError", "MatrixIO", "VectorIO", "io_formats", "IRSolver", "MGData", "MGSolver", "Norm", "NotFinite", "Product",
     "Prolongation", "RISmoother", "Restriction", "Scale", "ScaledSum", "SparseMatrixELL", "Sum",
     "VectorSizeDoesNotMatch", "batch_params", "convert", "copy", "fill", "launch_count", "methods", "mg_params", "tags",
 ]

@@ -55,7 +55,7 @@ class MgParams(ctypes.Structure):
     """hb2_mg_params"""
     _fields_ = [("n_pre_smooth", _u64), ("n_post_smooth", _u64), ("max_iters", _u64),
                 ("max_iters_coarse", _u64), ("eps_relative", _dbl), ("coarse_eps", _dbl), ("omega", _dbl),
-                ("coarse_exact", _int), ("no_fused_levels", _int), ("coarse_fp64", _int)]
+                ("coarse_exact", _int), ("no_fused_levels", _int), ("coarse_fp64", _int), ("cycle", _int)]
 
 
 class BatchParams(ctypes.Structure):
@@ -77,6 +77,9 @@ SIGNATURES = {
     "hb2_ell_info": (_int, [_vp, _pu64, _pu64, _pu64, _pu64, _pu64, _pu64]),
     "hb2_ell_export": (_int, [_vp, _vp, _vp, _vp]),
     "hb2_ell_layout": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
+    "hb2_ell_read": (_int, [_pvp, ctypes.c_char_p, _int, _vp]),
+    "hb2_ell_write": (_int, [_vp, ctypes.c_char_p]),
+    "hb2_ell_transpose": (_int, [_pvp, _vp, _vp]),
     "hb2_q1_create": (_int, [_pvp, _int, _u64, _vp, _int, _vp]),
     "hb2_q1_create_poisson": (_int, [_pvp, _int, ctypes.c_uint, _dbl, _vp]),
     "hb2_q1_destroy": (_int, [_vp]),

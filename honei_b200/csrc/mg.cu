@@ -153,6 +153,9 @@ namespace hb2
         if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
         if (! st) st = launch_ell(L.R, kRestrict, L.store, C.b, 0, 0, C.x, 0, 0, mg->ws, s, L.pass(L.rev_R));
         if (! st) st = record_cycle(mg, i - 1, s);
+        // W-cycle (math/mg.hh:720-722): the coarser level's cycle twice, except
+        // directly above the coarsest level
+        if (! st && mg->prm.cycle == 1 && i - 1 != 0) st = record_cycle(mg, i - 1, s);
         if (! st) st = launch_ell(L.P, kAdd, C.x, L.x, 0, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_P));
         if (! st) st = smooth(mg, L, mg->prm.n_post_smooth, s);
         return st;
@@ -340,7 +343,8 @@ namespace hb2
         mg->sub_t1 = 0;
         const uint64_t max_rows = env_u64("HB2_SUB_MAX_ROWS", kSubMaxRows);
         const uint64_t local_rows = env_u64("HB2_SUB_LOCAL_ROWS", kSubLocalRows);
-        if (! mg->prm.no_fused_levels && mg->prm.n_pre_smooth < (1u << 20) && mg->prm.n_post_smooth < (1u << 20))
+        if (! mg->prm.no_fused_levels && mg->prm.cycle == 0 && mg->prm.n_pre_smooth < (1u << 20) &&
+            mg->prm.n_post_smooth < (1u << 20))
             for (uint32_t i = 1; i < mg->nlev && i < 10; ++i)
                 if (mg->lev[i].n <= max_rows) mg->sub_top = (int)i;
         if (mg->sub_top >= 1)
@@ -390,6 +394,7 @@ namespace hb2
         p.coarse_exact = 1;
         p.no_fused_levels = 0;
         p.coarse_fp64 = 0;
+        p.cycle = 0;
         return p;
     }
 
@@ -488,6 +493,7 @@ extern "C" int hb2_mg_create(hb2_mg * out, uint32_t num_levels, const hb2_ell * 
     if (! out) return fail(HB2_ERR_ARG, "hb2_mg_create: null output");
     int st = validate(num_levels, A, prol, res);
     if (st) return st;
+    if (params && (params->cycle < 0 || params->cycle > 1)) return fail(HB2_ERR_ARG, "hb2_mg_create: cycle must be 0 (V) or 1 (W)");
     hb2_mg_s * mg = new hb2_mg_s();
     mg->dtype = A[0]->dtype;
     cudaGetDevice(&mg->device);

@@ -134,6 +134,20 @@ class SparseMatrixELL:
         P._dtype = R._dtype = dtype_code(dtype)
         return P, R
 
+    @classmethod
+    def _from_handle(cls, h, dtype):
+        m = cls(h.value)
+        m._dtype = dtype_code(dtype)
+        return m
+
+    def transposed(self, stream=None) -> "SparseMatrixELL":
+        """Transposition<tags::B200>::value(A) (math/transposition.hh:36-50)."""
+        h = ctypes.c_void_p()
+        call("hb2_ell_transpose", ctypes.byref(h), self._h, _stream(stream))
+        m = SparseMatrixELL(h.value)
+        m._dtype = self._dtype
+        return m
+
     def converted(self, dtype, stream=None) -> "SparseMatrixELL":
         h = ctypes.c_void_p()
         call("hb2_ell_convert", ctypes.byref(h), self._h, dtype_code(dtype), _stream(stream))

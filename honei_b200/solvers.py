@@ -96,9 +96,12 @@ class CGSolver:
 
 
 def mg_params(n_pre=4, n_post=4, max_iters=100, max_iters_coarse=100, eps=1e-10, coarse_eps=None, omega=0.7,
-              coarse_exact=True, fused_levels=True, coarse_fp64=False) -> MgParams:
+              coarse_exact=True, fused_levels=True, coarse_fp64=False, cycle="V") -> MgParams:
+    """cycle: "V" (MGCycleCreation<V::STATIC>) or "W" (W::STATIC)"""
+    if cycle not in ("V", "W"):
+        raise ValueError("cycle must be 'V' or 'W'")
     return MgParams(n_pre, n_post, max_iters, max_iters_coarse, eps, eps if coarse_eps is None else coarse_eps,
-                    omega, int(coarse_exact), int(not fused_levels), int(coarse_fp64))
+                    omega, int(coarse_exact), int(not fused_levels), int(coarse_fp64), 1 if cycle == "W" else 0)
 
 
 class MGData:

@@ -111,6 +111,17 @@ HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_
 /* Download the matrix in the reference layout (host arrays of K*stride, K*stride
  * and rows elements); Arl as the reference computes it. */
 HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);
+/* MatrixIO<io_formats::ELL>::read_matrix / write_matrix (math/matrix_io.hh:433-560):
+ * the reference's binary ELL file (five uint64: size, rows, columns, stride,
+ * num_cols_per_row; then size uint64 column indices and size doubles), read
+ * into the device layout (values rounded to dtype) or written from an F64
+ * matrix with one thread per row. */
+HB2_API int hb2_ell_read(hb2_ell *out, const char *path, hb2_dtype dtype, cudaStream_t stream);
+HB2_API int hb2_ell_write(hb2_ell A, const char *path);
+/* Transposition<Tag>::value (math/transposition.hh:36-50): A^T assembled like the
+ * reference (each row's entries in ascending column order); MGUtil::load_data
+ * builds every restriction matrix this way from its prolongation. */
+HB2_API int hb2_ell_transpose(hb2_ell *out, hb2_ell A, cudaStream_t stream);
 
 /* BandedMatrixQx<Q1Type, DT> (la/banded_matrix_qx-impl.hh:45-466): 9 bands of n,
  * band-major LL LD LU DL DD DU UL UD UU; n must be (2^L+1)^2. */
@@ -236,6 +247,8 @@ typedef struct
                                                ~20k rows run as two thread-block-cluster kernels per cycle) */
     int coarse_fp64;                        /* F32 hierarchies: 1 runs the coarsest CG in FP64 on an FP64 copy
                                                of the coarse operator (<= 128 rows); 0: FP32 as the reference */
+    int cycle;                              /* 0: V-cycle (MGCycleCreation<V::STATIC>, math/mg.hh:567-656);
+                                               1: W-cycle (MGCycleCreation<W::STATIC>, math/mg.hh:658-740) */
 } hb2_mg_params;
 
 HB2_API int hb2_mg_create(hb2_mg *out, uint32_t num_levels, const hb2_ell *A, const hb2_ell *prol, const hb2_ell *res,

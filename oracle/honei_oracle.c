@@ -498,7 +498,23 @@ typedef struct {                                                                
     T_ *jac[32], *b[32], *x[32], *d[32], *c[32], *store[32], *t0[32], *t1[32];     \
     uint64_t n_pre, n_post, max_iters_coarse, coarse_used;                          \
     T_ coarse_eps;                                                                  \
+    int cycle;                      /* 0 V::STATIC, 1 W::STATIC */                  \
 } mg_##SFX;                                                                         \
+                                                                                    \
+/* per-level vectors and the "jac" preconditioner of level l (A[l] set) */         \
+static void mg_level_vectors_##SFX(mg_##SFX *h, unsigned l, double omega)           \
+{                                                                                   \
+    uint64_t n = h->A[l].rows;                                                      \
+    h->jac[l] = (T_ *)malloc(sizeof(T_) * n);                                       \
+    /* PreconFill "jac" (math/mg.hh:266-273): P[j] = omega, then /= A(j,j) */       \
+    for (uint64_t j = 0; j < n; ++j) {                                              \
+        T_ pj = (T_)omega; pj /= ell_diag_##SFX(&h->A[l], j); h->jac[l][j] = pj;    \
+    }                                                                               \
+    h->b[l] = (T_ *)calloc(n, sizeof(T_)); h->x[l] = (T_ *)calloc(n, sizeof(T_));   \
+    h->d[l] = (T_ *)calloc(n, sizeof(T_)); h->c[l] = (T_ *)calloc(n, sizeof(T_));   \
+    h->store[l] = (T_ *)calloc(n, sizeof(T_));                                      \
+    h->t0[l] = (T_ *)calloc(n, sizeof(T_)); h->t1[l] = (T_ *)calloc(n, sizeof(T_)); \
+}                                                                                   \
                                                                                     \
 static void mg_setup_##SFX(mg_##SFX *h, unsigned lmin, unsigned lmax, double aniso, \
                            double omega)                                            \
@@ -506,18 +522,9 @@ static void mg_setup_##SFX(mg_##SFX *h, unsigned lmin, unsigned lmax, double ani
     memset(h, 0, sizeof(*h));                                                       \
     h->min_level = lmin; h->max_level = lmax;                                       \
     for (unsigned l = lmin; l <= lmax; ++l) {                                       \
-        uint64_t n = hbo_q1_n(l);                                                   \
         q1_ell_##SFX(&h->A[l], l, aniso);                                           \
         if (l > lmin) transfer_ell_##SFX(&h->P[l], &h->R[l], l);                    \
-        h->jac[l] = (T_ *)malloc(sizeof(T_) * n);                                   \
-        /* PreconFill "jac" (math/mg.hh:266-273): P[j] = omega, then /= A(j,j) */   \
-        for (uint64_t j = 0; j < n; ++j) {                                          \
-            T_ pj = (T_)omega; pj /= ell_diag_##SFX(&h->A[l], j); h->jac[l][j] = pj;\
-        }                                                                           \
-        h->b[l] = (T_ *)calloc(n, sizeof(T_)); h->x[l] = (T_ *)calloc(n, sizeof(T_));\
-        h->d[l] = (T_ *)calloc(n, sizeof(T_)); h->c[l] = (T_ *)calloc(n, sizeof(T_));\
-        h->store[l] = (T_ *)calloc(n, sizeof(T_));                                  \
-        h->t0[l] = (T_ *)calloc(n, sizeof(T_)); h->t1[l] = (T_ *)calloc(n, sizeof(T_));\
+        mg_level_vectors_##SFX(h, l, omega);                                        \
     }                                                                               \
 }                                                                                   \
                                                                                     \
@@ -542,7 +549,7 @@ static void smooth_##SFX(mg_##SFX *h, unsigned l, T_ *b, T_ *x, uint64_t sweeps)
     }                                                                               \
 }                                                                                   \
                                                                                     \
-/* math/mg.hh:577-640, executed directly instead of through an OperatorList */     \
+/* math/mg.hh:577-640 (V), 673-742 (W), executed directly, not as an OperatorList */     \
 static void vcycle_##SFX(mg_##SFX *h, unsigned l, T_ *x, T_ *b)                     \
 {                                                                                   \
     if (l == h->min_level) {                                                        \
@@ -555,6 +562,10 @@ static void vcycle_##SFX(mg_##SFX *h, unsigned l, T_ *x, T_ *b)                 
     spmv_##SFX(&h->R[l], h->store[l], h->d[l - 1]);                                 \
     memset(h->c[l - 1], 0, sizeof(T_) * h->A[l - 1].rows);                          \
     vcycle_##SFX(h, l - 1, h->c[l - 1], h->d[l - 1]);                               \
+    /* W::STATIC (math/mg.hh:719-721): the coarser cycle twice, except directly   \
+       above the coarsest level */                                                  \
+    if (h->cycle == 1 && l - 1 != h->min_level)                                     \
+        vcycle_##SFX(h, l - 1, h->c[l - 1], h->d[l - 1]);                           \
     spmv_##SFX(&h->P[l], h->c[l - 1], h->store[l]);                                 \
     for (uint64_t i = 0; i < n; ++i) x[i] += h->store[l][i];                        \
     smooth_##SFX(h, l, b, x, h->n_post);                                            \
@@ -586,8 +597,21 @@ uint64_t hbo_mg_q1_##SFX(unsigned min_level, unsigned max_level, double aniso,  
                          uint64_t max_iters, uint64_t max_iters_coarse, double eps, \
                          double coarse_eps, const T_ *b, T_ *x, double *stats)      \
 {                                                                                   \
+    return hbo_mg_q1_cycle_##SFX(0, min_level, max_level, aniso, omega, n_pre,      \
+                                 n_post, max_iters, max_iters_coarse, eps,          \
+                                 coarse_eps, b, x, stats);                          \
+}                                                                                   \
+                                                                                    \
+uint64_t hbo_mg_q1_cycle_##SFX(int cycle, unsigned min_level, unsigned max_level,  \
+                               double aniso, double omega, uint64_t n_pre,         \
+                               uint64_t n_post, uint64_t max_iters,                \
+                               uint64_t max_iters_coarse, double eps,              \
+                               double coarse_eps, const T_ *b, T_ *x,              \
+                               double *stats)                                      \
+{                                                                                   \
     mg_##SFX h;                                                                     \
     mg_setup_##SFX(&h, min_level, max_level, aniso, omega);                         \
+    h.cycle = cycle;                                                                \
     h.n_pre = n_pre; h.n_post = n_post; h.max_iters_coarse = max_iters_coarse;      \
     h.coarse_eps = (T_)coarse_eps;                                                  \
     uint64_t n = hbo_q1_n(max_level);                                               \
@@ -601,6 +625,45 @@ uint64_t hbo_mg_q1_##SFX(unsigned min_level, unsigned max_level, double aniso,  
 
 DEFINE_SOLVERS(double, f64, DBL_EPSILON, MULADD)
 DEFINE_SOLVERS(float, f32, FLT_EPSILON, MULADD)
+
+static void ell_copy_f64(ell_f64 *e, const hbo_ell_view *v)
+{
+    const uint64_t size = v->K * v->stride;
+    e->rows = v->rows; e->cols = v->cols; e->stride = v->stride; e->K = v->K;
+    e->Aj = (uint64_t *)malloc(sizeof(uint64_t) * size);
+    e->Ax = (double *)malloc(sizeof(double) * size);
+    e->Arl = (uint64_t *)malloc(sizeof(uint64_t) * (v->rows ? v->rows : 1));
+    memcpy(e->Aj, v->Aj, sizeof(uint64_t) * size);
+    memcpy(e->Ax, v->Ax, sizeof(double) * size);
+    memcpy(e->Arl, v->Arl, sizeof(uint64_t) * v->rows);
+}
+
+/* MGUtil::load_data (math/mg.hh:442-545) on given matrices: level l = 1..nlev holds
+ * A[l-1]; prol[l-2] / res[l-2] connect level l and l-1; P = omega / diag(A). */
+uint64_t hbo_mg_ell_f64(int cycle, unsigned nlev, const hbo_ell_view *A, const hbo_ell_view *prol,
+                        const hbo_ell_view *res, double omega, uint64_t n_pre, uint64_t n_post,
+                        uint64_t max_iters, uint64_t max_iters_coarse, double eps, double coarse_eps,
+                        const double *b, double *x, double *stats)
+{
+    mg_f64 h;
+    if (nlev < 1 || nlev > 31) return 0;
+    memset(&h, 0, sizeof(h));
+    h.min_level = 1; h.max_level = nlev; h.cycle = cycle;
+    for (unsigned l = 1; l <= nlev; ++l) {
+        ell_copy_f64(&h.A[l], &A[l - 1]);
+        if (l > 1) { ell_copy_f64(&h.P[l], &prol[l - 2]); ell_copy_f64(&h.R[l], &res[l - 2]); }
+        mg_level_vectors_f64(&h, l, omega);
+    }
+    h.n_pre = n_pre; h.n_post = n_post; h.max_iters_coarse = max_iters_coarse;
+    h.coarse_eps = coarse_eps;
+    const uint64_t n = h.A[nlev].rows;
+    memcpy(h.b[nlev], b, sizeof(double) * n);
+    memcpy(h.x[nlev], x, sizeof(double) * n);
+    uint64_t used = mg_solve_f64(&h, max_iters, eps, stats);
+    memcpy(x, h.x[nlev], sizeof(double) * n);
+    mg_free_f64(&h);
+    return used;
+}
 
 uint64_t hbo_cg_q1_f64(unsigned L, double aniso, const double *b, double *x,
                        uint64_t max_iters, double eps)

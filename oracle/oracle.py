@@ -58,6 +58,14 @@ def lib():
             f.restype = _u64
             f.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                           _ptr, _ptr, _ptr]
+        for sfx in ("f64", "f32"):
+            f = getattr(L, "hbo_mg_q1_cycle_" + sfx)
+            f.restype = _u64
+            f.argtypes = [ctypes.c_int, ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl,
+                          _dbl, _ptr, _ptr, _ptr]
+        L.hbo_mg_ell_f64.restype = _u64
+        L.hbo_mg_ell_f64.argtypes = [ctypes.c_int, ctypes.c_uint, _ptr, _ptr, _ptr, _dbl, _u64, _u64, _u64, _u64,
+                                     _dbl, _dbl, _ptr, _ptr, _ptr]
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
@@ -234,15 +242,76 @@ def jacobi_q1(L: int, b: np.ndarray, x0, sweeps: int, omega=0.7, aniso=1.0):
 
 
 def mg_q1(max_level: int, b: np.ndarray, x0=None, min_level=3, omega=0.7, n_pre=4, n_post=4, max_iters=100,
-          max_iters_coarse=1000, eps=1e-10, coarse_eps=None, aniso=1.0):
-    """MG V-cycle solver; returns (x, used_iters, stats[4])."""
+          max_iters_coarse=1000, eps=1e-10, coarse_eps=None, aniso=1.0, cycle="V"):
+    """MG solver with V or W cycles; returns (x, used_iters, stats[4])."""
     dtype = b.dtype
     x = np.zeros(q1_n(max_level), dtype) if x0 is None else np.array(x0, dtype)
     stats = np.zeros(4)
-    f = getattr(lib(), "hbo_mg_q1_" + _sfx(dtype))
-    it = f(min_level, max_level, aniso, omega, n_pre, n_post, max_iters, max_iters_coarse, eps,
-           eps if coarse_eps is None else coarse_eps, _p(b), _p(x), _p(stats))
+    f = getattr(lib(), "hbo_mg_q1_cycle_" + _sfx(dtype))
+    it = f({"V": 0, "W": 1}[cycle], min_level, max_level, aniso, omega, n_pre, n_post, max_iters, max_iters_coarse,
+           eps, eps if coarse_eps is None else coarse_eps, _p(b), _p(x), _p(stats))
     return x, int(it), stats
+
+
+class _EllView(ctypes.Structure):
+    _fields_ = [("rows", _u64), ("cols", _u64), ("stride", _u64), ("K", _u64),
+                ("Aj", _ptr), ("Ax", _ptr), ("Arl", _ptr)]
+
+
+def _views(mats):
+    arr = (_EllView * max(1, len(mats)))()
+    for i, m in enumerate(mats):
+        arr[i] = _EllView(m.rows, m.cols, m.stride, m.K, _p(m.Aj).value, _p(m.Ax).value, _p(m.Arl).value)
+    return arr
+
+
+def mg_ell(A, prol, res, b: np.ndarray, x0: np.ndarray, cycle="V", omega=0.7, n_pre=4, n_post=4, max_iters=100,
+           max_iters_coarse=100, eps=1e-8, coarse_eps=None):
+    """MGSolver on a hierarchy of reference ELL matrices (coarsest first; prol[i] / res[i]
+    between levels i+1 and i).  Returns (x, used_iters, stats[4])."""
+    x = np.array(x0, np.float64)
+    stats = np.zeros(4)
+    it = lib().hbo_mg_ell_f64({"V": 0, "W": 1}[cycle], len(A), _views(A), _views(prol), _views(res), omega, n_pre,
+                              n_post, max_iters, max_iters_coarse, eps, eps if coarse_eps is None else coarse_eps,
+                              _p(np.ascontiguousarray(b, np.float64)), _p(x), _p(stats))
+    return x, int(it), stats
+
+
+def ell_from_file_arrays(head, Aj, Ax) -> Ell:
+    """MatrixIO<io_formats::ELL>::read_matrix (math/matrix_io.hh:466-560) on the file's
+    header (size, rows, columns, stride, num_cols_per_row) and arrays; row lengths as
+    the raw-array constructor computes them (la/sparse_matrix_ell-impl.hh:185-208)."""
+    size, rows, cols, stride, K = (int(v) for v in head)
+    E = Ell(rows, cols, stride, K, 1, np.ascontiguousarray(Aj, np.uint64), np.ascontiguousarray(Ax, np.float64),
+            np.zeros(rows, np.uint64))
+    E.Arl = ell_row_length(E)
+    return E
+
+
+def ell_transpose(A: Ell) -> Ell:
+    """Transposition<Tag>::value (math/transposition.hh:36-50) followed by the
+    SparseMatrixELL(SparseMatrix) constructor (la/sparse_matrix_ell-impl.hh:75-122,
+    threads = 1): the nonzeros of A, each row in ascending column order, stored at
+    (column, row); every result row in ascending column order; stride = rows rounded up
+    to 32; num_cols_per_row = the longest row (at least 1)."""
+    S = A.stride
+    trows = [[] for _ in range(A.cols)]
+    for r in range(A.rows):
+        ent = [(int(A.Aj[r + k * S]), A.Ax[r + k * S]) for k in range(int(A.Arl[r])) if A.Ax[r + k * S] != 0]
+        ent.sort(key=lambda e: e[0])
+        for c, v in ent:
+            trows[c].append((r, v))
+    K = max([1] + [len(t) for t in trows])
+    stride = 32 * ((A.cols + 31) // 32)
+    Aj = np.zeros(K * stride, np.uint64)
+    Ax = np.zeros(K * stride, A.Ax.dtype)
+    Arl = np.zeros(A.cols, np.uint64)
+    for r, t in enumerate(trows):
+        Arl[r] = len(t)
+        for k, (c, v) in enumerate(t):
+            Aj[r + k * stride] = c
+            Ax[r + k * stride] = v
+    return Ell(A.cols, A.rows, stride, K, 1, Aj, Ax, Arl)
 
 
 def ir_q1(max_level: int, b: np.ndarray, x0=None, min_level=3, omega=0.7, n_pre=4, n_post=4, max_inner=100,

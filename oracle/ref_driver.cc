@@ -5,6 +5,10 @@
 //       writes golden fixtures computed by the reference's tags::CPU code
 //       (raw little-endian arrays + scalars.txt); tests/golden/make_golden.py
 //       packs them into the committed fixtures.
+//   honei_ref mgquad <datadir> <outdir>
+//       the reference's MGSolverTestQuad on its FEAST test data (W-cycle); writes
+//       the solution (raw doubles), the iteration counts and the restriction
+//       matrices (res_<level>.ell, reference ELL files)
 //   honei_ref bench <cg|mg|ir|spmv> <cpu|generic|sse|mc> <level> <reps> [warmup]
 //       times the solve phase (operator setup excluded; `warmup` untimed solves
 //       first) and prints one "RESULT {json}" line.  The thread count of the MultiCore tag comes from
@@ -19,7 +23,9 @@
 #include <honei/math/cg.hh>
 #include <honei/math/defect.hh>
 #include <honei/math/ir.hh>
+#include <honei/math/matrix_io.hh>
 #include <honei/math/mg.hh>
+#include <honei/math/vector_io.hh>
 #include <honei/math/prolongation.hh>
 #include <honei/math/restriction.hh>
 #include <honei/math/ri.hh>
@@ -405,8 +411,42 @@ namespace
     }
 }
 
+namespace
+{
+    // The reference's own MGSolverTestQuad flow (math/mg_TEST.cc:398-463): FEAST
+    // matrices A_1..A_6 and prol_2..prol_6 read by MatrixIO<ELL>, rhs_6 / init_6
+    // by VectorIO<EXP>, Jacobi 0.7, W-cycle, V(4,4), coarse CG on level 1, eps 1e-8.
+    int mgquad(const std::string & dir, const std::string & out)
+    {
+        typedef MGUtil<tags::CPU, SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>,
+                       DenseVector<double>, MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, double> Util;
+        const unsigned long max_level(6), min_level(1);
+        MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
+            data(Util::load_data(dir, max_level, double(0.7), "jac"));
+        Util::configure(data, 100, 100, 4, 4, min_level, double(1e-8));
+        OperatorList ol(MGCycleCreation<tags::CPU, methods::CYCLE::W::STATIC, CGSolver<tags::CPU, methods::NONE>,
+                        RISmoother<tags::CPU>, Restriction<tags::CPU, methods::PROLMAT>,
+                        Prolongation<tags::CPU, methods::PROLMAT>, double>::value(data));
+        MGSolver<tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(data, ol);
+        DenseVector<double> & x(data.x.at(MGDataIndex::internal_index_A(max_level)));
+        write_raw(out + "/mgquad_x", x.elements(), x.size());
+        // the restriction matrices load_data built (Transposition of each prol file),
+        // written by the reference's own ELL writer
+        for (unsigned long i(0); i < data.resmat.size(); ++i)
+        {
+            std::string name(out + "/res_" + stringify(i + 2) + ".ell");
+            MatrixIO<io_formats::ELL>::write_matrix(name, data.resmat.at(i));
+        }
+        std::ofstream sc((out + "/mgquad_scalars.txt").c_str());
+        sc.precision(17);
+        sc << "used_iters " << data.used_iters << "\n" << "used_iters_coarse " << data.used_iters_coarse << "\n";
+        return 0;
+    }
+}
+
 int main(int argc, char ** argv)
 {
+    if (argc >= 4 && std::string(argv[1]) == "mgquad") return mgquad(argv[2], argv[3]);
     if (argc >= 3 && std::string(argv[1]) == "golden")
     {
         outdir = argv[2];

@@ -71,3 +71,35 @@ def oracle():
     from oracle import oracle as o
     o.lib()
     return o
+
+
+class Feast:
+    """The reference's FEAST Q1 test data and its MGSolverTestQuad result
+    (tests/golden/make_feast_fixture.py)."""
+
+    def __init__(self):
+        self.z = dict(np.load(os.path.join(GOLDEN, "feast_poisson.npz")))
+        with open(os.path.join(GOLDEN, "feast_poisson.json")) as f:
+            self.meta = json.load(f)
+
+    def head(self, name):
+        return [int(v) for v in self.z[name + ".head"]]
+
+    def file_bytes(self, name) -> bytes:
+        """the matrix as the reference's ELL file (five uint64, Aj as uint64, Ax)"""
+        return (self.z[name + ".head"].astype("<u8").tobytes() + self.z[name + ".Aj"].astype("<u8").tobytes()
+                + self.z[name + ".Ax"].astype("<f8").tobytes())
+
+    def write(self, directory, name) -> str:
+        path = os.path.join(str(directory), name + ".ell")
+        with open(path, "wb") as f:
+            f.write(self.file_bytes(name))
+        return path
+
+    def ell(self, oracle, name):
+        return oracle.ell_from_file_arrays(self.z[name + ".head"], self.z[name + ".Aj"], self.z[name + ".Ax"])
+
+
+@pytest.fixture(scope="session")
+def feast():
+    return Feast()
