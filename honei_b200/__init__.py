@@ -7,13 +7,13 @@ operator call without the built library raises ImportError.
 from ._lib import DeviceTimeout, HoneiError, NotFinite, VectorSizeDoesNotMatch, launch_count
 from .io import MatrixIO, VectorIO, io_formats
 from .la import (BandedMatrixQx, Defect, DenseVector, Difference, DotProduct, ElementProduct, Norm, Product, Scale,
-                 ScaledSum, SparseMatrixELL, Sum, convert, copy, fill, tags)
+                 ScaledSum, SparseMatrixCSR, SparseMatrixELL, Sum, convert, copy, fill, tags)
 from .solvers import (BatchedPoissonSolver, CGSolver, IRSolver, MGData, MGSolver, Prolongation, Restriction,
                       RISmoother, batch_params, methods, mg_params)
 
 __all__ = [
     "BandedMatrixQx", "BatchedPoissonSolver", "CGSolver", "Defect", "DenseVector", "DeviceTimeout", "Difference", "DotProduct",
     "ElementProduct", "HoneiError", "MatrixIO", "VectorIO", "io_formats", "IRSolver", "MGData", "MGSolver", "Norm", "NotFinite", "Product",
-    "Prolongation", "RISmoother", "Restriction", "Scale", "ScaledSum", "SparseMatrixELL", "Sum",
+    "Prolongation", "RISmoother", "Restriction", "Scale", "ScaledSum", "SparseMatrixCSR", "SparseMatrixELL", "Sum",
     "VectorSizeDoesNotMatch", "batch_params", "convert", "copy", "fill", "launch_count", "methods", "mg_params", "tags",
 ]

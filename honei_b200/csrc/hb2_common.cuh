@@ -31,9 +31,10 @@ namespace hb2
 
     // ------------------------------------------------------------------
     // Arithmetic with explicit rounding.  The reference's compiled CPU loops
-    // round a*b and then the sum separately (no fma) for products and
-    // element-wise updates, and contract to fma only in the dot product; the
-    // kernels reproduce that exactly so results are bit-identical.
+    // round a*b and then the sum separately (no fma) in the ELL and banded
+    // products and the element-wise updates, and contract to fma in the dot
+    // product and the CSR product; the kernels reproduce each exactly so
+    // results are bit-identical.
     template <typename T> struct Arith;
     template <> struct Arith<double>
     {

@@ -1,6 +1,6 @@
 """Per-kernel timing of the hot kernels on one Q1 level.
 
-    python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong]
+    python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
 
 Each launch is preceded by an L2 flush (256 MiB write) and timed alone with CUDA
@@ -79,6 +79,21 @@ def main(argv=None) -> int:
                                nc * (rbr + s) + n * s)
         kernels["prolong"] = (lambda: _lib.call("hb2_product_add_ell", Pm.handle, c.ptr, y2.ptr, stream),
                               n * (rbp + 2 * s) + nc * s)
+    if a.kernel in ("all", "csr_spmv", "csr_defect"):
+        from .la import SparseMatrixCSR
+        C = SparseMatrixCSR.from_ell(A)
+        # algorithmic: the CSR arrays (uint32 row offsets, per block a 4-byte
+        # column and its values), x and y (and rhs); the device layout reads
+        # slots (incl. padding) and a 4-byte row index per row instead
+        cb = (n + 1) * 4 + C.used_blocks() * (4 + s * C.blocksize())
+        slots, long_rows, long_entries, unroll = C.layout()
+        print(json.dumps({"csr_layout": {"slots": slots, "padding": slots - C.used_blocks() * C.blocksize() + long_entries,
+                                         "long_rows": long_rows, "unroll": unroll,
+                                         "device_bytes_per_launch": slots * (4 + s) + 4 * n + long_entries * (4 + s) + 2 * n * s}}),
+              flush=True)
+        kernels["csr_spmv"] = (lambda: _lib.call("hb2_product_csr", C.handle, x.ptr, y.ptr, stream), cb + 2 * n * s)
+        kernels["csr_defect"] = (lambda: _lib.call("hb2_defect_csr", C.handle, b.ptr, x.ptr, y.ptr, stream),
+                                 cb + 3 * n * s)
     names = list(kernels) if a.kernel == "all" else [a.kernel]
     peak = peak_gbs()
     for name in names:

@@ -254,6 +254,90 @@ def _check_size(a: int, b: int):
         raise VectorSizeDoesNotMatch(_lib.HB2_ERR_SIZE, f"VectorSizeDoesNotMatch: {a} != {b}")
 
 
+class SparseMatrixCSR:
+    """SparseMatrixCSR<DT> on the device (la/sparse_matrix_csr.hh:44-125): Ar block
+    offsets, Aj first column of each block, Ax csr::blocksize values per block."""
+
+    def __init__(self, handle: int, dtype=None):
+        self._h = ctypes.c_void_p(handle)
+        rows, cols, bs, nb, nbytes = (ctypes.c_uint64() for _ in range(5))
+        call("hb2_csr_info", self._h, ctypes.byref(rows), ctypes.byref(cols), ctypes.byref(bs), ctypes.byref(nb),
+             ctypes.byref(nbytes))
+        self._rows, self._cols, self._bs, self._nblocks = rows.value, cols.value, bs.value, nb.value
+        self.device_bytes = nbytes.value
+        self._dtype = dtype
+
+    @classmethod
+    def from_arrays(cls, rows, columns, Ar, Aj, Ax, blocksize=1, stream=None):
+        """SparseMatrixCSR(blocksize, rows, columns, Aj, Ax, Ar, used) with host arrays."""
+        Ar = np.ascontiguousarray(Ar, np.uint64)
+        Ax = np.ascontiguousarray(Ax)
+        if Ar.size != rows + 1:
+            raise VectorSizeDoesNotMatch(_lib.HB2_ERR_SIZE, "Ar must hold rows + 1 offsets")
+        nb = int(Ar[-1])
+        Aj = np.ascontiguousarray(np.asarray(Aj)[:nb], np.uint64)
+        if Aj.size != nb or Ax.size < nb * blocksize:
+            raise VectorSizeDoesNotMatch(_lib.HB2_ERR_SIZE, "Aj / Ax shorter than Ar[rows] blocks")
+        h = ctypes.c_void_p()
+        call("hb2_csr_create", ctypes.byref(h), dtype_code(Ax.dtype), rows, columns, blocksize,
+             Ar.ctypes.data_as(ctypes.c_void_p), Aj.ctypes.data_as(ctypes.c_void_p),
+             Ax.ctypes.data_as(ctypes.c_void_p), 1, _stream(stream))
+        return cls(h.value, dtype_code(Ax.dtype))
+
+    @classmethod
+    def from_ell(cls, A: "SparseMatrixELL", blocksize=1, stream=None):
+        """SparseMatrixCSR(SparseMatrixELL) with csr::blocksize = blocksize."""
+        h = ctypes.c_void_p()
+        call("hb2_csr_from_ell", ctypes.byref(h), A.handle, blocksize, _stream(stream))
+        return cls(h.value, A.dtype)
+
+    def rows(self) -> int:
+        return self._rows
+
+    def columns(self) -> int:
+        return self._cols
+
+    def blocksize(self) -> int:
+        return self._bs
+
+    def used_blocks(self) -> int:
+        return self._nblocks
+
+    @property
+    def dtype(self) -> int:
+        return self._dtype
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def layout(self):
+        """(slots, long_rows, long_entries, unroll) of the device layout: slot-major
+        32-row slices of the rows of at most 128 entries (slots incl. padding) and
+        128-entry chunks of the longer rows."""
+        sl, lr, le, u = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        call("hb2_csr_layout", self._h, ctypes.byref(sl), ctypes.byref(lr), ctypes.byref(le), ctypes.byref(u))
+        return sl.value, lr.value, le.value, u.value
+
+    def export(self):
+        """(Ar, Aj, Ax) as host arrays."""
+        torch.cuda.synchronize()
+        Ar = np.zeros(self._rows + 1, np.uint64)
+        Aj = np.zeros(self._nblocks, np.uint64)
+        Ax = np.zeros(self._nblocks * self._bs, _NP[self._dtype])
+        call("hb2_csr_export", self._h, Ar.ctypes.data_as(ctypes.c_void_p), Aj.ctypes.data_as(ctypes.c_void_p),
+             Ax.ctypes.data_as(ctypes.c_void_p))
+        return Ar, Aj, Ax
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.load().hb2_csr_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
 class Product:
     """Product<tags::B200>::value (la/product.hh)."""
 
@@ -266,6 +350,8 @@ class Product:
         _check_size(A.rows(), y.size())
         if isinstance(A, BandedMatrixQx):
             call("hb2_product_q1", A.handle, x.ptr, y.ptr, _stream(stream))
+        elif isinstance(A, SparseMatrixCSR):
+            call("hb2_product_csr", A.handle, x.ptr, y.ptr, _stream(stream))
         else:
             call("hb2_product_ell", A.handle, x.ptr, y.ptr, _stream(stream))
         return y
@@ -278,6 +364,11 @@ class Defect:
     def value(r, rhs, A, x, norm2_out: torch.Tensor | None = None, stream=None):
         r, rhs, x = _vec(r), _vec(rhs), _vec(x)
         _check_size(x.size(), A.columns())
+        if isinstance(A, SparseMatrixCSR):
+            _check_size(rhs.size(), A.rows())
+            _check_size(r.size(), A.rows())
+            call("hb2_defect_csr", A.handle, rhs.ptr, x.ptr, r.ptr, _stream(stream))
+            return r
         _check_size(rhs.size(), A.columns())
         _check_size(r.size(), A.rows())
         if isinstance(A, BandedMatrixQx):

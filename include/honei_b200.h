@@ -66,6 +66,7 @@ typedef struct hb2_ell_s *hb2_ell; /* SparseMatrixELL<DT> resident on the device
 typedef struct hb2_q1_s *hb2_q1;   /* BandedMatrixQx<Q1Type, DT> resident on the device */
 typedef struct hb2_mg_s *hb2_mg;   /* MGData + V-cycle OperatorList resident on the device */
 typedef struct hb2_batch_s *hb2_batch; /* many Q1 systems solved together (batched PCG) */
+typedef struct hb2_csr_s *hb2_csr; /* SparseMatrixCSR<DT> resident on the device */
 
 /* ---------------------------------------------------------------- runtime */
 HB2_API const char *hb2_last_error(void);
@@ -123,6 +124,27 @@ HB2_API int hb2_ell_write(hb2_ell A, const char *path);
  * builds every restriction matrix this way from its prolongation. */
 HB2_API int hb2_ell_transpose(hb2_ell *out, hb2_ell A, cudaStream_t stream);
 
+/* SparseMatrixCSR<DT>(blocksize, rows, columns, Aj, Ax, Ar, used) (la/sparse_matrix_csr-impl.hh:40-71,
+ * 140-145): Ar[rows + 1] block offsets, Aj[Ar[rows]] first column of each block,
+ * Ax[Ar[rows] * blocksize] values (dtype).  Replaces the upload that
+ * Product<tags::GPU::CUDA>(DV, SMCSR, DV) performs (la/product-cuda.cc:317-400).
+ * host_ptrs != 0: host arrays; else device arrays. */
+HB2_API int hb2_csr_create(hb2_csr *out, hb2_dtype dtype, uint64_t rows, uint64_t cols, uint64_t blocksize,
+                   const uint64_t *Ar, const uint64_t *Aj, const void *Ax, int host_ptrs, cudaStream_t stream);
+/* SparseMatrixCSR(SparseMatrixELL) (la/sparse_matrix_csr-impl.hh:85-135) with csr::blocksize = blocksize */
+HB2_API int hb2_csr_from_ell(hb2_csr *out, hb2_ell A, uint64_t blocksize, cudaStream_t stream);
+HB2_API int hb2_csr_destroy(hb2_csr A);
+/* rows, cols, blocksize, blocks (Ar[rows]), device bytes */
+HB2_API int hb2_csr_info(hb2_csr A, uint64_t *rows, uint64_t *cols, uint64_t *blocksize, uint64_t *nblocks,
+                 uint64_t *device_bytes);
+/* Ar (rows + 1), Aj (blocks), Ax (blocks * blocksize) into host arrays */
+HB2_API int hb2_csr_export(hb2_csr A, uint64_t *Ar, uint64_t *Aj, void *Ax);
+/* Device layout the products run on: rows of at most 128 entries in 32-row
+ * slices stored slot-major (SELL-C-sigma; *slots = slots incl. padding), longer
+ * rows as 128-entry chunks (*long_rows, *long_entries); *unroll = slots per lane
+ * and round (8 or 16, timed at creation). */
+HB2_API int hb2_csr_layout(hb2_csr A, uint64_t *slots, uint64_t *long_rows, uint64_t *long_entries, uint32_t *unroll);
+
 /* BandedMatrixQx<Q1Type, DT> (la/banded_matrix_qx-impl.hh:45-466): 9 bands of n,
  * band-major LL LD LU DL DD DU UL UD UU; n must be (2^L+1)^2. */
 HB2_API int hb2_q1_create(hb2_q1 *out, hb2_dtype dtype, uint64_t n, const void *bands, int host_ptrs,
@@ -134,6 +156,13 @@ HB2_API int hb2_q1_destroy(hb2_q1 A);
 /* Product<Tag>::value(y, A, x) on ELL (la/product.hh:148-206; old CUDA launcher
  * cuda_product_smell_dv_{float,double}, backends/cuda/operations.hh:93-99). */
 HB2_API int hb2_product_ell(hb2_ell A, const void *x, void *y, cudaStream_t stream);
+/* Product<Tag>::value(y, A, x) on CSR (la/product.hh:208-244; old launcher
+ * cuda_product_csr_dv_{float,double}, backends/cuda/operations.hh:95-99): each row
+ * one fma chain over its blocks in order, a block value past x skipped. */
+HB2_API int hb2_product_csr(hb2_csr A, const void *x, void *y, cudaStream_t stream);
+/* Defect<Tag>::value(r, rhs, A, x) on CSR (math/defect.hh:385-420; old launcher
+ * cuda_defect_csr_dv_*, operations.hh:49-53): r = rhs - (the product's row sum). */
+HB2_API int hb2_defect_csr(hb2_csr A, const void *rhs, const void *x, void *r, cudaStream_t stream);
 /* Defect<Tag>::value(r, rhs, A, x) = rhs - A x (math/defect.hh:357-383; old launcher
  * cuda_defect_smell_dv_*, operations.hh:40-46).  norm2_dev (nullable, device double):
  * receives ||r||_2^2 computed in the same pass (Norm<vnt_l_two,false>, la/norm.hh:290-305). */

@@ -260,6 +260,34 @@ void hbo_ell_defect_##SFX(uint64_t rows, uint64_t stride, uint64_t T,           
 DEFINE_ELL_SPMV(double, f64, MULADD)
 DEFINE_ELL_SPMV(float, f32, MULADD)
 
+/* la/product.hh:208-244, math/defect.hh:385-420: SparseMatrixCSR with csr::blocksize
+ * bs -- Ar[row]..Ar[row+1] blocks, block i starting at column Aj[i] with bs values
+ * Ax[i*bs ..]; a block value whose column is >= the vector size is skipped */
+#define DEFINE_CSR_SPMV(T_, SFX, FMA)                                               \
+static T_ csr_row_##SFX(uint64_t row, uint64_t bs, uint64_t ncols, const uint64_t *Ar, \
+                        const uint64_t *Aj, const T_ *Ax, const T_ *x)              \
+{                                                                                   \
+    T_ sum = 0;                                                                     \
+    for (uint64_t i = Ar[row]; i < Ar[row + 1]; ++i)                                \
+        for (uint64_t b = 0; b < bs; ++b)                                           \
+            if (Aj[i] + b < ncols) sum = FMA(Ax[i * bs + b], x[Aj[i] + b], sum);    \
+    return sum;                                                                     \
+}                                                                                   \
+void hbo_csr_spmv_##SFX(uint64_t rows, uint64_t bs, uint64_t ncols, const uint64_t *Ar, \
+                        const uint64_t *Aj, const T_ *Ax, const T_ *x, T_ *y)       \
+{                                                                                   \
+    for (uint64_t r = 0; r < rows; ++r) y[r] = csr_row_##SFX(r, bs, ncols, Ar, Aj, Ax, x); \
+}                                                                                   \
+void hbo_csr_defect_##SFX(uint64_t rows, uint64_t bs, uint64_t ncols, const uint64_t *Ar, \
+                          const uint64_t *Aj, const T_ *Ax, const T_ *rhs, const T_ *x, \
+                          T_ *res)                                                  \
+{                                                                                   \
+    for (uint64_t r = 0; r < rows; ++r)                                             \
+        res[r] = rhs[r] - csr_row_##SFX(r, bs, ncols, Ar, Aj, Ax, x);               \
+}
+DEFINE_CSR_SPMV(double, f64, fma)
+DEFINE_CSR_SPMV(float, f32, fmaf)
+
 /* la/product.hh:370-403 */
 #define DEFINE_Q1_SPMV(T_, SFX, FMA)                                                \
 void hbo_q1_spmv_##SFX(uint64_t n, uint64_t m, const T_ *bands, const T_ *x, T_ *y)\

@@ -66,6 +66,9 @@ def lib():
         L.hbo_mg_ell_f64.restype = _u64
         L.hbo_mg_ell_f64.argtypes = [ctypes.c_int, ctypes.c_uint, _ptr, _ptr, _ptr, _dbl, _u64, _u64, _u64, _u64,
                                      _dbl, _dbl, _ptr, _ptr, _ptr]
+        for sfx in ("f64", "f32"):
+            getattr(L, "hbo_csr_spmv_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, _ptr, _ptr]
+            getattr(L, "hbo_csr_defect_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, _ptr, _ptr, _ptr]
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
@@ -324,3 +327,107 @@ def ir_q1(max_level: int, b: np.ndarray, x0=None, min_level=3, omega=0.7, n_pre=
                          inner_eps if coarse_eps is None else coarse_eps, max_outer, eps, int(reset_inner),
                          _p(b), _p(x), _p(stats))
     return x, int(it), stats
+
+
+class Csr:
+    """Reference SparseMatrixCSR arrays: Ar (rows + 1 block offsets), Aj (first column of
+    each block), Ax (bs values per block), blocksize bs."""
+
+    def __init__(self, rows, cols, bs, Ar, Aj, Ax):
+        self.rows, self.cols, self.bs = int(rows), int(cols), int(bs)
+        self.Ar = np.ascontiguousarray(Ar, np.uint64)
+        self.Aj = np.ascontiguousarray(Aj, np.uint64)
+        self.Ax = np.ascontiguousarray(Ax)
+
+    @property
+    def dtype(self):
+        return self.Ax.dtype
+
+
+def csr_blocked(rows, cols, indptr, indices, values, bs=1) -> Csr:
+    """SparseMatrixCSR::Implementation::_create (la/sparse_matrix_csr-impl.hh:98-135) on
+    rows given as CSR with ascending columns: consecutive entries of a row that fall in
+    one aligned block of bs columns share a block; Aj = the block's first column, the
+    block's bs values with zeros at the missing columns."""
+    indptr = np.asarray(indptr, np.int64)
+    indices = np.asarray(indices, np.int64)
+    values = np.asarray(values)
+    if bs == 1:
+        return Csr(rows, cols, 1, indptr, indices, values.copy())
+    row_of = np.repeat(np.arange(rows, dtype=np.int64), np.diff(indptr))
+    blk = indices // bs
+    new = np.ones(indices.size, bool)
+    new[1:] = (blk[1:] != blk[:-1]) | (row_of[1:] != row_of[:-1])
+    block_id = np.cumsum(new) - 1
+    nblocks = int(new.sum())
+    Aj = (blk[new] * bs).astype(np.uint64)
+    Ax = np.zeros(nblocks * bs, values.dtype)
+    Ax[block_id * bs + indices % bs] = values
+    counts = np.bincount(row_of[new], minlength=rows)
+    Ar = np.zeros(rows + 1, np.uint64)
+    Ar[1:] = np.cumsum(counts)
+    return Csr(rows, cols, bs, Ar, Aj, Ax)
+
+
+def csr_from_ell(E: Ell, bs=1) -> Csr:
+    """SparseMatrixCSR(SparseMatrixELL) (la/sparse_matrix_csr-impl.hh:85-96): every nonzero
+    slot of the ELL arrays (la/sparse_matrix.hh:157-185), rows in ascending column order."""
+    S, T = E.stride, E.T
+    rows_c, rows_v = [], []
+    for r in range(E.rows):
+        ent = {}
+        for i in range(r * T, E.K * S, S):
+            for t in range(T):
+                if E.Ax[i + t] != 0:
+                    ent[int(E.Aj[i + t])] = E.Ax[i + t]
+        cs = sorted(ent)
+        rows_c.append(cs)
+        rows_v.append([ent[c] for c in cs])
+    indptr = np.zeros(E.rows + 1, np.int64)
+    indptr[1:] = np.cumsum([len(c) for c in rows_c])
+    indices = np.array([c for cs in rows_c for c in cs], np.int64)
+    vals = np.array([v for vs in rows_v for v in vs], E.Ax.dtype)
+    return csr_blocked(E.rows, E.cols, indptr, indices, vals, bs)
+
+
+def skewed_csr(n=5000, m=4700, bs=1) -> Csr:
+    """The skewed test matrix of the reference driver's csr case: empty rows (r % 11 == 3),
+    one full row (n/2 + 1), rows of ~2m/3 entries (r % 500 == 7), otherwise 1..17 entries."""
+    L = lib()
+    u = L.hbo_uniform
+    indptr, indices, vals = [0], [], []
+    for r in range(n):
+        ent = {}
+        if r % 11 == 3:
+            pass
+        elif r == n // 2 + 1:
+            for c in range(m):
+                ent[c] = u(99, r * 10007 + c, 0.25, 1.0)
+        elif r % 500 == 7:
+            for c in range(m):
+                if (c + r) % 3 != 2:
+                    ent[c] = u(99, r * 10007 + c, -1.0, -0.25)
+        else:
+            for j in range(1 + (r * 7) % 17):
+                c = (r + j * j * 31 + j) % m
+                ent[c] = u(99, r * 10007 + c, 0.25, 1.0) * (1.0 if (r + j) % 2 else -1.0)
+        cs = sorted(ent)
+        indices += cs
+        vals += [ent[c] for c in cs]
+        indptr.append(len(indices))
+    return csr_blocked(n, m, np.array(indptr), np.array(indices, np.int64), np.array(vals, np.float64), bs)
+
+
+def csr_spmv(A: Csr, x: np.ndarray) -> np.ndarray:
+    y = np.empty(A.rows, A.dtype)
+    getattr(lib(), "hbo_csr_spmv_" + _sfx(A.dtype))(A.rows, A.bs, x.size, _p(A.Ar), _p(A.Aj), _p(A.Ax),
+                                                     _p(np.ascontiguousarray(x, A.dtype)), _p(y))
+    return y
+
+
+def csr_defect(A: Csr, rhs: np.ndarray, x: np.ndarray) -> np.ndarray:
+    r = np.empty(A.rows, A.dtype)
+    getattr(lib(), "hbo_csr_defect_" + _sfx(A.dtype))(A.rows, A.bs, x.size, _p(A.Ar), _p(A.Aj), _p(A.Ax),
+                                                       _p(np.ascontiguousarray(rhs, A.dtype)),
+                                                       _p(np.ascontiguousarray(x, A.dtype)), _p(r))
+    return r

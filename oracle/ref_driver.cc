@@ -5,6 +5,8 @@
 //       writes golden fixtures computed by the reference's tags::CPU code
 //       (raw little-endian arrays + scalars.txt); tests/golden/make_golden.py
 //       packs them into the committed fixtures.
+//   honei_ref csr <outdir>
+//       SparseMatrixCSR arrays (csr::blocksize 1..4) and their Product / Defect
 //   honei_ref mgquad <datadir> <outdir>
 //       the reference's MGSolverTestQuad on its FEAST test data (W-cycle); writes
 //       the solution (raw doubles), the iteration counts and the restriction
@@ -16,6 +18,7 @@
 #include "ref_common.hh"
 
 #include <honei/la/dot_product.hh>
+#include <honei/la/sparse_matrix_csr.hh>
 #include <honei/la/norm.hh>
 #include <honei/la/product.hh>
 #include <honei/la/scaled_sum.hh>
@@ -444,9 +447,96 @@ namespace
     }
 }
 
+namespace
+{
+    template <typename DT_>
+    void put_csr_case(const std::string & name, const SparseMatrixCSR<DT_> & A)
+    {
+        put_vec(name + ".Ar", A.Ar());
+        put_vec(name + ".Aj", A.Aj());
+        put_vec(name + ".Ax", A.Ax());
+        scalars << name << ".rows " << A.rows() << "\n" << name << ".cols " << A.columns() << "\n"
+                << name << ".bs " << A.blocksize() << "\n" << name << ".used " << A.used_elements() << "\n";
+        DenseVector<DT_> x(uniform<DT_>(A.columns(), 7)), rhs(uniform<DT_>(A.rows(), 11));
+        DenseVector<DT_> y(A.rows()), r(A.rows());
+        Product<tags::CPU>::value(y, A, x);
+        Defect<tags::CPU>::value(r, rhs, A, x);
+        put_vec(name + ".spmv", y);
+        put_vec(name + ".defect", r);
+    }
+
+    // rows of very different lengths: empty rows, short rows, rows of a few
+    // thousand entries and one full row; a column count that is not a multiple
+    // of the block sizes tested
+    SparseMatrix<double> skewed(unsigned long n, unsigned long m)
+    {
+        SparseMatrix<double> S(n, m);
+        for (unsigned long r(0); r < n; ++r)
+        {
+            if (r % 11 == 3) continue;
+            if (r == n / 2 + 1)
+            {
+                for (unsigned long c(0); c < m; ++c) S(r, c, hbo_uniform(99, r * 10007 + c, 0.25, 1.0));
+                continue;
+            }
+            if (r % 500 == 7)
+            {
+                for (unsigned long c(0); c < m; ++c)
+                    if ((c + r) % 3 != 2) S(r, c, hbo_uniform(99, r * 10007 + c, -1.0, -0.25));
+                continue;
+            }
+            const unsigned long k(1 + (r * 7) % 17);
+            for (unsigned long j(0); j < k; ++j)
+            {
+                const unsigned long c((r + j * j * 31 + j) % m);
+                S(r, c, hbo_uniform(99, r * 10007 + c, 0.25, 1.0) * ((r + j) % 2 ? 1.0 : -1.0));
+            }
+        }
+        return S;
+    }
+
+    // SparseMatrixCSR (la/sparse_matrix_csr-impl.hh:73-135) with csr::blocksize
+    // 1, 2, 4 on the Q1 operator and 1, 3 on the skewed matrix; Product and Defect
+    // (la/product.hh:208-244, math/defect.hh:385-420) on seeded vectors
+    int csr()
+    {
+        scalars.open((outdir + "/scalars.txt").c_str());
+        scalars.precision(17);
+        const unsigned long bss[] = {1, 2, 4};
+        for (unsigned L(4); L <= 6; L += 2)
+            for (unsigned i(0); i < 3; ++i)
+            {
+                Configuration::instance()->set_value("csr::blocksize", int(bss[i]));
+                SparseMatrixCSR<double> A(q1_ell_assembled<double>(L));
+                char nm[64];
+                snprintf(nm, sizeof nm, "q1_L%u_bs%lu_f64", L, bss[i]);
+                put_csr_case(nm, A);
+            }
+        Configuration::instance()->set_value("csr::blocksize", 1);
+        {
+            SparseMatrixCSR<float> Af(q1_ell_assembled<float>(6));
+            put_csr_case("q1_L6_bs1_f32", Af);
+        }
+        SparseMatrix<double> S(skewed(5000, 4700));
+        for (unsigned long bs(1); bs <= 3; bs += 2)
+        {
+            Configuration::instance()->set_value("csr::blocksize", int(bs));
+            SparseMatrixCSR<double> A(S);
+            put_csr_case(bs == 1 ? "skew_bs1_f64" : "skew_bs3_f64", A);
+        }
+        Configuration::instance()->set_value("csr::blocksize", 1);
+        return 0;
+    }
+}
+
 int main(int argc, char ** argv)
 {
     if (argc >= 4 && std::string(argv[1]) == "mgquad") return mgquad(argv[2], argv[3]);
+    if (argc >= 3 && std::string(argv[1]) == "csr")
+    {
+        outdir = argv[2];
+        return csr();
+    }
     if (argc >= 3 && std::string(argv[1]) == "golden")
     {
         outdir = argv[2];

@@ -34,12 +34,12 @@ def pytest_collection_modifyitems(config, items):
 class Golden:
     """Fixtures produced by the reference's own tags::CPU code (tests/golden/make_golden.py)."""
 
-    def __init__(self):
-        with open(os.path.join(GOLDEN, "reference_cpu.json")) as f:
+    def __init__(self, base="reference_cpu"):
+        with open(os.path.join(GOLDEN, base + ".json")) as f:
             meta = json.load(f)
         self.scalars = meta["scalars"]
         self.digests = meta["digests"]
-        self.full = dict(np.load(os.path.join(GOLDEN, "reference_cpu.npz")))
+        self.full = dict(np.load(os.path.join(GOLDEN, base + ".npz")))
 
     def has(self, name):
         return name in self.digests
@@ -64,6 +64,12 @@ class Golden:
 @pytest.fixture(scope="session")
 def golden():
     return Golden()
+
+
+@pytest.fixture(scope="session")
+def golden_csr():
+    """reference SparseMatrixCSR fixtures (tests/golden/make_csr_fixture.py)"""
+    return Golden("reference_csr")
 
 
 @pytest.fixture(scope="session")
