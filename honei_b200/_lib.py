@@ -80,6 +80,9 @@ SIGNATURES = {
     "hb2_ell_read": (_int, [_pvp, ctypes.c_char_p, _int, _vp]),
     "hb2_ell_write": (_int, [_vp, ctypes.c_char_p]),
     "hb2_ell_transpose": (_int, [_pvp, _vp, _vp]),
+    "hb2_krylov_create": (_int, [_pvp, _int, _vp, _vp, _vp, _u64, _dbl, _vp]),
+    "hb2_krylov_destroy": (_int, [_vp]),
+    "hb2_krylov_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "hb2_csr_create": (_int, [_pvp, _int, _u64, _u64, _u64, _vp, _vp, _vp, _int, _vp]),
     "hb2_csr_from_ell": (_int, [_pvp, _vp, _u64, _vp]),
     "hb2_csr_destroy": (_int, [_vp]),

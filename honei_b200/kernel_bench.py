@@ -1,6 +1,7 @@
 """Per-kernel timing of the hot kernels on one Q1 level.
 
-    python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect]
+    python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect|
+                                                cgvar|bicgstab]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
 
 Each launch is preceded by an L2 flush (256 MiB write) and timed alone with CUDA
@@ -94,6 +95,39 @@ def main(argv=None) -> int:
         kernels["csr_spmv"] = (lambda: _lib.call("hb2_product_csr", C.handle, x.ptr, y.ptr, stream), cb + 2 * n * s)
         kernels["csr_defect"] = (lambda: _lib.call("hb2_defect_csr", C.handle, b.ptr, x.ptr, y.ptr, stream),
                                  cb + 3 * n * s)
+    if a.kernel in ("cgvar", "bicgstab") and a.dtype == "f64":
+        from .solvers import HB2_BICGSTAB_VAR, HB2_CG_VAR, KrylovSolver
+        # Jacobi vector preconditioner; a fixed number of iterations (eps = 0)
+        dvec = torch.empty(n, dtype=dt, device=dev)
+        _lib.call("hb2_jacobi_precon", A.handle, 1.0, ctypes.c_void_p(dvec.data_ptr()), stream)
+        iters = 200
+        K = KrylovSolver(HB2_CG_VAR if a.kernel == "cgvar" else HB2_BICGSTAB_VAR, A, DenseVector(dvec), iters, 0.0)
+        x0 = DenseVector(n, dtype=dt)
+        K.solve(b, DenseVector(n, dtype=dt))        # warm-up
+        ts = []
+        for _ in range(3):
+            x0.elements.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, used, _ = K.solve(b, x0)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        its = used - 1 if a.kernel == "bicgstab" else used
+        # algorithmic bytes per iteration: the SpMV(s) (matrix bytes + x + y) and the
+        # vector passes (CG VAR: update 48, Jacobi + dot 24, direction 24 bytes per
+        # row; BiCGStab: 2 Jacobi products 2*24, s 40, t dots 16, update 56, r~ 32,
+        # direction 32 bytes per row)
+        per_row = (rb + 16 + 96) if a.kernel == "cgvar" else (2 * (rb + 16) + 48 + 40 + 16 + 56 + 32 + 32)
+        nbytes = n * per_row
+        us_it = 1000 * ms / its
+        print(json.dumps({"kernel": a.kernel, "level": L, "rows": n, "iterations": its, "solve_ms": ms,
+                          "us_per_iteration": us_it, "algorithmic_bytes_per_iteration": nbytes,
+                          "gbs": nbytes / (us_it * 1e-6) / 1e9, "frac_of_measured_peak": nbytes / (us_it * 1e-6) / 1e9 / peak_gbs()}),
+              flush=True)
+        return 0
     names = list(kernels) if a.kernel == "all" else [a.kernel]
     peak = peak_gbs()
     for name in names:

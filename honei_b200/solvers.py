@@ -1,7 +1,8 @@
-"""HONEI's solver layer for the B200 tag: grid transfer, smoother, CG, MG, IR.
+"""HONEI's solver layer for the B200 tag: grid transfer, smoother, CG (NONE and
+VAR), CGSmoother, BiCGStab, MG, IR.
 
 Mirrors math/prolongation.hh, math/restriction.hh, math/ri.hh, math/cg.hh,
-math/mg.hh and math/ir.hh.  Each solver is one call into libhonei_b200.so; the
+math/bicgstab.hh, math/mg.hh and math/ir.hh.  Each solver is one call into libhonei_b200.so; the
 MG cycle runs as a captured CUDA graph.
 """
 from __future__ import annotations
@@ -23,6 +24,10 @@ class methods:
         pass
 
     class PROLMAT:
+        pass
+
+    class VAR:
+        """variable preconditioning (CGSolver / BiCGStabSolver<Tag, methods::VAR>)"""
         pass
 
 
@@ -78,13 +83,64 @@ class RISmoother:
         return P
 
 
+HB2_CG_VAR, HB2_BICGSTAB_VAR, HB2_CG_SMOOTHER = 0, 1, 2
+
+
+class KrylovSolver:
+    """A Krylov solver resident on the device (hb2_krylov): its vectors and the CUDA
+    graph of a whole solve, for repeated solves with one A and P.
+
+    method: HB2_CG_VAR (CGSolver<Tag, methods::VAR>, math/cg.hh:142-210),
+    HB2_BICGSTAB_VAR (BiCGStabSolver<Tag, methods::VAR>, math/bicgstab.hh:60-210) or
+    HB2_CG_SMOOTHER (CGSmoother, math/cg.hh:217-290).  P: a DenseVector (element-wise
+    preconditioner) or a SparseMatrixELL."""
+
+    def __init__(self, method, A, P, max_iters, eps_relative=1e-8, stream=None):
+        if isinstance(P, SparseMatrixELL):
+            pm, pd = P.handle, None
+            _check_size(P.rows(), A.rows())
+        else:
+            P = _vec(P)
+            _check_size(P.size(), A.rows())
+            pm, pd = None, P.ptr
+        self._keep = (A, P)
+        self.method = method
+        h = ctypes.c_void_p()
+        call("hb2_krylov_create", ctypes.byref(h), int(method), A.handle, pm, pd, int(max_iters),
+             float(eps_relative), _stream(stream))
+        self._h = h
+        self.n = A.rows()
+
+    def solve(self, b, x, stream=None):
+        """x = the solution from the initial guess x; returns (x, used_iters, final_defect)."""
+        b, x = _vec(b), _vec(x)
+        _check_size(b.size(), self.n)
+        _check_size(x.size(), self.n)
+        used = ctypes.c_uint64()
+        defect = ctypes.c_double()
+        call("hb2_krylov_solve", self._h, b.ptr, x.ptr, ctypes.byref(used), ctypes.byref(defect), _stream(stream))
+        return x, used.value, defect.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.load().hb2_krylov_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
 class CGSolver:
-    """CGSolver<tags::B200, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps) (math/cg.hh:64-135).
+    """CGSolver<tags::B200, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps) (math/cg.hh:64-135);
+    with method=methods.VAR, CGSolver<tags::B200, methods::VAR> (math/cg.hh:142-210), P a DenseVector
+    (element-wise) or a SparseMatrixELL.
 
     Returns (x, used_iters, final_defect)."""
 
     @staticmethod
-    def value(A, P, b, x, max_iters, eps_relative=1e-8, stream=None):
+    def value(A, P, b, x, max_iters, eps_relative=1e-8, method=methods.NONE, stream=None):
+        if method is methods.VAR:
+            return KrylovSolver(HB2_CG_VAR, A, P, max_iters, eps_relative, stream).solve(b, x, stream)
         b, x = _vec(b), _vec(x)
         _check_size(b.size(), A.rows())
         _check_size(x.size(), A.columns())
@@ -93,6 +149,24 @@ class CGSolver:
         call("hb2_cg_solve", A.handle, b.ptr, x.ptr, int(max_iters), float(eps_relative), ctypes.byref(used),
              ctypes.byref(defect), _stream(stream))
         return x, used.value, defect.value
+
+
+class BiCGStabSolver:
+    """BiCGStabSolver<tags::B200, methods::VAR>::value(A, P, b, x, max_iters, used_iters, eps)
+    (math/bicgstab.hh:60-210).  Returns (x, used_iters, squared final defect)."""
+
+    @staticmethod
+    def value(A, P, b, x, max_iters, eps_relative=1e-8, stream=None):
+        return KrylovSolver(HB2_BICGSTAB_VAR, A, P, max_iters, eps_relative, stream).solve(b, x, stream)
+
+
+class CGSmoother:
+    """CGSmoother<tags::B200>::value(A, P, b, x, temp_vecs, max_iters) (math/cg.hh:217-290):
+    exactly max_iters preconditioned CG steps from x.  Returns x."""
+
+    @staticmethod
+    def value(A, P, b, x, max_iters, stream=None):
+        return KrylovSolver(HB2_CG_SMOOTHER, A, P, max_iters, 0.0, stream).solve(b, x, stream)[0]
 
 
 def mg_params(n_pre=4, n_post=4, max_iters=100, max_iters_coarse=100, eps=1e-10, coarse_eps=None, omega=0.7,

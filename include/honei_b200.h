@@ -67,6 +67,7 @@ typedef struct hb2_q1_s *hb2_q1;   /* BandedMatrixQx<Q1Type, DT> resident on the
 typedef struct hb2_mg_s *hb2_mg;   /* MGData + V-cycle OperatorList resident on the device */
 typedef struct hb2_batch_s *hb2_batch; /* many Q1 systems solved together (batched PCG) */
 typedef struct hb2_csr_s *hb2_csr; /* SparseMatrixCSR<DT> resident on the device */
+typedef struct hb2_krylov_s *hb2_krylov; /* a Krylov solver with its vectors and CUDA graph */
 
 /* ---------------------------------------------------------------- runtime */
 HB2_API const char *hb2_last_error(void);
@@ -256,6 +257,27 @@ HB2_API int hb2_jacobi_precon(hb2_ell A, double omega, void *P, cudaStream_t str
  * Synchronises `stream`. */
 HB2_API int hb2_cg_solve(hb2_ell A, const void *b, void *x, uint64_t max_iters, double eps, uint64_t *used_iters,
                  double *final_defect, cudaStream_t stream);
+
+/* Krylov solvers with a variable preconditioner, FP64:
+ *   HB2_CG_VAR        CGSolver<Tag, methods::VAR> (math/cg.hh:142-210)
+ *   HB2_BICGSTAB_VAR  BiCGStabSolver<Tag, methods::VAR> (math/bicgstab.hh:60-210)
+ *   HB2_CG_SMOOTHER   CGSmoother (math/cg.hh:217-290): exactly max_iters steps
+ * P is either the ELL matrix P or the vector pdiag (n doubles, host or device,
+ * copied: the element-wise product P (.) r); the other is NULL.  The handle
+ * keeps a reference to A and P (they must outlive it) and owns its vectors and
+ * the CUDA graph of the solve (prefix, a conditional WHILE node over the
+ * iterations, IF nodes for BiCGStab's early exits). */
+enum { HB2_CG_VAR = 0, HB2_BICGSTAB_VAR = 1, HB2_CG_SMOOTHER = 2 };
+HB2_API int hb2_krylov_create(hb2_krylov *out, int method, hb2_ell A, hb2_ell P, const double *pdiag,
+                      uint64_t max_iters, double eps_relative, cudaStream_t stream);
+HB2_API int hb2_krylov_destroy(hb2_krylov K);
+/* b, x: device vectors (x: initial guess in, result out).  used_iters: the
+ * reference's used_iters (CG VAR: the iteration that met a stop test, 0 if none
+ * ran; BiCGStab: iterations + 1; smoother: max_iters); final_defect: ||r||
+ * (CG VAR), the squared defect norm (BiCGStab, as the reference's
+ * Norm<vnt_l_two, false>), 0 (smoother).  Synchronises `stream`. */
+HB2_API int hb2_krylov_solve(hb2_krylov K, const void *b, void *x, uint64_t *used_iters, double *final_defect,
+                     cudaStream_t stream);
 
 /* MG hierarchy: MGData (math/mg.hh:57-240) + MGCycleCreation<V::STATIC,
  * CGSolver<NONE>, RISmoother, Restriction<PROLMAT>, Prolongation<PROLMAT>>

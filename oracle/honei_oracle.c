@@ -751,3 +751,140 @@ uint64_t hbo_ir_q1(unsigned min_level, unsigned max_level, double aniso, double 
     mg_free_f32(&h);
     return used;
 }
+
+
+/* ---- Krylov solvers with a variable preconditioner ------------------------ */
+/* P: a vector (Product of two DenseVectors = ElementProduct, la/product.hh:1198-1204)
+ * when pdiag != NULL, else an ELL matrix (Product ELL, la/product.hh:148-206) */
+static void pc_apply_f64(const double *pdiag, const ell_f64 *P, uint64_t n, const double *r, double *z)
+{
+    if (pdiag) for (uint64_t i = 0; i < n; ++i) z[i] = pdiag[i] * r[i];
+    else spmv_f64(P, r, z);
+}
+
+/* the reference's guard against division by a tiny number */
+static double eps_guard(double t)
+{
+    return fabs(t) > DBL_EPSILON ? t : DBL_EPSILON * (t / fabs(t));
+}
+
+/* ScaledSum<Tag>::value(x, y, b) x += b*y and value(r, x, y, b) r = b*y + x
+ * (la/scaled_sum.hh:73-108), each product and sum rounded */
+static void axpy(uint64_t n, double *x, const double *y, double b)
+{ for (uint64_t i = 0; i < n; ++i) x[i] = MULADD(b, y[i], x[i]); }
+static void axpy3(uint64_t n, double *r, const double *x, const double *y, double b)
+{ for (uint64_t i = 0; i < n; ++i) r[i] = MULADD(b, y[i], x[i]); }
+
+uint64_t hbo_cgvar_f64(const hbo_ell_view *Av, const double *pdiag, const hbo_ell_view *Pv, const double *b,
+                       double *x, uint64_t max_iters, double eps, int smoother)
+{
+    ell_f64 A, P;
+    ell_copy_f64(&A, Av);
+    if (! pdiag) ell_copy_f64(&P, Pv);
+    const uint64_t n = A.rows;
+    double *p = (double *)malloc(sizeof(double) * n), *r = (double *)malloc(sizeof(double) * n);
+    double *v = (double *)malloc(sizeof(double) * n), *z = (double *)malloc(sizeof(double) * n);
+    uint64_t it = 0, used = 0;
+    /* math/cg.hh:161-210 (CGSolver VAR); CGSmoother (math/cg.hh:230-288) has no
+       convergence test and stops after max_iters */
+    defect_f64(&A, b, x, r);
+    pc_apply_f64(pdiag, &P, n, r, p);
+    const double initial = sqrt(hbo_dot_f64(n, r, r));
+    double alpha_new = hbo_dot_f64(n, r, p), alpha, lambda, temp;
+    while (it < max_iters) {
+        spmv_f64(&A, p, v);
+        temp = hbo_dot_f64(n, v, p);
+        lambda = alpha_new / eps_guard(temp);
+        ++it;
+        axpy(n, x, p, lambda);
+        axpy(n, r, v, -lambda);
+        if (smoother) {
+            if (it == max_iters) break;
+        } else {
+            const double cur = sqrt(hbo_dot_f64(n, r, r));
+            if (cur < eps * initial) { used = it; break; }
+            if (cur < eps) { used = it; break; }
+            if (it == max_iters) { used = it; break; }
+        }
+        pc_apply_f64(pdiag, &P, n, r, z);
+        alpha = alpha_new;
+        alpha_new = hbo_dot_f64(n, r, z);
+        const double talpha = alpha_new / eps_guard(alpha);
+        for (uint64_t i = 0; i < n; ++i) { p[i] = p[i] * talpha; p[i] = p[i] + z[i]; }
+    }
+    free(p); free(r); free(v); free(z);
+    ell_free_f64(&A);
+    if (! pdiag) ell_free_f64(&P);
+    return smoother ? it : used;
+}
+
+/* BiCGStabSolver<Tag, methods::VAR> (math/bicgstab.hh:71-210); the norms are
+ * Norm<vnt_l_two, false> (squared), compared with eps times the squared initial
+ * defect; returns the reference's used_iters (iterations + 1) */
+uint64_t hbo_bicgstab_f64(const hbo_ell_view *Av, const double *pdiag, const hbo_ell_view *Pv, const double *b,
+                          double *x, uint64_t max_iters, double eps)
+{
+    ell_f64 A, P;
+    ell_copy_f64(&A, Av);
+    if (! pdiag) ell_copy_f64(&P, Pv);
+    const uint64_t n = A.rows;
+    double *vec[10];
+    for (int i = 0; i < 10; ++i) vec[i] = (double *)malloc(sizeof(double) * (n ? n : 1));
+    double *r = vec[0], *rt = vec[1], *rt0 = vec[2], *pt = vec[3], *v = vec[4], *vt = vec[5], *s = vec[6],
+           *st = vec[7], *t = vec[8], *tt = vec[9];
+    double defnorm, defnorm_0, defnorm_00 = 1e14, rho, rho_old, alpha, omega, beta, gamma;
+    uint64_t iter = 0;
+    int restarted = 0, converged = 0;
+    do {
+        defect_f64(&A, b, x, r);
+        defnorm_0 = hbo_dot_f64(n, r, r);
+        defnorm = defnorm_0;
+        pc_apply_f64(pdiag, &P, n, r, rt0);
+        if (! restarted) defnorm_00 = defnorm_0;
+        memcpy(rt, rt0, sizeof(double) * n);
+        memcpy(pt, rt0, sizeof(double) * n);
+        rho = hbo_dot_f64(n, rt0, rt0);
+        do {
+            iter = iter + 1;
+            spmv_f64(&A, pt, v);
+            pc_apply_f64(pdiag, &P, n, v, vt);
+            gamma = hbo_dot_f64(n, vt, rt0);
+            if (fabs(gamma) < fabs(rho) * 1e-14) { restarted = 1; break; }
+            alpha = rho / gamma;
+            /* the reference also sets `restarted` (without leaving the loop) when
+               |alpha| ||vt||^2 / defnorm < 1e-5; the flag is read only before the
+               first pass, so it changes nothing and is not computed here */
+            axpy3(n, s, r, v, -alpha);
+            defnorm = hbo_dot_f64(n, s, s);
+            if (defnorm < eps * defnorm_00) {
+                axpy(n, x, pt, alpha);
+                converged = 1;
+                break;
+            }
+            axpy3(n, st, rt, vt, -alpha);
+            spmv_f64(&A, st, t);
+            pc_apply_f64(pdiag, &P, n, t, tt);
+            gamma = hbo_dot_f64(n, tt, tt);
+            omega = hbo_dot_f64(n, tt, st);
+            if (fabs(gamma) < fabs(omega) * 1e-14) { restarted = 1; break; }
+            omega = omega / gamma;
+            axpy(n, x, st, omega);
+            axpy(n, x, pt, alpha);
+            axpy3(n, r, s, t, -omega);
+            defnorm = hbo_dot_f64(n, r, r);
+            if (defnorm < eps * defnorm_00) { converged = 1; break; }
+            axpy3(n, rt, st, tt, -omega);
+            rho_old = rho;
+            rho = hbo_dot_f64(n, rt, rt0);
+            beta = (alpha / omega) * (rho / rho_old);
+            axpy(n, pt, vt, -omega);
+            for (uint64_t i = 0; i < n; ++i) pt[i] = pt[i] * beta;
+            for (uint64_t i = 0; i < n; ++i) pt[i] = pt[i] + rt[i];
+        } while (iter <= max_iters);
+    } while (converged == 0 && iter < max_iters);
+    (void)defnorm;
+    for (int i = 0; i < 10; ++i) free(vec[i]);
+    ell_free_f64(&A);
+    if (! pdiag) ell_free_f64(&P);
+    return iter + 1;
+}

@@ -69,6 +69,10 @@ def lib():
         for sfx in ("f64", "f32"):
             getattr(L, "hbo_csr_spmv_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, _ptr, _ptr]
             getattr(L, "hbo_csr_defect_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, _ptr, _ptr, _ptr]
+        for f in ("hbo_cgvar_f64", "hbo_bicgstab_f64"):
+            getattr(L, f).restype = _u64
+        L.hbo_cgvar_f64.argtypes = [_ptr, _ptr, _ptr, _ptr, _ptr, _u64, _dbl, ctypes.c_int]
+        L.hbo_bicgstab_f64.argtypes = [_ptr, _ptr, _ptr, _ptr, _ptr, _u64, _dbl]
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
@@ -431,3 +435,75 @@ def csr_defect(A: Csr, rhs: np.ndarray, x: np.ndarray) -> np.ndarray:
                                                        _p(np.ascontiguousarray(rhs, A.dtype)),
                                                        _p(np.ascontiguousarray(x, A.dtype)), _p(r))
     return r
+
+
+def _precon_args(P):
+    """P: a numpy vector (diagonal) or an Ell matrix"""
+    if isinstance(P, np.ndarray):
+        return _p(np.ascontiguousarray(P, np.float64)), None, P
+    return None, _views([P]), P
+
+
+def cg_var(A: Ell, P, b, x0=None, max_iters=1000, eps=1e-8, smoother=False):
+    """CGSolver<Tag, methods::VAR> (or CGSmoother); returns (x, used_iters)."""
+    x = np.zeros(A.rows) if x0 is None else np.array(x0, np.float64)
+    pd, pv, keep = _precon_args(P)
+    it = lib().hbo_cgvar_f64(_views([A]), pd, pv, _p(np.ascontiguousarray(b, np.float64)), _p(x), max_iters, eps,
+                             int(smoother))
+    return x, int(it)
+
+
+def bicgstab(A: Ell, P, b, x0=None, max_iters=1000, eps=1e-8):
+    """BiCGStabSolver<Tag, methods::VAR>; returns (x, used_iters)."""
+    x = np.zeros(A.rows) if x0 is None else np.array(x0, np.float64)
+    pd, pv, keep = _precon_args(P)
+    it = lib().hbo_bicgstab_f64(_views([A]), pd, pv, _p(np.ascontiguousarray(b, np.float64)), _p(x), max_iters, eps)
+    return x, int(it)
+
+
+def jacobi_vector(A: Ell) -> np.ndarray:
+    """DenseVector(n, 1) then /= A(j, j) (math/mg.hh:266-273 with damping 1)"""
+    d = np.zeros(A.rows)
+    S = A.stride
+    for k in range(A.K):
+        sl = slice(k * S, k * S + A.rows)
+        hit = (A.Aj[sl] == np.arange(A.rows, dtype=np.uint64)) & (np.arange(A.rows) >= 0)
+        hit &= k < A.Arl.astype(np.int64)
+        d[hit] = A.Ax[sl][hit]
+    return 1.0 / d
+
+
+def neumann2(A: Ell) -> Ell:
+    """P = 2 D^-1 - D^-1 A D^-1 on A's pattern, as the reference driver's krylov case
+    builds it: p_rc = -(a_rc / (a_rr a_cc)), plus 2 / a_rr on the diagonal; rows in
+    ascending column order, zeros dropped (then SparseMatrixELL(SparseMatrix))."""
+    diag = 1.0 / jacobi_vector(A)
+    rows_c, rows_v = [], []
+    S = A.stride
+    for r in range(A.rows):
+        ent = {}
+        for k in range(int(A.Arl[r])):
+            c, a = int(A.Aj[r + k * S]), A.Ax[r + k * S]
+            if a != 0:
+                ent[c] = a
+        cs, vs = [], []
+        for c in sorted(ent):
+            v = -(ent[c]) / (diag[r] * diag[c])
+            if c == r:
+                v += 2.0 / diag[r]
+            if v != 0.0:
+                cs.append(c)
+                vs.append(v)
+        rows_c.append(cs)
+        rows_v.append(vs)
+    K = max([1] + [len(c) for c in rows_c])
+    stride = 32 * ((A.rows + 31) // 32)
+    Aj = np.zeros(K * stride, np.uint64)
+    Ax = np.zeros(K * stride)
+    Arl = np.zeros(A.rows, np.uint64)
+    for r in range(A.rows):
+        Arl[r] = len(rows_c[r])
+        for k, (c, v) in enumerate(zip(rows_c[r], rows_v[r])):
+            Aj[r + k * stride] = c
+            Ax[r + k * stride] = v
+    return Ell(A.rows, A.cols, stride, K, 1, Aj, Ax, Arl)

@@ -5,6 +5,8 @@
 //       writes golden fixtures computed by the reference's tags::CPU code
 //       (raw little-endian arrays + scalars.txt); tests/golden/make_golden.py
 //       packs them into the committed fixtures.
+//   honei_ref krylov <outdir>
+//       CGSolver VAR, BiCGStabSolver VAR and CGSmoother on the Q1 operator
 //   honei_ref csr <outdir>
 //       SparseMatrixCSR arrays (csr::blocksize 1..4) and their Product / Defect
 //   honei_ref mgquad <datadir> <outdir>
@@ -23,6 +25,7 @@
 #include <honei/la/product.hh>
 #include <honei/la/scaled_sum.hh>
 #include <honei/la/sum.hh>
+#include <honei/math/bicgstab.hh>
 #include <honei/math/cg.hh>
 #include <honei/math/defect.hh>
 #include <honei/math/ir.hh>
@@ -529,8 +532,76 @@ namespace
     }
 }
 
+namespace
+{
+    // P = 2 D^-1 - D^-1 A D^-1 (two terms of the Neumann series of A^-1 around
+    // its diagonal D), on A's pattern
+    SparseMatrixELL<double> neumann2(const SparseMatrixELL<double> & A)
+    {
+        SparseMatrix<double> S(A);
+        SparseMatrix<double> P(A.rows(), A.columns());
+        for (unsigned long r(0); r < A.rows(); ++r)
+            for (typename SparseVector<double>::NonZeroConstElementIterator i(S[r].begin_non_zero_elements()),
+                     i_end(S[r].end_non_zero_elements()); i != i_end; ++i)
+            {
+                const unsigned long c(i.index());
+                double v = -(*i) / (S(r, r) * S(c, c));
+                if (c == r) v += 2.0 / S(r, r);
+                if (v != 0.0) P(r, c, v);
+            }
+        return SparseMatrixELL<double>(P);
+    }
+
+    template <typename Solver_, typename PT_>
+    void krylov_case(const std::string & name, SparseMatrixELL<double> & A, PT_ & P, DenseVector<double> & b)
+    {
+        DenseVector<double> x(A.rows(), 0.0);
+        unsigned long used(0);
+        Solver_::value(A, P, b, x, 1000ul, used, 1e-8);
+        put_vec(name + ".x", x);
+        scalars << name << ".iters " << used << "\n" << name << ".relres " << rel_residual(A, b, x) << "\n";
+    }
+
+    // CGSolver<tags::CPU, methods::VAR> (math/cg.hh:142-210), BiCGStabSolver<tags::CPU,
+    // methods::VAR> (math/bicgstab.hh:60-210) and CGSmoother (math/cg.hh:217-290) on the
+    // Q1 operator, b = A u, x0 = 0, eps 1e-8, 1000 iterations at most; P the Jacobi
+    // vector 1 / diag(A) or the ELL matrix neumann2(A)
+    int krylov()
+    {
+        scalars.open((outdir + "/scalars.txt").c_str());
+        scalars.precision(17);
+        for (unsigned L(5); L <= 6; ++L)
+        {
+            SparseMatrixELL<double> A(q1_ell_assembled<double>(L));
+            DenseVector<double> u(uniform<double>(A.rows(), 42)), b(A.rows());
+            Product<tags::CPU>::value(b, A, u);
+            put_vec(key("kr_L%u.b", L), b);
+            DenseVector<double> Pj(A.rows(), 1.0);
+            for (unsigned long j(0); j < Pj.size(); ++j) Pj[j] /= A(j, j);
+            SparseMatrixELL<double> Pn(neumann2(A));
+            put_ell(key("kr_L%u.Pn", L), Pn);
+            krylov_case<CGSolver<tags::CPU, methods::VAR> >(key("kr_L%u.cgvar_jac", L), A, Pj, b);
+            krylov_case<CGSolver<tags::CPU, methods::VAR> >(key("kr_L%u.cgvar_neu", L), A, Pn, b);
+            krylov_case<BiCGStabSolver<tags::CPU, methods::VAR> >(key("kr_L%u.bicg_jac", L), A, Pj, b);
+            krylov_case<BiCGStabSolver<tags::CPU, methods::VAR> >(key("kr_L%u.bicg_neu", L), A, Pn, b);
+            // CGSmoother: 5 iterations from x0 = 0
+            std::vector<DenseVector<double> > tmp;
+            for (int i(0); i < 4; ++i) tmp.push_back(DenseVector<double>(A.rows(), 0.0));
+            DenseVector<double> xs(A.rows(), 0.0);
+            CGSmoother<tags::CPU>::value(A, Pj, b, xs, tmp, 5ul);
+            put_vec(key("kr_L%u.cgsmooth_jac.x", L), xs);
+        }
+        return 0;
+    }
+}
+
 int main(int argc, char ** argv)
 {
+    if (argc >= 3 && std::string(argv[1]) == "krylov")
+    {
+        outdir = argv[2];
+        return krylov();
+    }
     if (argc >= 4 && std::string(argv[1]) == "mgquad") return mgquad(argv[2], argv[3]);
     if (argc >= 3 && std::string(argv[1]) == "csr")
     {
