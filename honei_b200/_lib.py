@@ -58,6 +58,13 @@ class MgParams(ctypes.Structure):
                 ("coarse_exact", _int), ("no_fused_levels", _int), ("coarse_fp64", _int), ("cycle", _int)]
 
 
+class MGInfoParams(ctypes.Structure):
+    """hb2_lmg_params (MGInfo, math/multigrid.hh:65-149)"""
+    _fields_ = [("n_max_iter", _u64), ("initial_zero", _int), ("convergence_check", _int), ("is_smoother", _int),
+                ("tolerance", _dbl), ("n_pre_smooth", _u64), ("adapt_correction_factor", _dbl), ("omega", _dbl),
+                ("macro_border_mask", _u64 * 8)]
+
+
 class BatchParams(ctypes.Structure):
     """hb2_batch_params"""
     _fields_ = [("max_iters", _u64), ("eps_relative", _dbl), ("n_pre_smooth", _u64), ("n_post_smooth", _u64),
@@ -80,6 +87,9 @@ SIGNATURES = {
     "hb2_ell_read": (_int, [_pvp, ctypes.c_char_p, _int, _vp]),
     "hb2_ell_write": (_int, [_vp, ctypes.c_char_p]),
     "hb2_ell_transpose": (_int, [_pvp, _vp, _vp]),
+    "hb2_lmg_create": (_int, [_pvp, ctypes.c_uint, ctypes.c_uint, _vp, _vp, _vp]),
+    "hb2_lmg_destroy": (_int, [_vp]),
+    "hb2_lmg_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "hb2_krylov_create": (_int, [_pvp, _int, _vp, _vp, _vp, _u64, _dbl, _vp]),
     "hb2_krylov_destroy": (_int, [_vp]),
     "hb2_krylov_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),

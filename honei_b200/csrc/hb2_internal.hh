@@ -212,6 +212,11 @@ namespace hb2
     // BLAS-1 helpers (blas1.cu) usable from other translation units.
     int launch_fill(int dt, void * x, double value, uint64_t n, cudaStream_t stream);
     int launch_copy(int dt, void * dst, const void * src, uint64_t n, cudaStream_t stream);
+
+    // banded Q1 kernels (q1.cu): mode 0 y = A x, 1 y = rhs - A x, 2 the Jacobi sweep
+    // y = x + (rhs - A x) (.) dinv (y != x); err: device flag of the bounded copy wait
+    int launch_q1(const hb2_q1_s * A, int mode, const void * x, void * y, const void * rhs, const void * dinv,
+                  int * err, cudaStream_t stream);
     int launch_norm(int dt, const void * x, uint64_t n, int root, double * dev_out, const Workspace * ws,
                     cudaStream_t stream);
     int launch_convert(int dst_dt, void * dst, int src_dt, const void * src, uint64_t n, cudaStream_t stream);

@@ -65,10 +65,12 @@ namespace hb2
         int64_t lo, hi; // valid global range [lo, hi)
     };
 
-    template <typename T, bool DEFECT>
+    // MODE 0: y = A x; 1: y = rhs - A x; 2 (Jacobi, math/jacobi.hh MG variant):
+    // y = x + (rhs - A x) (.) dinv, each product, sum and difference rounded
+    template <typename T, int MODE>
     __global__ void __launch_bounds__(kQ1Threads)
     q1_kernel(const T * __restrict__ bands, const T * __restrict__ x, T * __restrict__ y, const T * __restrict__ rhs,
-              int64_t n, int64_t m, int * err)
+              const T * __restrict__ dinv, int64_t n, int64_t m, int * err)
     {
         typedef Arith<T> M;
         constexpr int R = RowsPerThread<T>::value;
@@ -130,14 +132,16 @@ namespace hb2
                 const int w = b / 3;
                 s = M::add(s, M::mul(__ldcs(bands + b * n + i), win[w][j - base[w]]));
             }
-            y[i] = DEFECT ? M::sub(rhs[i], s) : s;
+            if (MODE == 0) y[i] = s;
+            else if (MODE == 1) y[i] = M::sub(rhs[i], s);
+            else y[i] = M::add(win[1][i - base[1]], M::mul(M::sub(rhs[i], s), dinv[i]));
         }
     }
 
     // plain-load variant for x pointers that are not 16-byte aligned
-    template <typename T, bool DEFECT>
+    template <typename T, int MODE>
     __global__ void q1_kernel_direct(const T * __restrict__ bands, const T * __restrict__ x, T * __restrict__ y,
-                                     const T * __restrict__ rhs, int64_t n, int64_t m)
+                                     const T * __restrict__ rhs, const T * __restrict__ dinv, int64_t n, int64_t m)
     {
         typedef Arith<T> M;
         const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -151,7 +155,9 @@ namespace hb2
             if (j < 0 || j >= n) continue;
             s = M::add(s, M::mul(bands[b * n + i], __ldg(x + j)));
         }
-        y[i] = DEFECT ? M::sub(rhs[i], s) : s;
+        if (MODE == 0) y[i] = s;
+        else if (MODE == 1) y[i] = M::sub(rhs[i], s);
+        else y[i] = M::add(x[i], M::mul(M::sub(rhs[i], s), dinv[i]));
     }
 
     template <typename T>
@@ -173,52 +179,57 @@ namespace hb2
         }
     }
 
-    static int q1_launch(const hb2_q1_s * A, const void * x, void * y, const void * rhs, bool defect,
-                         cudaStream_t stream)
+    template <typename T, int MODE>
+    static void q1_launch_typed(const hb2_q1_s * A, const void * x, void * y, const void * rhs, const void * dinv,
+                                int * err, cudaStream_t stream)
     {
-        if (A->n == 0) return HB2_OK;
-        const bool aligned = ((uintptr_t)x % 16) == 0;
-        int * err = 0;
-        Workspace * ws = 0;
-        int st = stream_workspace(stream, &ws);
-        if (st) return st;
-        err = ws->error;
         const int64_t n = (int64_t)A->n, m = (int64_t)A->m;
-        if (A->dtype == HB2_F64)
+        const T * b = (const T *)A->bands;
+        if (((uintptr_t)x % 16) == 0)
         {
-            const double * b = (const double *)A->bands;
-            if (aligned)
-            {
-                unsigned grid = ceil_div(A->n, kQ1Threads * RowsPerThread<double>::value);
-                if (defect) q1_kernel<double, true><<<grid, kQ1Threads, 0, stream>>>(b, (const double *)x, (double *)y, (const double *)rhs, n, m, err);
-                else q1_kernel<double, false><<<grid, kQ1Threads, 0, stream>>>(b, (const double *)x, (double *)y, 0, n, m, err);
-            }
-            else
-            {
-                unsigned grid = ceil_div(A->n, 256);
-                if (defect) q1_kernel_direct<double, true><<<grid, 256, 0, stream>>>(b, (const double *)x, (double *)y, (const double *)rhs, n, m);
-                else q1_kernel_direct<double, false><<<grid, 256, 0, stream>>>(b, (const double *)x, (double *)y, 0, n, m);
-            }
+            const unsigned grid = ceil_div(A->n, kQ1Threads * RowsPerThread<T>::value);
+            q1_kernel<T, MODE><<<grid, kQ1Threads, 0, stream>>>(b, (const T *)x, (T *)y, (const T *)rhs,
+                                                                (const T *)dinv, n, m, err);
         }
         else
         {
-            const float * b = (const float *)A->bands;
-            if (aligned)
-            {
-                unsigned grid = ceil_div(A->n, kQ1Threads * RowsPerThread<float>::value);
-                if (defect) q1_kernel<float, true><<<grid, kQ1Threads, 0, stream>>>(b, (const float *)x, (float *)y, (const float *)rhs, n, m, err);
-                else q1_kernel<float, false><<<grid, kQ1Threads, 0, stream>>>(b, (const float *)x, (float *)y, 0, n, m, err);
-            }
-            else
-            {
-                unsigned grid = ceil_div(A->n, 256);
-                if (defect) q1_kernel_direct<float, true><<<grid, 256, 0, stream>>>(b, (const float *)x, (float *)y, (const float *)rhs, n, m);
-                else q1_kernel_direct<float, false><<<grid, 256, 0, stream>>>(b, (const float *)x, (float *)y, 0, n, m);
-            }
+            const unsigned grid = ceil_div(A->n, 256);
+            q1_kernel_direct<T, MODE><<<grid, 256, 0, stream>>>(b, (const T *)x, (T *)y, (const T *)rhs,
+                                                                (const T *)dinv, n, m);
+        }
+    }
+
+    // mode 0: y = A x, 1: y = rhs - A x, 2: y = x + (rhs - A x) (.) dinv (y != x);
+    // err: device flag set when a block's bulk copies of x never completed
+    int launch_q1(const hb2_q1_s * A, int mode, const void * x, void * y, const void * rhs, const void * dinv,
+                  int * err, cudaStream_t stream)
+    {
+        if (A->n == 0) return HB2_OK;
+        if (A->dtype == HB2_F64)
+        {
+            if (mode == 0) q1_launch_typed<double, 0>(A, x, y, rhs, dinv, err, stream);
+            else if (mode == 1) q1_launch_typed<double, 1>(A, x, y, rhs, dinv, err, stream);
+            else q1_launch_typed<double, 2>(A, x, y, rhs, dinv, err, stream);
+        }
+        else
+        {
+            if (mode == 0) q1_launch_typed<float, 0>(A, x, y, rhs, dinv, err, stream);
+            else if (mode == 1) q1_launch_typed<float, 1>(A, x, y, rhs, dinv, err, stream);
+            else q1_launch_typed<float, 2>(A, x, y, rhs, dinv, err, stream);
         }
         count_launches(1);
         HB2_LAUNCH_CHECK("q1 kernel launch");
         return HB2_OK;
+    }
+
+    static int q1_launch(const hb2_q1_s * A, const void * x, void * y, const void * rhs, bool defect,
+                         cudaStream_t stream)
+    {
+        if (A->n == 0) return HB2_OK;
+        Workspace * ws = 0;
+        int st = stream_workspace(stream, &ws);
+        if (st) return st;
+        return launch_q1(A, defect ? 1 : 0, x, y, rhs, nullptr, ws->error, stream);
     }
 }
 

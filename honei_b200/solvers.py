@@ -1,8 +1,8 @@
 """HONEI's solver layer for the B200 tag: grid transfer, smoother, CG (NONE and
-VAR), CGSmoother, BiCGStab, MG, IR.
+VAR), CGSmoother, BiCGStab, MG, the legacy banded Multigrid, IR.
 
 Mirrors math/prolongation.hh, math/restriction.hh, math/ri.hh, math/cg.hh,
-math/bicgstab.hh, math/mg.hh and math/ir.hh.  Each solver is one call into libhonei_b200.so; the
+math/bicgstab.hh, math/mg.hh, math/multigrid.hh and math/ir.hh.  Each solver is one call into libhonei_b200.so; the
 MG cycle runs as a captured CUDA graph.
 """
 from __future__ import annotations
@@ -167,6 +167,53 @@ class CGSmoother:
     @staticmethod
     def value(A, P, b, x, max_iters, stream=None):
         return KrylovSolver(HB2_CG_SMOOTHER, A, P, max_iters, 0.0, stream).solve(b, x, stream)[0]
+
+
+def mg_info(n_max_iter=16, initial_zero=True, convergence_check=False, is_smoother=False, tolerance=1e-8,
+            n_pre_smooth=2, adapt_correction_factor=1.0, omega=0.7, macro_border_mask=None) -> _lib.MGInfoParams:
+    """MGInfo of the legacy Multigrid (math/multigrid.hh:65-149); defaults of the reference's
+    banded tests (math/poisson_mg_double_banded_TEST.cc).  omega scales the inverted diagonal."""
+    mask = ALL_DIRICHLET if macro_border_mask is None else np.asarray(macro_border_mask, np.uint64)
+    p = _lib.MGInfoParams(n_max_iter, int(initial_zero), int(convergence_check), int(is_smoother), tolerance,
+                          n_pre_smooth, adapt_correction_factor, omega)
+    for i in range(8):
+        p.macro_border_mask[i] = int(mask[i])
+    return p
+
+
+class Multigrid:
+    """Multigrid<tags::B200, tags::B200, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>
+    on BandedMatrixQx (math/multigrid.hh:151-466, 781-825), resident on the device.
+
+    ``Multigrid(A, min_level, info)``: A lists the banded matrices of levels min_level ..
+    max_level, coarsest first.  ``value(b, x)`` solves from x and returns (x, cycles, defect)."""
+
+    def __init__(self, A, min_level, info: _lib.MGInfoParams | None = None, stream=None):
+        self.info = info or mg_info()
+        self._keep = list(A)
+        arr = (ctypes.c_void_p * len(A))(*[m.handle.value for m in A])
+        h = ctypes.c_void_p()
+        call("hb2_lmg_create", ctypes.byref(h), int(min_level), int(min_level) + len(A) - 1, arr,
+             ctypes.byref(self.info), _stream(stream))
+        self._h = h
+        self.n = A[-1].rows()
+
+    def value(self, b, x, stream=None):
+        b, x = _vec(b), _vec(x)
+        _check_size(b.size(), self.n)
+        _check_size(x.size(), self.n)
+        cycles = ctypes.c_uint64()
+        defect = ctypes.c_double()
+        call("hb2_lmg_solve", self._h, b.ptr, x.ptr, ctypes.byref(cycles), ctypes.byref(defect), _stream(stream))
+        return x, cycles.value, defect.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.load().hb2_lmg_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
 
 
 def mg_params(n_pre=4, n_post=4, max_iters=100, max_iters_coarse=100, eps=1e-10, coarse_eps=None, omega=0.7,

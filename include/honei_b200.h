@@ -68,6 +68,7 @@ typedef struct hb2_mg_s *hb2_mg;   /* MGData + V-cycle OperatorList resident on 
 typedef struct hb2_batch_s *hb2_batch; /* many Q1 systems solved together (batched PCG) */
 typedef struct hb2_csr_s *hb2_csr; /* SparseMatrixCSR<DT> resident on the device */
 typedef struct hb2_krylov_s *hb2_krylov; /* a Krylov solver with its vectors and CUDA graph */
+typedef struct hb2_lmg_s *hb2_lmg; /* the legacy banded multigrid solver (MGInfo + its CUDA graph) */
 
 /* ---------------------------------------------------------------- runtime */
 HB2_API const char *hb2_last_error(void);
@@ -278,6 +279,33 @@ HB2_API int hb2_krylov_destroy(hb2_krylov K);
  * Norm<vnt_l_two, false>), 0 (smoother).  Synchronises `stream`. */
 HB2_API int hb2_krylov_solve(hb2_krylov K, const void *b, void *x, uint64_t *used_iters, double *final_defect,
                      cudaStream_t stream);
+
+/* The legacy multigrid solver Multigrid<Tag, OuterTag, methods::NONE, methods::JAC,
+ * methods::CYCLE::V, methods::FIXED> on BandedMatrixQx (math/multigrid.hh:151-466,
+ * 781-825): its MGInfo configuration (math/multigrid.hh:65-149); the levels'
+ * diags_inverted are built as the reference's tests build them, omega * (1 / DD). */
+typedef struct
+{
+    uint64_t n_max_iter;               /* 16: cycles at most */
+    int initial_zero;                  /* 1: d = b (the initial guess is not applied to the defect) */
+    int convergence_check;             /* 0: skip the solve when ||d0|| <= tolerance */
+    int is_smoother;                   /* 0: 1 = no norms, exactly n_max_iter cycles */
+    double tolerance;                  /* 1e-8: stop when ||d|| <= ||d0|| * tolerance */
+    uint64_t n_pre_smooth;             /* 2: Jacobi sweeps before and after the coarse correction */
+    double adapt_correction_factor;    /* 1.0: x += factor * P x(coarser) */
+    double omega;                      /* 0.7 */
+    uint64_t macro_border_mask[8];     /* 2 = Dirichlet, 1 = Neumann (edges and corners) */
+} hb2_lmg_params;
+/* A: max_level - min_level + 1 banded matrices, levels min_level (>= 1) .. max_level,
+ * one element type; the handle keeps references to them. */
+HB2_API int hb2_lmg_create(hb2_lmg *out, unsigned min_level, unsigned max_level, const hb2_q1 *A,
+                   const hb2_lmg_params *params, cudaStream_t stream);
+HB2_API int hb2_lmg_destroy(hb2_lmg mg);
+/* Multigrid::value(system, b, x, ...): b, x device vectors of the finest level (x:
+ * initial guess in -- its first row, last row and first column replaced by b's values
+ * -- result out).  cycles: cycles run; defect: the last ||d|| of the finest level.
+ * Synchronises `stream`. */
+HB2_API int hb2_lmg_solve(hb2_lmg mg, const void *b, void *x, uint64_t *cycles, double *defect, cudaStream_t stream);
 
 /* MG hierarchy: MGData (math/mg.hh:57-240) + MGCycleCreation<V::STATIC,
  * CGSolver<NONE>, RISmoother, Restriction<PROLMAT>, Prolongation<PROLMAT>>

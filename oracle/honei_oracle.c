@@ -888,3 +888,134 @@ uint64_t hbo_bicgstab_f64(const hbo_ell_view *Av, const double *pdiag, const hbo
     if (! pdiag) ell_free_f64(&P);
     return iter + 1;
 }
+
+/* ---- legacy Multigrid<Tag, OuterTag, NONE, JAC, CYCLE::V, FIXED> on BandedMatrixQx ---- */
+/* math/conjugate_gradients.hh:491-560 with the banded cg_kernel (:108-151): x = 0,
+ * g = A x - b, u = -g; while ||x||^2 grows by more than konv_rad: one CG step with
+ * the gradient recomputed as A x - b.  Norm<l2, false> = the fma dot of x with itself.
+ * A cap of 100000 steps guards the loop (the reference has none). */
+#define DEFINE_LMG(T_, SFX, EPS_MACH)                                               \
+static uint64_t lmg_cg_##SFX(uint64_t n, uint64_t m, const T_ *bands, const T_ *rhs, \
+                             T_ *x, double konv_rad)                                \
+{                                                                                   \
+    T_ *ng = (T_ *)malloc(sizeof(T_) * n), *g = (T_ *)malloc(sizeof(T_) * n);       \
+    T_ *u = (T_ *)malloc(sizeof(T_) * n), *e = (T_ *)malloc(sizeof(T_) * n);        \
+    for (uint64_t i = 0; i < n; ++i) x[i] = 0;                                      \
+    hbo_q1_spmv_##SFX(n, m, bands, x, g);                                           \
+    for (uint64_t i = 0; i < n; ++i) g[i] = g[i] - rhs[i];                          \
+    for (uint64_t i = 0; i < n; ++i) u[i] = g[i] * (T_)-1;                          \
+    T_ norm_x = hbo_dot_##SFX(n, x, x), norm_x_last = (T_)(norm_x - 1);             \
+    uint64_t it = 0;                                                                \
+    while (norm_x - norm_x_last > konv_rad && it < 100000) {                        \
+        T_ upper = hbo_dot_##SFX(n, g, g);                                          \
+        hbo_q1_spmv_##SFX(n, m, bands, u, e);                                       \
+        T_ lower = hbo_dot_##SFX(n, e, u);                                          \
+        T_ f = fabs(lower) >= EPS_MACH ? upper / lower : upper / EPS_MACH;          \
+        for (uint64_t i = 0; i < n; ++i) { e[i] = u[i] * f; e[i] = e[i] + x[i]; }   \
+        lower = upper;                                                              \
+        hbo_q1_spmv_##SFX(n, m, bands, e, ng);                                      \
+        for (uint64_t i = 0; i < n; ++i) ng[i] = ng[i] - rhs[i];                    \
+        upper = hbo_dot_##SFX(n, ng, ng);                                           \
+        f = fabs(lower) >= EPS_MACH ? upper / lower : upper / EPS_MACH;             \
+        for (uint64_t i = 0; i < n; ++i) { u[i] = u[i] * f; u[i] = u[i] - ng[i]; }  \
+        memcpy(g, ng, sizeof(T_) * n);                                              \
+        memcpy(x, e, sizeof(T_) * n);                                               \
+        norm_x_last = norm_x;                                                       \
+        norm_x = hbo_dot_##SFX(n, x, x);                                            \
+        ++it;                                                                       \
+    }                                                                               \
+    free(ng); free(g); free(u); free(e);                                            \
+    return it;                                                                      \
+}                                                                                   \
+                                                                                    \
+/* math/jacobi.hh (the MG variants): x = d^-1 (.) b, then sweeps of                \
+ * t = b - A x; x += t (.) d^-1 (in place, t computed from the whole old x) */      \
+static void lmg_sweeps_##SFX(uint64_t n, uint64_t m, const T_ *bands, const T_ *b,  \
+                             T_ *x, const T_ *dinv, uint64_t sweeps, T_ *t)         \
+{                                                                                   \
+    for (uint64_t s = 0; s < sweeps; ++s) {                                         \
+        hbo_q1_defect_##SFX(n, m, bands, b, x, t);                                  \
+        for (uint64_t i = 0; i < n; ++i) x[i] = x[i] + t[i] * dinv[i];              \
+    }                                                                               \
+}                                                                                   \
+                                                                                    \
+/* Multigrid<..., JAC, CYCLE::V, FIXED>::value (math/multigrid.hh:781-825) and its  \
+ * banded _multigrid_kernel (:159-466).  Levels lmin..lmax (lmin >= 1):             \
+ * bands[l] band-major LL..UU, n = (2^l + 1)^2; dinv[l] the inverted diagonal       \
+ * scaled as the caller chose; rhs: the finest right-hand side; x: initial guess in, \
+ * result out.  Returns the cycles run. */                                          \
+uint64_t hbo_lmg_##SFX(unsigned lmin, unsigned lmax, const T_ *const *bands,        \
+                       const T_ *const *dinv, const T_ *rhs_in, T_ *x_io,           \
+                       uint64_t n_max_iter, int initial_zero, int convergence_check, \
+                       int is_smoother, double tolerance, uint64_t n_pre,           \
+                       double adapt, const uint64_t *mask)                          \
+{                                                                                   \
+    T_ *x[32], *c[32], *d[32], *rhs[32], *t[32];                                    \
+    uint64_t N[32], M[32];                                                          \
+    for (unsigned l = lmin; l <= lmax; ++l) {                                       \
+        M[l] = ((uint64_t)1 << l) + 1; N[l] = M[l] * M[l];                           \
+        x[l] = (T_ *)calloc(N[l], sizeof(T_)); c[l] = (T_ *)calloc(N[l], sizeof(T_)); \
+        d[l] = (T_ *)calloc(N[l], sizeof(T_)); rhs[l] = (T_ *)calloc(N[l], sizeof(T_)); \
+        t[l] = (T_ *)calloc(N[l], sizeof(T_));                                      \
+    }                                                                               \
+    const unsigned L = lmax;                                                        \
+    const uint64_t n = N[L], sq = M[L];                                             \
+    memcpy(rhs[L], rhs_in, sizeof(T_) * n);                                         \
+    /* value(): Dirichlet values of b on the first row, the last row and the first column */ \
+    memcpy(x[L], x_io, sizeof(T_) * n);                                             \
+    for (uint64_t i = 0; i < sq; ++i) x[L][i] = rhs_in[i];                          \
+    for (uint64_t i = n - sq; i < n; ++i) x[L][i] = rhs_in[i];                      \
+    for (uint64_t i = 0; i < n; i += sq) x[L][i] = rhs_in[i];                       \
+    if (initial_zero) memcpy(d[L], rhs[L], sizeof(T_) * n);                         \
+    else hbo_q1_defect_##SFX(n, M[L], bands[L], rhs[L], x[L], d[L]);                \
+    T_ defect, initial;                                                             \
+    if (! is_smoother) { defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L])); initial = defect; } \
+    else { defect = (T_)1e8; initial = defect; }                                    \
+    uint64_t iter = 0, cycles = 0;                                                  \
+    if (! (convergence_check && defect <= (T_)tolerance)) {                         \
+        for (iter = 1; iter <= n_max_iter; ++iter) {                                \
+            unsigned l = L;                                                         \
+            int started = 1;                                                        \
+            cycles = iter;                                                          \
+            while (lmin != L) {                                                     \
+                if (started) {                                                      \
+                    for (uint64_t i = 0; i < N[l]; ++i) c[l][i] = dinv[l][i] * d[l][i]; \
+                    lmg_sweeps_##SFX(N[l], M[l], bands[l], d[l], c[l], dinv[l], n_pre - 1, t[l]); \
+                    for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = x[l][i] + c[l][i];  \
+                } else {                                                            \
+                    for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = dinv[l][i] * d[l][i]; \
+                    lmg_sweeps_##SFX(N[l], M[l], bands[l], d[l], x[l], dinv[l], n_pre - 1, t[l]); \
+                }                                                                   \
+                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
+                --l;                                                                \
+                hbo_restriction_##SFX(N[l], d[l], N[l + 1], d[l + 1], mask);        \
+                memcpy(rhs[l], d[l], sizeof(T_) * N[l]);                            \
+                if (l == lmin) break;                                               \
+                started = 0;                                                        \
+            }                                                                       \
+            lmg_cg_##SFX(N[l], M[l], bands[l], d[l], x[l], (double)EPS_MACH);       \
+            if (lmin == L) {                                                        \
+                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
+                break;                                                              \
+            }                                                                       \
+            while (1) {                                                             \
+                ++l;                                                                \
+                hbo_prolongation_##SFX(N[l], c[l], N[l - 1], x[l - 1], mask);       \
+                const T_ alpha = (T_)adapt;                                         \
+                for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = x[l][i] + alpha * c[l][i]; \
+                lmg_sweeps_##SFX(N[l], M[l], bands[l], rhs[l], x[l], dinv[l], n_pre, t[l]); \
+                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
+                if (l == L) break;                                                  \
+            }                                                                       \
+            if (! is_smoother) {                                                    \
+                defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L]));                    \
+                if (defect <= initial * (T_)tolerance) break;                       \
+            }                                                                       \
+        }                                                                           \
+    }                                                                               \
+    memcpy(x_io, x[L], sizeof(T_) * n);                                             \
+    for (unsigned l = lmin; l <= lmax; ++l) { free(x[l]); free(c[l]); free(d[l]); free(rhs[l]); free(t[l]); } \
+    return cycles;                                                                  \
+}
+DEFINE_LMG(double, f64, DBL_EPSILON)
+DEFINE_LMG(float, f32, FLT_EPSILON)

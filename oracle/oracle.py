@@ -73,6 +73,11 @@ def lib():
             getattr(L, f).restype = _u64
         L.hbo_cgvar_f64.argtypes = [_ptr, _ptr, _ptr, _ptr, _ptr, _u64, _dbl, ctypes.c_int]
         L.hbo_bicgstab_f64.argtypes = [_ptr, _ptr, _ptr, _ptr, _ptr, _u64, _dbl]
+        for sfx in ("f64", "f32"):
+            f = getattr(L, "hbo_lmg_" + sfx)
+            f.restype = _u64
+            f.argtypes = [ctypes.c_uint, ctypes.c_uint, _ptr, _ptr, _ptr, _ptr, _u64, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, _dbl, _u64, _dbl, _ptr]
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
@@ -507,3 +512,46 @@ def neumann2(A: Ell) -> Ell:
             Aj[r + k * stride] = c
             Ax[r + k * stride] = v
     return Ell(A.rows, A.cols, stride, K, 1, Aj, Ax, Arl)
+
+
+def read_feast_bin(raw: bytes, dtype=np.float64):
+    """math/testdata/<n>.bin of the reference: int32 n, then n doubles each of DD LL LD LU
+    DL DU UL UD UU, b, the analytic solution and the reference solution.  Returns
+    (bands band-major LL LD LU DL DD DU UL UD UU, b, analytic, reference) in dtype."""
+    n = int(np.frombuffer(raw[:4], dtype="<i4")[0])
+    v = np.frombuffer(raw[4:4 + 8 * 12 * n], dtype="<f8").reshape(12, n)
+    order = [1, 2, 3, 4, 0, 5, 6, 7, 8]
+    bands = np.ascontiguousarray(v[order].reshape(-1)).astype(dtype)
+    return bands, v[9].astype(dtype), v[10].copy(), v[11].copy()
+
+
+def lmg_dinv(bands: np.ndarray, n: int, omega=0.7) -> np.ndarray:
+    """the reference tests' diags_inverted: ElementInverse(DD) then Scale by omega, in dtype"""
+    dt = bands.dtype.type
+    dd = bands[4 * n:5 * n]
+    inv = np.where(dd == 0, dt(0), dt(1) / np.where(dd == 0, dt(1), dd)).astype(bands.dtype)
+    return (inv * dt(omega)).astype(bands.dtype)
+
+
+def legacy_mg(bands_by_level: dict, rhs, x0, n_max_iter=16, initial_zero=True, convergence_check=False,
+              is_smoother=False, tolerance=1e-8, n_pre=2, adapt=1.0, mask=ALL_DIRICHLET, dinv_by_level=None):
+    """Multigrid<..., JAC, CYCLE::V, FIXED> on banded Q1 levels {level: bands}; returns (x, cycles)."""
+    levels = sorted(bands_by_level)
+    lmin, lmax = levels[0], levels[-1]
+    dt = bands_by_level[lmax].dtype
+    keep = []
+    bp = (_ptr * 32)()
+    dp = (_ptr * 32)()
+    for l in levels:
+        b = np.ascontiguousarray(bands_by_level[l], dt)
+        n = b.size // 9
+        d = np.ascontiguousarray(dinv_by_level[l] if dinv_by_level else lmg_dinv(b, n), dt)
+        keep += [b, d]
+        bp[l] = _p(b).value
+        dp[l] = _p(d).value
+    x = np.array(x0, dt)
+    m = np.ascontiguousarray(np.asarray(mask, np.uint64))
+    f = getattr(lib(), "hbo_lmg_" + _sfx(dt))
+    cycles = f(lmin, lmax, bp, dp, _p(np.ascontiguousarray(rhs, dt)), _p(x), n_max_iter, int(initial_zero),
+               int(convergence_check), int(is_smoother), tolerance, n_pre, adapt, _p(m))
+    return x, int(cycles)

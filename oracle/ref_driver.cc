@@ -5,6 +5,8 @@
 //       writes golden fixtures computed by the reference's tags::CPU code
 //       (raw little-endian arrays + scalars.txt); tests/golden/make_golden.py
 //       packs them into the committed fixtures.
+//   honei_ref mglegacy <testdata dir> <outdir>
+//       Multigrid<..., JAC, CYCLE::V, FIXED> on the banded Q1 test data
 //   honei_ref krylov <outdir>
 //       CGSolver VAR, BiCGStabSolver VAR and CGSmoother on the Q1 operator
 //   honei_ref csr <outdir>
@@ -31,6 +33,7 @@
 #include <honei/math/ir.hh>
 #include <honei/math/matrix_io.hh>
 #include <honei/math/mg.hh>
+#include <honei/math/multigrid.hh>
 #include <honei/math/vector_io.hh>
 #include <honei/math/prolongation.hh>
 #include <honei/math/restriction.hh>
@@ -595,8 +598,129 @@ namespace
     }
 }
 
+namespace
+{
+    // one level of the reference's FEAST banded Q1 test data (math/testdata/<n>.bin:
+    // int32 n, then n doubles each of DD LL LD LU DL DU UL UD UU, b, the analytic
+    // and the reference solution)
+    template <typename DT_>
+    void read_bin(const std::string & dir, unsigned long n, BandedMatrixQx<Q1Type, DT_> *& A, DenseVector<DT_> & b)
+    {
+        std::string path(dir + "/" + stringify(n) + ".bin");
+        FILE * f(fopen(path.c_str(), "rb"));
+        if (! f) throw InternalError("cannot open " + path);
+        int k(0);
+        if (1 != fread(&k, sizeof(int), 1, f) || (unsigned long)k != n) throw InternalError("bad header in " + path);
+        std::vector<double> v(10 * n);
+        if (10 * n != fread(&v[0], sizeof(double), 10 * n, f)) throw InternalError("short file " + path);
+        fclose(f);
+        // file order DD LL LD LU DL DU UL UD UU; BandedMatrixQx takes LL LD LU DL DD DU UL UD UU
+        const unsigned long order[9] = {1, 2, 3, 4, 0, 5, 6, 7, 8};
+        DenseVector<DT_> band[9] = {DenseVector<DT_>(n), DenseVector<DT_>(n), DenseVector<DT_>(n), DenseVector<DT_>(n),
+                                    DenseVector<DT_>(n), DenseVector<DT_>(n), DenseVector<DT_>(n), DenseVector<DT_>(n),
+                                    DenseVector<DT_>(n)};
+        for (unsigned long q(0); q < 9; ++q)
+            for (unsigned long i(0); i < n; ++i) band[q][i] = DT_(v[order[q] * n + i]);
+        for (unsigned long i(0); i < n; ++i) b[i] = DT_(v[9 * n + i]);
+        A = new BandedMatrixQx<Q1Type, DT_>(n, band[0], band[1], band[2], band[3], band[4], band[5], band[6], band[7],
+                                            band[8]);
+    }
+
+    // The setup of math/poisson_mg_double_banded_TEST.cc (MGInfo levels 0..L, the
+    // matrices and right-hand sides of levels 1..L from the test data, diags_inverted =
+    // 0.7 / DD, zero x below the finest level) and Multigrid<tags::CPU, tags::CPU,
+    // methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value on it.
+    template <typename DT_>
+    DenseVector<DT_> legacy_mg(const std::string & dir, unsigned long L, unsigned long iters, bool initial_zero,
+                               bool convergence_check, bool is_smoother, double tolerance, unsigned long n_pre,
+                               double adapt, const unsigned long * mask, const DenseVector<DT_> & x0)
+    {
+        MGInfo<DT_, BandedMatrixQx<Q1Type, DT_> > info;
+        info.is_smoother = is_smoother;
+        for (int i(0); i < 8; ++i) info.macro_border_mask[i] = mask[i];
+        info.min_level = 1;
+        info.max_level = L;
+        info.n_max_iter = iters;
+        info.initial_zero = initial_zero;
+        info.tolerance = tolerance;
+        info.convergence_check = convergence_check;
+        info.n_pre_smooth = n_pre;
+        info.n_post_smooth = n_pre;
+        info.n_max_iter_coarse = 0;
+        info.tolerance_coarse = 1e-2;
+        info.adapt_correction_factor = adapt;
+        std::vector<BandedMatrixQx<Q1Type, DT_> *> keep;
+        for (unsigned long i(0); i <= L; ++i)
+        {
+            unsigned long size(((1ul << i) + 1) * ((1ul << i) + 1));
+            if (i == 0) size = 9;
+            DenseVector<DT_> zero(size, DT_(0));
+            info.c.push_back(zero.copy());
+            info.d.push_back(zero.copy());
+            info.x.push_back(zero.copy());
+            info.diags_inverted.push_back(zero.copy());
+            if (i < info.min_level)
+            {
+                BandedMatrixQx<Q1Type, DT_> ac(size, zero.copy(), zero.copy(), zero.copy(), zero.copy(), zero.copy(),
+                                               zero.copy(), zero.copy(), zero.copy(), zero.copy());
+                info.a.push_back(ac);
+                info.rhs.push_back(zero.copy());
+            }
+            else
+            {
+                BandedMatrixQx<Q1Type, DT_> * A(0);
+                DenseVector<DT_> b(size);
+                read_bin<DT_>(dir, size, A, b);
+                keep.push_back(A);
+                info.a.push_back(*A);
+                info.rhs.push_back(b);
+            }
+        }
+        for (unsigned long i(0); i <= L; ++i)
+        {
+            DenseVector<DT_> sdi(info.a[i].band(DD).copy());
+            ElementInverse<tags::CPU>::value(sdi);
+            Scale<tags::CPU>::value(sdi, DT_(0.7));
+            info.diags_inverted[i] = sdi.copy();
+        }
+        DenseVector<DT_> b(info.rhs[L].copy());
+        DenseVector<DT_> result(x0.copy());
+        Multigrid<tags::CPU, tags::CPU, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value(
+            info.a[L], b, result, (unsigned long)11, std::numeric_limits<DT_>::epsilon(), info);
+        for (size_t i(0); i < keep.size(); ++i) delete keep[i];
+        return result;
+    }
+
+    int mglegacy(const std::string & dir)
+    {
+        scalars.open((outdir + "/scalars.txt").c_str());
+        scalars.precision(17);
+        const unsigned long dirichlet[8] = {2, 2, 2, 2, 2, 2, 2, 2};
+        const unsigned long mixed[8] = {2, 1, 2, 1, 2, 2, 1, 2};
+        const unsigned long n5(1089);
+        // A: the reference test's configuration
+        put_vec("lmg_A.x", legacy_mg<double>(dir, 5, 16, true, false, false, 1e-8, 2, 1.0, dirichlet,
+                                             DenseVector<double>(n5, 0.0)));
+        // B: a nonzero start, V(3,3), damped correction, Neumann edges, the tolerance stop
+        put_vec("lmg_B.x", legacy_mg<double>(dir, 5, 30, false, true, false, 1e-6, 3, 0.8, mixed,
+                                             uniform<double>(n5, 5)));
+        // C: smoother mode, 3 cycles, level 4
+        put_vec("lmg_C.x", legacy_mg<double>(dir, 4, 3, true, false, true, 1e-8, 2, 1.0, dirichlet,
+                                             DenseVector<double>(289, 0.0)));
+        // D: configuration A in single precision
+        put_vec("lmg_D.x", legacy_mg<float>(dir, 5, 16, true, false, false, 1e-8, 2, 1.0, dirichlet,
+                                            DenseVector<float>(n5, 0.0f)));
+        return 0;
+    }
+}
+
 int main(int argc, char ** argv)
 {
+    if (argc >= 4 && std::string(argv[1]) == "mglegacy")
+    {
+        outdir = argv[3];
+        return mglegacy(argv[2]);
+    }
     if (argc >= 3 && std::string(argv[1]) == "krylov")
     {
         outdir = argv[2];
