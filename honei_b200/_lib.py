@@ -62,7 +62,7 @@ class MGInfoParams(ctypes.Structure):
     """hb2_lmg_params (MGInfo, math/multigrid.hh:65-149)"""
     _fields_ = [("n_max_iter", _u64), ("initial_zero", _int), ("convergence_check", _int), ("is_smoother", _int),
                 ("tolerance", _dbl), ("n_pre_smooth", _u64), ("adapt_correction_factor", _dbl), ("omega", _dbl),
-                ("macro_border_mask", _u64 * 8)]
+                ("macro_border_mask", _u64 * 8), ("adaptive", _int)]
 
 
 class BatchParams(ctypes.Structure):
@@ -90,6 +90,7 @@ SIGNATURES = {
     "hb2_lmg_create": (_int, [_pvp, ctypes.c_uint, ctypes.c_uint, _vp, _vp, _vp]),
     "hb2_lmg_destroy": (_int, [_vp]),
     "hb2_lmg_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "hb2_lmg_solve_mixed": (_int, [_vp, _vp, _vp, _vp, _u64, _vp, _vp, _vp, _vp]),
     "hb2_krylov_create": (_int, [_pvp, _int, _vp, _vp, _vp, _u64, _dbl, _vp]),
     "hb2_krylov_destroy": (_int, [_vp]),
     "hb2_krylov_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),

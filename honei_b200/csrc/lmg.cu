@@ -36,14 +36,44 @@ namespace
         double defect, initial;
         unsigned long long cycles;
         int err;            // coarse CG step cap reached
-        int pad;
+        int bc;             // 1: value()'s initial guess (b's Dirichlet values), 0: x as given
+        double dots[32][2]; // adaptive correction: <d, c>, <A c, c> per level
     };
 
     template <typename T>
-    __global__ void k_bc_init(T * x, const T * x_in, const T * rhs, uint64_t n, uint64_t sq)
+    __global__ void k_bc_init(T * x, const T * x_in, const T * rhs, uint64_t n, uint64_t sq, const LState * st)
     {
+        const bool bc = st ? st->bc != 0 : true;
         for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-            x[i] = (i < sq || i >= n - sq || i % sq == 0) ? rhs[i] : x_in[i];
+            x[i] = (bc && (i < sq || i >= n - sq || i % sq == 0)) ? rhs[i] : x_in[i];
+    }
+
+    // out0 = <a, b>, out1 = <c, b> (the adaptive correction's two dots)
+    template <typename T>
+    __global__ void __launch_bounds__(256) k_dot2(const T * a, const T * b, const T * c, uint64_t n, ReduceSlot rs,
+                                                  double * out)
+    {
+        __shared__ double scratch[32];
+        double acc0 = 0.0, acc1 = 0.0;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        {
+            acc0 = fma((double)a[i], (double)b[i], acc0);
+            acc1 = fma((double)c[i], (double)b[i], acc1);
+        }
+        const unsigned G = gridDim.x, ng = (G + kReduceGroup - 1) / kReduceGroup;
+        double v = block_sum(acc0, scratch);
+        sum_finish(v, rs.partials, rs.gpart, rs.ticket, G, blockIdx.x, out, 0, scratch);
+        v = block_sum(acc1, scratch);
+        sum_finish(v, rs.partials + G, rs.gpart + ng, rs.ticket + ng + 1, G, blockIdx.x, out + 1, 0, scratch);
+    }
+
+    // x = x + alpha c with alpha = <d, c> / <A c, c> in the vectors' type
+    template <typename T>
+    __global__ void k_axpy_adaptive(T * x, const T * c, const double * dots, uint64_t n)
+    {
+        const T alpha = Arith<T>::div((T)dots[0], (T)dots[1]);
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+            x[i] = Arith<T>::add(x[i], Arith<T>::mul(alpha, c[i]));
     }
 
     template <typename T>
@@ -170,6 +200,9 @@ namespace
     }
 
     uint32_t grid_of(uint64_t n) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 8ull * num_sms())); }
+
+    // host sources of the bc flag copy (static storage: valid while a copy is in flight)
+    const int kOne = 1, kZero = 0;
 }
 
 struct hb2_lmg_s
@@ -272,8 +305,22 @@ namespace
             st = hb2_prolongation((hb2_dtype)G->dtype, L.c, L.n, G->lev[i - 1].x, G->lev[i - 1].n,
                                   G->prm.macro_border_mask, s);
             if (st) break;
-            k_axpy<T><<<grid_of(L.n), 256, 0, s>>>((T *)L.x, (const T *)L.c, alpha, L.n);
-            count_launches(1);
+            if (G->prm.adaptive && G->prm.adapt_correction_factor == 0.0)
+            {
+                // math/multigrid.hh:1712-1721 (the MIXED kernel): alpha = <d, c> / <A c, c>
+                double * dots = G->st->dots[G->lmin + i];
+                st = launch_q1(L.A, 0, L.c, L.tmp, nullptr, nullptr, G->ws->error, s);
+                if (st) break;
+                k_dot2<T><<<grid_of(L.n), 256, 0, s>>>((const T *)L.d, (const T *)L.c, (const T *)L.tmp, L.n,
+                                                       G->ws->slot(), dots);
+                k_axpy_adaptive<T><<<grid_of(L.n), 256, 0, s>>>((T *)L.x, (const T *)L.c, dots, L.n);
+                count_launches(2);
+            }
+            else
+            {
+                k_axpy<T><<<grid_of(L.n), 256, 0, s>>>((T *)L.x, (const T *)L.c, alpha, L.n);
+                count_launches(1);
+            }
             HB2_LAUNCH_CHECK("lmg correction");
             st = sweeps<T>(G, L, L.x, L.rhs, npre, s);
             if (! st) st = launch_q1(L.A, 1, L.x, L.d, L.rhs, nullptr, G->ws->error, s);
@@ -308,7 +355,7 @@ namespace
         if (ce != cudaSuccess) return capture_fail(G, ce, "cudaGraphConditionalHandleCreate");
         // value(): the initial guess with b's values on the first row, the last row and
         // the first column; then d = b (initial_zero) or b - A x, and ||d||
-        k_bc_init<T><<<grid_of(F.n), 256, 0, G->cap>>>((T *)F.x, (const T *)G->xin, (const T *)F.rhs, F.n, F.m);
+        k_bc_init<T><<<grid_of(F.n), 256, 0, G->cap>>>((T *)F.x, (const T *)G->xin, (const T *)F.rhs, F.n, F.m, G->st);
         count_launches(1);
         int st;
         if (p.initial_zero) st = launch_copy(G->dtype, F.d, F.rhs, F.n, G->cap);
@@ -363,15 +410,16 @@ namespace
     }
 
     // diags_inverted as the reference's tests build them: ElementInverse(DD) (0 stays 0),
-    // then Scale by omega
+    // then Scale by the double omega
     template <typename T>
-    __global__ void k_dinv(T * dinv, const T * bands, uint64_t n, T omega)
+    __global__ void k_dinv(T * dinv, const T * bands, uint64_t n, double omega)
     {
         for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         {
             const T dd = bands[4 * n + i];
             const T inv = dd == T(0) ? T(0) : Arith<T>::div(T(1), dd);
-            dinv[i] = Arith<T>::mul(inv, omega);
+            // Scale<tags::CPU> with a double factor: the product formed in double
+            dinv[i] = (T)__dmul_rn((double)inv, omega);
         }
     }
 
@@ -441,7 +489,7 @@ extern "C" int hb2_lmg_create(hb2_lmg * out, unsigned min_level, unsigned max_le
                                                               params->omega);
         else
             k_dinv<float><<<grid_of(L.n), 256, 0, stream>>>((float *)L.dinv, (const float *)L.A->bands, L.n,
-                                                             (float)params->omega);
+                                                             params->omega);
         count_launches(1);
     }
     G->xin = take(nf);
@@ -462,14 +510,122 @@ extern "C" int hb2_lmg_destroy(hb2_lmg G)
     return HB2_OK;
 }
 
+namespace
+{
+    // one run of the graph: bc = 1 applies value()'s initial guess, 0 runs the kernel
+    // on x as given (the MIXED driver's persistent inner iterate)
+    int lmg_run(hb2_lmg G, const void * b, void * x, int bc, uint64_t * cycles, double * defect, cudaStream_t stream);
+}
+
 extern "C" int hb2_lmg_solve(hb2_lmg G, const void * b, void * x, uint64_t * cycles, double * defect,
                              cudaStream_t stream)
 {
     if (! G || ! b || ! x) return fail(HB2_ERR_ARG, "hb2_lmg_solve: null argument");
+    return lmg_run(G, b, x, 1, cycles, defect, stream);
+}
+
+namespace
+{
+    __global__ void k_res_update(double * res, const float * xi, double scale, uint64_t n)
+    {
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+            res[i] = __dadd_rn(res[i], __dmul_rn(scale, (double)xi[i]));
+    }
+    __global__ void k_scale64(double * v, double a, uint64_t n)
+    {
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+            v[i] = __dmul_rn(v[i], a);
+    }
+    __global__ void k_to_f32(float * o, const double * v, uint64_t n)
+    {
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+            o[i] = (float)v[i];
+    }
+
+    double host_norm(hb2_lmg G, const double * v, uint64_t n, cudaStream_t stream, int * st)
+    {
+        double * out = &G->st->dots[0][0];
+        k_norm2<double><<<grid_of(n), 256, 0, stream>>>(v, n, G->ws->slot(), out);
+        count_launches(1);
+        double h = 0;
+        cudaError_t e = cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) *st = cuda_status(e, "hb2_lmg_solve_mixed (norm)");
+        return sqrt(h);
+    }
+}
+
+extern "C" int hb2_lmg_solve_mixed(hb2_lmg G, hb2_q1 A, const void * b, void * x, uint64_t max_outer,
+                                   uint64_t * outer_steps, uint64_t * inner_cycles, double * final_defect,
+                                   cudaStream_t stream)
+{
+    if (! G || ! A || ! b || ! x) return fail(HB2_ERR_ARG, "hb2_lmg_solve_mixed: null argument");
+    if (G->dtype != HB2_F32 || A->dtype != HB2_F64)
+        return fail(HB2_ERR_ARG, "hb2_lmg_solve_mixed: an F32 hierarchy and an F64 matrix");
+    auto & F = G->lev.back();
+    if (A->n != F.n) return fail(HB2_ERR_SIZE, "hb2_lmg_solve_mixed: MatrixRowsDoNotMatch (finest level)");
+    const uint64_t n = F.n;
+    double * buf = nullptr;
+    // ig, od, res (F64), then two 256-byte aligned F32 vectors padded to 64 elements
+    const size_t bytes = 3 * n * sizeof(double) + 256 + 2 * ((n + 63) / 64 * 64) * sizeof(float);
+    HB2_CUDA(cudaMallocAsync((void **)&buf, bytes, stream));
+    double * ig = buf, * od = buf + n, * res = buf + 2 * n;
+    float * x32 = (float *)(((uintptr_t)(buf + 3 * n) + 255) & ~(uintptr_t)255);
+    float * r32 = x32 + ((n + 63) / 64) * 64;
+    const uint32_t g = grid_of(n);
+    int st = HB2_OK;
+    uint64_t outer = 0, inner = 0;
+    double def = 0.0;
+    // value(): the initial guess with b's Dirichlet values; the inner iterate starts at it
+    k_bc_init<double><<<g, 256, 0, stream>>>(ig, (const double *)x, (const double *)b, n, F.m, nullptr);
+    k_to_f32<<<g, 256, 0, stream>>>(x32, ig, n);
+    cudaError_t ce = cudaMemsetAsync(res, 0, n * sizeof(double), stream);
+    count_launches(2);
+    if (ce != cudaSuccess) st = cuda_status(ce, "hb2_lmg_solve_mixed");
+    if (! st) st = launch_q1(A, 1, ig, od, b, nullptr, G->ws->error, stream);
+    const double initial = st ? 0.0 : host_norm(G, od, n, stream, &st);
+    const double outer_eps = (double)(float)G->prm.tolerance;
+    double scale = 1.0;
+    while (! st && outer < max_outer)
+    {
+        k_to_f32<<<g, 256, 0, stream>>>(r32, od, n);
+        count_launches(1);
+        uint64_t c = 0;
+        st = lmg_run(G, r32, x32, 0, &c, nullptr, stream);
+        if (st) break;
+        inner += c;
+        ++outer;
+        k_res_update<<<g, 256, 0, stream>>>(res, x32, scale, n);
+        count_launches(1);
+        st = launch_q1(A, 1, res, od, b, nullptr, G->ws->error, stream);
+        if (st) break;
+        def = host_norm(G, od, n, stream, &st);
+        if (st || def < outer_eps * initial) break;
+        scale = def;
+        k_scale64<<<g, 256, 0, stream>>>(od, 1.0 / scale, n);
+        count_launches(1);
+    }
+    if (! st) st = launch_copy(HB2_F64, x, res, n, stream);
+    cudaFreeAsync(buf, stream);
+    ce = cudaStreamSynchronize(stream);
+    if (! st && ce != cudaSuccess) st = cuda_status(ce, "hb2_lmg_solve_mixed");
+    if (outer_steps) *outer_steps = outer;
+    if (inner_cycles) *inner_cycles = inner;
+    if (final_defect) *final_defect = def;
+    if (! st && outer == max_outer && ! (def < outer_eps * initial))
+        return fail(HB2_ERR_NOT_FINITE, "hb2_lmg_solve_mixed: no convergence within max_outer steps");
+    return st;
+}
+
+namespace
+{
+int lmg_run(hb2_lmg G, const void * b, void * x, int bc, uint64_t * cycles, double * defect, cudaStream_t stream)
+{
     auto & F = G->lev.back();
     int st = launch_copy(G->dtype, F.rhs, b, F.n, stream);
     if (! st) st = launch_copy(G->dtype, G->xin, x, F.n, stream);
     if (st) return st;
+    HB2_CUDA(cudaMemcpyAsync(&G->st->bc, bc ? &kOne : &kZero, sizeof(int), cudaMemcpyHostToDevice, stream));
     HB2_CUDA(cudaGraphLaunch(G->exec, stream));
     st = launch_copy(G->dtype, x, F.x, F.n, stream);
     if (st) return st;
@@ -483,4 +639,5 @@ extern "C" int hb2_lmg_solve(hb2_lmg G, const void * b, void * x, uint64_t * cyc
     if (err) return fail(HB2_ERR_TIMEOUT, "hb2_lmg_solve: a banded kernel's copy wait expired");
     if (h.err) return fail(HB2_ERR_TIMEOUT, "hb2_lmg_solve: the coarse CG reached its step cap");
     return HB2_OK;
+}
 }

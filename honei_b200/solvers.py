@@ -170,14 +170,17 @@ class CGSmoother:
 
 
 def mg_info(n_max_iter=16, initial_zero=True, convergence_check=False, is_smoother=False, tolerance=1e-8,
-            n_pre_smooth=2, adapt_correction_factor=1.0, omega=0.7, macro_border_mask=None) -> _lib.MGInfoParams:
+            n_pre_smooth=2, adapt_correction_factor=1.0, omega=0.7, macro_border_mask=None,
+            adaptive=False) -> _lib.MGInfoParams:
     """MGInfo of the legacy Multigrid (math/multigrid.hh:65-149); defaults of the reference's
-    banded tests (math/poisson_mg_double_banded_TEST.cc).  omega scales the inverted diagonal."""
+    banded tests (math/poisson_mg_double_banded_TEST.cc).  omega scales the inverted diagonal;
+    adaptive: the MIXED class's kernel (a correction factor of 0 = alpha <d, c> / <A c, c>)."""
     mask = ALL_DIRICHLET if macro_border_mask is None else np.asarray(macro_border_mask, np.uint64)
     p = _lib.MGInfoParams(n_max_iter, int(initial_zero), int(convergence_check), int(is_smoother), tolerance,
                           n_pre_smooth, adapt_correction_factor, omega)
     for i in range(8):
         p.macro_border_mask[i] = int(mask[i])
+    p.adaptive = int(adaptive)
     return p
 
 
@@ -206,6 +209,19 @@ class Multigrid:
         defect = ctypes.c_double()
         call("hb2_lmg_solve", self._h, b.ptr, x.ptr, ctypes.byref(cycles), ctypes.byref(defect), _stream(stream))
         return x, cycles.value, defect.value
+
+    def value_mixed(self, A, b, x, max_outer=1000, stream=None):
+        """Multigrid<..., MIXED>::value (math/multigrid.hh:2252-2394): this FP32 hierarchy
+        under FP64 defect correction with the FP64 finest matrix A; b, x FP64.
+        Returns (x, outer_steps, inner_cycles, final_defect)."""
+        b, x = _vec(b), _vec(x)
+        _check_size(b.size(), self.n)
+        _check_size(x.size(), self.n)
+        outer, inner = ctypes.c_uint64(), ctypes.c_uint64()
+        defect = ctypes.c_double()
+        call("hb2_lmg_solve_mixed", self._h, A.handle, b.ptr, x.ptr, int(max_outer), ctypes.byref(outer),
+             ctypes.byref(inner), ctypes.byref(defect), _stream(stream))
+        return x, outer.value, inner.value, defect.value
 
     def __del__(self):
         try:

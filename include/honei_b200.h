@@ -295,6 +295,8 @@ typedef struct
     double adapt_correction_factor;    /* 1.0: x += factor * P x(coarser) */
     double omega;                      /* 0.7 */
     uint64_t macro_border_mask[8];     /* 2 = Dirichlet, 1 = Neumann (edges and corners) */
+    int adaptive;                      /* 0; 1 = the MIXED class's kernel: a correction factor of 0
+                                          means alpha = <d, c> / <A c, c> (math/multigrid.hh:1712-1721) */
 } hb2_lmg_params;
 /* A: max_level - min_level + 1 banded matrices, levels min_level (>= 1) .. max_level,
  * one element type; the handle keeps references to them. */
@@ -306,6 +308,15 @@ HB2_API int hb2_lmg_destroy(hb2_lmg mg);
  * -- result out).  cycles: cycles run; defect: the last ||d|| of the finest level.
  * Synchronises `stream`. */
 HB2_API int hb2_lmg_solve(hb2_lmg mg, const void *b, void *x, uint64_t *cycles, double *defect, cudaStream_t stream);
+/* Multigrid<Tag, OuterTag, NONE, JAC, CYCLE::V, MIXED>::value (math/multigrid.hh:2252-2394):
+ * `mg` an F32 hierarchy (its MGInfo), A the F64 finest matrix, b and x F64 device vectors.
+ * The FP64 defect of the initial guess (b's Dirichlet values applied) is scaled into the
+ * inner right-hand side, the inner kernel runs on its persistent iterate, result (from 0)
+ * += scale x_inner, until ||b - A result|| < tolerance (the MGInfo's, through float)
+ * times the initial norm; at most max_outer outer steps (the reference has no cap:
+ * HB2_ERR_NOT_FINITE when it is reached).  Synchronises `stream`. */
+HB2_API int hb2_lmg_solve_mixed(hb2_lmg mg, hb2_q1 A, const void *b, void *x, uint64_t max_outer,
+                        uint64_t *outer_steps, uint64_t *inner_cycles, double *final_defect, cudaStream_t stream);
 
 /* MG hierarchy: MGData (math/mg.hh:57-240) + MGCycleCreation<V::STATIC,
  * CGSolver<NONE>, RISmoother, Restriction<PROLMAT>, Prolongation<PROLMAT>>

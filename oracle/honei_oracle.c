@@ -939,83 +939,172 @@ static void lmg_sweeps_##SFX(uint64_t n, uint64_t m, const T_ *bands, const T_ *
     }                                                                               \
 }                                                                                   \
                                                                                     \
-/* Multigrid<..., JAC, CYCLE::V, FIXED>::value (math/multigrid.hh:781-825) and its  \
- * banded _multigrid_kernel (:159-466).  Levels lmin..lmax (lmin >= 1):             \
- * bands[l] band-major LL..UU, n = (2^l + 1)^2; dinv[l] the inverted diagonal       \
- * scaled as the caller chose; rhs: the finest right-hand side; x: initial guess in, \
- * result out.  Returns the cycles run. */                                          \
+typedef struct {                                                                    \
+    unsigned lmin, lmax;                                                            \
+    uint64_t N[32], M[32];                                                          \
+    const T_ *bands[32], *dinv[32];                                                 \
+    T_ *x[32], *c[32], *d[32], *rhs[32], *t[32];                                    \
+} lmg_##SFX;                                                                        \
+                                                                                    \
+static void lmg_alloc_##SFX(lmg_##SFX *h, unsigned lmin, unsigned lmax,             \
+                            const T_ *const *bands, const T_ *const *dinv)          \
+{                                                                                   \
+    h->lmin = lmin; h->lmax = lmax;                                                 \
+    for (unsigned l = lmin; l <= lmax; ++l) {                                       \
+        h->M[l] = ((uint64_t)1 << l) + 1; h->N[l] = h->M[l] * h->M[l];              \
+        h->bands[l] = bands[l]; h->dinv[l] = dinv[l];                               \
+        h->x[l] = (T_ *)calloc(h->N[l], sizeof(T_)); h->c[l] = (T_ *)calloc(h->N[l], sizeof(T_)); \
+        h->d[l] = (T_ *)calloc(h->N[l], sizeof(T_)); h->rhs[l] = (T_ *)calloc(h->N[l], sizeof(T_)); \
+        h->t[l] = (T_ *)calloc(h->N[l], sizeof(T_));                                \
+    }                                                                               \
+}                                                                                   \
+static void lmg_release_##SFX(lmg_##SFX *h)                                         \
+{                                                                                   \
+    for (unsigned l = h->lmin; l <= h->lmax; ++l) {                                 \
+        free(h->x[l]); free(h->c[l]); free(h->d[l]); free(h->rhs[l]); free(h->t[l]); \
+    }                                                                               \
+}                                                                                   \
+                                                                                    \
+/* _multigrid_kernel (math/multigrid.hh:159-466 FIXED, 1619-1934 MIXED) on the      \
+ * state's finest x (iterate) and rhs.  mixed: the MIXED class's kernel, whose      \
+ * coarse-grid correction factor 0 means alpha = <d, c> / <A c, c>.  Returns the    \
+ * cycles run. */                                                                   \
+static uint64_t lmg_kernel_##SFX(lmg_##SFX *h, uint64_t n_max_iter, int initial_zero, \
+                                 int convergence_check, int is_smoother,            \
+                                 double tolerance, uint64_t n_pre, double adapt,    \
+                                 const uint64_t *mask, int mixed)                   \
+{                                                                                   \
+    const unsigned L = h->lmax, lmin = h->lmin;                                     \
+    const uint64_t n = h->N[L];                                                     \
+    T_ **x = h->x, **c = h->c, **d = h->d, **rhs = h->rhs, **t = h->t;              \
+    if (initial_zero) memcpy(d[L], rhs[L], sizeof(T_) * n);                         \
+    else hbo_q1_defect_##SFX(n, h->M[L], h->bands[L], rhs[L], x[L], d[L]);          \
+    T_ defect, initial;                                                             \
+    if (! is_smoother) { defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L])); initial = defect; } \
+    else { defect = (T_)1e8; initial = defect; }                                    \
+    uint64_t cycles = 0;                                                            \
+    if (convergence_check && defect <= (T_)tolerance) return 0;                     \
+    for (uint64_t iter = 1; iter <= n_max_iter; ++iter) {                           \
+        unsigned l = L;                                                             \
+        int started = 1;                                                            \
+        cycles = iter;                                                              \
+        while (lmin != L) {                                                         \
+            const uint64_t Nl = h->N[l], Ml = h->M[l];                              \
+            if (started) {                                                          \
+                for (uint64_t i = 0; i < Nl; ++i) c[l][i] = h->dinv[l][i] * d[l][i]; \
+                lmg_sweeps_##SFX(Nl, Ml, h->bands[l], d[l], c[l], h->dinv[l], n_pre - 1, t[l]); \
+                for (uint64_t i = 0; i < Nl; ++i) x[l][i] = x[l][i] + c[l][i];      \
+            } else {                                                                \
+                for (uint64_t i = 0; i < Nl; ++i) x[l][i] = h->dinv[l][i] * d[l][i]; \
+                lmg_sweeps_##SFX(Nl, Ml, h->bands[l], d[l], x[l], h->dinv[l], n_pre - 1, t[l]); \
+            }                                                                       \
+            hbo_q1_defect_##SFX(Nl, Ml, h->bands[l], rhs[l], x[l], d[l]);           \
+            --l;                                                                    \
+            hbo_restriction_##SFX(h->N[l], d[l], h->N[l + 1], d[l + 1], mask);      \
+            memcpy(rhs[l], d[l], sizeof(T_) * h->N[l]);                             \
+            if (l == lmin) break;                                                   \
+            started = 0;                                                            \
+        }                                                                           \
+        lmg_cg_##SFX(h->N[l], h->M[l], h->bands[l], d[l], x[l], (double)EPS_MACH);  \
+        if (lmin == L) {                                                            \
+            hbo_q1_defect_##SFX(h->N[l], h->M[l], h->bands[l], rhs[l], x[l], d[l]); \
+            break;                                                                  \
+        }                                                                           \
+        while (1) {                                                                 \
+            ++l;                                                                    \
+            const uint64_t Nl = h->N[l], Ml = h->M[l];                              \
+            hbo_prolongation_##SFX(Nl, c[l], h->N[l - 1], x[l - 1], mask);          \
+            T_ alpha = (T_)adapt;                                                   \
+            if (mixed && adapt == 0.0) {                                            \
+                const T_ d1 = hbo_dot_##SFX(Nl, d[l], c[l]);                        \
+                hbo_q1_spmv_##SFX(Nl, Ml, h->bands[l], c[l], t[l]);                 \
+                const T_ d2 = hbo_dot_##SFX(Nl, t[l], c[l]);                        \
+                alpha = (T_)(d1 / d2);                                              \
+            }                                                                       \
+            for (uint64_t i = 0; i < Nl; ++i) x[l][i] = x[l][i] + alpha * c[l][i];  \
+            lmg_sweeps_##SFX(Nl, Ml, h->bands[l], rhs[l], x[l], h->dinv[l], n_pre, t[l]); \
+            hbo_q1_defect_##SFX(Nl, Ml, h->bands[l], rhs[l], x[l], d[l]);           \
+            if (l == L) break;                                                      \
+        }                                                                           \
+        if (! is_smoother) {                                                        \
+            defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L]));                        \
+            if (defect <= initial * (T_)tolerance) break;                           \
+        }                                                                           \
+    }                                                                               \
+    return cycles;                                                                  \
+}                                                                                   \
+                                                                                    \
+/* Multigrid<..., JAC, CYCLE::V, FIXED>::value (math/multigrid.hh:781-825) */       \
 uint64_t hbo_lmg_##SFX(unsigned lmin, unsigned lmax, const T_ *const *bands,        \
                        const T_ *const *dinv, const T_ *rhs_in, T_ *x_io,           \
                        uint64_t n_max_iter, int initial_zero, int convergence_check, \
                        int is_smoother, double tolerance, uint64_t n_pre,           \
                        double adapt, const uint64_t *mask)                          \
 {                                                                                   \
-    T_ *x[32], *c[32], *d[32], *rhs[32], *t[32];                                    \
-    uint64_t N[32], M[32];                                                          \
-    for (unsigned l = lmin; l <= lmax; ++l) {                                       \
-        M[l] = ((uint64_t)1 << l) + 1; N[l] = M[l] * M[l];                           \
-        x[l] = (T_ *)calloc(N[l], sizeof(T_)); c[l] = (T_ *)calloc(N[l], sizeof(T_)); \
-        d[l] = (T_ *)calloc(N[l], sizeof(T_)); rhs[l] = (T_ *)calloc(N[l], sizeof(T_)); \
-        t[l] = (T_ *)calloc(N[l], sizeof(T_));                                      \
-    }                                                                               \
+    lmg_##SFX h;                                                                    \
+    lmg_alloc_##SFX(&h, lmin, lmax, bands, dinv);                                   \
     const unsigned L = lmax;                                                        \
-    const uint64_t n = N[L], sq = M[L];                                             \
-    memcpy(rhs[L], rhs_in, sizeof(T_) * n);                                         \
-    /* value(): Dirichlet values of b on the first row, the last row and the first column */ \
-    memcpy(x[L], x_io, sizeof(T_) * n);                                             \
-    for (uint64_t i = 0; i < sq; ++i) x[L][i] = rhs_in[i];                          \
-    for (uint64_t i = n - sq; i < n; ++i) x[L][i] = rhs_in[i];                      \
-    for (uint64_t i = 0; i < n; i += sq) x[L][i] = rhs_in[i];                       \
-    if (initial_zero) memcpy(d[L], rhs[L], sizeof(T_) * n);                         \
-    else hbo_q1_defect_##SFX(n, M[L], bands[L], rhs[L], x[L], d[L]);                \
-    T_ defect, initial;                                                             \
-    if (! is_smoother) { defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L])); initial = defect; } \
-    else { defect = (T_)1e8; initial = defect; }                                    \
-    uint64_t iter = 0, cycles = 0;                                                  \
-    if (! (convergence_check && defect <= (T_)tolerance)) {                         \
-        for (iter = 1; iter <= n_max_iter; ++iter) {                                \
-            unsigned l = L;                                                         \
-            int started = 1;                                                        \
-            cycles = iter;                                                          \
-            while (lmin != L) {                                                     \
-                if (started) {                                                      \
-                    for (uint64_t i = 0; i < N[l]; ++i) c[l][i] = dinv[l][i] * d[l][i]; \
-                    lmg_sweeps_##SFX(N[l], M[l], bands[l], d[l], c[l], dinv[l], n_pre - 1, t[l]); \
-                    for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = x[l][i] + c[l][i];  \
-                } else {                                                            \
-                    for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = dinv[l][i] * d[l][i]; \
-                    lmg_sweeps_##SFX(N[l], M[l], bands[l], d[l], x[l], dinv[l], n_pre - 1, t[l]); \
-                }                                                                   \
-                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
-                --l;                                                                \
-                hbo_restriction_##SFX(N[l], d[l], N[l + 1], d[l + 1], mask);        \
-                memcpy(rhs[l], d[l], sizeof(T_) * N[l]);                            \
-                if (l == lmin) break;                                               \
-                started = 0;                                                        \
-            }                                                                       \
-            lmg_cg_##SFX(N[l], M[l], bands[l], d[l], x[l], (double)EPS_MACH);       \
-            if (lmin == L) {                                                        \
-                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
-                break;                                                              \
-            }                                                                       \
-            while (1) {                                                             \
-                ++l;                                                                \
-                hbo_prolongation_##SFX(N[l], c[l], N[l - 1], x[l - 1], mask);       \
-                const T_ alpha = (T_)adapt;                                         \
-                for (uint64_t i = 0; i < N[l]; ++i) x[l][i] = x[l][i] + alpha * c[l][i]; \
-                lmg_sweeps_##SFX(N[l], M[l], bands[l], rhs[l], x[l], dinv[l], n_pre, t[l]); \
-                hbo_q1_defect_##SFX(N[l], M[l], bands[l], rhs[l], x[l], d[l]);      \
-                if (l == L) break;                                                  \
-            }                                                                       \
-            if (! is_smoother) {                                                    \
-                defect = (T_)sqrt(hbo_dot_##SFX(n, d[L], d[L]));                    \
-                if (defect <= initial * (T_)tolerance) break;                       \
-            }                                                                       \
-        }                                                                           \
-    }                                                                               \
-    memcpy(x_io, x[L], sizeof(T_) * n);                                             \
-    for (unsigned l = lmin; l <= lmax; ++l) { free(x[l]); free(c[l]); free(d[l]); free(rhs[l]); free(t[l]); } \
+    const uint64_t n = h.N[L], sq = h.M[L];                                         \
+    memcpy(h.rhs[L], rhs_in, sizeof(T_) * n);                                       \
+    /* the initial guess with b's values on the first row, the last row and the first column */ \
+    memcpy(h.x[L], x_io, sizeof(T_) * n);                                           \
+    for (uint64_t i = 0; i < sq; ++i) h.x[L][i] = rhs_in[i];                        \
+    for (uint64_t i = n - sq; i < n; ++i) h.x[L][i] = rhs_in[i];                    \
+    for (uint64_t i = 0; i < n; i += sq) h.x[L][i] = rhs_in[i];                     \
+    const uint64_t cycles = lmg_kernel_##SFX(&h, n_max_iter, initial_zero, convergence_check, \
+                                             is_smoother, tolerance, n_pre, adapt, mask, 0); \
+    memcpy(x_io, h.x[L], sizeof(T_) * n);                                           \
+    lmg_release_##SFX(&h);                                                          \
     return cycles;                                                                  \
 }
 DEFINE_LMG(double, f64, DBL_EPSILON)
 DEFINE_LMG(float, f32, FLT_EPSILON)
+
+
+/* Multigrid<Tag, OuterTag, NONE, JAC, CYCLE::V, MIXED>::value on BandedMatrixQx
+ * (math/multigrid.hh:2252-2394): the FP64 defect of the initial guess (b's Dirichlet
+ * values on the first row, the last row and the first column) scaled into the FP32
+ * inner right-hand side, the inner kernel on its persistent iterate, result (starting
+ * at 0) += scale x_inner, the FP64 defect, its norm, stop below tolerance (the inner
+ * MGInfo's float, widened) times the initial norm, else scale by 1 / norm.  At most
+ * max_outer outer steps (the reference has no cap).  Returns the outer steps;
+ * *inner_total: the inner cycles. */
+uint64_t hbo_lmg_mixed(unsigned lmin, unsigned lmax, const float *const *bands, const float *const *dinv,
+                       const double *bands64, const double *b, double *x, uint64_t n_max_iter, int initial_zero,
+                       double tolerance, uint64_t n_pre, double adapt, const uint64_t *mask, uint64_t max_outer,
+                       uint64_t *inner_total)
+{
+    lmg_f32 h;
+    lmg_alloc_f32(&h, lmin, lmax, bands, dinv);
+    const unsigned L = lmax;
+    const uint64_t n = h.N[L], sq = h.M[L];
+    double *ig = (double *)malloc(sizeof(double) * n), *od = (double *)malloc(sizeof(double) * n);
+    double *res = (double *)calloc(n, sizeof(double));
+    memcpy(ig, x, sizeof(double) * n);
+    for (uint64_t i = 0; i < sq; ++i) ig[i] = b[i];
+    for (uint64_t i = n - sq; i < n; ++i) ig[i] = b[i];
+    for (uint64_t i = 0; i < n; i += sq) ig[i] = b[i];
+    for (uint64_t i = 0; i < n; ++i) h.x[L][i] = (float)ig[i];
+    hbo_q1_defect_f64(n, sq, bands64, b, ig, od);
+    const double initial = sqrt(hbo_dot_f64(n, od, od));
+    const double outer_eps = (double)(float)tolerance;
+    double scale = 1.0;
+    uint64_t outer = 0, inner = 0;
+    while (outer < max_outer) {
+        for (uint64_t i = 0; i < n; ++i) h.rhs[L][i] = (float)od[i];
+        inner += lmg_kernel_f32(&h, n_max_iter, initial_zero, 0, 0, (double)(float)tolerance, n_pre, adapt, mask, 1);
+        ++outer;
+        for (uint64_t i = 0; i < n; ++i) res[i] = res[i] + scale * (double)h.x[L][i];
+        hbo_q1_defect_f64(n, sq, bands64, b, res, od);
+        const double def = sqrt(hbo_dot_f64(n, od, od));
+        if (def < outer_eps * initial) break;
+        scale = def;
+        const double inv = 1.0 / scale;
+        for (uint64_t i = 0; i < n; ++i) od[i] = od[i] * inv;
+    }
+    memcpy(x, res, sizeof(double) * n);
+    free(ig); free(od); free(res);
+    lmg_release_f32(&h);
+    if (inner_total) *inner_total = inner;
+    return outer;
+}

@@ -78,6 +78,9 @@ def lib():
             f.restype = _u64
             f.argtypes = [ctypes.c_uint, ctypes.c_uint, _ptr, _ptr, _ptr, _ptr, _u64, ctypes.c_int, ctypes.c_int,
                           ctypes.c_int, _dbl, _u64, _dbl, _ptr]
+        L.hbo_lmg_mixed.restype = _u64
+        L.hbo_lmg_mixed.argtypes = [ctypes.c_uint, ctypes.c_uint, _ptr, _ptr, _ptr, _ptr, _ptr, _u64, ctypes.c_int, _dbl,
+                                    _u64, _dbl, _ptr, _u64, _ptr]
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
@@ -526,11 +529,12 @@ def read_feast_bin(raw: bytes, dtype=np.float64):
 
 
 def lmg_dinv(bands: np.ndarray, n: int, omega=0.7) -> np.ndarray:
-    """the reference tests' diags_inverted: ElementInverse(DD) then Scale by omega, in dtype"""
+    """the reference tests' diags_inverted: ElementInverse(DD) in the vectors' type, then
+    Scale by the double omega (the product formed in double, rounded to the type)"""
     dt = bands.dtype.type
     dd = bands[4 * n:5 * n]
     inv = np.where(dd == 0, dt(0), dt(1) / np.where(dd == 0, dt(1), dd)).astype(bands.dtype)
-    return (inv * dt(omega)).astype(bands.dtype)
+    return (inv.astype(np.float64) * omega).astype(bands.dtype)
 
 
 def legacy_mg(bands_by_level: dict, rhs, x0, n_max_iter=16, initial_zero=True, convergence_check=False,
@@ -555,3 +559,27 @@ def legacy_mg(bands_by_level: dict, rhs, x0, n_max_iter=16, initial_zero=True, c
     cycles = f(lmin, lmax, bp, dp, _p(np.ascontiguousarray(rhs, dt)), _p(x), n_max_iter, int(initial_zero),
                int(convergence_check), int(is_smoother), tolerance, n_pre, adapt, _p(m))
     return x, int(cycles)
+
+
+def legacy_mg_mixed(bands32_by_level: dict, bands64, b, x0, n_max_iter=2, initial_zero=True, tolerance=1e-8,
+                    n_pre=2, adapt=1.0, mask=ALL_DIRICHLET, max_outer=1000):
+    """Multigrid<..., MIXED>: FP32 levels {level: bands} under FP64 defect correction with
+    the finest FP64 bands64 and b.  Returns (x, outer_steps, inner_cycles)."""
+    levels = sorted(bands32_by_level)
+    keep = []
+    bp = (_ptr * 32)()
+    dp = (_ptr * 32)()
+    for l in levels:
+        bb = np.ascontiguousarray(bands32_by_level[l], np.float32)
+        d = lmg_dinv(bb, bb.size // 9)
+        keep += [bb, d]
+        bp[l] = _p(bb).value
+        dp[l] = _p(d).value
+    b64 = np.ascontiguousarray(bands64, np.float64)
+    x = np.array(x0, np.float64)
+    m = np.ascontiguousarray(np.asarray(mask, np.uint64))
+    inner = _u64()
+    outer = lib().hbo_lmg_mixed(levels[0], levels[-1], bp, dp, _p(b64), _p(np.ascontiguousarray(b, np.float64)), _p(x),
+                                n_max_iter, int(initial_zero), tolerance, n_pre, adapt, _p(m), max_outer,
+                                ctypes.byref(inner))
+    return x, int(outer), int(inner.value)

@@ -626,16 +626,16 @@ namespace
                                             band[8]);
     }
 
-    // The setup of math/poisson_mg_double_banded_TEST.cc (MGInfo levels 0..L, the
-    // matrices and right-hand sides of levels 1..L from the test data, diags_inverted =
-    // 0.7 / DD, zero x below the finest level) and Multigrid<tags::CPU, tags::CPU,
-    // methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value on it.
+    // The setup of math/poisson_mg_double_banded_TEST.cc / poisson_mg_mixed_banded_TEST.cc:
+    // MGInfo levels 0..L, the matrices and right-hand sides of levels 1..L from the
+    // test data, diags_inverted = ElementInverse(DD) scaled by 0.7 (a double, as the
+    // tests pass it), zero x below the finest level.
     template <typename DT_>
-    DenseVector<DT_> legacy_mg(const std::string & dir, unsigned long L, unsigned long iters, bool initial_zero,
-                               bool convergence_check, bool is_smoother, double tolerance, unsigned long n_pre,
-                               double adapt, const unsigned long * mask, const DenseVector<DT_> & x0)
+    void fill_info(MGInfo<DT_, BandedMatrixQx<Q1Type, DT_> > & info, std::vector<BandedMatrixQx<Q1Type, DT_> *> & keep,
+                   const std::string & dir, unsigned long L, unsigned long iters, bool initial_zero,
+                   bool convergence_check, bool is_smoother, double tolerance, unsigned long n_pre, double adapt,
+                   const unsigned long * mask)
     {
-        MGInfo<DT_, BandedMatrixQx<Q1Type, DT_> > info;
         info.is_smoother = is_smoother;
         for (int i(0); i < 8; ++i) info.macro_border_mask[i] = mask[i];
         info.min_level = 1;
@@ -649,7 +649,6 @@ namespace
         info.n_max_iter_coarse = 0;
         info.tolerance_coarse = 1e-2;
         info.adapt_correction_factor = adapt;
-        std::vector<BandedMatrixQx<Q1Type, DT_> *> keep;
         for (unsigned long i(0); i <= L; ++i)
         {
             unsigned long size(((1ul << i) + 1) * ((1ul << i) + 1));
@@ -680,13 +679,45 @@ namespace
         {
             DenseVector<DT_> sdi(info.a[i].band(DD).copy());
             ElementInverse<tags::CPU>::value(sdi);
-            Scale<tags::CPU>::value(sdi, DT_(0.7));
+            Scale<tags::CPU>::value(sdi, 0.7);
             info.diags_inverted[i] = sdi.copy();
         }
+    }
+
+    // Multigrid<tags::CPU, tags::CPU, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>
+    template <typename DT_>
+    DenseVector<DT_> legacy_mg(const std::string & dir, unsigned long L, unsigned long iters, bool initial_zero,
+                               bool convergence_check, bool is_smoother, double tolerance, unsigned long n_pre,
+                               double adapt, const unsigned long * mask, const DenseVector<DT_> & x0)
+    {
+        MGInfo<DT_, BandedMatrixQx<Q1Type, DT_> > info;
+        std::vector<BandedMatrixQx<Q1Type, DT_> *> keep;
+        fill_info<DT_>(info, keep, dir, L, iters, initial_zero, convergence_check, is_smoother, tolerance, n_pre, adapt,
+                       mask);
         DenseVector<DT_> b(info.rhs[L].copy());
         DenseVector<DT_> result(x0.copy());
         Multigrid<tags::CPU, tags::CPU, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value(
             info.a[L], b, result, (unsigned long)11, std::numeric_limits<DT_>::epsilon(), info);
+        for (size_t i(0); i < keep.size(); ++i) delete keep[i];
+        return result;
+    }
+
+    // Multigrid<tags::CPU, tags::CPU, methods::NONE, methods::JAC, methods::CYCLE::V, methods::MIXED>:
+    // an FP32 MGInfo under FP64 defect correction with the FP64 finest matrix and b
+    DenseVector<double> legacy_mg_mixed(const std::string & dir, unsigned long L, unsigned long iters,
+                                        double adapt, const unsigned long * mask, const DenseVector<double> & x0)
+    {
+        MGInfo<float, BandedMatrixQx<Q1Type, float> > info;
+        std::vector<BandedMatrixQx<Q1Type, float> *> keep;
+        fill_info<float>(info, keep, dir, L, iters, true, false, false, 1e-8, 2, adapt, mask);
+        const unsigned long n(((1ul << L) + 1) * ((1ul << L) + 1));
+        BandedMatrixQx<Q1Type, double> * A(0);
+        DenseVector<double> b(n);
+        read_bin<double>(dir, n, A, b);
+        DenseVector<double> result(x0.copy());
+        Multigrid<tags::CPU, tags::CPU, methods::NONE, methods::JAC, methods::CYCLE::V, methods::MIXED>::value(
+            *A, b, result, (unsigned long)11, std::numeric_limits<double>::epsilon(), info);
+        delete A;
         for (size_t i(0); i < keep.size(); ++i) delete keep[i];
         return result;
     }
@@ -710,6 +741,10 @@ namespace
         // D: configuration A in single precision
         put_vec("lmg_D.x", legacy_mg<float>(dir, 5, 16, true, false, false, 1e-8, 2, 1.0, dirichlet,
                                             DenseVector<float>(n5, 0.0f)));
+        // E: the mixed-precision test's configuration (math/poisson_mg_mixed_banded_TEST.cc)
+        put_vec("lmg_E.x", legacy_mg_mixed(dir, 5, 2, 1.0, dirichlet, DenseVector<double>(n5, 0.0)));
+        // F: E with the adaptive coarse-grid correction (factor 0) and a nonzero start
+        put_vec("lmg_F.x", legacy_mg_mixed(dir, 5, 2, 0.0, dirichlet, uniform<double>(n5, 6)));
         return 0;
     }
 }

@@ -10,7 +10,10 @@ methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value on it:
 * B: a seeded nonzero start, 30 cycles with the tolerance stop (1e-6), V(3,3), factor 0.8,
   Neumann edges (mask 2 1 2 1 2 2 1 2);
 * C: smoother mode, 3 cycles, level 4;
-* D: configuration A in single precision.
+* D: configuration A in single precision;
+* E: Multigrid<..., MIXED> in the configuration of math/poisson_mg_mixed_banded_TEST.cc
+  (an FP32 MGInfo with 2 cycles per outer step under FP64 defect correction);
+* F: E with the adaptive coarse-grid correction (factor 0) and a seeded nonzero start.
 
 Writes ``reference_legacy_mg.npz`` (the data arrays, shape (12, n) per level, and the
 four solutions) and ``reference_legacy_mg.json`` (SHA-256 of the data files).
@@ -49,7 +52,7 @@ def main() -> int:
         out[f"bin_{n}"] = np.frombuffer(raw[4:], "<f8").reshape(12, n).copy()
     with tempfile.TemporaryDirectory() as tmp:
         subprocess.check_call([REF_BIN, "mglegacy", data, tmp], stdout=subprocess.DEVNULL)
-        for c in "ABCD":
+        for c in "ABCDEF":
             out[f"lmg_{c}.x"] = np.fromfile(os.path.join(tmp, f"lmg_{c}.x"), "<f4" if c == "D" else "<f8")
     np.savez_compressed(os.path.join(OUT_DIR, "reference_legacy_mg.npz"), **out)
     with open(os.path.join(OUT_DIR, "reference_legacy_mg.json"), "w") as f:

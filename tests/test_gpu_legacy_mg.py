@@ -69,3 +69,37 @@ def test_handle_reuse(lmg_golden):
     x1 = mg.value(hb.DenseVector(b), hb.DenseVector(b.size))[0].numpy()
     x2 = mg.value(hb.DenseVector(b), hb.DenseVector(b.size))[0].numpy()
     assert same_bits(x1, x2) and same_bits(x1, lmg_golden["lmg_A.x"])
+
+
+@pytest.mark.parametrize("case", ["E", "F"])
+def test_mixed(lmg_golden, oracle, case):
+    """Multigrid<..., MIXED>: the inner FP32 cycles are bit-identical; the outer FP64 norm
+    (a tree reduction here, sequential in the reference) also scales the defect, so the
+    result agrees to rounding and the step counts agree exactly."""
+    from test_legacy_mg_host import MIXED_CASES, mixed_levels
+    c = MIXED_CASES[case]
+    b32, a64, b = mixed_levels(lmg_golden)
+    x0 = oracle.uniform(b.size, c["x0"]) if c["x0"] else np.zeros(b.size)
+    xo, outer_o, inner_o = oracle.legacy_mg_mixed(b32, a64, b, x0, adapt=c["adapt"])
+    info = hb.mg_info(n_max_iter=2, adapt_correction_factor=c["adapt"], adaptive=True)
+    mg = hb.Multigrid(device_levels(b32), 1, info)
+    A64 = hb.BandedMatrixQx.from_bands(a64.reshape(9, -1))
+    x, outer, inner, _ = mg.value_mixed(A64, hb.DenseVector(b), hb.DenseVector(x0))
+    assert (outer, inner) == (outer_o, inner_o)
+    ref = lmg_golden[f"lmg_{case}.x"]
+    assert np.abs(x.numpy() - ref).max() <= 1e-9 * np.abs(ref).max()
+    assert np.abs(x.numpy() - lmg_golden["bin_1089"][11]).max() < 1e-4
+
+
+def test_mixed_assembled_level9(oracle):
+    """FP32 levels 1-9 under FP64 defect correction on the assembled Q1 operator"""
+    L = 9
+    b32 = {l: oracle.q1_bands(l, np.float32).reshape(-1) for l in range(1, L + 1)}
+    a64 = oracle.q1_bands(L, np.float64)
+    b = oracle.q1_spmv(a64, oracle.uniform(oracle.q1_n(L), 3))
+    xo, outer_o, inner_o = oracle.legacy_mg_mixed(b32, a64.reshape(-1), b, np.zeros(b.size), n_max_iter=4)
+    mg = hb.Multigrid([hb.BandedMatrixQx.poisson_q1(l, torch.float32) for l in range(1, L + 1)], 1,
+                      hb.mg_info(n_max_iter=4, adaptive=True))
+    x, outer, inner, _ = mg.value_mixed(hb.BandedMatrixQx.poisson_q1(L), hb.DenseVector(b), hb.DenseVector(b.size))
+    assert (outer, inner) == (outer_o, inner_o)
+    assert np.abs(x.numpy() - xo).max() <= 1e-9 * np.abs(xo).max()

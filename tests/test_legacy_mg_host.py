@@ -76,3 +76,24 @@ def test_lmg_entry_points_check_arguments():
     assert lib.hb2_lmg_create(ctypes.byref(h), 3, 2, arr, ctypes.byref(p), None) == _lib.HB2_ERR_ARG
     assert lib.hb2_lmg_create(ctypes.byref(h), 1, 1, arr, None, None) == _lib.HB2_ERR_ARG
     assert lib.hb2_lmg_solve(None, None, None, None, None, None) == _lib.HB2_ERR_ARG
+
+
+MIXED_CASES = {"E": dict(adapt=1.0, x0=None), "F": dict(adapt=0.0, x0=6)}
+
+
+def mixed_levels(golden):
+    b32, _ = levels(golden, 5, np.float32)
+    b64, b = levels(golden, 5, np.float64)
+    return b32, b64[5], b
+
+
+@pytest.mark.parametrize("case", sorted(MIXED_CASES))
+def test_oracle_mixed_is_the_reference(lmg_golden, oracle, case):
+    """Multigrid<..., MIXED> in the configuration of math/poisson_mg_mixed_banded_TEST.cc"""
+    c = MIXED_CASES[case]
+    b32, a64, b = mixed_levels(lmg_golden)
+    x0 = oracle.uniform(b.size, c["x0"]) if c["x0"] else np.zeros(b.size)
+    x, outer, inner = oracle.legacy_mg_mixed(b32, a64, b, x0, adapt=c["adapt"])
+    assert np.array_equal(x.view(np.uint8), lmg_golden[f"lmg_{case}.x"].view(np.uint8))
+    assert inner == 2 * outer
+    assert np.abs(x - lmg_golden["bin_1089"][11]).max() < 1e-4   # the reference test's check
