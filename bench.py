@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the CSR / Krylov / legacy-multigrid timings")
     return ap.parse_args()
 
 
@@ -385,6 +386,8 @@ def main():
         line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
     if not args.no_serving:
         line["serving"] = serving_loop(rank)
+    if not args.no_next:
+        line["next_rows"] = next_rows(hb, dev, flush, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(L)
     if rank == 0:
@@ -394,6 +397,79 @@ def main():
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def next_rows(hb, dev, flush, rank, reps=3):
+    """Device timings of the paths beside the MG solve (CUDA events on the launching
+    stream, L2 flushed before each timed call): SparseMatrixCSR Product on the level-11
+    Q1 operator, CGSolver VAR and BiCGStabSolver VAR per iteration (level 10, Jacobi
+    vector P, 200 iterations), the legacy banded Multigrid (levels 1-10, V(2,2), to 1e-8;
+    FIXED in FP64 and MIXED with FP32 levels)."""
+    import torch
+    from honei_b200 import _lib
+    from honei_b200.inputs import uniform
+    stream = torch.cuda.current_stream()
+    s_ptr = ctypes_stream(stream)
+    peak = load_peaks()[0]
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts), r
+
+    out = {}
+    # CSR
+    L = 11
+    n = ((1 << L) + 1) ** 2
+    E = hb.SparseMatrixELL.poisson_q1(L)
+    C = hb.SparseMatrixCSR.from_ell(E)
+    del E
+    x = hb.DenseVector(torch.from_numpy(uniform(n, 1)).to(dev))
+    y = hb.DenseVector(n)
+    ms, _ = timed(lambda: _lib.call("hb2_product_csr", C.handle, x.ptr, y.ptr, s_ptr))
+    nbytes = (n + 1) * 4 + C.used_blocks() * 12 + 16 * n
+    out["csr_spmv"] = {"workload": "Q1 level 11, %d rows, %d entries, FP64" % (n, C.used_blocks()),
+                       "launch_us": 1000 * ms, "algorithmic_bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                       "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
+    del C, x, y
+    # Krylov
+    L = 10
+    n = ((1 << L) + 1) ** 2
+    A = hb.SparseMatrixELL.poisson_q1(L)
+    d = hb.DenseVector(n)
+    _lib.call("hb2_jacobi_precon", A.handle, 1.0, d.ptr, s_ptr)
+    b = hb.DenseVector(n)
+    hb.Product.value(b, A, hb.DenseVector(torch.from_numpy(uniform(n, 42)).to(dev)))
+    for name, method in (("cg_var", hb.HB2_CG_VAR), ("bicgstab", hb.HB2_BICGSTAB_VAR)):
+        K = hb.KrylovSolver(method, A, d, 200, 0.0)
+        x0 = hb.DenseVector(n)
+        ms, r = timed(lambda: K.solve(b, x0))
+        its = r[1] - 1 if method == hb.HB2_BICGSTAB_VAR else r[1]
+        out[name] = {"workload": "Q1 level 10, Jacobi vector P, %d iterations" % its, "solve_ms": ms,
+                     "us_per_iteration": 1000 * ms / its}
+        del K
+    # legacy banded multigrid
+    A64 = [hb.BandedMatrixQx.poisson_q1(l) for l in range(1, L + 1)]
+    A32 = [hb.BandedMatrixQx.poisson_q1(l, torch.float32) for l in range(1, L + 1)]
+    bq = hb.DenseVector(n)
+    hb.Product.value(bq, A64[-1], hb.DenseVector(torch.from_numpy(uniform(n, 42)).to(dev)))
+    mg = hb.Multigrid(A64, 1, hb.mg_info(n_max_iter=100, tolerance=1e-8))
+    ms, r = timed(lambda: mg.value(bq, hb.DenseVector(n)))
+    out["legacy_mg_fixed"] = {"workload": "banded Q1 levels 1-10, V(2,2), FP64, to 1e-8", "solve_ms": ms,
+                              "cycles": r[1]}
+    mg32 = hb.Multigrid(A32, 1, hb.mg_info(n_max_iter=2, tolerance=1e-8, adaptive=True))
+    ms, r = timed(lambda: mg32.value_mixed(A64[-1], bq, hb.DenseVector(n)))
+    out["legacy_mg_mixed"] = {"workload": "FP32 banded levels 1-10 under FP64 defect correction, to 1e-8",
+                              "solve_ms": ms, "outer_steps": r[1], "inner_cycles": r[2]}
+    return out
 
 
 def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
