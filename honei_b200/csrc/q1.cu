@@ -6,7 +6,8 @@
 // windows of x: [r0-m-1, r0+B-m+1), [r0-1, r0+B+1), [r0+m-1, r0+B+m+1).  Each is
 // clamped to [0, n), rounded to 16-byte boundaries for the bulk copy, and a
 // ragged tail (n is odd) is fetched with plain loads.  Band values stream with
-// evict-first loads.  Summation: DD*x first, then LL LD LU DL DU UL UD UU with
+// evict-first loads issued before the wait for the windows (rows interleaved
+// across the block's threads, so they are coalesced).  Summation: DD*x first, then LL LD LU DL DU UL UD UU with
 // the reference's bounds tests, each product and sum separately rounded, so
 // the result is bit-identical to the reference.
 #include "hb2_common.cuh"
@@ -82,6 +83,20 @@ namespace hb2
         __shared__ int64_t base[3];
 
         const int64_t r0 = (int64_t)blockIdx.x * B;
+        // rows r0 + k * kQ1Threads + threadIdx.x: the band (and rhs, dinv) loads are
+        // coalesced and independent of x, so every thread issues them before the
+        // block waits for its x windows
+        T bv[R][9], rh[R], dv[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = r0 + (int64_t)k * kQ1Threads + threadIdx.x;
+            const bool ok = i < n;
+#pragma unroll
+            for (int b = 0; b < 9; ++b) bv[k][b] = ok ? __ldcs(bands + b * n + i) : T(0);
+            rh[k] = (MODE != 0 && ok) ? rhs[i] : T(0);
+            dv[k] = (MODE == 2 && ok) ? dinv[i] : T(0);
+        }
         if (threadIdx.x == 0)
         {
             mbar_init(&bar, 1);
@@ -120,9 +135,9 @@ namespace hb2
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
-            const int64_t i = r0 + (int64_t)threadIdx.x * R + k;
+            const int64_t i = r0 + (int64_t)k * kQ1Threads + threadIdx.x;
             if (i >= n) break;
-            T s = M::mul(__ldcs(bands + 4 * n + i), win[1][i - base[1]]);
+            T s = M::mul(bv[k][4], win[1][i - base[1]]);
 #pragma unroll
             for (int b = 0; b < 9; ++b)
             {
@@ -130,11 +145,11 @@ namespace hb2
                 const int64_t j = i + off[b];
                 if (j < 0 || j >= n) continue;
                 const int w = b / 3;
-                s = M::add(s, M::mul(__ldcs(bands + b * n + i), win[w][j - base[w]]));
+                s = M::add(s, M::mul(bv[k][b], win[w][j - base[w]]));
             }
             if (MODE == 0) y[i] = s;
-            else if (MODE == 1) y[i] = M::sub(rhs[i], s);
-            else y[i] = M::add(win[1][i - base[1]], M::mul(M::sub(rhs[i], s), dinv[i]));
+            else if (MODE == 1) y[i] = M::sub(rh[k], s);
+            else y[i] = M::add(win[1][i - base[1]], M::mul(M::sub(rh[k], s), dv[k]));
         }
     }
 
