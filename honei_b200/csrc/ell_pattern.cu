@@ -172,6 +172,19 @@ namespace hb2
                 if (MODE == kDot) ex[i] = ok ? x[r] : T(0);
                 if (MODE == kAdd) ex[i] = ok ? y[r] : T(0);
             }
+            // per row, once: the bound test, the row's x pointer (a gather is then one
+            // sign-extended offset) and its pattern's table entries
+            bool rok[R];
+            const T * xr[R];
+            const PatEnt<T> * te[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+            {
+                const uint64_t r = r0 + 32 * i;
+                rok[i] = r < A.rows;
+                xr[i] = x + (rok[i] ? r : 0);
+                te[i] = tab + p[i] * (uint32_t)K;
+            }
 #pragma unroll
             for (int k = 0; k < (KT > 0 ? KT : kPatMaxK); ++k)
             {
@@ -179,10 +192,8 @@ namespace hb2
 #pragma unroll
                 for (int i = 0; i < R; ++i)
                 {
-                    const uint64_t r = r0 + 32 * i;
-                    const PatEnt<T> e = tab[p[i] * (uint32_t)K + k];
-                    if (r < A.rows && e.off != kPatEmpty)
-                        acc[i] = M::add(acc[i], M::mul(e.val, __ldg(x + (uint32_t)((int32_t)r + e.off))));
+                    const PatEnt<T> e = te[i][k];
+                    if (rok[i] && e.off != kPatEmpty) acc[i] = M::add(acc[i], M::mul(e.val, __ldg(xr[i] + e.off)));
                 }
             }
             double part = 0.0;

@@ -171,8 +171,10 @@ namespace hb2
     uint64_t list_grid_cap();
 
     // one slot of a row pattern: value and column - row (kPatEmpty past the row)
+    // aligned to its size so that one entry is one 128-bit (FP64) / 64-bit (FP32)
+    // shared-memory load
     template <typename T>
-    struct PatEnt
+    struct alignas(2 * sizeof(T)) PatEnt
     {
         T val;
         int32_t off;
