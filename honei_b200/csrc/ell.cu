@@ -206,7 +206,7 @@ namespace hb2
     uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)
     {
         const int cls = reducing ? 1 : 0;
-        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * A->rpt[cls];
+        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * (A->rpt[cls] & ~kPatWin);
         if (A->layout[cls] == kLayoutCompact) return (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt);
         return (uint64_t)kEllThreads * (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
     }

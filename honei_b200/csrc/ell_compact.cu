@@ -511,6 +511,8 @@ namespace hb2
                                                      {kLayoutCompact, 8}};
         if (A->pat)
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
+        if (A->pat && A->pat_win_m)
+            for (int r : {1, 2}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatWin));
         float best[2] = {1e30f, 1e30f};
         Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}};
         for (int cls = 0; cls < (square ? 2 : 1); ++cls)
@@ -575,14 +577,19 @@ namespace hb2
         {
             // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
             // rows per thread; pattern[1|2|4]: the row-pattern layout (square
+            // matrices that admit it; patternwin[1|2] its windowed kernel where the
+            // offsets allow;
             // matrices that admit it; the others compressed, 2 rows per thread);
             // no autotuning
             Choice c;
             if (v[0] == 'p' && A->pat)
             {
-                const int r = atoi(v + 7);
+                // patternwin[1|2]: the windowed kernel where the matrix admits it
+                const bool win = strncmp(v, "patternwin", 10) == 0;
+                const int r = atoi(v + (win ? 10 : 7));
                 c.layout[0] = c.layout[1] = kLayoutPattern;
                 c.rpt[0] = c.rpt[1] = (r == 2 || r == 4) ? r : 1;
+                if (win && A->pat_win_m && c.rpt[0] <= 2) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatWin;
             }
             else
             {

@@ -17,6 +17,7 @@
 // kernel class whether this layout is the fastest.
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
+#include "tma.cuh"
 
 #include <climits>
 #include <cstdlib>
@@ -227,6 +228,149 @@ namespace hb2
         }
     }
 
+    // diagnostic: set when a windowed block's copies did not complete in time (the
+    // block then computed from global memory)
+    __device__ int g_pat_win_timeout = 0;
+
+    // The row-pattern kernel for a square matrix whose pattern offsets all lie in the
+    // three bands around -m, 0, +m (the Q1 operators, m^2 rows).  A block owns
+    // B = 256 R rows, interleaved over its threads; thread 0 stages the three windows
+    // of x that the bands touch with bulk copies (as the banded kernel does) while
+    // every thread loads its rows' pattern ids and vectors; the gathers then read
+    // shared memory.  Each table entry carries its window-relative offset for this
+    // block.  If the copies have not completed within the bounded wait, the block
+    // computes from global memory (same bits) and waits for them once more before
+    // it exits.
+    template <typename T, int MODE, int R>
+    __global__ void __launch_bounds__(kEllThreads)
+    ell_pattern_win_kernel(EllPatternView<T> A, int64_t m, const T * __restrict__ x, T * __restrict__ y,
+                           const T * __restrict__ aux, const T * __restrict__ aux2, T * __restrict__ zero,
+                           ReduceSlot rs, double * red, int want_sqrt)
+    {
+        typedef Arith<T> M;
+        constexpr int K = 9;
+        constexpr int B = kEllThreads * R;
+        constexpr int E = 16 / sizeof(T);
+        constexpr int W = (B + 2 + 2 * E + E - 1) / E * E;
+        struct alignas(16) WEnt
+        {
+            T val;
+            int32_t off;    // column - row (kPatEmpty past the row)
+            int32_t rel;    // index in `win` minus the row
+        };
+        __shared__ WEnt tab[kPatMax * K];
+        __shared__ alignas(128) T win[3 * W];
+        __shared__ alignas(8) uint64_t bar;
+        __shared__ int64_t base[3];
+        const int64_t n = (int64_t)A.rows;
+        const int64_t r0 = (int64_t)blockIdx.x * B;
+        const unsigned t = threadIdx.x;
+        uint32_t p[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = r0 + (int64_t)k * kEllThreads + t;
+            p[k] = i < n ? (uint32_t)__ldcs(A.pat + i) : 0u;
+        }
+        pdl_entry();   // the vectors below may come from the previous kernel
+        T ea[R], ep[R], ey[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = r0 + (int64_t)k * kEllThreads + t;
+            const bool ok = i < n;
+            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi)) ? aux[i] : T(0);
+            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+            ey[k] = (ok && MODE == kAdd) ? y[i] : T(0);
+        }
+        if (t == 0)
+        {
+            mbar_init(&bar, 1);
+            const int64_t starts[3] = {r0 - m - 1, r0 - 1, r0 + m - 1};
+            unsigned total = 0;
+            int64_t lo[3], ahi[3], alo[3], hi[3];
+            for (int w = 0; w < 3; ++w)
+            {
+                lo[w] = starts[w] < 0 ? 0 : starts[w];
+                hi[w] = starts[w] + B + 2 > n ? n : starts[w] + B + 2;
+                if (hi[w] < lo[w]) hi[w] = lo[w];
+                alo[w] = lo[w] - (lo[w] % E);
+                ahi[w] = hi[w] - (hi[w] % E);
+                if (ahi[w] < alo[w]) ahi[w] = alo[w];
+                base[w] = alo[w];
+                total += (unsigned)((ahi[w] - alo[w]) * sizeof(T));
+            }
+            mbar_expect_tx(&bar, total);
+            for (int w = 0; w < 3; ++w)
+            {
+                if (ahi[w] > alo[w])
+                    bulk_g2s(&win[w * W], x + alo[w], (unsigned)((ahi[w] - alo[w]) * sizeof(T)), &bar);
+                for (int64_t j = (ahi[w] > lo[w] ? ahi[w] : lo[w]); j < hi[w]; ++j) win[w * W + (j - alo[w])] = x[j];
+            }
+        }
+        __syncthreads();
+        for (uint32_t j = t; j < A.npat * (uint32_t)K; j += kEllThreads)
+        {
+            const PatEnt<T> e = A.tab[j];
+            WEnt q;
+            q.val = e.val;
+            q.off = e.off;
+            q.rel = 0;
+            if (e.off != kPatEmpty)
+            {
+                const int w = e.off <= -2 ? 0 : (e.off <= 1 ? 1 : 2);
+                q.rel = (int32_t)((int64_t)e.off - base[w] + (int64_t)w * W);
+            }
+            tab[j] = q;
+        }
+        __syncthreads();
+        const bool fast = mbar_wait_bounded(&bar, 0, 1000000000ull);
+        if (! fast && t == 0) atomicExch(&g_pat_win_timeout, 1);
+        double part = 0.0;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = r0 + (int64_t)k * kEllThreads + t;
+            if (i >= n) continue;
+            const WEnt * te = tab + p[k] * K;
+            T acc = T(0);
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+            {
+                const WEnt e = te[j];
+                if (e.off != kPatEmpty)
+                {
+                    const T xv = fast ? win[i + e.rel] : __ldg(x + (i + e.off));
+                    acc = M::add(acc, M::mul(e.val, xv));
+                }
+            }
+            const T xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[(i - base[1]) + W] : x[i]) : T(0);
+            if (MODE == kPlain) y[i] = acc;
+            else if (MODE == kDefect)
+            {
+                const T d = M::sub(ea[k], acc);
+                y[i] = d;
+                part = fma((double)d, (double)d, part);
+            }
+            else if (MODE == kDot)
+            {
+                y[i] = acc;
+                part = fma((double)acc, (double)xc, part);
+            }
+            else if (MODE == kAdd) y[i] = M::add(ey[k], acc);
+            else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep[k], M::sub(ea[k], acc)));
+            else if (MODE == kRestrict) { y[i] = acc; zero[i] = T(0); }
+        }
+        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        {
+            __shared__ double scratch[32];
+            const double sum = block_sum(part, scratch);
+            grid_sum_finish(sum, rs, red, want_sqrt, scratch);
+        }
+        // copies still in flight must land before the block's shared memory is reused
+        if (! fast) mbar_wait_bounded(&bar, 0, 1000000000ull);
+    }
+
     template <typename T, int MODE>
     static void pattern_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
                              void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
@@ -238,6 +382,20 @@ namespace hb2
         v.rows = A->rows;
         v.K = A->K;
         v.npat = A->npat;
+        // the window copies need a 16-byte aligned x
+        if ((R & kPatWin) && A->pat_win_m && A->K == 9 && ! b.list && b.nvec == 1 && ! b.active &&
+            ((uintptr_t)x & 15) == 0)
+        {
+            const int Rw = R & ~kPatWin;
+            if (Rw == 1)
+                launch_pdl(ell_pattern_win_kernel<T, MODE, 1>, grid, dim3(kEllThreads), 0, s, v, A->pat_win_m,
+                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt);
+            else
+                launch_pdl(ell_pattern_win_kernel<T, MODE, 2>, grid, dim3(kEllThreads), 0, s, v, A->pat_win_m,
+                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt);
+            return;
+        }
+        R &= ~kPatWin;
 #define HB2_PAT_LAUNCH(KT_, R_)                                                                              \
         launch_pdl(ell_pattern_kernel<T, KT_, MODE, R_>, grid, dim3(kEllThreads), 0, s, v, (const T *)x, (T *)y, \
                    (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags, b)
@@ -358,6 +516,26 @@ namespace hb2
             return e == cudaSuccess ? HB2_OK : cuda_status(e, "ELL row patterns");
         }
         A->pattern_bytes = rows + (uint64_t)np * A->K * sizeof(PatEnt<T>);
+        // the windowed kernel applies when every offset lies in the bands around -m, 0, +m
+        {
+            std::vector<PatEnt<T>> htab((size_t)np * A->K);
+            A->pat_win_m = 0;
+            int64_t mm = 1;
+            while (mm * mm < (int64_t)rows) ++mm;
+            if (A->K == 9 && mm * mm == (int64_t)rows && mm >= 3 && (int64_t)rows < (1ll << 31) &&
+                cudaMemcpy(htab.data(), A->ptab, htab.size() * sizeof(PatEnt<T>), cudaMemcpyDeviceToHost) == cudaSuccess)
+            {
+                bool ok_win = true;
+                for (const auto & e : htab)
+                {
+                    if (e.off == kPatEmpty) continue;
+                    const int64_t o = e.off;
+                    if (! ((o >= -mm - 1 && o <= -mm + 1) || (o >= -1 && o <= 1) || (o >= mm - 1 && o <= mm + 1)))
+                        ok_win = false;
+                }
+                if (ok_win) A->pat_win_m = mm;
+            }
+        }
         return HB2_OK;
     }
 

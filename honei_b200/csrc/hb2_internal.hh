@@ -86,6 +86,10 @@ struct hb2_ell_s
     void * ptab = nullptr;
     uint32_t npat = 0;
     uint64_t pattern_bytes = 0;
+    // m when every pattern offset lies in the three bands around -m, 0, +m of a
+    // square matrix of m^2 rows (the Q1 operators): the windowed pattern kernel
+    // applies (rpt | kPatWin); 0 otherwise
+    int64_t pat_win_m = 0;
     // row patterns of a small square matrix for the fused small-level kernels
     // (subcycle.cu), built on the host when the matrix joins a hierarchy
     uint8_t * spat = nullptr;
@@ -180,6 +184,7 @@ namespace hb2
         int32_t off;
     };
     constexpr int32_t kPatEmpty = (-2147483647 - 1);
+    constexpr int kPatWin = 0x10;    // rpt flag: the windowed row-pattern kernel
     constexpr int kSubPatMax = 8;    // patterns of a small-level operator in the fused kernels
     int ell_small_patterns(hb2_ell_s * A);
 

@@ -12,52 +12,12 @@
 // the result is bit-identical to the reference.
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
+#include "tma.cuh"
 
 namespace hb2
 {
     constexpr int kQ1Threads = 256;
 
-    __device__ __forceinline__ uint32_t smem_addr(const void * p)
-    {
-        return (uint32_t)__cvta_generic_to_shared(p);
-    }
-
-    __device__ __forceinline__ void mbar_init(uint64_t * bar, unsigned count)
-    {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-
-    __device__ __forceinline__ void mbar_expect_tx(uint64_t * bar, unsigned bytes)
-    {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(bytes)
-                     : "memory");
-    }
-
-    __device__ __forceinline__ void bulk_g2s(void * dst, const void * src, unsigned bytes, uint64_t * bar)
-    {
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                     :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
-    }
-
-    __device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, unsigned parity)
-    {
-        uint32_t ok;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
-        return ok != 0;
-    }
-
-    // bounded wait: false after limit_ns without completion
-    __device__ __forceinline__ bool mbar_wait_bounded(uint64_t * bar, unsigned parity, unsigned long long limit_ns)
-    {
-        if (mbar_try_wait(bar, parity)) return true;
-        unsigned long long t0 = global_ns();
-        while (! mbar_try_wait(bar, parity))
-            if (global_ns() - t0 > limit_ns) return false;
-        return true;
-    }
 
     template <typename T>
     struct Window

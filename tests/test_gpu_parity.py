@@ -429,11 +429,13 @@ def test_ir_mixed_fp64_coarse(oracle):
     assert it <= 6
 
 
-@pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4"])
+@pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4", "patternwin1",
+                                    "patternwin2"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     """Value-dictionary + 16-bit offset layout (forceR) and row-pattern layout (patternR,
-    square matrices; the rectangular transfers stay compressed): same bits as the plain
+    square matrices, patternwinR with x staged in shared-memory windows; the rectangular
+    transfers stay compressed): same bits as the plain
     layout (and the oracle) for every ELL kernel mode, square and rectangular."""
     from honei_b200 import _lib
     npdt = np.float64 if dt == torch.float64 else np.float32
