@@ -32,6 +32,7 @@ namespace
     struct KState
     {
         double alpha_new, alpha, temp, init, cur;          // CG
+        double alpha_next;                                 // CG, vector P: <r, d (.) r> of the new r
         double rho, rho_new, gamma, omega, ab, d0, d00, defnorm;   // BiCGStab
         unsigned long long iter, used;
         int stage, restart, first, converged;
@@ -115,6 +116,39 @@ namespace
             p[i] = __dadd_rn(__dmul_rn(p[i], ta), z[i]);
     }
 
+    // CG with a vector P: the update also forms z = d (.) r of the new r and
+    // alpha_next = <z, r> (plus ||r||^2 unless smoothing); z is not stored
+    template <bool NORM>
+    __global__ void __launch_bounds__(kVecThreads) k_cg_update_diag(uint64_t n, double * x, double * r,
+                                                                    const double * p, const double * v,
+                                                                    const double * d, const KState * st,
+                                                                    ReduceSlot rs, double * out_z, double * out_n)
+    {
+        __shared__ double scratch[32];
+        const double lambda = st->alpha_new / eps_guard(st->temp), ml = -lambda;
+        double acc[2] = {0.0, 0.0};
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        {
+            x[i] = axpy(lambda, p[i], x[i]);
+            const double ri = axpy(ml, v[i], r[i]);
+            r[i] = ri;
+            const double zi = __dmul_rn(d[i], ri);
+            acc[0] = fma(zi, ri, acc[0]);
+            if (NORM) acc[1] = fma(ri, ri, acc[1]);
+        }
+        if (NORM) finish<2>(acc, rs, out_z, out_n, scratch);
+        else finish<1>(acc, rs, out_z, nullptr, scratch);
+    }
+
+    // CG with a vector P: p = p * talpha + d (.) r (z formed again, each step rounded)
+    __global__ void __launch_bounds__(kVecThreads) k_cg_p_diag(uint64_t n, double * p, const double * d,
+                                                               const double * r, const KState * st)
+    {
+        const double ta = st->alpha_new / eps_guard(st->alpha);
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+            p[i] = __dadd_rn(__dmul_rn(p[i], ta), __dmul_rn(d[i], r[i]));
+    }
+
     __global__ void k_cg_init(KState * st, uint64_t max_iters, cudaGraphConditionalHandle h)
     {
         st->iter = 0;
@@ -122,8 +156,9 @@ namespace
         cudaGraphSetConditional(h, max_iters > 0 ? 1u : 0u);
     }
 
-    // math/cg.hh:178-198 (smoother: math/cg.hh:263-267)
-    __global__ void k_cg_decide(KState * st, uint64_t max_iters, double eps, int smoother,
+    // math/cg.hh:178-198 (smoother: math/cg.hh:263-267); fused: the next alpha_new
+    // was already reduced by the update (vector P)
+    __global__ void k_cg_decide(KState * st, uint64_t max_iters, double eps, int smoother, int fused,
                                 cudaGraphConditionalHandle h)
     {
         const unsigned long long it = st->iter + 1;
@@ -138,6 +173,7 @@ namespace
         }
         if (stop) st->used = it;
         st->alpha = st->alpha_new;
+        if (fused) st->alpha_new = st->alpha_next;
         cudaGraphSetConditional(h, stop ? 0u : 1u);
     }
 
@@ -414,9 +450,25 @@ namespace
         cudaStream_t s = K->cap2;
         int e = launch_ell(K->A, kDot, p, v, 0, 0, 0, &st->temp, 0, K->ws, s);
         if (e) return e;
+        if (K->pdiag)
+        {
+            // vector P: z = d (.) r and <z, r> fused into the update, z formed again in
+            // the direction update -- four kernels per iteration
+            if (smoother)
+                k_cg_update_diag<false><<<vgrid(n), kVecThreads, 0, s>>>(n, x, r, p, v, K->pdiag, st, K->ws->slot(),
+                                                                          &st->alpha_next, nullptr);
+            else
+                k_cg_update_diag<true><<<vgrid(n), kVecThreads, 0, s>>>(n, x, r, p, v, K->pdiag, st, K->ws->slot(),
+                                                                         &st->alpha_next, &st->cur);
+            k_cg_decide<<<1, 1, 0, s>>>(st, K->max_iters, K->eps, smoother ? 1 : 0, 1, h_loop);
+            k_cg_p_diag<<<vgrid(n), kVecThreads, 0, s>>>(n, p, K->pdiag, r, st);
+            count_launches(3);
+            HB2_LAUNCH_CHECK("krylov CG (vector P)");
+            return HB2_OK;
+        }
         if (smoother) k_cg_update<false><<<vgrid(n), kVecThreads, 0, s>>>(n, x, r, p, v, st, K->ws->slot(), nullptr);
         else k_cg_update<true><<<vgrid(n), kVecThreads, 0, s>>>(n, x, r, p, v, st, K->ws->slot(), &st->cur);
-        k_cg_decide<<<1, 1, 0, s>>>(st, K->max_iters, K->eps, smoother ? 1 : 0, h_loop);
+        k_cg_decide<<<1, 1, 0, s>>>(st, K->max_iters, K->eps, smoother ? 1 : 0, 0, h_loop);
         count_launches(2);
         HB2_LAUNCH_CHECK("krylov CG update");
         if (K->pdiag) e = precond(K, r, z, r, &st->alpha_new, nullptr, nullptr, nullptr, nullptr, s);

@@ -117,10 +117,10 @@ def main(argv=None) -> int:
         ms = statistics.median(ts)
         its = used - 1 if a.kernel == "bicgstab" else used
         # algorithmic bytes per iteration: the SpMV(s) (matrix bytes + x + y) and the
-        # vector passes (CG VAR: update 48, Jacobi + dot 24, direction 24 bytes per
-        # row; BiCGStab: 2 Jacobi products 2*24, s 40, t dots 16, update 56, r~ 32,
-        # direction 32 bytes per row)
-        per_row = (rb + 16 + 96) if a.kernel == "cgvar" else (2 * (rb + 16) + 48 + 40 + 16 + 56 + 32 + 32)
+        # vector passes (CG VAR: update with z = d (.) r and its dot 56, direction 32
+        # bytes per row; BiCGStab: 2 Jacobi products 2*24, s 40, t dots 16, update 56,
+        # r~ 32, direction 32 bytes per row)
+        per_row = (rb + 16 + 88) if a.kernel == "cgvar" else (2 * (rb + 16) + 48 + 40 + 16 + 56 + 32 + 32)
         nbytes = n * per_row
         us_it = 1000 * ms / its
         print(json.dumps({"kernel": a.kernel, "level": L, "rows": n, "iterations": its, "solve_ms": ms,
