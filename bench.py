@@ -339,7 +339,7 @@ def main():
     xa = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
     xb = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
     kms = []
-    for i in range(args.warmup + max(args.steps, 10)):
+    for i in range(args.warmup + max(args.steps, 30)):
         flush.zero_()
         k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k0.record(stream)

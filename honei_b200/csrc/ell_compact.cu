@@ -48,6 +48,20 @@ namespace hb2
         return rows == cols ? (int64_t)r : (int64_t)((r * cols) / rows);
     }
 
+    // row_base without the 64-bit division, for the kernels: ratio = cols / rows
+    // rounded to double.  For r < rows < 2^32 and cols < 2^31 the estimate
+    // r * ratio is within 2^-20 of r * cols / rows, so its truncation is off by at
+    // most one, and the exact integer products settle which way.
+    __device__ __forceinline__ int64_t row_base_est(uint64_t r, uint64_t rows, uint64_t cols, double ratio)
+    {
+        if (rows == cols) return (int64_t)r;
+        const uint64_t num = r * cols;
+        uint64_t q = (uint64_t)((double)r * ratio);
+        if (q * rows > num) --q;
+        else if ((q + 1) * rows <= num) ++q;
+        return (int64_t)q;
+    }
+
     // one insert per distinct value of a warp: matrices with few values would
     // otherwise send every slot's atomic to the same few addresses
     template <typename T>
@@ -113,6 +127,7 @@ namespace hb2
         const T * table;
         uint64_t rows, cols, ld;
         uint32_t K, ntable;
+        double ratio;   // cols / rows (row_base_est)
     };
 
     // one thread: R consecutive rows; per slot it loads R one-byte codes and R
@@ -187,7 +202,7 @@ namespace hb2
         {
             int64_t base[R];
 #pragma unroll
-            for (int i = 0; i < R; ++i) base[i] = row_base(r0 + i, A.rows, A.cols);
+            for (int i = 0; i < R; ++i) base[i] = row_base_est(r0 + i, A.rows, A.cols, A.ratio);
             if constexpr (KT > 0)
             {
                 CW cw[KT];
@@ -268,6 +283,7 @@ namespace hb2
         v.ld = A->ld;
         v.K = A->K;
         v.ntable = A->ntable;
+        v.ratio = (double)A->cols / (double)A->rows;
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         const T * ap = (const T *)aux;
@@ -513,38 +529,47 @@ namespace hb2
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         if (A->pat && A->pat_win_m)
             for (int r : {1, 2}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatWin));
-        float best[2] = {1e30f, 1e30f};
+        // Each candidate is timed as a burst of back-to-back launches (the way the
+        // solvers issue them, and long enough for the event clock's granularity),
+        // the candidates interleaved over several rounds so that clock or
+        // neighbour drift hits all of them; a candidate's time is its best round.
+        constexpr int kRounds = 4, kBurst = 8;
         Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}};
-        for (int cls = 0; cls < (square ? 2 : 1); ++cls)
-            for (const auto & v : variants)
-            {
+        for (int cls = 0; cls < (square ? 2 : 1) && ! st; ++cls)
+        {
+            std::vector<float> best(variants.size(), 1e30f);
+            auto select = [&](const std::pair<int, int> & v) {
                 A->layout[cls] = v.first;
                 A->rpt[cls] = v.second;
                 if (v.first == kLayoutCompact) (cls ? A->compact_rpt_red : A->compact_rpt) = v.second;
-                // a fused reduction needs one partial per row block: shapes beyond
-                // the workspace are not candidates
-                if (cls == 1 && (uint64_t)ell_grid(A, true) > ws->max_blocks) continue;
-                float total = 0.f;
-                for (int rep = 0; rep < 4; ++rep)
+            };
+            for (int round = 0; round <= kRounds && ! st; ++round)   // round 0 warms up
+                for (size_t vi = 0; vi < variants.size() && ! st; ++vi)
                 {
+                    select(variants[vi]);
+                    // a fused reduction needs one partial per row block: shapes beyond
+                    // the workspace are not candidates
+                    if (cls == 1 && (uint64_t)ell_grid(A, true) > ws->max_blocks) continue;
                     cudaEventRecord(e0, s);
-                    st = cls == 0 ? launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s)
-                                  : launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s);
+                    for (int b = 0; b < kBurst && ! st; ++b)
+                        st = cls == 0 ? launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s)
+                                      : launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s);
                     cudaEventRecord(e1, s);
                     if (st) break;
                     cudaEventSynchronize(e1);
                     float ms = 0.f;
                     cudaEventElapsedTime(&ms, e0, e1);
-                    if (rep > 0) total += ms;
+                    if (round > 0 && ms < best[vi]) best[vi] = ms;
                 }
-                if (st) break;
-                if (total < best[cls])
+            float best_ms = 1e30f;
+            for (size_t vi = 0; vi < variants.size(); ++vi)
+                if (best[vi] < best_ms)
                 {
-                    best[cls] = total;
-                    c.layout[cls] = v.first;
-                    c.rpt[cls] = v.second;
+                    best_ms = best[vi];
+                    c.layout[cls] = variants[vi].first;
+                    c.rpt[cls] = variants[vi].second;
                 }
-            }
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaStreamSynchronize(s);
