@@ -355,7 +355,9 @@ def main():
     k_bytes = (row_bytes + 4 * 8) * n
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
     peaks = load_peaks()
-    traffic = load_traffic()
+    vkind, vrpt, vwin = A.layout_variant(0)
+    variant = variant_name(vkind, vrpt, vwin)
+    traffic = load_traffic(variant)
 
     solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)),
                                  layout_row_bytes(hb, torch.float64, range(MIN_LEVEL, L + 1)))
@@ -368,8 +370,9 @@ def main():
         "latency_ms": {"p50": percentile(step_ms, 50), "p99": percentile(step_ms, 99), "max": max(step_ms)},
         "cycles": int(statistics.median(cycles)), "relres": relres,
         "wall_ms_per_step_incl_flush": 1000 * t_wall / args.steps,
-        "roofline": {"bound": "hbm", "kernel": "%s<double,9,kJacobi> (fused Jacobi sweep, level %d)" % (
-                         KERNEL_OF_LAYOUT[kind], L),
+        "roofline": {"bound": "hbm", "kernel": "%s, Jacobi mode, %d rows per thread (fused Jacobi sweep, level %d)" % (
+                         "ell_pattern_win_kernel" if vwin else KERNEL_OF_LAYOUT[kind], vrpt, L),
+                     "variant": variant,
                      "layout": layout_text(kind, table_size, row_bytes + 32),
                      "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
                      "peak_source": peaks[1], "traffic": traffic, "algorithmic_bytes": k_bytes,
@@ -685,12 +688,24 @@ def load_peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def load_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def variant_name(kind, rows_per_thread, windowed):
+    """Name of an ELL kernel variant as HB2_ELL_COMPACT spells it (plain, forceR,
+    patternR, patternwinR)."""
+    if kind == 2:
+        return ("patternwin%d" if windowed else "pattern%d") % rows_per_thread
+    if kind == 1:
+        return "force%d" % rows_per_thread
+    return "plain"
+
+
+def load_traffic(variant):
+    """DRAM bytes per launch of the dominant kernel, for the variant the autotuner
+    chose, from the committed ncu summary (None when that variant was not captured)."""
     path = os.path.join(ROOT, "profiles", "ell_jacobi_sweep_fp64_level10.md")
+    key = "traffic_bytes_per_launch[%s]:" % variant
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key):
                 return float(line.split(":", 1)[1])
     except Exception:
         pass

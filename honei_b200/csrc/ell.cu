@@ -658,6 +658,17 @@ extern "C" int hb2_ell_layout(hb2_ell A, int * layout, uint32_t * table_size, ui
     return HB2_OK;
 }
 
+extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * rows_per_thread, int * windowed)
+{
+    if (! A) return fail(HB2_ERR_ARG, "hb2_ell_layout_variant: null matrix");
+    if (cls != 0 && cls != 1) return fail(HB2_ERR_ARG, "hb2_ell_layout_variant: class must be 0 or 1");
+    const int l = A->layout[cls];
+    if (layout) *layout = l;
+    if (rows_per_thread) *rows_per_thread = (int)(ell_rows_per_block(A, cls == 1) / kEllThreads);
+    if (windowed) *windowed = (l == kLayoutPattern && (A->rpt[cls] & kPatWin)) ? 1 : 0;
+    return HB2_OK;
+}
+
 extern "C" int hb2_ell_export(hb2_ell A, uint64_t * Aj, void * Ax, uint64_t * Arl)
 {
     if (! A || ! Aj || ! Ax || ! Arl) return fail(HB2_ERR_ARG, "hb2_ell_export: null argument");

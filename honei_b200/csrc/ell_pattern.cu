@@ -232,15 +232,38 @@ namespace hb2
     // block then computed from global memory)
     __device__ int g_pat_win_timeout = 0;
 
+    // Extent of one x window of the windowed kernel: rows [lo, hi) of x (the
+    // window's B + 2 rows clipped to the vector), of which the bulk copy moves
+    // [alo, ahi) (ends rounded down to 16 bytes); plain loads fetch the ragged
+    // tail [max(ahi, lo), hi), at most E - 1 elements.
+    struct WinGeom
+    {
+        int64_t lo, hi, alo, ahi;
+    };
+
+    template <int B, int E>
+    __device__ __forceinline__ WinGeom win_geom(int64_t start, int64_t n)
+    {
+        WinGeom g;
+        g.lo = start < 0 ? 0 : start;
+        g.hi = start + B + 2 > n ? n : start + B + 2;
+        if (g.hi < g.lo) g.hi = g.lo;
+        g.alo = g.lo - (g.lo % E);
+        g.ahi = g.hi - (g.hi % E);
+        return g;
+    }
+
     // The row-pattern kernel for a square matrix whose pattern offsets all lie in the
     // three bands around -m, 0, +m (the Q1 operators, m^2 rows).  A block owns
     // B = 256 R rows, interleaved over its threads; thread 0 stages the three windows
-    // of x that the bands touch with bulk copies (as the banded kernel does) while
-    // every thread loads its rows' pattern ids and vectors; the gathers then read
-    // shared memory.  Each table entry carries its window-relative offset for this
-    // block.  If the copies have not completed within the bounded wait, the block
-    // computes from global memory (same bits) and waits for them once more before
-    // it exits.
+    // of x that the bands touch with bulk copies (as the banded kernel does) and
+    // threads 1 .. 3 (E - 1) fetch the windows' ragged tails, while every thread loads
+    // its rows' pattern ids and vectors and its share of the pattern table; the
+    // block meets once, and the gathers then read shared memory.  Each table entry
+    // carries its window-relative offset for this block (every thread computes the
+    // window geometry itself).  If the copies have not completed within the bounded
+    // wait, the block computes from global memory (same bits) and waits for them
+    // once more before it exits.
     template <typename T, int MODE, int R>
     __global__ void __launch_bounds__(kEllThreads)
     ell_pattern_win_kernel(EllPatternView<T> A, int64_t m, const T * __restrict__ x, T * __restrict__ y,
@@ -252,6 +275,7 @@ namespace hb2
         constexpr int B = kEllThreads * R;
         constexpr int E = 16 / sizeof(T);
         constexpr int W = (B + 2 + 2 * E + E - 1) / E * E;
+        constexpr int TE = (kPatMax * K + kEllThreads - 1) / kEllThreads;   // table entries per thread
         struct alignas(16) WEnt
         {
             T val;
@@ -261,16 +285,25 @@ namespace hb2
         __shared__ WEnt tab[kPatMax * K];
         __shared__ alignas(128) T win[3 * W];
         __shared__ alignas(8) uint64_t bar;
-        __shared__ int64_t base[3];
         const int64_t n = (int64_t)A.rows;
         const int64_t r0 = (int64_t)blockIdx.x * B;
         const unsigned t = threadIdx.x;
+        const int64_t starts[3] = {r0 - m - 1, r0 - 1, r0 + m - 1};
         uint32_t p[R];
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
             const int64_t i = r0 + (int64_t)k * kEllThreads + t;
             p[k] = i < n ? (uint32_t)__ldcs(A.pat + i) : 0u;
+        }
+        // the pattern table is constant: fetched before the wait on the previous kernel
+        const uint32_t nent = A.npat * (uint32_t)K;
+        PatEnt<T> mine[TE];
+#pragma unroll
+        for (int q = 0; q < TE; ++q)
+        {
+            const uint32_t j = t + q * kEllThreads;
+            if (j < nent) mine[q] = A.tab[j];
         }
         pdl_entry();   // the vectors below may come from the previous kernel
         T ea[R], ep[R], ey[R];
@@ -286,42 +319,49 @@ namespace hb2
         if (t == 0)
         {
             mbar_init(&bar, 1);
-            const int64_t starts[3] = {r0 - m - 1, r0 - 1, r0 + m - 1};
+            WinGeom g[3];
             unsigned total = 0;
-            int64_t lo[3], ahi[3], alo[3], hi[3];
+#pragma unroll
             for (int w = 0; w < 3; ++w)
             {
-                lo[w] = starts[w] < 0 ? 0 : starts[w];
-                hi[w] = starts[w] + B + 2 > n ? n : starts[w] + B + 2;
-                if (hi[w] < lo[w]) hi[w] = lo[w];
-                alo[w] = lo[w] - (lo[w] % E);
-                ahi[w] = hi[w] - (hi[w] % E);
-                if (ahi[w] < alo[w]) ahi[w] = alo[w];
-                base[w] = alo[w];
-                total += (unsigned)((ahi[w] - alo[w]) * sizeof(T));
+                g[w] = win_geom<B, E>(starts[w], n);
+                total += (unsigned)((g[w].ahi - g[w].alo) * sizeof(T));
             }
             mbar_expect_tx(&bar, total);
+#pragma unroll
             for (int w = 0; w < 3; ++w)
-            {
-                if (ahi[w] > alo[w])
-                    bulk_g2s(&win[w * W], x + alo[w], (unsigned)((ahi[w] - alo[w]) * sizeof(T)), &bar);
-                for (int64_t j = (ahi[w] > lo[w] ? ahi[w] : lo[w]); j < hi[w]; ++j) win[w * W + (j - alo[w])] = x[j];
-            }
+                if (g[w].ahi > g[w].alo)
+                    bulk_g2s(&win[w * W], x + g[w].alo, (unsigned)((g[w].ahi - g[w].alo) * sizeof(T)), &bar);
         }
-        __syncthreads();
-        for (uint32_t j = t; j < A.npat * (uint32_t)K; j += kEllThreads)
+        else if (t <= 3 * (E - 1))
         {
-            const PatEnt<T> e = A.tab[j];
-            WEnt q;
-            q.val = e.val;
-            q.off = e.off;
-            q.rel = 0;
-            if (e.off != kPatEmpty)
+            const int w = (int)(t - 1) / (E - 1), e = (int)(t - 1) % (E - 1);
+            const WinGeom g = win_geom<B, E>(w == 0 ? starts[0] : (w == 1 ? starts[1] : starts[2]), n);
+            const int64_t j = (g.ahi > g.lo ? g.ahi : g.lo) + e;
+            if (j < g.hi) win[w * W + (j - g.alo)] = x[j];
+        }
+        int64_t wbase[3];
+#pragma unroll
+        for (int w = 0; w < 3; ++w) wbase[w] = win_geom<B, E>(starts[w], n).alo;
+#pragma unroll
+        for (int q = 0; q < TE; ++q)
+        {
+            const uint32_t j = t + q * kEllThreads;
+            if (j < nent)
             {
-                const int w = e.off <= -2 ? 0 : (e.off <= 1 ? 1 : 2);
-                q.rel = (int32_t)((int64_t)e.off - base[w] + (int64_t)w * W);
+                const PatEnt<T> e = mine[q];
+                WEnt qe;
+                qe.val = e.val;
+                qe.off = e.off;
+                qe.rel = 0;
+                if (e.off != kPatEmpty)
+                {
+                    const int w = e.off <= -2 ? 0 : (e.off <= 1 ? 1 : 2);
+                    const int64_t wb = w == 0 ? wbase[0] : (w == 1 ? wbase[1] : wbase[2]);
+                    qe.rel = (int32_t)((int64_t)e.off - wb + (int64_t)w * W);
+                }
+                tab[j] = qe;
             }
-            tab[j] = q;
         }
         __syncthreads();
         const bool fast = mbar_wait_bounded(&bar, 0, 1000000000ull);
@@ -344,7 +384,7 @@ namespace hb2
                     acc = M::add(acc, M::mul(e.val, xv));
                 }
             }
-            const T xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[(i - base[1]) + W] : x[i]) : T(0);
+            const T xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[(i - wbase[1]) + W] : x[i]) : T(0);
             if (MODE == kPlain) y[i] = acc;
             else if (MODE == kDefect)
             {

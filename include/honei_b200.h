@@ -111,6 +111,11 @@ HB2_API int hb2_ell_info(hb2_ell A, uint64_t *rows, uint64_t *cols, uint64_t *st
  * *row_bytes = matrix bytes read per row.  Every layout gives the same bits.
  * No counterpart in the reference (its device copy is the raw arrays). */
 HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_t *row_bytes);
+/* The kernel behind that choice, per kernel class (cls 0: products, sweeps and
+ * transfers; 1: defects with a fused norm): its layout (as above), rows per thread,
+ * and *windowed = 1 for the row-pattern kernel that stages x in shared-memory
+ * windows.  No counterpart in the reference. */
+HB2_API int hb2_ell_layout_variant(hb2_ell A, int cls, int *layout, int *rows_per_thread, int *windowed);
 /* Download the matrix in the reference layout (host arrays of K*stride, K*stride
  * and rows elements); Arl as the reference computes it. */
 HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);

@@ -446,8 +446,11 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     if layout.startswith("pattern"):
         # two row patterns: interior stencil, Dirichlet identity row; 1 matrix byte per row
         assert A.layout() == (2, 2, 1)
+        want = (2, int(layout[-1]), layout.startswith("patternwin"))
     else:
         assert A.layout() == (1, 3, 27)
+        want = (1, int(layout[-1]), False)
+    assert A.layout_variant(0) == want and A.layout_variant(1) == want
     assert P.layout()[0] == 1 and R.layout()[0] == 1
     monkeypatch.setenv("HB2_ELL_COMPACT", "0")
     A0 = SparseMatrixELL.poisson_q1(L, dt)
