@@ -385,6 +385,7 @@ def main():
     if not args.no_mixed:
         line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5), min(args.warmup, 2),
                                               rank)
+        line["mixed_vs_fp64"]["anisotropic"] = anisotropic_probe(hb, dev, flush, MIXED_LEVEL, rank)
     if not args.no_batch:
         line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
     if not args.no_serving:
@@ -475,26 +476,36 @@ def next_rows(hb, dev, flush, rank, reps=3):
     return out
 
 
-def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
+def finite_or_text(v):
+    """A float for the JSON line; inf / nan (a diverged solve) as text, which strict
+    JSON parsers accept."""
+    import math
+    return v if math.isfinite(v) else str(v)
+
+
+def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cycles=100, max_outer=100):
     """Config 2: level-11 Q1 Poisson (4,198,401 unknowns) to 1e-10 relative residual,
     plain FP64 MG vs iterative refinement (FP64 defect / update / norm around an FP32
     MG V(4,4) inner solve to 1e-3, restarted from zero each outer step, coarse CG
-    cap 100 at eps 1e-10).  Times are CUDA-event times per solve, L2 flushed before each."""
+    cap 100 at eps 1e-10).  Times are CUDA-event times per solve, L2 flushed before each.
+    aniso scales the x-coupling of every level's operator (the anisotropic variant);
+    max_cycles caps the MG cycles of both solvers, max_outer the IR steps."""
     import statistics
 
     import torch
 
     from honei_b200.inputs import uniform
     n = ((1 << level) + 1) ** 2
-    A = hb.SparseMatrixELL.poisson_q1(level)
+    A = hb.SparseMatrixELL.poisson_q1(level, aniso=aniso)
     u = hb.DenseVector(torch.from_numpy(uniform(n, 42 + rank)).to(dev))
     b = hb.DenseVector(n)
     hb.Product.value(b, A, u)
-    fp64 = hb.MGData.poisson_q1(MIN_LEVEL, level, params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10,
-                                                                        coarse_exact=False))
-    inner = hb.MGData.poisson_q1(MIN_LEVEL, level, dtype=torch.float32,
-                                 params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-3, coarse_eps=1e-10,
-                                                     coarse_exact=False, coarse_fp64=True))
+    fp64 = hb.MGData.poisson_q1(MIN_LEVEL, level, aniso=aniso,
+                                params=hb.mg_params(max_iters=max_cycles, max_iters_coarse=COARSE_CAP, eps=1e-10,
+                                                    coarse_exact=False))
+    inner = hb.MGData.poisson_q1(MIN_LEVEL, level, dtype=torch.float32, aniso=aniso,
+                                 params=hb.mg_params(max_iters=max_cycles, max_iters_coarse=COARSE_CAP, eps=1e-3,
+                                                     coarse_eps=1e-10, coarse_exact=False, coarse_fp64=True))
     x64 = hb.DenseVector(n)
     xir = hb.DenseVector(n)
 
@@ -513,14 +524,24 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
 
     info = {}
 
+    # a diverging solve (the anisotropic variant) ends with a NaN / Inf defect norm,
+    # which the solvers report as NotFinite after their last cycle
     def run64():
         hb.fill(x64, 0.0)
-        hb.MGSolver.value(fp64, b, x64)
+        try:
+            hb.MGSolver.value(fp64, b, x64)
+        except hb.NotFinite:
+            info["fp64_not_finite"] = True
 
     def runir():
         hb.fill(xir, 0.0)
-        _, it, st = hb.IRSolver.value(A, b, xir, inner, eps=1e-10, reset_inner=True)
-        info["outer"], info["inner"] = it, int(st[3])
+        info["outer"], info["inner"] = None, None
+        try:
+            _, it, st = hb.IRSolver.value(A, b, xir, inner, eps=1e-10, max_iters=max_outer, reset_inner=True)
+            info["outer"], info["inner"] = it, int(st[3])
+        except hb.NotFinite as e:
+            info["mixed_not_finite"] = True
+            info["outer"], info["inner"] = int(e.stats[0]), int(e.stats[3])
 
     t64 = timed(run64)
     tir = timed(runir)
@@ -532,10 +553,33 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank):
     relir = hb.Norm.value(r) / nb
     d = hb.DenseVector(x64.elements - xir.elements)
     err = hb.Norm.value(d) / hb.Norm.value(x64)
-    return {"level": level, "unknowns": n, "fp64_mg_ms": t64, "fp64_cycles": fp64.used_iters, "fp64_relres": rel64,
-            "mixed_ir_ms": tir, "ir_outer_iters": info["outer"], "ir_inner_fp32_cycles": info["inner"],
-            "mixed_relres": relir, "mixed_rel_error_vs_fp64": err, "speedup_mixed_over_fp64": t64 / tir,
-            "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-10"}
+    res = {"level": level, "unknowns": n, "fp64_mg_ms": t64, "fp64_cycles": fp64.used_iters,
+           "fp64_relres": finite_or_text(rel64), "mixed_ir_ms": tir, "ir_outer_iters": info["outer"],
+           "ir_inner_fp32_cycles": info["inner"], "mixed_relres": finite_or_text(relir),
+           "mixed_rel_error_vs_fp64": finite_or_text(err), "speedup_mixed_over_fp64": t64 / tir,
+           "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-10"}
+    if aniso != 1.0:
+        res["x_coupling"] = aniso
+        res["cycle_cap"], res["outer_cap"] = max_cycles, max_outer
+        res["fp64_converged"] = bool(rel64 <= 1e-10)
+        res["mixed_converged"] = bool(relir <= 1e-10)
+        res["fp64_not_finite"] = info.get("fp64_not_finite", False)
+        res["mixed_not_finite"] = info.get("mixed_not_finite", False)
+    return res
+
+
+def anisotropic_probe(hb, dev, flush, level, rank):
+    """Config 2's anisotropic variant: every level's x-coupling (DL/DU) scaled by a
+    factor, the diagonal raised to keep zero interior row sums.  The reference's
+    method (V(4,4) damped Jacobi on rediscretised coarse operators, coarse CG)
+    diverges for the factor 100 -- in FP64, and on the CPU oracle as well -- and
+    converges up to a factor of about 10.  The factor 100 runs for a bounded number of
+    cycles and is reported with the defect it reached; the factor 10 is solved to
+    1e-10 in FP64 and in mixed precision like the isotropic case."""
+    return {"x_coupling_100": mixed_vs_fp64(hb, dev, flush, level, 1, 0, rank, aniso=100.0, max_cycles=10,
+                                            max_outer=3),
+            "x_coupling_10": mixed_vs_fp64(hb, dev, flush, level, 2, 1, rank, aniso=10.0, max_cycles=300,
+                                           max_outer=30)}
 
 
 def batch_workload(seed, nsys=512, lo=4, hi=9, multi_frac=0.25, multi_rhs=8):

@@ -13,7 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import MgParams, call
+from ._lib import MgParams, NotFinite, call
 from .la import DenseVector, SparseMatrixELL, _check_size, _stream, _vec, dtype_code
 
 
@@ -294,24 +294,32 @@ class MGSolver:
     def value(data: MGData, b, x, stream=None):
         b, x = _vec(b), _vec(x)
         stats = (ctypes.c_double * 4)()
-        call("hb2_mg_solve", data.handle, b.ptr, x.ptr, stats, _stream(stream))
-        data.used_iters = int(stats[0])
-        data.rnorm_initial, data.rnorm_final = stats[1], stats[2]
-        data.used_iters_coarse = int(stats[3])
+        try:
+            call("hb2_mg_solve", data.handle, b.ptr, x.ptr, stats, _stream(stream))
+        finally:
+            # filled also when the solve ends on a NaN defect norm (NotFinite)
+            data.used_iters = int(stats[0])
+            data.rnorm_initial, data.rnorm_final = stats[1], stats[2]
+            data.used_iters_coarse = int(stats[3])
         return x
 
 
 class IRSolver:
     """IRSolver<B200 FP64, B200 inner, Norm<l2, true>>::value (math/ir.hh:31-80).
 
-    Returns (x, outer_iters, stats[4])."""
+    Returns (x, outer_iters, stats[4]): outer steps, initial and last defect norm, inner
+    cycles.  A NotFinite error (NaN defect norm) carries the same list as .stats."""
 
     @staticmethod
     def value(A: SparseMatrixELL, b, x, inner: MGData, eps=1e-10, max_iters=100, reset_inner=False, stream=None):
         b, x = _vec(b), _vec(x)
         stats = (ctypes.c_double * 4)()
-        call("hb2_ir_solve", A.handle, inner.handle, b.ptr, x.ptr, float(eps), int(max_iters), int(bool(reset_inner)),
-             stats, _stream(stream))
+        try:
+            call("hb2_ir_solve", A.handle, inner.handle, b.ptr, x.ptr, float(eps), int(max_iters),
+                 int(bool(reset_inner)), stats, _stream(stream))
+        except NotFinite as e:
+            e.stats = list(stats)
+            raise
         return x, int(stats[0]), list(stats)
 
 
