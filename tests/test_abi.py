@@ -47,6 +47,8 @@ def test_argument_checks_without_gpu():
     h = ctypes.c_void_p()
     assert lib.hb2_mg_create(ctypes.byref(h), 0, None, None, None, None, None) == HB2_ERR_ARG
     assert lib.hb2_q1_create(None, 0, 81, None, 1, None) == HB2_ERR_ARG
+    assert lib.hb2_ell_layout(None, None, None, None) == HB2_ERR_ARG
+    assert lib.hb2_ell_layout_variant(None, 0, None, None, None) == HB2_ERR_ARG
     # batched solver: coarse level above 3, or a system below the coarse level
     lv = (ctypes.c_uint32 * 2)(4, 2)
     assert lib.hb2_batch_create_q1(ctypes.byref(h), 1, lv, None, 4, None, None) == HB2_ERR_ARG
