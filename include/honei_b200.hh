@@ -19,6 +19,16 @@
  *                                                OperatorList lives inside MGData here)
  *   IRSolver<Outer, Inner, Norm>::value(A, b, x, inner, eps, max_iters, used_iters)
  *                                                math/ir.hh:42-80
+ *   Prolongation / Restriction<Tag, NONE|PROLMAT>::value(fine|coarse, coarse|fine, mask, matrix)
+ *                                                math/prolongation.hh:42-155, math/restriction.hh:41-185
+ *   Transposition<Tag>::value(A)                 math/transposition.hh:36-50
+ *   MatrixIO<io_formats::ELL>::read_matrix / write_matrix      math/matrix_io.hh:433-560
+ *   SparseMatrixCSR Product / Defect             la/product.hh:208-244, math/defect.hh:385-420
+ *   CGSolver<Tag, methods::VAR>, BiCGStabSolver<Tag, methods::VAR>, CGSmoother<Tag>
+ *                                                math/cg.hh:142-290, math/bicgstab.hh:60-210
+ *   Multigrid<Tag, OuterTag, NONE, JAC, CYCLE::V, FIXED|MIXED>::value(system, b, x,
+ *                                                max_levels, conv_rad, info)
+ *                                                math/multigrid.hh:781-825, 2252-2394
  * Size mismatches throw VectorSizeDoesNotMatch / MatrixRowsDoNotMatch /
  * MatrixColumnsDoNotMatch before anything is launched (la/vector_error.hh:48,
  * la/matrix_error.hh:46-75); a failing library call throws InternalError with the
@@ -53,6 +63,34 @@ namespace honei_b200
     namespace methods
     {
         struct NONE
+        {
+        };
+        struct PROLMAT
+        {
+        };
+        struct VAR
+        {
+        };
+        struct JAC
+        {
+        };
+        struct FIXED
+        {
+        };
+        struct MIXED
+        {
+        };
+        namespace CYCLE
+        {
+            struct V
+            {
+            };
+        }
+    }
+
+    namespace io_formats
+    {
+        struct ELL
         {
         };
     }
@@ -225,6 +263,9 @@ namespace honei_b200
                 return SparseMatrixELL(h);
             }
 
+            /* takes ownership of a matrix handle made by the C ABI */
+            static SparseMatrixELL adopt(hb2_ell h) { return SparseMatrixELL(h); }
+
             uint64_t rows() const { info(); return _rows; }
             uint64_t columns() const { info(); return _cols; }
             uint64_t stride() const { info(); return _stride; }
@@ -289,6 +330,62 @@ namespace honei_b200
             std::shared_ptr<hb2_q1_s> _h;
     };
 
+    /* SparseMatrixCSR<DT_> (la/sparse_matrix_csr-impl.hh:40-71): Ar (rows + 1 block offsets),
+     * Aj (first column of each block), Ax (blocksize values per block) */
+    template <typename DT_>
+    class SparseMatrixCSR
+    {
+        public:
+            SparseMatrixCSR(uint64_t rows, uint64_t columns, uint64_t blocksize, const std::vector<uint64_t> & Ar,
+                            const std::vector<uint64_t> & Aj, const std::vector<DT_> & Ax)
+            {
+                if (Ar.size() != rows + 1) throw VectorSizeDoesNotMatch(Ar.size(), rows + 1);
+                hb2_csr h = nullptr;
+                detail::check(hb2_csr_create(&h, detail::Dtype<DT_>::value, rows, columns, blocksize, Ar.data(),
+                                             Aj.data(), Ax.data(), 1, nullptr),
+                              "SparseMatrixCSR");
+                _h = std::shared_ptr<hb2_csr_s>(h, [](hb2_csr p) { hb2_csr_destroy(p); });
+            }
+
+            /* SparseMatrixCSR(SparseMatrix(ELL)) with csr::blocksize */
+            static SparseMatrixCSR from_ell(const SparseMatrixELL<DT_> & A, uint64_t blocksize = 1)
+            {
+                hb2_csr h = nullptr;
+                detail::check(hb2_csr_from_ell(&h, A.handle(), blocksize, nullptr), "SparseMatrixCSR");
+                return SparseMatrixCSR(h);
+            }
+
+            uint64_t rows() const { uint64_t r, c, bs, nb, bytes; info(r, c, bs, nb, bytes); return r; }
+            uint64_t columns() const { uint64_t r, c, bs, nb, bytes; info(r, c, bs, nb, bytes); return c; }
+            uint64_t blocksize() const { uint64_t r, c, bs, nb, bytes; info(r, c, bs, nb, bytes); return bs; }
+            hb2_csr handle() const { return _h.get(); }
+
+            void export_arrays(std::vector<uint64_t> & Ar, std::vector<uint64_t> & Aj, std::vector<DT_> & Ax) const
+            {
+                uint64_t r, c, bs, nb, bytes;
+                info(r, c, bs, nb, bytes);
+                Ar.assign(r + 1, 0);
+                Aj.assign(nb, 0);
+                Ax.assign(nb * bs, DT_(0));
+                detail::check(hb2_csr_export(handle(), Ar.data(), Aj.data(), Ax.data()), "export");
+            }
+
+        private:
+            explicit SparseMatrixCSR(hb2_csr h) : _h(h, [](hb2_csr p) { hb2_csr_destroy(p); }) {}
+
+            void info(uint64_t & r, uint64_t & c, uint64_t & bs, uint64_t & nb, uint64_t & bytes) const
+            {
+                detail::check(hb2_csr_info(handle(), &r, &c, &bs, &nb, &bytes), "info");
+            }
+
+            std::shared_ptr<hb2_csr_s> _h;
+    };
+
+    /* ProlongationMatrix (level fine_level - 1 -> fine_level, identity index maps,
+     * math/prolongation_matrix.hh:44-100) and its Transposition, the restriction */
+    template <typename DT_>
+    std::pair<SparseMatrixELL<DT_>, SparseMatrixELL<DT_>> q1_transfer(unsigned fine_level);
+
     // ------------------------------------------------------------------ operators
     template <typename Tag_> struct Product;
     template <typename Tag_> struct Defect;
@@ -322,6 +419,16 @@ namespace honei_b200
             detail::check(hb2_product_q1(a.handle(), b.elements(), result.elements(), nullptr), "Product (Q1)");
             return result;
         }
+
+        template <typename DT_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & result, const SparseMatrixCSR<DT_> & a,
+                                        const DenseVector<DT_> & b)
+        {
+            detail::check_size(b.size(), a.columns());
+            detail::check_size(result.size(), a.rows());
+            detail::check(hb2_product_csr(a.handle(), b.elements(), result.elements(), nullptr), "Product (CSR)");
+            return result;
+        }
     };
 
     template <>
@@ -352,6 +459,20 @@ namespace honei_b200
             detail::check(hb2_defect_q1(system.handle(), right_hand_side.elements(), x.elements(), result.elements(),
                                         nullptr),
                           "Defect (Q1)");
+            return result;
+        }
+
+        template <typename DT_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & result, const DenseVector<DT_> & right_hand_side,
+                                        const SparseMatrixCSR<DT_> & system, const DenseVector<DT_> & x)
+        {
+            detail::check_size(x.size(), system.columns());
+            if (right_hand_side.size() != system.rows())
+                throw MatrixRowsDoNotMatch(system.rows(), right_hand_side.size());
+            detail::check_size(result.size(), system.rows());
+            detail::check(hb2_defect_csr(system.handle(), right_hand_side.elements(), x.elements(), result.elements(),
+                                         nullptr),
+                          "Defect (CSR)");
             return result;
         }
     };
@@ -608,6 +729,289 @@ namespace honei_b200
                                         stats, nullptr);
             used_iters = (uint64_t)stats[0];
             detail::check(st, "IRSolver");
+        }
+    };
+
+    // ------------------------------------------------------------------ grid transfer
+    template <typename DT_>
+    std::pair<SparseMatrixELL<DT_>, SparseMatrixELL<DT_>> q1_transfer(unsigned fine_level)
+    {
+        hb2_ell p = nullptr, r = nullptr;
+        detail::check(hb2_ell_create_transfer(&p, &r, detail::Dtype<DT_>::value, fine_level, nullptr), "q1_transfer");
+        return std::make_pair(SparseMatrixELL<DT_>::adopt(p), SparseMatrixELL<DT_>::adopt(r));
+    }
+
+    /* the 8 boundary entries of a macro (edges and corners): 2 = Dirichlet, 1 = Neumann */
+    inline std::vector<uint64_t> all_dirichlet() { return std::vector<uint64_t>(8, 2); }
+
+    template <typename Tag_, typename Method_> struct Prolongation;
+    template <typename Tag_, typename Method_> struct Restriction;
+
+    template <>
+    struct Prolongation<tags::B200, methods::NONE>
+    {
+        /* matrix-free bilinear prolongation (level sizes (2^l + 1)^2) and the mask's
+         * Dirichlet boundaries; the matrix argument is unused as in the reference */
+        template <typename DT_, typename MatrixType_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & fine, const DenseVector<DT_> & coarse,
+                                        const std::vector<uint64_t> & mask, const MatrixType_ &)
+        {
+            detail::check_size(mask.size(), 8);
+            detail::check(hb2_prolongation(detail::Dtype<DT_>::value, fine.elements(), fine.size(), coarse.elements(),
+                                           coarse.size(), mask.data(), nullptr),
+                          "Prolongation");
+            return fine;
+        }
+    };
+
+    template <>
+    struct Prolongation<tags::B200, methods::PROLMAT>
+    {
+        /* fine = prolmat coarse; the mask is unused as in the reference */
+        template <typename DT_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & fine, const DenseVector<DT_> & coarse,
+                                        const std::vector<uint64_t> &, const SparseMatrixELL<DT_> & prolmat)
+        {
+            return Product<tags::B200>::value(fine, prolmat, coarse);
+        }
+    };
+
+    template <>
+    struct Restriction<tags::B200, methods::NONE>
+    {
+        template <typename DT_, typename MatrixType_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & coarse, const DenseVector<DT_> & fine,
+                                        const std::vector<uint64_t> & mask, const MatrixType_ &)
+        {
+            detail::check_size(mask.size(), 8);
+            detail::check(hb2_restriction(detail::Dtype<DT_>::value, coarse.elements(), coarse.size(), fine.elements(),
+                                          fine.size(), mask.data(), nullptr),
+                          "Restriction");
+            return coarse;
+        }
+    };
+
+    template <>
+    struct Restriction<tags::B200, methods::PROLMAT>
+    {
+        template <typename DT_>
+        static DenseVector<DT_> & value(DenseVector<DT_> & coarse, const DenseVector<DT_> & fine,
+                                        const std::vector<uint64_t> &, const SparseMatrixELL<DT_> & resmat)
+        {
+            return Product<tags::B200>::value(coarse, resmat, fine);
+        }
+    };
+
+    template <typename Tag_> struct Transposition;
+
+    template <>
+    struct Transposition<tags::B200>
+    {
+        template <typename DT_>
+        static SparseMatrixELL<DT_> value(const SparseMatrixELL<DT_> & a)
+        {
+            hb2_ell h = nullptr;
+            detail::check(hb2_ell_transpose(&h, a.handle(), nullptr), "Transposition");
+            return SparseMatrixELL<DT_>::adopt(h);
+        }
+    };
+
+    // ------------------------------------------------------------------ files
+    template <typename Format_> struct MatrixIO;
+
+    template <>
+    struct MatrixIO<io_formats::ELL>
+    {
+        /* the reference's binary ELL file, values rounded to DT_ */
+        template <typename DT_>
+        static SparseMatrixELL<DT_> read_matrix(const std::string & input, DT_)
+        {
+            hb2_ell h = nullptr;
+            detail::check(hb2_ell_read(&h, input.c_str(), detail::Dtype<DT_>::value, nullptr), "MatrixIO::read_matrix");
+            return SparseMatrixELL<DT_>::adopt(h);
+        }
+
+        static void write_matrix(const std::string & output, const SparseMatrixELL<double> & smatrix)
+        {
+            detail::check(hb2_ell_write(smatrix.handle(), output.c_str()), "MatrixIO::write_matrix");
+        }
+    };
+
+    // ------------------------------------------------------------------ Krylov solvers (FP64)
+    template <typename Tag_, typename Method_> struct BiCGStabSolver;
+    template <typename Tag_> struct CGSmoother;
+
+    namespace detail
+    {
+        /* one solve of a hb2_krylov handle built for (A, P); P an element-wise vector or an ELL matrix */
+        inline void krylov(int method, const SparseMatrixELL<double> & A, hb2_ell Pm, const double * Pd,
+                           const DenseVector<double> & b, DenseVector<double> & x, uint64_t max_iters,
+                           double eps_relative, uint64_t & used_iters, const char * what)
+        {
+            check_size(b.size(), A.rows());
+            check_size(x.size(), A.columns());
+            hb2_krylov K = nullptr;
+            check(hb2_krylov_create(&K, method, A.handle(), Pm, Pd, max_iters, eps_relative, nullptr), what);
+            std::unique_ptr<hb2_krylov_s, int (*)(hb2_krylov)> keep(K, hb2_krylov_destroy);
+            double defect = 0.0;
+            check(hb2_krylov_solve(K, b.elements(), x.elements(), &used_iters, &defect, nullptr), what);
+        }
+    }
+
+    template <>
+    struct CGSolver<tags::B200, methods::VAR>
+    {
+        /* P (.) r as the preconditioner */
+        static DenseVector<double> & value(const SparseMatrixELL<double> & A, const DenseVector<double> & P,
+                                           const DenseVector<double> & b, DenseVector<double> & x,
+                                           uint64_t max_iters, uint64_t & used_iters, double eps_relative = 1e-8)
+        {
+            detail::check_size(P.size(), A.rows());
+            detail::krylov(HB2_CG_VAR, A, nullptr, P.elements(), b, x, max_iters, eps_relative, used_iters,
+                           "CGSolver<VAR>");
+            return x;
+        }
+
+        /* P r (an ELL matrix, e.g. an SPAI) as the preconditioner */
+        static DenseVector<double> & value(const SparseMatrixELL<double> & A, const SparseMatrixELL<double> & P,
+                                           const DenseVector<double> & b, DenseVector<double> & x,
+                                           uint64_t max_iters, uint64_t & used_iters, double eps_relative = 1e-8)
+        {
+            if (P.rows() != A.rows()) throw MatrixRowsDoNotMatch(P.rows(), A.rows());
+            detail::krylov(HB2_CG_VAR, A, P.handle(), nullptr, b, x, max_iters, eps_relative, used_iters,
+                           "CGSolver<VAR>");
+            return x;
+        }
+    };
+
+    template <>
+    struct BiCGStabSolver<tags::B200, methods::VAR>
+    {
+        /* used_iters as the reference counts them (iterations + 1) */
+        static DenseVector<double> & value(const SparseMatrixELL<double> & A, const DenseVector<double> & P,
+                                           const DenseVector<double> & b, DenseVector<double> & x,
+                                           uint64_t max_iters, uint64_t & used_iters, double eps_relative = 1e-8)
+        {
+            detail::check_size(P.size(), A.rows());
+            detail::krylov(HB2_BICGSTAB_VAR, A, nullptr, P.elements(), b, x, max_iters, eps_relative, used_iters,
+                           "BiCGStabSolver<VAR>");
+            return x;
+        }
+    };
+
+    template <>
+    struct CGSmoother<tags::B200>
+    {
+        /* exactly max_iters preconditioned CG steps from x; temp_vecs are unused (the
+         * solver keeps its vectors on the device) */
+        static DenseVector<double> & value(const SparseMatrixELL<double> & A, const DenseVector<double> & P,
+                                           const DenseVector<double> & b, DenseVector<double> & x,
+                                           std::vector<DenseVector<double>> &, uint64_t max_iters)
+        {
+            detail::check_size(P.size(), A.rows());
+            uint64_t used = 0;
+            detail::krylov(HB2_CG_SMOOTHER, A, nullptr, P.elements(), b, x, max_iters, 0.0, used, "CGSmoother");
+            return x;
+        }
+    };
+
+    // ------------------------------------------------------------------ legacy banded multigrid
+    /* MGInfo's configuration (math/multigrid.hh:65-149), defaults of the reference's
+     * banded tests */
+    inline hb2_lmg_params mg_info_params(uint64_t n_max_iter = 16, bool initial_zero = true, double tolerance = 1e-8,
+                                         uint64_t n_pre_smooth = 2)
+    {
+        hb2_lmg_params p;
+        p.n_max_iter = n_max_iter;
+        p.initial_zero = initial_zero ? 1 : 0;
+        p.convergence_check = 0;
+        p.is_smoother = 0;
+        p.tolerance = tolerance;
+        p.n_pre_smooth = n_pre_smooth;
+        p.adapt_correction_factor = 1.0;
+        p.omega = 0.7;
+        for (int i = 0; i < 8; ++i) p.macro_border_mask[i] = 2;
+        p.adaptive = 0;
+        return p;
+    }
+
+    /* MGInfo with its levels' banded operators (coarsest first, levels min_level ..),
+     * resident on the device with the solver's graph; cycles / defect of the last solve */
+    template <typename DT_>
+    class MGInfo
+    {
+        public:
+            MGInfo(unsigned min_level, const std::vector<BandedMatrixQx<DT_>> & a,
+                   const hb2_lmg_params & params = mg_info_params()) :
+                _a(a), _n(a.empty() ? 0 : a.back().rows())
+            {
+                std::vector<hb2_q1> h;
+                for (const auto & m : a) h.push_back(m.handle());
+                hb2_lmg g = nullptr;
+                detail::check(hb2_lmg_create(&g, min_level, min_level + (unsigned)a.size() - 1, h.data(), &params,
+                                             nullptr),
+                              "MGInfo");
+                _h = std::shared_ptr<hb2_lmg_s>(g, [](hb2_lmg p) { hb2_lmg_destroy(p); });
+            }
+
+            uint64_t size() const { return _n; }
+            hb2_lmg handle() const { return _h.get(); }
+
+            uint64_t cycles = 0, outer_steps = 0;
+            double defect = 0.0;
+
+        private:
+            std::vector<BandedMatrixQx<DT_>> _a;
+            uint64_t _n;
+            std::shared_ptr<hb2_lmg_s> _h;
+    };
+
+    template <typename Tag_, typename OuterTag_, typename ProlType_, typename SmootherType_, typename CycleType_,
+              typename Mode_>
+    struct Multigrid;
+
+    template <>
+    struct Multigrid<tags::B200, tags::B200, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>
+    {
+        /* x: initial guess in, result out; max_levels and conv_rad are unused as in the
+         * reference (the levels are the info's) */
+        template <typename DT_>
+        static void value(const BandedMatrixQx<DT_> & system, const DenseVector<DT_> & right_hand_side,
+                          DenseVector<DT_> & x, unsigned long, DT_, MGInfo<DT_> & info)
+        {
+            detail::check_size(system.rows(), info.size());
+            detail::check_size(right_hand_side.size(), info.size());
+            detail::check_size(x.size(), info.size());
+            uint64_t cycles = 0;
+            double defect = 0.0;
+            detail::check(hb2_lmg_solve(info.handle(), right_hand_side.elements(), x.elements(), &cycles, &defect,
+                                        nullptr),
+                          "Multigrid<FIXED>");
+            info.cycles = cycles;
+            info.defect = defect;
+        }
+    };
+
+    template <>
+    struct Multigrid<tags::B200, tags::B200, methods::NONE, methods::JAC, methods::CYCLE::V, methods::MIXED>
+    {
+        /* FP64 defect correction around the FP32 hierarchy of info (the reference has no
+         * cap on the outer steps; max_outer bounds them and NotFinite reports reaching it) */
+        static void value(const BandedMatrixQx<double> & system, const DenseVector<double> & right_hand_side,
+                          DenseVector<double> & x, unsigned long, double, MGInfo<float> & info,
+                          uint64_t max_outer = 1000)
+        {
+            detail::check_size(system.rows(), info.size());
+            detail::check_size(right_hand_side.size(), info.size());
+            detail::check_size(x.size(), info.size());
+            uint64_t outer = 0, inner = 0;
+            double defect = 0.0;
+            const int st = hb2_lmg_solve_mixed(info.handle(), system.handle(), right_hand_side.elements(),
+                                               x.elements(), max_outer, &outer, &inner, &defect, nullptr);
+            info.outer_steps = outer;
+            info.cycles = inner;
+            info.defect = defect;
+            detail::check(st, "Multigrid<MIXED>");
         }
     };
 }

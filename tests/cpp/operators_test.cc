@@ -11,6 +11,8 @@
 #include "honei_b200.hh"
 #include "honei_oracle.h"
 
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -274,6 +276,181 @@ namespace
         TEST_CHECK(rel_diff(x.to_host(), xr) < 1e-9);
     }
 
+    void transfer_test()
+    {
+        const unsigned L = 6;
+        const uint64_t nf = hbo_q1_n(L), nc = hbo_q1_n(L - 1);
+        const std::vector<uint64_t> mask = all_dirichlet();
+        const std::vector<double> ch = uniform(nc, 51), fh = uniform(nf, 52);
+        DenseVector<double> c(ch), f(fh), fine(nf), coarse(nc);
+        std::pair<SparseMatrixELL<double>, SparseMatrixELL<double>> PR = q1_transfer<double>(L);
+        Prolongation<tags::B200, methods::NONE>::value(fine, c, mask, PR.first);
+        std::vector<double> want(nf);
+        hbo_prolongation_f64(nf, want.data(), nc, ch.data(), mask.data());
+        TEST_CHECK(same_bits(fine.to_host(), want));
+        Restriction<tags::B200, methods::NONE>::value(coarse, f, mask, PR.second);
+        std::vector<double> wantc(nc);
+        hbo_restriction_f64(nc, wantc.data(), nf, fh.data(), mask.data());
+        TEST_CHECK(same_bits(coarse.to_host(), wantc));
+        // PROLMAT: the ProlongationMatrix of the oracle, as ELL, applied on the host
+        std::vector<uint64_t> rowptr(nf + 1), col(4 * nf);
+        std::vector<double> val(4 * nf);
+        hbo_prolmat_csr_f64(L, rowptr.data(), col.data(), val.data());
+        uint64_t stride = 0, K = 0;
+        hbo_ell_dims(nf, rowptr.data(), 1, &stride, &K);
+        std::vector<uint64_t> Aj(K * stride, 0), Arl(nf, 0);
+        std::vector<double> Ax(K * stride, 0.0);
+        hbo_ell_from_csr_f64(nf, rowptr.data(), col.data(), val.data(), 1, stride, K, Aj.data(), Ax.data(), Arl.data());
+        std::vector<uint64_t> dAj, dArl;
+        std::vector<double> dAx;
+        PR.first.export_arrays(dAj, dAx, dArl);
+        TEST_CHECK(same_bits(dAj, Aj) && same_bits(dAx, Ax) && same_bits(dArl, Arl));
+        Prolongation<tags::B200, methods::PROLMAT>::value(fine, c, mask, PR.first);
+        hbo_ell_spmv_f64(nf, stride, 1, Aj.data(), Ax.data(), Arl.data(), ch.data(), want.data());
+        TEST_CHECK(same_bits(fine.to_host(), want));
+        // the restriction matrix is the Transposition of the prolongation matrix
+        SparseMatrixELL<double> Rt = Transposition<tags::B200>::value(PR.first);
+        std::vector<uint64_t> rAj, rArl, tAj, tArl;
+        std::vector<double> rAx, tAx;
+        PR.second.export_arrays(rAj, rAx, rArl);
+        Rt.export_arrays(tAj, tAx, tArl);
+        TEST_CHECK(same_bits(rAj, tAj) && same_bits(rAx, tAx) && same_bits(rArl, tArl));
+        Restriction<tags::B200, methods::PROLMAT>::value(coarse, f, mask, Rt);
+        DenseVector<double> coarse2(nc);
+        Product<tags::B200>::value(coarse2, PR.second, f);
+        TEST_CHECK(same_bits(coarse.to_host(), coarse2.to_host()));
+    }
+
+    void matrix_io_test()
+    {
+        SparseMatrixELL<double> A = SparseMatrixELL<double>::poisson_q1(5);
+        char path[] = "/tmp/hb2_matrix_io_XXXXXX";
+        const int fd = mkstemp(path);
+        TEST_CHECK(fd >= 0);
+        close(fd);
+        MatrixIO<io_formats::ELL>::write_matrix(path, A);
+        SparseMatrixELL<double> B = MatrixIO<io_formats::ELL>::read_matrix(path, double(0));
+        std::remove(path);
+        std::vector<uint64_t> aj, arl, bj, brl;
+        std::vector<double> ax, bx;
+        A.export_arrays(aj, ax, arl);
+        B.export_arrays(bj, bx, brl);
+        TEST_CHECK(same_bits(aj, bj) && same_bits(ax, bx) && same_bits(arl, brl));
+        bool thrown = false;
+        try
+        {
+            MatrixIO<io_formats::ELL>::read_matrix("/nonexistent/file.ell", double(0));
+        }
+        catch (const InternalError &)
+        {
+            thrown = true;
+        }
+        TEST_CHECK(thrown);
+    }
+
+    void csr_test()
+    {
+        const unsigned L = 7;
+        SparseMatrixELL<double> A = SparseMatrixELL<double>::poisson_q1(L);
+        for (uint64_t bs : {1ull, 2ull})
+        {
+            SparseMatrixCSR<double> C = SparseMatrixCSR<double>::from_ell(A, bs);
+            TEST_CHECK(C.rows() == A.rows() && C.columns() == A.columns() && C.blocksize() == bs);
+            std::vector<uint64_t> Ar, Aj;
+            std::vector<double> Ax;
+            C.export_arrays(Ar, Aj, Ax);
+            SparseMatrixCSR<double> C2(C.rows(), C.columns(), bs, Ar, Aj, Ax);
+            const uint64_t n = A.rows();
+            const std::vector<double> xh = uniform(n, 61), bh = uniform(n, 62);
+            DenseVector<double> x(xh), b(bh), y(n), r(n);
+            Product<tags::B200>::value(y, C2, x);
+            std::vector<double> want(n);
+            hbo_csr_spmv_f64(n, bs, n, Ar.data(), Aj.data(), Ax.data(), xh.data(), want.data());
+            TEST_CHECK(same_bits(y.to_host(), want));
+            Defect<tags::B200>::value(r, b, C, x);
+            hbo_csr_defect_f64(n, bs, n, Ar.data(), Aj.data(), Ax.data(), bh.data(), xh.data(), want.data());
+            TEST_CHECK(same_bits(r.to_host(), want));
+        }
+    }
+
+    void krylov_test()
+    {
+        const unsigned L = 5;
+        const RefEll e = q1_ell(L);
+        SparseMatrixELL<double> A(e.rows, e.rows, e.stride, e.K, e.Aj, e.Ax, e.Arl);
+        const std::vector<double> bh = ref_spmv(e, uniform(e.rows, 42));
+        DenseVector<double> P = RISmoother<tags::B200>::jacobi_precon(A, 1.0);   // 1 / diag
+        const std::vector<double> ph = P.to_host();
+        hbo_ell_view v{e.rows, e.rows, e.stride, e.K, e.Aj.data(), e.Ax.data(), e.Arl.data()};
+        DenseVector<double> b(bh);
+        {
+            DenseVector<double> x(e.rows);
+            uint64_t used = 0;
+            CGSolver<tags::B200, methods::VAR>::value(A, P, b, x, 1000, used, 1e-8);
+            std::vector<double> xr(e.rows, 0.0);
+            const uint64_t ref = hbo_cgvar_f64(&v, ph.data(), nullptr, bh.data(), xr.data(), 1000, 1e-8, 0);
+            TEST_CHECK(used + 1 >= ref && used <= ref + 1);
+            TEST_CHECK(rel_diff(x.to_host(), xr) < 1e-6);
+        }
+        {
+            DenseVector<double> x(e.rows);
+            uint64_t used = 0;
+            BiCGStabSolver<tags::B200, methods::VAR>::value(A, P, b, x, 1000, used, 1e-8);
+            std::vector<double> xr(e.rows, 0.0);
+            const uint64_t ref = hbo_bicgstab_f64(&v, ph.data(), nullptr, bh.data(), xr.data(), 1000, 1e-8);
+            TEST_CHECK(used + 1 >= ref && used <= ref + 1);
+            TEST_CHECK(rel_diff(x.to_host(), xr) < 1e-3);
+        }
+        {
+            DenseVector<double> x(e.rows);
+            std::vector<DenseVector<double>> temps;
+            CGSmoother<tags::B200>::value(A, P, b, x, temps, 5);
+            std::vector<double> xr(e.rows, 0.0);
+            hbo_cgvar_f64(&v, ph.data(), nullptr, bh.data(), xr.data(), 5, 0.0, 1);
+            TEST_CHECK(rel_diff(x.to_host(), xr) < 1e-10);
+        }
+    }
+
+    void legacy_multigrid_test()
+    {
+        // FIXED on an assembled hierarchy, levels 1..8: the oracle's cycles and iterates
+        const unsigned lmin = 1, L = 8;
+        std::vector<std::vector<double>> bands(L + 1), dinv(L + 1);
+        std::vector<BandedMatrixQx<double>> levels;
+        const double * bp[32] = {nullptr};
+        const double * dp[32] = {nullptr};
+        for (unsigned l = lmin; l <= L; ++l)
+        {
+            const uint64_t n = hbo_q1_n(l);
+            bands[l].resize(9 * n);
+            hbo_q1_bands_f64(l, 1.0, bands[l].data());
+            dinv[l].resize(n);
+            for (uint64_t i = 0; i < n; ++i)
+            {
+                const double dd = bands[l][4 * n + i];
+                const double inv = dd == 0.0 ? 0.0 : 1.0 / dd;
+                dinv[l][i] = inv * 0.7;
+            }
+            bp[l] = bands[l].data();
+            dp[l] = dinv[l].data();
+            levels.push_back(BandedMatrixQx<double>::poisson_q1(l));
+        }
+        const uint64_t n = hbo_q1_n(L), m = hbo_q1_m(L);
+        std::vector<double> bh(n), x0 = uniform(n, 4);
+        const std::vector<double> u = uniform(n, 3);
+        hbo_q1_spmv_f64(n, m, bands[L].data(), u.data(), bh.data());
+        for (double & v : x0) v *= 0.01;
+        MGInfo<double> info(lmin, levels, mg_info_params(40, true, 1e-10, 2));
+        DenseVector<double> b(bh), x(x0);
+        Multigrid<tags::B200, tags::B200, methods::NONE, methods::JAC, methods::CYCLE::V, methods::FIXED>::value(
+            levels.back(), b, x, L, 0.0, info);
+        std::vector<double> xr = x0;
+        const uint64_t mask[8] = {2, 2, 2, 2, 2, 2, 2, 2};
+        const uint64_t cycles = hbo_lmg_f64(lmin, L, bp, dp, bh.data(), xr.data(), 40, 1, 0, 0, 1e-10, 2, 1.0, mask);
+        TEST_CHECK(info.cycles == cycles);
+        TEST_CHECK(same_bits(x.to_host(), xr));
+    }
+
     void size_error_test()
     {
         SparseMatrixELL<double> A = SparseMatrixELL<double>::poisson_q1(4);
@@ -319,6 +496,9 @@ int main()
         {"banded_q1_test", banded_q1_test},     {"blas1_test", blas1_test},
         {"ri_smoother_test", ri_smoother_test}, {"cg_solver_test", cg_solver_test},
         {"mg_solver_test", mg_solver_test},     {"ir_solver_test", ir_solver_test},
+        {"transfer_test", transfer_test},       {"matrix_io_test", matrix_io_test},
+        {"csr_test", csr_test},                 {"krylov_test", krylov_test},
+        {"legacy_multigrid_test", legacy_multigrid_test},
         {"size_error_test", size_error_test}};
     int failed = 0;
     for (const auto & t : tests)

@@ -42,4 +42,4 @@ def test_cpp_layer_matches_oracle(tmp_path):
     exe = build(tmp_path)
     res = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stdout + res.stderr
-    assert "9 tests, 0 failed" in res.stdout, res.stdout
+    assert "14 tests, 0 failed" in res.stdout, res.stdout
