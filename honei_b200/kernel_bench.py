@@ -1,7 +1,7 @@
 """Per-kernel timing of the hot kernels on one Q1 level.
 
     python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect|
-                                                cgvar|bicgstab]
+                                                cgvar|bicgstab|coarse_cg]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
 
 Each launch is preceded by an L2 flush (256 MiB write) and timed alone with CUDA
@@ -95,6 +95,30 @@ def main(argv=None) -> int:
         kernels["csr_spmv"] = (lambda: _lib.call("hb2_product_csr", C.handle, x.ptr, y.ptr, stream), cb + 2 * n * s)
         kernels["csr_defect"] = (lambda: _lib.call("hb2_defect_csr", C.handle, b.ptr, x.ptr, y.ptr, stream),
                                  cb + 3 * n * s)
+    if a.kernel == "coarse_cg":
+        # the MG's coarsest-level solve: CG on the level-3 operator (81 unknowns) for
+        # 100 iterations (the cap of the bench; eps 0 never stops early), which runs
+        # as one warp with the operator and vectors in registers
+        from .solvers import CGSolver
+        A3 = SparseMatrixELL.poisson_q1(3, dt)
+        n3 = A3.rows()
+        b3 = vec(n3, 9)
+        x3 = DenseVector(n3, dtype=dt)
+        ts = []
+        used = 0
+        for i in range(a.iters + 1):
+            x3.elements.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, used, _ = CGSolver.value(A3, None, b3, x3, 100, 0.0)
+            e1.record()
+            e1.synchronize()
+            if i > 0:
+                ts.append(1000 * e0.elapsed_time(e1))
+        us = statistics.median(ts)
+        print(json.dumps({"kernel": "coarse_cg", "level": 3, "rows": n3, "iterations": used, "solve_us": us,
+                          "us_per_iteration": us / max(used, 1)}), flush=True)
+        return 0
     if a.kernel in ("cgvar", "bicgstab") and a.dtype == "f64":
         from .solvers import HB2_BICGSTAB_VAR, HB2_CG_VAR, KrylovSolver
         # Jacobi vector preconditioner; a fixed number of iterations (eps = 0)
