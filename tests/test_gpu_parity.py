@@ -55,6 +55,24 @@ def test_transfer_assembly_on_device(oracle, L):
         assert same_bits(Aj, ref.Aj) and same_bits(Ax, ref.Ax) and same_bits(Arl, ref.Arl)
 
 
+@pytest.mark.parametrize("L", [10, 11])
+def test_assembly_at_config_levels(oracle, L):
+    """The config levels 10 and 11 (1,050,625 and 4,198,401 rows): operator and transfer
+    matrices assembled on the device are the reference's arrays, bit for bit."""
+    ref = oracle.q1_ell(L)
+    A = SparseMatrixELL.poisson_q1(L)
+    assert (A.rows(), A.columns(), A.stride(), A.num_cols_per_row()) == (ref.rows, ref.cols, ref.stride, ref.K)
+    Aj, Ax, Arl = A.export()
+    assert same_bits(Aj, ref.Aj) and same_bits(Ax, ref.Ax) and same_bits(Arl, ref.Arl)
+    del A, Aj, Ax, Arl, ref
+    Pr, Rr = oracle.transfer_ell(L)
+    P, R = SparseMatrixELL.transfer(L)
+    for dev, r in ((P, Pr), (R, Rr)):
+        assert (dev.rows(), dev.columns(), dev.stride(), dev.num_cols_per_row()) == (r.rows, r.cols, r.stride, r.K)
+        Aj, Ax, Arl = dev.export()
+        assert same_bits(Aj, r.Aj) and same_bits(Ax, r.Ax) and same_bits(Arl, r.Arl)
+
+
 @pytest.mark.parametrize("T", [1, 2, 3])
 def test_upload_reference_arrays_roundtrip(oracle, T):
     ref = oracle.q1_ell(5, T=T)
