@@ -36,6 +36,7 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "honei_ref")
 MIN_LEVEL = 3
 COARSE_CAP = 100
 MIXED_LEVEL = 11
+SUB_MAX_ROWS = 20000    # levels up to this many rows run in the fused small-level kernels
 
 
 def parse():
@@ -59,7 +60,8 @@ def mg_solve_bytes(level: int, cycles: int, row_bytes, min_level: int = MIN_LEVE
 
     row_bytes(l, which) = matrix bytes per row of the layout the level-l operator
     ("A"), its restriction ("R", rows = level l-1) or prolongation ("P") runs on
-    (plain FP64: 9 x 12 = 108; compressed: 3 per slot; row patterns: 1).
+    (plain FP64: 9 x 12 = 108; compressed: 3 per slot; row patterns: 1; transfers
+    applied by the Q1 transfer kernels: 0).
     Jacobi sweep rb + 4s per row; defect rb + 3s; restriction rb(R) + 2s per
     coarse row + the fine input; prolongation-add rb(P) + 2s per fine row + the
     coarse input; convergence defect once per cycle plus the initial one; the
@@ -83,12 +85,17 @@ def layout_row_bytes(hb, dtype, levels):
     """row_bytes(l, which) for mg_solve_bytes, from matrices of the same shapes as the
     hierarchy's (the layout choice is made once per shape and process)."""
     import torch
+    # levels above SUB_MAX_ROWS rows apply their transfers with the Q1 transfer kernels,
+    # which read no matrix (unless HB2_Q1_TRANSFER=0); the fused small levels read them
+    q1t = os.environ.get("HB2_Q1_TRANSFER", "1") != "0"
     table = {}
     for l in levels:
         table[(l, "A")] = hb.SparseMatrixELL.poisson_q1(l, dtype).layout()[2]
         if l > min(levels):
             P, R = hb.SparseMatrixELL.transfer(l, dtype)
             table[(l, "P")], table[(l, "R")] = P.layout()[2], R.layout()[2]
+            if q1t and ((1 << l) + 1) ** 2 > SUB_MAX_ROWS:
+                table[(l, "P")] = table[(l, "R")] = 0
     return lambda l, which: table[(l, which)]
 
 

@@ -213,6 +213,14 @@ namespace hb2
 
     unsigned ell_grid(const hb2_ell_s * A, bool reducing) { return ceil_div(A->rows, ell_rows_per_block(A, reducing)); }
 
+    // HB2_Q1_TRANSFER=0 runs the Q1 transfer matrices on their stored layout instead
+    // (read at every launch, so a process can compare both)
+    static bool q1_transfer_kernels_enabled()
+    {
+        const char * v = getenv("HB2_Q1_TRANSFER");
+        return ! (v && strcmp(v, "0") == 0);
+    }
+
     int launch_ell(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux, const void * aux2,
                    void * zero, double * red, int want_sqrt, const Workspace * ws, cudaStream_t stream, int flags,
                    const Batch * batch)
@@ -248,6 +256,9 @@ namespace hb2
                 return fail(HB2_ERR_UNSUPPORTED, "matrix / batch too large for the reduction workspace");
             rs = ws->slot();
         }
+        if (A->q1_transfer && ! red && b.nvec == 1 && ! b.list && ! b.active &&
+            (mode == kPlain || mode == kAdd || mode == kRestrict) && q1_transfer_kernels_enabled())
+            return launch_q1_transfer(A, mode, x, y, zero, stream);
         const int cls = red != 0;
         if (A->layout[cls] == kLayoutPattern)
             launch_ell_pattern(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, A->rpt[cls]);
@@ -590,6 +601,8 @@ extern "C" int hb2_ell_create_transfer(hb2_ell * prol, hb2_ell * res, hb2_dtype 
     int cst = ell_build_compact(P, stream);
     if (! cst) cst = ell_build_compact(R, stream);
     if (cst) { hb2_ell_destroy(P); hb2_ell_destroy(R); return cst; }
+    P->q1_transfer = (int)fine_level;
+    R->q1_transfer = -(int)fine_level;
     *prol = P;
     *res = R;
     return HB2_OK;

@@ -100,6 +100,11 @@ struct hb2_ell_s
     // its rows per thread
     int layout[2] = {0, 0};
     int rpt[2] = {2, 2};
+    // the Q1 transfer matrices of hb2_ell_create_transfer: +L for the prolongation
+    // into fine level L, -L for its transposition, the restriction; 0 otherwise.
+    // Their products run on kernels that know the rows' columns and weights
+    // (launch_q1_transfer) instead of reading the matrix.
+    int q1_transfer = 0;
 
     template <typename T> hb2::EllView<T> view() const
     {
@@ -222,6 +227,11 @@ namespace hb2
 
     // banded Q1 kernels (q1.cu): mode 0 y = A x, 1 y = rhs - A x, 2 the Jacobi sweep
     // y = x + (rhs - A x) (.) dinv (y != x); err: device flag of the bounded copy wait
+    // y = P x, y += P x (kAdd) or y = R x with zero[] cleared (kRestrict) for a matrix
+    // with q1_transfer set: the products and slot-ordered sums of its rows, bit-identical
+    // to the ELL kernels, without the matrix reads (transfer.cu)
+    int launch_q1_transfer(const hb2_ell_s * A, int mode, const void * x, void * y, void * zero,
+                           cudaStream_t stream);
     int launch_q1(const hb2_q1_s * A, int mode, const void * x, void * y, const void * rhs, const void * dinv,
                   int * err, cudaStream_t stream);
     int launch_norm(int dt, const void * x, uint64_t n, int root, double * dev_out, const Workspace * ws,

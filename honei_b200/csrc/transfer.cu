@@ -128,6 +128,104 @@ namespace hb2
         for (int i = 0; i < 8; ++i) mk.bit[i] = mask ? (mask[i] == 2) : 1;
         return mk;
     }
+
+    // ------------------------------------------------------------------
+    // The ProlongationMatrix of the identity index maps (math/prolongation_matrix.hh:44-100)
+    // and its Transposition, applied without reading them.  Fine node (i, j) of a grid
+    // with mf points per line, coarse node (I, J) = (i / 2, j / 2): the prolongation row
+    // holds, in ascending column order, (I, J) with weight 1 (i, j even), (I, J) and
+    // (I, J + 1) or (I, J) and (I + 1, J) with 1/2 (one odd), and (I, J), (I, J + 1),
+    // (I + 1, J), (I + 1, J + 1) with 1/4 (both odd); the restriction row of (I, J)
+    // holds the fine nodes (2I + di, 2J + dj), di, dj in -1..1 inside the grid, in
+    // ascending column order, with weight (1 or 1/2) x (1 or 1/2).  Each row is summed
+    // as the ELL kernels sum it (0 + v0 x0 + v1 x1 ..., products and sums rounded
+    // separately), so the results are bit-identical to the matrix products.
+    template <typename T, int MODE>
+    __global__ void __launch_bounds__(256)
+    q1_prolong_kernel(const T * __restrict__ c, T * __restrict__ y, uint32_t mf, uint32_t mc, uint64_t nf)
+    {
+        typedef Arith<T> M;
+        pdl_entry();
+        const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (r >= nf) return;
+        const uint32_t i = (uint32_t)(r / mf), j = (uint32_t)(r - (uint64_t)i * mf);
+        const T * cp = c + (uint64_t)(i >> 1) * mc + (j >> 1);
+        const T h = T(0.5), q = T(0.25);
+        T acc;
+        if (! (i & 1) && ! (j & 1)) acc = M::add(T(0), M::mul(T(1), cp[0]));
+        else if (! (i & 1)) acc = M::add(M::add(T(0), M::mul(h, cp[0])), M::mul(h, cp[1]));
+        else if (! (j & 1)) acc = M::add(M::add(T(0), M::mul(h, cp[0])), M::mul(h, cp[mc]));
+        else
+            acc = M::add(M::add(M::add(M::add(T(0), M::mul(q, cp[0])), M::mul(q, cp[1])), M::mul(q, cp[mc])),
+                         M::mul(q, cp[mc + 1]));
+        y[r] = MODE == kAdd ? M::add(y[r], acc) : acc;
+    }
+
+    template <typename T, int MODE>
+    __global__ void __launch_bounds__(256)
+    q1_restrict_kernel(const T * __restrict__ x, T * __restrict__ y, T * __restrict__ zero, uint32_t mf,
+                       uint32_t mc, uint64_t nc)
+    {
+        typedef Arith<T> M;
+        pdl_entry();
+        const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (r >= nc) return;
+        const int I = (int)(r / mc), J = (int)(r - (uint64_t)I * mc);
+        T acc = T(0);
+#pragma unroll
+        for (int di = -1; di <= 1; ++di)
+        {
+            const int i = 2 * I + di;
+            if (i < 0 || i >= (int)mf) continue;
+            const T * xr = x + (uint64_t)i * mf;
+            const T wi = di == 0 ? T(1) : T(0.5);
+#pragma unroll
+            for (int dj = -1; dj <= 1; ++dj)
+            {
+                const int jj = 2 * J + dj;
+                if (jj < 0 || jj >= (int)mf) continue;
+                const T w = dj == 0 ? wi : (di == 0 ? T(0.5) : T(0.25));
+                acc = M::add(acc, M::mul(w, xr[jj]));
+            }
+        }
+        y[r] = acc;
+        if (MODE == kRestrict) zero[r] = T(0);
+    }
+
+    template <typename T>
+    static int q1_transfer_typed(const hb2_ell_s * A, int mode, const void * x, void * y, void * zero,
+                                 cudaStream_t s)
+    {
+        const int L = A->q1_transfer > 0 ? A->q1_transfer : -A->q1_transfer;
+        const uint32_t mf = (1u << L) + 1, mc = (1u << (L - 1)) + 1;
+        const T * xp = (const T *)x;
+        T * yp = (T *)y;
+        const dim3 grid(ceil_div(A->rows, 256));
+        if (A->q1_transfer > 0)
+        {
+            if (mode == kAdd) launch_pdl(q1_prolong_kernel<T, kAdd>, grid, dim3(256), 0, s, xp, yp, mf, mc, A->rows);
+            else launch_pdl(q1_prolong_kernel<T, kPlain>, grid, dim3(256), 0, s, xp, yp, mf, mc, A->rows);
+        }
+        else
+        {
+            if (mode == kRestrict)
+                launch_pdl(q1_restrict_kernel<T, kRestrict>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows);
+            else launch_pdl(q1_restrict_kernel<T, kPlain>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows);
+        }
+        return HB2_OK;
+    }
+
+    int launch_q1_transfer(const hb2_ell_s * A, int mode, const void * x, void * y, void * zero, cudaStream_t stream)
+    {
+        // a prolongation computes kPlain / kAdd rows, a restriction kPlain / kRestrict rows
+        if ((A->q1_transfer > 0 && mode == kRestrict) || (A->q1_transfer < 0 && mode == kAdd))
+            return fail(HB2_ERR_UNSUPPORTED, "Q1 transfer kernel: mode");
+        const int st = A->dtype == HB2_F64 ? q1_transfer_typed<double>(A, mode, x, y, zero, stream)
+                                           : q1_transfer_typed<float>(A, mode, x, y, zero, stream);
+        count_launches(1);
+        HB2_LAUNCH_CHECK("Q1 transfer kernel launch");
+        return st;
+    }
 }
 
 using namespace hb2;

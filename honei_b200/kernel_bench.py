@@ -75,7 +75,11 @@ def main(argv=None) -> int:
     if a.kernel in ("all", "restrict", "prolong"):
         Pm, Rm = SparseMatrixELL.transfer(L, dt)
         c = vec(nc, 5)
-        rbr, rbp = Rm.layout()[2], Pm.layout()[2]
+        # the Q1 transfer kernels read no matrix (HB2_Q1_TRANSFER=0: the stored layout)
+        if os.environ.get("HB2_Q1_TRANSFER", "1") != "0":
+            rbr, rbp = 0, 0
+        else:
+            rbr, rbp = Rm.layout()[2], Pm.layout()[2]
         kernels["restrict"] = (lambda: _lib.call("hb2_product_ell", Rm.handle, x.ptr, c.ptr, stream),
                                nc * (rbr + s) + n * s)
         kernels["prolong"] = (lambda: _lib.call("hb2_product_add_ell", Pm.handle, c.ptr, y2.ptr, stream),

@@ -459,6 +459,7 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     npdt = np.float64 if dt == torch.float64 else np.float32
     L = 9
     monkeypatch.setenv("HB2_ELL_COMPACT", layout)   # that layout, no autotuning
+    monkeypatch.setenv("HB2_Q1_TRANSFER", "0")      # the transfers on their stored layout too
     A = SparseMatrixELL.poisson_q1(L, dt)
     P, R = SparseMatrixELL.transfer(L, dt)
     if layout.startswith("pattern"):
@@ -494,6 +495,30 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     # the fused norm's tree order follows the launch shape (rows per thread)
     assert abs(outs[0][5] - outs[1][5]) <= 1e-12 * outs[1][5]
     assert same_bits(outs[0][0], oracle.ell_spmv(oracle.q1_ell(L, npdt), x))
+
+
+@pytest.mark.parametrize("L", [2, 3, 6, 10])
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_q1_transfer_kernels_match_matrix_products(oracle, monkeypatch, L, dt):
+    """The transfer matrices' products without reading them (y = P c, y += P c,
+    y = R f) are the ELL kernels' and the oracle's bits."""
+    from honei_b200 import _lib
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    Pr, Rr = oracle.transfer_ell(L, npdt)
+    P, R = SparseMatrixELL.transfer(L, dt)
+    c, f, y0 = oracle.uniform(Pr.cols, 41, npdt), oracle.uniform(Pr.rows, 42, npdt), oracle.uniform(Pr.rows, 43, npdt)
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HB2_Q1_TRANSFER", flag)
+        yp, yr, ya = dvec(np.zeros(Pr.rows, npdt)), dvec(np.zeros(Rr.rows, npdt)), dvec(y0.copy())
+        hb.Product.value(yp, P, dvec(c))
+        hb.Product.value(yr, R, dvec(f))
+        _lib.call("hb2_product_add_ell", P.handle, dvec(c).ptr, ya.ptr, None)
+        outs.append([host(yp), host(yr), host(ya)])
+    for a, b in zip(outs[0], outs[1]):
+        assert same_bits(a, b)
+    assert same_bits(outs[0][0], oracle.ell_spmv(Pr, c))
+    assert same_bits(outs[0][1], oracle.ell_spmv(Rr, f))
 
 
 def test_compressed_layout_falls_back_when_not_eligible(oracle):
