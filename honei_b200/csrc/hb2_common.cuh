@@ -260,6 +260,60 @@ namespace hb2
 
     inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
+    // Rows of the Q1 transfer matrices of the identity index maps, from the grid (mf,
+    // mc points per fine / coarse line): the products and slot-ordered sums of the
+    // matrix rows, bit-identical to an ELL row sum over them.  Prolongation row of fine
+    // node (i, j), coarse (I, J) = (i/2, j/2): (I,J) x 1; (I,J), (I,J+1) or (I,J),
+    // (I+1,J) x 1/2; (I,J), (I,J+1), (I+1,J), (I+1,J+1) x 1/4.  Restriction row of coarse
+    // node (I, J): the fine nodes (2I+di, 2J+dj) inside the grid, di, dj = -1, 0, 1 in
+    // that order, x (1 or 1/2)(1 or 1/2).  L2: vector loads through L2 (data written
+    // by other blocks of the same launch).
+    template <typename T, bool L2>
+    __device__ __forceinline__ T q1_load(const T * p)
+    {
+        return L2 ? __ldcg(p) : *p;
+    }
+
+    template <typename T, bool L2>
+    __device__ __forceinline__ T q1_prolong_row(uint64_t r, const T * c, uint32_t mf, uint32_t mc)
+    {
+        typedef Arith<T> M;
+        const uint32_t i = (uint32_t)(r / mf), j = (uint32_t)(r - (uint64_t)i * mf);
+        const T * cp = c + (uint64_t)(i >> 1) * mc + (j >> 1);
+        const T h = T(0.5), q = T(0.25);
+        if (! (i & 1) && ! (j & 1)) return M::add(T(0), M::mul(T(1), q1_load<T, L2>(cp)));
+        if (! (i & 1)) return M::add(M::add(T(0), M::mul(h, q1_load<T, L2>(cp))), M::mul(h, q1_load<T, L2>(cp + 1)));
+        if (! (j & 1)) return M::add(M::add(T(0), M::mul(h, q1_load<T, L2>(cp))), M::mul(h, q1_load<T, L2>(cp + mc)));
+        const T a0 = q1_load<T, L2>(cp), a1 = q1_load<T, L2>(cp + 1), a2 = q1_load<T, L2>(cp + mc),
+                a3 = q1_load<T, L2>(cp + mc + 1);
+        return M::add(M::add(M::add(M::add(T(0), M::mul(q, a0)), M::mul(q, a1)), M::mul(q, a2)), M::mul(q, a3));
+    }
+
+    template <typename T, bool L2>
+    __device__ __forceinline__ T q1_restrict_row(uint64_t r, const T * x, uint32_t mf, uint32_t mc)
+    {
+        typedef Arith<T> M;
+        const int I = (int)(r / mc), J = (int)(r - (uint64_t)I * mc);
+        T acc = T(0);
+#pragma unroll
+        for (int di = -1; di <= 1; ++di)
+        {
+            const int i = 2 * I + di;
+            if (i < 0 || i >= (int)mf) continue;
+            const T * xr = x + (uint64_t)i * mf;
+            const T wi = di == 0 ? T(1) : T(0.5);
+#pragma unroll
+            for (int dj = -1; dj <= 1; ++dj)
+            {
+                const int jj = 2 * J + dj;
+                if (jj < 0 || jj >= (int)mf) continue;
+                const T w = dj == 0 ? wi : (di == 0 ? T(0.5) : T(0.25));
+                acc = M::add(acc, M::mul(w, q1_load<T, L2>(xr + jj)));
+            }
+        }
+        return acc;
+    }
+
     extern int g_num_sms;
     int num_sms();
 }

@@ -47,6 +47,9 @@ namespace hb2
         const uint8_t * pat;
         const PatEnt<T> * ptab;
         uint32_t npat;
+        // R and P are the Q1 transfer matrices of grid level q1l (mf, mc points per
+        // line): their rows come from q1_restrict_row / q1_prolong_row; 0: read R, P
+        uint32_t q1l, mf, mc;
     };
 
     constexpr int kSubMaxLevels = 10;
@@ -209,7 +212,8 @@ namespace hb2
         tm.sync();
         for (uint32_t r = tm.tid; r < C.n; r += tm.nth)
         {
-            C.b[r] = row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.R, r, L.store);
+            C.b[r] = L.q1l ? q1_restrict_row<T, ! Team<LOCAL, PL>::plain>(r, L.store, L.mf, L.mc)
+                           : row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.R, r, L.store);
             C.x[r] = T(0);
         }
         tm.sync();
@@ -222,7 +226,8 @@ namespace hb2
     {
         typedef Arith<T> M;
         for (uint32_t r = tm.tid; r < L.n; r += tm.nth)
-            L.x[r] = M::add(tm.ld(L.x + r), row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.P, r, C.x));
+            L.x[r] = M::add(tm.ld(L.x + r), L.q1l ? q1_prolong_row<T, ! Team<LOCAL, PL>::plain>(r, C.x, L.mf, L.mc)
+                                                  : row_sum_any<T, ! Team<LOCAL, PL>::plain>(L.P, r, C.x));
         tm.sync();
         sub_smooth(L, n_post, tm, sp);
     }
@@ -369,6 +374,13 @@ namespace hb2
         for (int i = sc.t1 + 1; i <= sc.top; ++i) up_level(sc.lev[i], sc.lev[i - 1], sc.n_post, all, none);
     }
 
+    // HB2_Q1_TRANSFER=0: the fused small levels read the transfer matrices too
+    static bool q1_transfer_rows_enabled()
+    {
+        const char * v = getenv("HB2_Q1_TRANSFER");
+        return ! (v && strcmp(v, "0") == 0);
+    }
+
     // HB2_SUB_PATTERNS=0: the fused small levels read the plain ELL arrays
     static bool sub_patterns_enabled()
     {
@@ -383,6 +395,13 @@ namespace hb2
         s.A = d.A->view<T>();
         if (d.R) s.R = d.R->view<T>(); else s.R = s.A;
         if (d.P) s.P = d.P->view<T>(); else s.P = s.A;
+        s.q1l = s.mf = s.mc = 0;
+        if (d.R && d.P && d.P->q1_transfer > 1 && d.R->q1_transfer == -d.P->q1_transfer && q1_transfer_rows_enabled())
+        {
+            s.q1l = (uint32_t)d.P->q1_transfer;
+            s.mf = (1u << s.q1l) + 1;
+            s.mc = (1u << (s.q1l - 1)) + 1;
+        }
         s.x = (T *)d.x;
         s.b = (T *)d.b;
         s.store = (T *)d.store;

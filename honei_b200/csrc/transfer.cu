@@ -139,7 +139,8 @@ namespace hb2
     // holds the fine nodes (2I + di, 2J + dj), di, dj in -1..1 inside the grid, in
     // ascending column order, with weight (1 or 1/2) x (1 or 1/2).  Each row is summed
     // as the ELL kernels sum it (0 + v0 x0 + v1 x1 ..., products and sums rounded
-    // separately), so the results are bit-identical to the matrix products.
+    // separately; q1_prolong_row / q1_restrict_row), so the results are bit-identical
+    // to the matrix products.
     template <typename T, int MODE>
     __global__ void __launch_bounds__(256)
     q1_prolong_kernel(const T * __restrict__ c, T * __restrict__ y, uint32_t mf, uint32_t mc, uint64_t nf)
@@ -148,16 +149,7 @@ namespace hb2
         pdl_entry();
         const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= nf) return;
-        const uint32_t i = (uint32_t)(r / mf), j = (uint32_t)(r - (uint64_t)i * mf);
-        const T * cp = c + (uint64_t)(i >> 1) * mc + (j >> 1);
-        const T h = T(0.5), q = T(0.25);
-        T acc;
-        if (! (i & 1) && ! (j & 1)) acc = M::add(T(0), M::mul(T(1), cp[0]));
-        else if (! (i & 1)) acc = M::add(M::add(T(0), M::mul(h, cp[0])), M::mul(h, cp[1]));
-        else if (! (j & 1)) acc = M::add(M::add(T(0), M::mul(h, cp[0])), M::mul(h, cp[mc]));
-        else
-            acc = M::add(M::add(M::add(M::add(T(0), M::mul(q, cp[0])), M::mul(q, cp[1])), M::mul(q, cp[mc])),
-                         M::mul(q, cp[mc + 1]));
+        const T acc = q1_prolong_row<T, false>(r, c, mf, mc);
         y[r] = MODE == kAdd ? M::add(y[r], acc) : acc;
     }
 
@@ -166,29 +158,10 @@ namespace hb2
     q1_restrict_kernel(const T * __restrict__ x, T * __restrict__ y, T * __restrict__ zero, uint32_t mf,
                        uint32_t mc, uint64_t nc)
     {
-        typedef Arith<T> M;
         pdl_entry();
         const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= nc) return;
-        const int I = (int)(r / mc), J = (int)(r - (uint64_t)I * mc);
-        T acc = T(0);
-#pragma unroll
-        for (int di = -1; di <= 1; ++di)
-        {
-            const int i = 2 * I + di;
-            if (i < 0 || i >= (int)mf) continue;
-            const T * xr = x + (uint64_t)i * mf;
-            const T wi = di == 0 ? T(1) : T(0.5);
-#pragma unroll
-            for (int dj = -1; dj <= 1; ++dj)
-            {
-                const int jj = 2 * J + dj;
-                if (jj < 0 || jj >= (int)mf) continue;
-                const T w = dj == 0 ? wi : (di == 0 ? T(0.5) : T(0.25));
-                acc = M::add(acc, M::mul(w, xr[jj]));
-            }
-        }
-        y[r] = acc;
+        y[r] = q1_restrict_row<T, false>(r, x, mf, mc);
         if (MODE == kRestrict) zero[r] = T(0);
     }
 
