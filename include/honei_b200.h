@@ -92,7 +92,10 @@ HB2_API int hb2_ell_create(hb2_ell *out, hb2_dtype dtype, uint64_t rows, uint64_
 HB2_API int hb2_ell_create_q1(hb2_ell *out, hb2_dtype dtype, unsigned level, double aniso, cudaStream_t stream);
 /* Assemble on the device P = ProlongationMatrix (level-1 -> level) with identity
  * index maps (math/prolongation_matrix.hh:44-100) and its transpose R
- * (math/transposition.hh:36-50), both as ELL. */
+ * (math/transposition.hh:36-50), both as ELL.  Their single-vector products
+ * (hb2_product_ell, hb2_product_add_ell, the MG hierarchy's transfers) run on
+ * kernels that derive each row's columns and weights from the grid instead of
+ * reading the matrix, with the same bits; HB2_Q1_TRANSFER=0 reads the matrices. */
 HB2_API int hb2_ell_create_transfer(hb2_ell *prol, hb2_ell *res, hb2_dtype dtype, unsigned fine_level,
                             cudaStream_t stream);
 /* Same matrix in another element type (values rounded like DT(double)). */
