@@ -76,6 +76,7 @@ SIGNATURES = {
     "hb2_last_error": (ctypes.c_char_p, []),
     "hb2_version": (ctypes.c_char_p, []),
     "hb2_launch_count": (_u64, []),
+    "hb2_workspace_count": (_u64, []),
     "hb2_ell_create": (_int, [_pvp, _int, _u64, _u64, _u64, _u64, _u64, _vp, _vp, _vp, _int, _vp]),
     "hb2_ell_create_q1": (_int, [_pvp, _int, ctypes.c_uint, _dbl, _vp]),
     "hb2_ell_create_transfer": (_int, [_pvp, _pvp, _int, ctypes.c_uint, _vp]),

@@ -206,7 +206,7 @@ namespace hb2
     uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)
     {
         const int cls = reducing ? 1 : 0;
-        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * (A->rpt[cls] & ~kPatWin);
+        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * (A->rpt[cls] & ~kPatFlags);
         if (A->layout[cls] == kLayoutCompact) return (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt);
         return (uint64_t)kEllThreads * (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
     }
@@ -678,7 +678,7 @@ extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * ro
     const int l = A->layout[cls];
     if (layout) *layout = l;
     if (rows_per_thread) *rows_per_thread = (int)(ell_rows_per_block(A, cls == 1) / kEllThreads);
-    if (windowed) *windowed = (l == kLayoutPattern && (A->rpt[cls] & kPatWin)) ? 1 : 0;
+    if (windowed) *windowed = l != kLayoutPattern ? 0 : (A->rpt[cls] & kPatWin) ? 1 : (A->rpt[cls] & kPatQ1) ? 2 : 0;
     return HB2_OK;
 }
 

@@ -529,6 +529,8 @@ namespace hb2
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         if (A->pat && A->pat_win_m)
             for (int r : {1, 2}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatWin));
+        if (A->pat && A->q1_full >= 0)
+            for (int r : {2, 4, 8}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatQ1));
         // Each candidate is timed as a burst of back-to-back launches (the way the
         // solvers issue them, and long enough for the event clock's granularity),
         // the candidates interleaved over several rounds so that clock or
@@ -598,14 +600,14 @@ namespace hb2
         st = ell_build_pattern(A, stream);
         if (st) return st;
         const char * v = getenv("HB2_ELL_COMPACT");
-        if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0))
+        if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0 || strncmp(v, "q1stencil", 9) == 0))
         {
             // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
             // rows per thread; pattern[1|2|4]: the row-pattern layout (square
-            // matrices that admit it; patternwin[1|2] its windowed kernel where the
-            // offsets allow;
             // matrices that admit it; the others compressed, 2 rows per thread);
-            // no autotuning
+            // patternwin[1|2] its windowed kernel where the offsets allow;
+            // q1stencil[2|4|8] the Q1 stencil kernel where the matrix holds the full
+            // nine-point stencil; no autotuning
             Choice c;
             if (v[0] == 'p' && A->pat)
             {
@@ -615,6 +617,15 @@ namespace hb2
                 c.layout[0] = c.layout[1] = kLayoutPattern;
                 c.rpt[0] = c.rpt[1] = (r == 2 || r == 4) ? r : 1;
                 if (win && A->pat_win_m && c.rpt[0] <= 2) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatWin;
+            }
+            else if (strncmp(v, "q1stencil", 9) == 0 && A->pat)
+            {
+                // q1stencil[2|4|8]: the Q1 stencil kernel where the matrix holds the
+                // full stencil, else the row-pattern kernel with as many rows per thread
+                const int r = atoi(v + 9);
+                c.layout[0] = c.layout[1] = kLayoutPattern;
+                c.rpt[0] = c.rpt[1] = (r == 4 || r == 8) ? r : 2;
+                if (A->q1_full >= 0) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatQ1;
             }
             else
             {

@@ -422,6 +422,11 @@ namespace hb2
         v.rows = A->rows;
         v.K = A->K;
         v.npat = A->npat;
+        if ((R & kPatQ1) && ell_q1_stencil_applies(A, MODE, x, b))
+        {
+            launch_ell_q1_stencil(A, MODE, x, y, aux, aux2, red, want_sqrt, rs, grid, s, flags, R & ~kPatFlags);
+            return;
+        }
         // the window copies need a 16-byte aligned x
         if ((R & kPatWin) && A->pat_win_m && A->K == 9 && ! b.list && b.nvec == 1 && ! b.active &&
             ((uintptr_t)x & 15) == 0)
@@ -435,11 +440,18 @@ namespace hb2
                            (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt);
             return;
         }
-        R &= ~kPatWin;
+        R &= ~kPatFlags;
 #define HB2_PAT_LAUNCH(KT_, R_)                                                                              \
         launch_pdl(ell_pattern_kernel<T, KT_, MODE, R_>, grid, dim3(kEllThreads), 0, s, v, (const T *)x, (T *)y, \
                    (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags, b)
-        if (A->K == 9) { if (R == 1) HB2_PAT_LAUNCH(9, 1); else if (R == 2) HB2_PAT_LAUNCH(9, 2); else HB2_PAT_LAUNCH(9, 4); }
+        // (8 rows per thread only as the fallback of the Q1 stencil kernel's widest shape)
+        if (A->K == 9)
+        {
+            if (R == 1) HB2_PAT_LAUNCH(9, 1);
+            else if (R == 2) HB2_PAT_LAUNCH(9, 2);
+            else if (R == 4) HB2_PAT_LAUNCH(9, 4);
+            else HB2_PAT_LAUNCH(9, 8);
+        }
         else { if (R == 1) HB2_PAT_LAUNCH(0, 1); else if (R == 2) HB2_PAT_LAUNCH(0, 2); else HB2_PAT_LAUNCH(0, 4); }
 #undef HB2_PAT_LAUNCH
     }
@@ -576,6 +588,7 @@ namespace hb2
                 if (ok_win) A->pat_win_m = mm;
             }
         }
+        ell_find_q1_stencil(A);
         return HB2_OK;
     }
 

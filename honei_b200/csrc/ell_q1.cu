@@ -1,0 +1,315 @@
+// Q1 stencil kernel for square row-pattern ELL matrices whose rows are the
+// nine-point stencil of an m x m node grid (the Q1 operators of
+// math/fill_matrix.hh:37-79 at every level, and any matrix with the same
+// structure).
+//
+// The general row-pattern kernels (ell_pattern.cu) look up each row's pattern
+// in a table and gather x through per-slot offsets: about 200-230 instructions
+// per row, most of them address arithmetic, so they issue-bind well below the
+// HBM roofline.  Here the pattern that holds the full stencil -- nine slots,
+// columns i-m-1, i-m, i-m+1, i-1, i, i+1, i+m-1, i+m, i+m+1 in that slot order --
+// is known when the layout is built, and its nine values travel as kernel
+// parameters (constant-bank operands of the multiplies).  A block owns
+// B = 256 R consecutive rows, interleaved over its threads; thread 0 stages the
+// three windows of x the stencil touches ([r0-m-1, r0+B-m+1), [r0-1, r0+B+1),
+// [r0+m-1, r0+B+m+1)) with bulk copies (cp.async.bulk, no multicast, completion
+// on an mbarrier with a bounded wait) while every thread streams its rows'
+// pattern ids, rhs and Jacobi vector.  A full-stencil row then reads its nine x
+// values at fixed shared-memory offsets from its own position: no table, no
+// per-slot integer work.  Rows of any other pattern (Dirichlet identity rows,
+// the grid's boundary) take the general slot loop over the pattern table.
+// Both paths form the products and slot-ordered sums of the plain layout
+// (la/product.hh:148-206: sum = 0, then sum += a_k x_k slot by slot, each
+// product and sum rounded), so results are bit-identical to it and to the
+// reference.  If the copies do not complete within the bounded wait, the block
+// computes from global memory instead (same bits) and records the event.
+#include "hb2_common.cuh"
+#include "hb2_internal.hh"
+#include "tma.cuh"
+
+#include <vector>
+
+namespace hb2
+{
+    template <typename T>
+    struct Q1Stencil
+    {
+        T v[9];                  // the full stencil row's values, in slot order
+        const uint8_t * pat;     // pattern id per row
+        const PatEnt<T> * tab;   // npat * 9 (value, column - row) entries
+        int64_t n, m;
+        uint32_t full;           // pattern id of the full stencil row
+    };
+
+    // diagnostic: set when a block's window copies did not complete in time
+    __device__ int g_q1_stencil_timeout = 0;
+
+    // x window w of the block starting at row r0: its first element's global index
+    // (16-byte aligned: the bulk copy's start), the valid range and the ragged tail
+    template <int B, int E>
+    __device__ __forceinline__ void q1_window(int64_t start, int64_t n, int64_t & lo, int64_t & hi, int64_t & alo,
+                                              int64_t & ahi)
+    {
+        lo = start < 0 ? 0 : start;
+        hi = start + B + 2 > n ? n : start + B + 2;
+        if (hi < lo) hi = lo;
+        alo = lo - (lo % E);
+        ahi = hi - (hi % E);
+    }
+
+    // one row of any pattern: slots in table order, x from the windows (or from
+    // global memory when the copies did not complete)
+    template <typename T, int W>
+    __device__ __noinline__ T q1_any_row(const PatEnt<T> * __restrict__ te, const T * __restrict__ x, int64_t i,
+                                         const T * win, int64_t alo0, int64_t alo1, int64_t alo2, bool fast)
+    {
+        typedef Arith<T> M;
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < 9; ++j)
+        {
+            const PatEnt<T> e = te[j];
+            if (e.off == kPatEmpty) continue;
+            const int64_t g = i + e.off;
+            T xv;
+            if (! fast) xv = __ldg(x + g);
+            else if (e.off <= -2) xv = win[g - alo0];
+            else if (e.off <= 1) xv = win[W + (g - alo1)];
+            else xv = win[2 * W + (g - alo2)];
+            acc = M::add(acc, M::mul(e.val, xv));
+        }
+        return acc;
+    }
+
+    template <typename T, int MODE, int R>
+    __global__ void __launch_bounds__(kEllThreads)
+    q1_stencil_kernel(const __grid_constant__ Q1Stencil<T> s, const T * __restrict__ x, T * __restrict__ y,
+                      const T * __restrict__ aux, const T * __restrict__ aux2, ReduceSlot rs, double * red,
+                      int want_sqrt, int flags)
+    {
+        typedef Arith<T> M;
+        constexpr int B = kEllThreads * R;
+        constexpr int E = 16 / sizeof(T);
+        constexpr int W = (B + 2 + 2 * E + E - 1) / E * E;
+        extern __shared__ __align__(128) unsigned char q1_smem[];
+        T * win = reinterpret_cast<T *>(q1_smem);
+        __shared__ alignas(8) uint64_t bar;
+        const int64_t n = s.n, m = s.m;
+        const int t = (int)threadIdx.x;
+        const int64_t blk = (flags & kReverse) ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
+        const int64_t r0 = blk * B;
+        const int64_t i0 = r0 + t;
+        // pattern ids are constant: fetched before waiting on the previous kernel
+        uint32_t p[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            p[k] = i < n ? (uint32_t)((flags & kKeepL2) ? __ldcg(s.pat + i) : __ldcs(s.pat + i)) : s.full;
+        }
+        pdl_entry();   // x, rhs and P may come from the previous kernel
+        T ea[R], ep[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            const bool ok = i < n;
+            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi)) ? aux[i] : T(0);
+            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+        }
+        int64_t lo[3], hi[3], alo[3], ahi[3];
+#pragma unroll
+        for (int w = 0; w < 3; ++w) q1_window<B, E>(r0 + (w - 1) * m - 1, n, lo[w], hi[w], alo[w], ahi[w]);
+        if (t == 0)
+        {
+            mbar_init(&bar, 1);
+            unsigned total = 0;
+#pragma unroll
+            for (int w = 0; w < 3; ++w) total += (unsigned)((ahi[w] - alo[w]) * sizeof(T));
+            mbar_expect_tx(&bar, total);
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+                if (ahi[w] > alo[w])
+                    bulk_g2s(win + w * W, x + alo[w], (unsigned)((ahi[w] - alo[w]) * sizeof(T)), &bar);
+        }
+        else if (t <= 3 * (E - 1))
+        {
+            // the windows' ragged tails (at most E - 1 elements each) by plain loads
+            const int w = (t - 1) / (E - 1), e = (t - 1) % (E - 1);
+            const int64_t from = w == 0 ? (ahi[0] > lo[0] ? ahi[0] : lo[0])
+                                        : (w == 1 ? (ahi[1] > lo[1] ? ahi[1] : lo[1]) : (ahi[2] > lo[2] ? ahi[2] : lo[2]));
+            const int64_t j = from + e;
+            const int64_t h = w == 0 ? hi[0] : (w == 1 ? hi[1] : hi[2]);
+            const int64_t a = w == 0 ? alo[0] : (w == 1 ? alo[1] : alo[2]);
+            if (j < h) win[w * W + (j - a)] = x[j];
+        }
+        __syncthreads();
+        const bool fast = mbar_wait_bounded(&bar, 0, 1000000000ull);
+        if (! fast && t == 0) atomicExch(&g_q1_stencil_timeout, 1);
+        // x[i - m - 1 + j], x[i - 1 + j], x[i + m - 1 + j] of row i = i0 + k * 256 at
+        // c0[k * 256 + j], c1[...], c2[...]: compile-time offsets from three
+        // per-thread positions (negative only for rows the full stencil does not reach)
+        const int o0 = (int)(i0 - m - 1 - alo[0]);
+        const int o1 = W + (int)(i0 - 1 - alo[1]);
+        const int o2 = 2 * W + (int)(i0 + m - 1 - alo[2]);
+        double part = 0.0;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            if (i >= n) break;
+            const int l = k * kEllThreads;
+            T acc, xc;
+            if (fast && p[k] == s.full)
+            {
+                const T * c0 = win + (o0 + l);
+                const T * c1 = win + (o1 + l);
+                const T * c2 = win + (o2 + l);
+                acc = M::add(T(0), M::mul(s.v[0], c0[0]));
+                acc = M::add(acc, M::mul(s.v[1], c0[1]));
+                acc = M::add(acc, M::mul(s.v[2], c0[2]));
+                acc = M::add(acc, M::mul(s.v[3], c1[0]));
+                xc = c1[1];
+                acc = M::add(acc, M::mul(s.v[4], xc));
+                acc = M::add(acc, M::mul(s.v[5], c1[2]));
+                acc = M::add(acc, M::mul(s.v[6], c2[0]));
+                acc = M::add(acc, M::mul(s.v[7], c2[1]));
+                acc = M::add(acc, M::mul(s.v[8], c2[2]));
+            }
+            else
+            {
+                acc = q1_any_row<T, W>(s.tab + p[k] * 9u, x, i, win, alo[0], alo[1], alo[2], fast);
+                xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[o1 + l + 1] : x[i]) : T(0);
+            }
+            if (MODE == kPlain) y[i] = acc;
+            else if (MODE == kDefect)
+            {
+                const T d = M::sub(ea[k], acc);
+                y[i] = d;
+                part = fma((double)d, (double)d, part);
+            }
+            else if (MODE == kDot)
+            {
+                y[i] = acc;
+                part = fma((double)acc, (double)xc, part);
+            }
+            else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep[k], M::sub(ea[k], acc)));
+        }
+        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        {
+            __shared__ double scratch[32];
+            const double sum = block_sum(part, scratch);
+            grid_sum_finish(sum, rs, red, want_sqrt, scratch);
+        }
+        // copies still in flight must land before the block's shared memory is reused
+        if (! fast) mbar_wait_bounded(&bar, 0, 1000000000ull);
+    }
+
+    template <typename T, int R>
+    static constexpr size_t q1_stencil_smem()
+    {
+        return (size_t)3 * ((kEllThreads * R + 2 + 2 * (16 / sizeof(T)) + 16 / sizeof(T) - 1) / (16 / sizeof(T)) *
+                            (16 / sizeof(T))) * sizeof(T);
+    }
+
+    template <typename T, int MODE, int R>
+    static void q1_stencil_launch(const Q1Stencil<T> & s, dim3 grid, cudaStream_t st, const void * x, void * y,
+                                  const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
+                                  int flags)
+    {
+        constexpr size_t smem = q1_stencil_smem<T, R>();
+        if (smem > 48 * 1024)
+        {
+            // dynamic shared memory above 48 KiB needs the kernel's opt-in, once per device
+            static bool done[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev >= 0 && dev < 64 && ! done[dev])
+            {
+                cudaFuncSetAttribute(q1_stencil_kernel<T, MODE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+                done[dev] = true;
+            }
+        }
+        launch_pdl(q1_stencil_kernel<T, MODE, R>, grid, dim3(kEllThreads), smem, st, s, (const T *)x, (T *)y,
+                   (const T *)aux, (const T *)aux2, rs, red, want_sqrt, flags);
+    }
+
+    template <typename T, int MODE>
+    static void q1_stencil_mode(const hb2_ell_s * A, int R, dim3 grid, cudaStream_t st, const void * x, void * y,
+                                const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
+                                int flags)
+    {
+        Q1Stencil<T> s;
+        for (int k = 0; k < 9; ++k) s.v[k] = (T)A->q1_val[k];
+        s.pat = A->pat;
+        s.tab = (const PatEnt<T> *)A->ptab;
+        s.n = (int64_t)A->rows;
+        s.m = A->pat_win_m;
+        s.full = (uint32_t)A->q1_full;
+        if (R == 2) q1_stencil_launch<T, MODE, 2>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
+        else if (R == 4) q1_stencil_launch<T, MODE, 4>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
+        else q1_stencil_launch<T, MODE, 8>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
+    }
+
+    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, const Batch & b)
+    {
+        return A->q1_full >= 0 && A->pat_win_m && A->K == 9 && ! b.list && b.nvec == 1 && ! b.active &&
+               (mode == kPlain || mode == kDefect || mode == kDot || mode == kJacobi) && ((uintptr_t)x & 15) == 0;
+    }
+
+    void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                               const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                               cudaStream_t stream, int flags, int R)
+    {
+#define HB2_Q1S(T_, M_) q1_stencil_mode<T_, M_>(A, R, grid, stream, x, y, aux, aux2, rs, red, want_sqrt, flags)
+        if (A->dtype == HB2_F64)
+        {
+            if (mode == kPlain) HB2_Q1S(double, kPlain);
+            else if (mode == kDefect) HB2_Q1S(double, kDefect);
+            else if (mode == kDot) HB2_Q1S(double, kDot);
+            else HB2_Q1S(double, kJacobi);
+        }
+        else
+        {
+            if (mode == kPlain) HB2_Q1S(float, kPlain);
+            else if (mode == kDefect) HB2_Q1S(float, kDefect);
+            else if (mode == kDot) HB2_Q1S(float, kDot);
+            else HB2_Q1S(float, kJacobi);
+        }
+#undef HB2_Q1S
+    }
+
+    // After the row-pattern layout is built: the pattern, if any, that holds the
+    // full nine-point stencil of an m x m grid in ascending column order (at most
+    // one is used; rows of other full patterns take the general slot loop).
+    template <typename T>
+    static void find_q1_stencil_typed(hb2_ell_s * A)
+    {
+        const int64_t m = A->pat_win_m;
+        std::vector<PatEnt<T>> tab((size_t)A->npat * 9);
+        if (cudaMemcpy(tab.data(), A->ptab, tab.size() * sizeof(PatEnt<T>), cudaMemcpyDeviceToHost) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return;
+        }
+        const int64_t want[9] = {-m - 1, -m, -m + 1, -1, 0, 1, m - 1, m, m + 1};
+        for (uint32_t q = 0; q < A->npat; ++q)
+        {
+            bool full = true;
+            for (int k = 0; k < 9 && full; ++k) full = tab[(size_t)q * 9 + k].off == want[k];
+            if (! full) continue;
+            A->q1_full = (int)q;
+            for (int k = 0; k < 9; ++k) A->q1_val[k] = (double)tab[(size_t)q * 9 + k].val;
+            return;
+        }
+    }
+
+    void ell_find_q1_stencil(hb2_ell_s * A)
+    {
+        A->q1_full = -1;
+        if (! A->pat || ! A->ptab || ! A->pat_win_m || A->K != 9 || A->pat_win_m > (1 << 20)) return;
+        if (A->dtype == HB2_F64) find_q1_stencil_typed<double>(A);
+        else find_q1_stencil_typed<float>(A);
+    }
+}

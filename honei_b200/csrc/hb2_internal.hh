@@ -90,6 +90,11 @@ struct hb2_ell_s
     // square matrix of m^2 rows (the Q1 operators): the windowed pattern kernel
     // applies (rpt | kPatWin); 0 otherwise
     int64_t pat_win_m = 0;
+    // the pattern holding the full nine-point stencil (columns i-m-1 .. i+m+1 in
+    // ascending slot order) and its values, or -1: the Q1 stencil kernel applies
+    // (rpt | kPatQ1, ell_q1.cu)
+    int q1_full = -1;
+    double q1_val[9] = {};
     // row patterns of a small square matrix for the fused small-level kernels
     // (subcycle.cu), built on the host when the matrix joins a hierarchy
     uint8_t * spat = nullptr;
@@ -190,6 +195,8 @@ namespace hb2
     };
     constexpr int32_t kPatEmpty = (-2147483647 - 1);
     constexpr int kPatWin = 0x10;    // rpt flag: the windowed row-pattern kernel
+    constexpr int kPatQ1 = 0x20;     // rpt flag: the Q1 stencil kernel (ell_q1.cu)
+    constexpr int kPatFlags = kPatWin | kPatQ1;
     constexpr int kSubPatMax = 8;    // patterns of a small-level operator in the fused kernels
     int ell_small_patterns(hb2_ell_s * A);
 
@@ -212,6 +219,13 @@ namespace hb2
     void launch_ell_pattern(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                             const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
                             cudaStream_t stream, int flags, Batch b, int R);
+
+    // Q1 stencil kernel for row-pattern matrices with the full nine-point stencil (ell_q1.cu)
+    void ell_find_q1_stencil(hb2_ell_s * A);
+    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, const Batch & b);
+    void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                               const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                               cudaStream_t stream, int flags, int R);
 
     // compressed ELL layout (ell_compact.cu)
     int ell_build_compact(hb2_ell_s * A, cudaStream_t stream);

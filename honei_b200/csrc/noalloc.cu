@@ -12,10 +12,11 @@
 // Limits and sharing:
 //  * the scratch holds kNoAllocMaxBlocks block partials, so the matrix may have
 //    at most kNoAllocMaxBlocks * 512 rows in FP64 (8,388,608) and
-//    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216), and at most
-//    kNoAllocMaxBlocks row blocks in the layout it runs on (the row-pattern
-//    layout at one row per thread: 4,194,304 rows); larger matrices are
-//    rejected with HB2_ERR_UNSUPPORTED before anything is launched;
+//    kNoAllocMaxBlocks * 1024 rows in FP32 (16,777,216); larger matrices are
+//    rejected with HB2_ERR_UNSUPPORTED before anything is launched.  The
+//    decision depends on the row count and element type only: where the
+//    matrix's tuned layout would need more row blocks than that, the kernel
+//    runs on the same layout with more rows per thread (same defect bits);
 //  * every GPU that loads the library holds the array (about 134 KiB) until the
 //    process exits;
 //  * all calls on a device share the one array: calls whose kernels overlap on
@@ -71,20 +72,41 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
     if (! A || ! norm2_dev) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null matrix or norm output");
     if (A->rows != A->cols) return fail(HB2_ERR_SIZE, "hb2_defect_ell_noalloc: VectorSizeDoesNotMatch (rhs vs columns)");
     if (A->rows > 0 && (! rhs || ! x || ! r)) return fail(HB2_ERR_ARG, "hb2_defect_ell_noalloc: null vector");
-    // at most max_rows rows (512 per scratch partial in FP64, 1024 in FP32), and
-    // the row blocks of the layout the matrix runs on must fit the scratch
+    // at most max_rows rows (512 per scratch partial in FP64, 1024 in FP32): the
+    // only condition, so the answer depends on the row count and element type
+    // alone, never on the layout the autotuner picked for this matrix
     const uint64_t rows_per_block = (uint64_t)kEllThreads *
                                     (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
     const uint64_t max_rows = (uint64_t)kNoAllocMaxBlocks * rows_per_block;
-    if (A->rows > max_rows || ell_grid(A, true) > kNoAllocMaxBlocks)
+    if (A->rows > max_rows)
         return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: " + std::to_string(A->rows) +
                     " rows exceed the static scratch limit of " + std::to_string(max_rows) +
                     " rows for this element type; use hb2_defect_ell");
+    // The kernel runs on the matrix's tuned layout unless that layout's row
+    // blocks outnumber the scratch partials (the row-pattern layout at one row
+    // per thread, or the compressed one at two in FP32): then on the same layout
+    // with enough rows per thread.  Every variant forms the same products and
+    // slot-ordered sums, so the defect vector is the same bit for bit; the norm's
+    // block partials follow the launch shape.
+    hb2_ell_s V = *A;
+    const int base = V.rpt[1] & ~kPatFlags, kflags = V.rpt[1] & kPatFlags;
+    for (int r = 2; r <= 8 && ell_grid(&V, true) > kNoAllocMaxBlocks; r *= 2)
+    {
+        if (V.layout[1] == kLayoutPattern && r > base && (r <= 4 || (kflags & kPatQ1)))
+            V.rpt[1] = r | (kflags & kPatQ1) | (r <= 2 ? (kflags & kPatWin) : 0);
+        else if (V.layout[1] == kLayoutCompact && r > V.compact_rpt_red) V.compact_rpt_red = r;
+    }
+    if (ell_grid(&V, true) > kNoAllocMaxBlocks)
+        return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: no layout variant fits the static scratch");
     double * scratch = 0;
     int st = noalloc_scratch(&scratch);
     if (st) return st;
-    // the ticket counters must start at zero; the previous call's contents are
-    // otherwise left as they were (the partials are written before they are read)
+    // The ticket counters must start at zero.  Every completed launch leaves them
+    // at zero again, but a launch that stopped part-way (an error on the device,
+    // or a call that raced with another on a second stream) would leave a
+    // counter off by some tickets and every later norm wrong, so they are
+    // cleared here each call.  The partials need no clearing: each block writes
+    // its own before the last block reads them.
     unsigned * ticket = (unsigned *)(scratch + kNoAllocMaxBlocks + kNoAllocGroups);
     HB2_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * (kNoAllocGroups + 1), stream));
     Workspace ws;
@@ -98,5 +120,5 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
     ws.max_blocks = kNoAllocMaxBlocks;
     ws.max_tickets = kNoAllocGroups + 1;
     ws.host_scalars = 0;
-    return launch_ell(A, kDefect, x, r, rhs, 0, 0, norm2_dev, 0, &ws, stream);
+    return launch_ell(&V, kDefect, x, r, rhs, 0, 0, norm2_dev, 0, &ws, stream);
 }

@@ -119,3 +119,9 @@ extern "C" const char * hb2_last_error(void) { return hb2::t_last_error.c_str();
 extern "C" const char * hb2_version(void) { return "honei_b200 0.1 (sm_100a)"; }
 
 extern "C" uint64_t hb2_launch_count(void) { return hb2::t_launches; }
+
+extern "C" uint64_t hb2_workspace_count(void)
+{
+    std::lock_guard<std::mutex> lock(hb2::g_ws_mutex);
+    return hb2::g_ws.size();
+}

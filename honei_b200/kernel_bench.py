@@ -4,7 +4,9 @@
                                                 cgvar|bicgstab|coarse_cg]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
 
-Each launch is preceded by an L2 flush (256 MiB write) and timed alone with CUDA
+Each launch is preceded by an L2 flush (256 MiB written, then 256 MiB read, so
+that no dirty line of the flush is written back during the launch; --flush write
+keeps only the write) and timed alone with CUDA
 events on the launching stream; the line reports the mean launch time and the
 algorithmic bandwidth (bytes per row as in the design notes) against the
 measured HBM peak.  The first launch of each kernel is a warm-up.
@@ -34,12 +36,32 @@ def peak_gbs() -> float:
         return 6650.0
 
 
+class L2Flush:
+    """Evicts L2 (126 MB on B200) before a timed launch: writes a 256 MiB buffer,
+    then (clean=True) reads another 256 MiB, so that the launch finds neither its
+    inputs in L2 nor dirty lines of the flush whose write-back it would pay for
+    during its own reads."""
+
+    def __init__(self, device, clean: bool = True):
+        self.w = torch.empty(64 << 20, dtype=torch.float32, device=device)
+        self.r = torch.ones(64 << 20, dtype=torch.float32, device=device) if clean else None
+        self.out = torch.empty((), dtype=torch.float32, device=device)
+
+    def __call__(self):
+        self.w.zero_()
+        if self.r is not None:
+            torch.sum(self.r, dim=0, out=self.out)
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="all")
     ap.add_argument("--level", type=int, default=10)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--flush", default="clean", choices=["clean", "write", "none"],
+                    help="clean: write then read 256 MiB before each launch; write: the write only; none: "
+                         "bursts of 8 back-to-back launches, no flush (warm L2), time per launch")
     a = ap.parse_args(argv)
     dt = torch.float64 if a.dtype == "f64" else torch.float32
     s = 8 if a.dtype == "f64" else 4
@@ -50,7 +72,7 @@ def main(argv=None) -> int:
     n = ((1 << L) + 1) ** 2
     nc = ((1 << (L - 1)) + 1) ** 2
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    flush = L2Flush(dev, clean=a.flush == "clean") if a.flush != "none" else None
 
     def vec(m, seed):
         return DenseVector(torch.from_numpy(uniform(m, seed, dtype=npdt)).to(dev))
@@ -62,7 +84,11 @@ def main(argv=None) -> int:
     P = DenseVector(n, dtype=dt)
     _lib.call("hb2_jacobi_precon", A.handle, 0.7, P.ptr, stream)
     nrm = torch.zeros(1, dtype=torch.float64, device=dev)
+    xc = torch.empty(n, dtype=dt, device=dev)
     kernels = {
+        # the floor for streaming this many bytes: torch's device copy of one vector
+        # (read n, write n elements), timed the same way
+        "copy": (lambda: xc.copy_(x.elements), 2 * n * s),
         "jacobi": (lambda: _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, b.ptr, x.ptr, y.ptr, stream),
                    n * (rb + 4 * s)),
         "spmv": (lambda: _lib.call("hb2_product_ell", A.handle, x.ptr, y.ptr, stream), n * (rb + 2 * s)),
@@ -162,17 +188,22 @@ def main(argv=None) -> int:
         fn, nbytes = kernels[name]
         times = []
         for i in range(a.iters + 1):
-            flush.zero_()
+            if a.flush != "none":
+                flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            fn()
+            for _ in range(1 if a.flush != "none" else 8):
+                fn()
             e1.record()
             e1.synchronize()
             if i > 0:
-                times.append(e0.elapsed_time(e1))
+                times.append(e0.elapsed_time(e1) / (1 if a.flush != "none" else 8))
         ms = statistics.mean(times)
         gbs = nbytes / (ms * 1e-3) / 1e9
-        print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "layout": A.layout()[0], "matrix_bytes_per_row": rb,
+        print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "layout": A.layout()[0],
+                          "variant": list(A.layout_variant(0 if name != "defect" else 1)) if name != "copy" else None,
+                          "flush": a.flush,
+                          "matrix_bytes_per_row": rb,
                           "launch_us": 1000 * ms,
                           "algorithmic_bytes": nbytes, "gbs": gbs, "frac_of_measured_peak": gbs / peak}),
               flush=True)

@@ -170,12 +170,14 @@ class SparseMatrixELL:
         return c.value, t.value, rb.value
 
     def layout_variant(self, cls: int = 0):
-        """(kind, rows_per_thread, windowed) of the kernel behind layout() for kernel
+        """(kind, rows_per_thread, kernel) of the kernel behind layout() for kernel
         class cls (0: products, sweeps, transfers; 1: defects with a fused norm);
-        windowed = True for the row-pattern kernel that stages x in shared memory."""
+        kernel 1 for the row-pattern kernel that stages x in shared-memory windows,
+        2 for the Q1 stencil kernel (row patterns holding the full nine-point
+        stencil), 0 otherwise."""
         k, r, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hb2_ell_layout_variant", self._h, cls, ctypes.byref(k), ctypes.byref(r), ctypes.byref(w))
-        return k.value, r.value, bool(w.value)
+        return k.value, r.value, w.value
 
     def stride(self) -> int:
         return self._stride

@@ -4,8 +4,8 @@
  *
  * This is the drop-in boundary.  It replaces the old CUDA backend's launcher
  * table (honei/backends/cuda/operations.hh:29-128) and the tag glue in
- * honei/la/ *-cuda.cc and honei/math/ *-cuda.cc.  A new HONEI tag (tags::B200,
- * see INTEGRATION.md) specialises Product, Defect, ScaledSum, DotProduct, Norm,
+ * honei/la/ *-cuda.cc and honei/math/ *-cuda.cc.  A new HONEI tag, tags::B200,
+ * specialises Product, Defect, ScaledSum, DotProduct, Norm,
  * Sum, Scale, Difference, ElementProduct, copy/fill/convert, Prolongation,
  * Restriction and the CG / MG / IR solvers with thin shims over these calls.
  *
@@ -75,6 +75,10 @@ HB2_API const char *hb2_last_error(void);
 HB2_API const char *hb2_version(void);
 /* number of kernels this library launched on this host thread since load */
 HB2_API uint64_t hb2_launch_count(void);
+/* number of per-(device, stream) reduction workspaces this library has
+ * allocated since load (each is created on the first fused reduction on a
+ * stream and kept until exit) */
+HB2_API uint64_t hb2_workspace_count(void);
 
 /* ---------------------------------------------------------------- matrices */
 /* Upload a SparseMatrixELL in the reference layout (la/sparse_matrix_ell-impl.hh:42-72:
@@ -185,10 +189,11 @@ HB2_API int hb2_defect_ell(hb2_ell A, const void *rhs, const void *x, void *r, d
  * hb2_defect_ell's reduction workspace is cudaMalloc'd on first use of a stream,
  * this variant keeps the reduction scratch in a fixed file-scope device array
  * (about 134 KiB per GPU that loads the library, held until exit).  norm2_dev
- * is required.  Limit: at most 8,388,608 rows in F64 and 16,777,216 in F32,
- * and at most 16,384 row blocks in the device layout the matrix runs on (the
- * row-pattern layout at one row per thread: 4,194,304 rows); larger matrices
- * return HB2_ERR_UNSUPPORTED before any launch.  All calls on a
+ * is required.  Limit: at most 8,388,608 rows in F64 and 16,777,216 in F32;
+ * larger matrices return HB2_ERR_UNSUPPORTED before any launch.  The answer
+ * depends on the row count and element type only (a tuned layout whose row
+ * blocks would not fit the scratch runs with more rows per thread: the same
+ * defect bits; the norm within rounding of hb2_defect_ell's).  All calls on a
  * device share the array, so calls that overlap on the GPU race; calls ordered on
  * one stream are safe.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) and caches it: make it before any stream capture. */

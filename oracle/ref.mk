@@ -2,7 +2,7 @@
 # tags::CPU::MultiCore::SSE) from the reference sources where they lie, plus the
 # driver programs in this directory that call it.  Outputs go to oracle/_ref/ only.
 #
-#   make -f oracle/ref.mk REF=/root/reference -j8
+#   make -f oracle/ref.mk REF=<reference checkout> -j8   (or HONEI_REFERENCE=<checkout>)
 #
 # The reference is gnu++98 code; -fpermissive silences its pre-C++11 idioms and
 # -std=gnu++98 is required (C++11 makes `bind` ambiguous in util/log.cc and
@@ -12,7 +12,10 @@
 # the CPU MemoryBackend registers itself from a static initialiser that a
 # plain archive link would drop.
 
-REF      ?= /root/reference
+REF      ?= $(HONEI_REFERENCE)
+ifeq ($(strip $(REF)),)
+$(error set REF=<reference checkout> or HONEI_REFERENCE)
+endif
 OUT      := oracle/_ref
 OBJ      := $(OUT)/obj
 CXX      ?= g++

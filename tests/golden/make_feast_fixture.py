@@ -40,7 +40,7 @@ def read_ell(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ["HONEI_REFERENCE"]
     data = os.path.join(ref, "honei", "math", "testdata", "poisson") + "/"
     from honei_b200.io import parse_exp
     out, digests = {}, {}

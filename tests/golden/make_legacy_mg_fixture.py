@@ -38,7 +38,7 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "honei_ref")
 
 
 def main() -> int:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ["HONEI_REFERENCE"]
     data = os.path.join(ref, "honei", "math", "testdata")
     if not os.path.exists(REF_BIN):
         print("build the reference driver first: make -f oracle/ref.mk -j8", file=sys.stderr)

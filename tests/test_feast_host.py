@@ -12,7 +12,7 @@ import pytest
 from honei_b200 import _lib
 from honei_b200.io import parse_exp
 
-REF_DATA = "/root/reference/honei/math/testdata/poisson/"
+REF_DATA = os.path.join(os.environ.get("HONEI_REFERENCE", "/nonexistent"), "honei/math/testdata/poisson/")
 
 
 def test_parse_exp_rules():

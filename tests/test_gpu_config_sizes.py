@@ -1,0 +1,136 @@
+"""Parity at the configs' own sizes and on the exact paths the benchmark times.
+
+* Config 1 (Q1 level 10, 1,050,625 unknowns) with the benchmark's MG parameters:
+  V(4,4), omega 0.7, coarse level 3, coarse CG capped at 100 iterations with
+  tree-ordered dots (coarse_exact=False), stop at 1e-10.  Against the oracle
+  (math/mg.hh:1094-1127 restated, reference-order coarse dots): cycle count within
+  +-1, true relative residual below 1e-10 on the oracle's operator, solution within
+  1e-8 relative of the oracle's.  (Each of the two solutions is about 5e-7 from the
+  exact solution at this stop; the 1e-8 bound says they are the same iterate up
+  to the coarse solve's rounding.)
+* Config 2 (level 11, 4,198,401 unknowns): FP64 MG with the reference-order coarse
+  solve bit for bit against the oracle; with the benchmark's coarse mode as above;
+  mixed-precision IR (math/ir.hh:31-80) with its error stated against the oracle's
+  FP64 MG solution (bound 5e-6 relative, about ten times the error either solution
+  has against the exact one) and its true residual below 1e-10.
+* SpMV, defect and the Jacobi sweep at level 11 on the plain layout and on the
+  layout the autotuner picks: bit for bit against the oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import honei_b200 as hb
+from honei_b200 import DenseVector, SparseMatrixELL
+
+pytestmark = pytest.mark.gpu
+
+SOL_TOL = 1e-8        # benched coarse mode vs the oracle's reference-order solve
+MIXED_TOL = 5e-6      # mixed IR vs the oracle's FP64 MG solution
+
+
+def dvec(a):
+    return DenseVector(torch.from_numpy(np.ascontiguousarray(a)).cuda())
+
+
+def host(v):
+    torch.cuda.synchronize()
+    return v.numpy()
+
+
+def same_bits(a, b):
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    return a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def bench_params(eps=1e-10):
+    return hb.mg_params(max_iters_coarse=100, eps=eps, coarse_exact=False)
+
+
+class Case:
+    def __init__(self, oracle, L):
+        self.L = L
+        self.A = oracle.q1_ell(L)
+        self.b = oracle.ell_spmv(self.A, oracle.uniform(self.A.rows, 42))
+        self.x, self.iters, _ = oracle.mg_q1(L, self.b, max_iters_coarse=100)
+        self.nb = np.linalg.norm(self.b)
+
+    def relres(self, oracle, x):
+        return np.linalg.norm(self.b - oracle.ell_spmv(self.A, x)) / self.nb
+
+
+@pytest.fixture(scope="module")
+def case10(oracle):
+    return Case(oracle, 10)
+
+
+@pytest.fixture(scope="module")
+def case11(oracle):
+    return Case(oracle, 11)
+
+
+def solve_mg(L, b, params, dtype=torch.float64):
+    data = hb.MGData.poisson_q1(3, L, dtype=dtype, params=params)
+    x = dvec(np.zeros(b.size))
+    hb.MGSolver.value(data, dvec(b), x)
+    return host(x), data.used_iters
+
+
+@pytest.mark.parametrize("L", [10, 11])
+def test_mg_benchmark_mode_against_the_oracle(oracle, case10, case11, L):
+    c = case10 if L == 10 else case11
+    x, it = solve_mg(L, c.b, bench_params())
+    assert abs(it - c.iters) <= 1, (it, c.iters)
+    assert c.relres(oracle, x) < 1e-10
+    assert np.linalg.norm(x - c.x) / np.linalg.norm(c.x) < SOL_TOL
+
+
+def test_mg_level11_reference_order_bit_exact(case11):
+    x, it = solve_mg(11, case11.b, hb.mg_params(max_iters_coarse=100, eps=1e-10, coarse_exact=True))
+    assert it == case11.iters
+    assert same_bits(x, case11.x)
+
+
+def test_mixed_ir_level11_against_the_oracle(oracle, case11):
+    """The benchmark's mixed-precision IR: FP32 MG V(4,4) inner solve to 1e-3 from a
+    zero start, FP64 coarse CG, FP64 outer defect / update / norm, stop at 1e-10."""
+    L = 11
+    A = SparseMatrixELL.poisson_q1(L)
+    inner = hb.MGData.poisson_q1(3, L, dtype=torch.float32,
+                                 params=hb.mg_params(max_iters_coarse=100, eps=1e-3, coarse_eps=1e-10,
+                                                     coarse_exact=False, coarse_fp64=True))
+    x = dvec(np.zeros(case11.b.size))
+    _, it, st = hb.IRSolver.value(A, dvec(case11.b), x, inner, eps=1e-10, reset_inner=True)
+    xs = host(x)
+    assert case11.relres(oracle, xs) < 1e-10
+    err = np.linalg.norm(xs - case11.x) / np.linalg.norm(case11.x)
+    assert err < MIXED_TOL, err
+    assert it <= 6
+
+
+@pytest.mark.parametrize("layout", ["0", None])
+def test_level11_operators_bit_exact(oracle, case11, monkeypatch, layout):
+    """y = A x, r = b - A x (+ ||r||^2) and one Jacobi sweep at level 11, on the plain
+    layout (HB2_ELL_COMPACT=0) and on the one the autotuner picks."""
+    if layout is not None:
+        monkeypatch.setenv("HB2_ELL_COMPACT", layout)
+    ref = case11.A
+    A = SparseMatrixELL.poisson_q1(11)
+    if layout == "0":
+        assert A.layout()[0] == 0
+    x, rhs = oracle.uniform(ref.cols, 7), oracle.uniform(ref.rows, 11)
+    y = dvec(np.zeros(ref.rows))
+    hb.Product.value(y, A, dvec(x))
+    assert same_bits(host(y), oracle.ell_spmv(ref, x))
+    r = dvec(np.zeros(ref.rows))
+    nrm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    hb.Defect.value(r, dvec(rhs), A, dvec(x), norm2_out=nrm)
+    rr = oracle.ell_defect(ref, rhs, x)
+    assert same_bits(host(r), rr)
+    expect = float(np.dot(rr, rr))
+    assert abs(nrm.item() - expect) <= 1e-12 * expect
+    P = hb.RISmoother.jacobi_precon(A, 0.7)
+    x0 = x * 0.1
+    xv = dvec(x0)
+    hb.RISmoother.value(A, P, dvec(rhs), xv, max_iters=2)
+    assert same_bits(host(xv), oracle.jacobi_q1(11, rhs, x0, 2))

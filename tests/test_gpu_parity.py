@@ -121,13 +121,14 @@ def test_product_dot_and_add(oracle):
     x = oracle.uniform(ref.cols, 3)
     y = dvec(np.zeros(ref.rows))
     dot = torch.zeros(1, dtype=torch.float64, device=DEV)
-    _lib.call("hb2_product_dot_ell", A.handle, dvec(x).ptr, y.ptr, dot.data_ptr(), None)
+    xd = dvec(x)
+    _lib.call("hb2_product_dot_ell", A.handle, xd.ptr, y.ptr, dot.data_ptr(), None)
     yr = oracle.ell_spmv(ref, x)
     assert same_bits(host(y), yr)
     assert abs(dot.item() - float(yr @ x)) <= 1e-12 * abs(float(yr @ x))
     z0 = oracle.uniform(ref.rows, 4)
     z = dvec(z0)
-    _lib.call("hb2_product_add_ell", A.handle, dvec(x).ptr, z.ptr, None)
+    _lib.call("hb2_product_add_ell", A.handle, xd.ptr, z.ptr, None)
     assert same_bits(host(z), z0 + yr)
 
 
@@ -448,12 +449,12 @@ def test_ir_mixed_fp64_coarse(oracle):
 
 
 @pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4", "patternwin1",
-                                    "patternwin2"])
+                                    "patternwin2", "q1stencil2", "q1stencil4", "q1stencil8"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     """Value-dictionary + 16-bit offset layout (forceR) and row-pattern layout (patternR,
-    square matrices, patternwinR with x staged in shared-memory windows; the rectangular
-    transfers stay compressed): same bits as the plain
+    square matrices, patternwinR with x staged in shared-memory windows, q1stencilR the
+    Q1 stencil kernel; the rectangular transfers stay compressed): same bits as the plain
     layout (and the oracle) for every ELL kernel mode, square and rectangular."""
     from honei_b200 import _lib
     npdt = np.float64 if dt == torch.float64 else np.float32
@@ -462,13 +463,13 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     monkeypatch.setenv("HB2_Q1_TRANSFER", "0")      # the transfers on their stored layout too
     A = SparseMatrixELL.poisson_q1(L, dt)
     P, R = SparseMatrixELL.transfer(L, dt)
-    if layout.startswith("pattern"):
+    if layout.startswith("pattern") or layout.startswith("q1stencil"):
         # two row patterns: interior stencil, Dirichlet identity row; 1 matrix byte per row
         assert A.layout() == (2, 2, 1)
-        want = (2, int(layout[-1]), layout.startswith("patternwin"))
+        want = (2, int(layout[-1]), 1 if layout.startswith("patternwin") else 2 if layout.startswith("q1") else 0)
     else:
         assert A.layout() == (1, 3, 27)
-        want = (1, int(layout[-1]), False)
+        want = (1, int(layout[-1]), 0)
     assert A.layout_variant(0) == want and A.layout_variant(1) == want
     assert P.layout()[0] == 1 and R.layout()[0] == 1
     monkeypatch.setenv("HB2_ELL_COMPACT", "0")
@@ -485,9 +486,10 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
         hb.Product.value(y, M, dvec(x))
         nrm = torch.zeros(1, dtype=torch.float64, device=DEV)
         hb.Defect.value(r, dvec(b), M, dvec(x), norm2_out=nrm)
-        _lib.call("hb2_jacobi_sweep_ell", M.handle, Pj.ptr, dvec(b).ptr, dvec(x).ptr, s.ptr, None)
+        bv, xv, cv = dvec(b), dvec(x), dvec(c)   # held until the launches have read them
+        _lib.call("hb2_jacobi_sweep_ell", M.handle, Pj.ptr, bv.ptr, xv.ptr, s.ptr, None)
         f, cc = dvec(x.copy()), dvec(np.zeros(nc, npdt))
-        _lib.call("hb2_product_add_ell", Pm.handle, dvec(c).ptr, f.ptr, None)
+        _lib.call("hb2_product_add_ell", Pm.handle, cv.ptr, f.ptr, None)
         hb.Restriction.value(cc, dvec(x), resmat=Rm, method=hb.methods.PROLMAT)
         outs.append([host(v) for v in (y, r, s, f, cc)] + [nrm.item()])
     for a, b_ in zip(outs[0][:5], outs[1][:5]):
@@ -513,7 +515,8 @@ def test_q1_transfer_kernels_match_matrix_products(oracle, monkeypatch, L, dt):
         yp, yr, ya = dvec(np.zeros(Pr.rows, npdt)), dvec(np.zeros(Rr.rows, npdt)), dvec(y0.copy())
         hb.Product.value(yp, P, dvec(c))
         hb.Product.value(yr, R, dvec(f))
-        _lib.call("hb2_product_add_ell", P.handle, dvec(c).ptr, ya.ptr, None)
+        cv = dvec(c)
+        _lib.call("hb2_product_add_ell", P.handle, cv.ptr, ya.ptr, None)
         outs.append([host(yp), host(yr), host(ya)])
     for a, b in zip(outs[0], outs[1]):
         assert same_bits(a, b)

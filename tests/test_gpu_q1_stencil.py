@@ -1,0 +1,138 @@
+"""The Q1 stencil kernel (honei_b200/csrc/ell_q1.cu) for row-pattern ELL matrices
+holding the full nine-point stencil, pinned with HB2_ELL_COMPACT=q1stencilR
+(R = 2, 4, 8 rows per thread).  Bit for bit against the oracle's ELL product
+(la/product.hh:148-206) in every mode it runs (y = A x, r = b - A x with the fused
+||r||^2, y = A x with <y, x>, the Jacobi sweep of math/ri.hh:97-133), at the
+levels where the layout applies (8..11), in both precisions; for the anisotropic
+operator (other stencil values), for a matrix with a second full-stencil pattern
+(its rows take the general slot loop), for an x that is not 16-byte aligned (the
+general kernel) and inside the MG solve (passes in alternating directions)."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import honei_b200 as hb
+from honei_b200 import DenseVector, SparseMatrixELL, _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def dvec(a):
+    return DenseVector(torch.from_numpy(np.ascontiguousarray(a)).cuda())
+
+
+def host(v):
+    torch.cuda.synchronize()
+    return v.numpy()
+
+
+def same_bits(a, b):
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    return a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def check_modes(oracle, A, ref, npdt, seed=3):
+    n = ref.rows
+    x, b = oracle.uniform(n, seed, npdt), oracle.uniform(n, seed + 1, npdt)
+    y = dvec(np.zeros(n, npdt))
+    hb.Product.value(y, A, dvec(x))
+    yr = oracle.ell_spmv(ref, x)
+    assert same_bits(host(y), yr)
+    r = dvec(np.zeros(n, npdt))
+    nrm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    hb.Defect.value(r, dvec(b), A, dvec(x), norm2_out=nrm)
+    rr = oracle.ell_defect(ref, b, x)
+    assert same_bits(host(r), rr)
+    e = float(np.dot(rr.astype(np.float64), rr.astype(np.float64)))
+    assert abs(nrm.item() - e) <= 1e-12 * e
+    dot = torch.zeros(1, dtype=torch.float64, device="cuda")
+    y2 = dvec(np.zeros(n, npdt))
+    xd = dvec(x)
+    _lib.call("hb2_product_dot_ell", A.handle, xd.ptr, y2.ptr, ctypes.c_void_p(dot.data_ptr()), None)
+    assert same_bits(host(y2), yr)
+    d = float(np.dot(yr.astype(np.float64), x.astype(np.float64)))
+    assert abs(dot.item() - d) <= 1e-12 * np.dot(np.abs(yr.astype(np.float64)), np.abs(x.astype(np.float64)))
+    # Jacobi sweep x' = x + P (b - A x) against the plain layout's bits
+    P = hb.RISmoother.jacobi_precon(A, 0.7)
+    s = dvec(np.zeros(n, npdt))
+    bv, xv = dvec(b), dvec(x)    # held: a temporary's memory could be reused before the launch reads it
+    _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, bv.ptr, xv.ptr, s.ptr, None)
+    Ph = host(P)
+    # each operation rounded as the kernels do: b - Ax, then P * (b - Ax), then x + it
+    d_ = (b - yr).astype(npdt)
+    expect = (x + (Ph * d_).astype(npdt)).astype(npdt)
+    assert same_bits(host(s), expect)
+
+
+@pytest.mark.parametrize("R", [2, 4, 8])
+@pytest.mark.parametrize("L", [8, 9, 10, 11])
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_q1_stencil_modes_bit_exact(oracle, monkeypatch, dt, L, R):
+    if L == 11 and dt == torch.float32 and R != 4:
+        pytest.skip("level 11 FP32: one shape is enough")
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    monkeypatch.setenv("HB2_ELL_COMPACT", f"q1stencil{R}")
+    A = SparseMatrixELL.poisson_q1(L, dt)
+    assert A.layout_variant(0) == (2, R, 2) and A.layout_variant(1) == (2, R, 2)
+    check_modes(oracle, A, oracle.q1_ell(L, npdt), npdt)
+
+
+@pytest.mark.parametrize("aniso", [10.0, 100.0])
+def test_q1_stencil_anisotropic(oracle, monkeypatch, aniso):
+    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+    A = SparseMatrixELL.poisson_q1(9, aniso=aniso)
+    assert A.layout_variant(0)[2] == 2
+    check_modes(oracle, A, oracle.q1_ell(9, aniso=aniso), np.float64)
+
+
+def test_q1_stencil_second_full_pattern(oracle, monkeypatch):
+    """Interior rows of one grid band carry other stencil values: a second
+    full-stencil pattern, whose rows take the general slot loop."""
+    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil2")
+    ref = oracle.q1_ell(9)
+    Ax = ref.Ax.copy().reshape(ref.K, ref.stride)
+    m = (1 << 9) + 1
+    rows = np.arange(100 * m, 140 * m)
+    full = (ref.Arl[rows] == 9)
+    Ax[:, rows[full]] *= 2.0
+    Ax = Ax.reshape(-1)
+    A = SparseMatrixELL.from_arrays(ref.rows, ref.cols, ref.stride, ref.K, ref.Aj, Ax, ref.Arl)
+    assert A.layout()[:2] == (2, 3) and A.layout_variant(0)[2] == 2
+    ref2 = oracle.Ell(ref.rows, ref.cols, ref.stride, ref.K, 1, ref.Aj, Ax, ref.Arl)
+    check_modes(oracle, A, ref2, np.float64)
+
+
+def test_q1_stencil_unaligned_x(oracle, monkeypatch):
+    """x not 16-byte aligned: the general row-pattern kernel runs instead, same bits."""
+    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+    L = 9
+    A = SparseMatrixELL.poisson_q1(L)
+    n = A.rows()
+    x = oracle.uniform(n, 7)
+    buf = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(x).cuda()
+    xv = DenseVector(buf[1:])
+    assert xv.elements.data_ptr() % 16 != 0
+    y = dvec(np.zeros(n))
+    hb.Product.value(y, A, xv)
+    assert same_bits(host(y), oracle.ell_spmv(oracle.q1_ell(L), x))
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_q1_stencil_in_the_mg_solve(oracle, monkeypatch, dt):
+    """MG V(4,4) with every eligible level on the Q1 stencil kernel: the oracle's
+    iterates bit for bit (reference-order coarse CG), cycle count equal."""
+    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    L = 10
+    A = oracle.q1_ell(L, npdt)
+    b = oracle.ell_spmv(A, oracle.uniform(A.rows, 42, npdt))
+    eps = 1e-10 if dt == torch.float64 else 1e-5
+    data = hb.MGData.poisson_q1(3, L, dtype=dt, params=hb.mg_params(max_iters_coarse=100, eps=eps, coarse_exact=True))
+    x = dvec(np.zeros(A.rows, npdt))
+    hb.MGSolver.value(data, dvec(b), x)
+    xo, it, _ = oracle.mg_q1(L, b, max_iters_coarse=100, eps=eps)
+    assert data.used_iters == it
+    assert same_bits(host(x), xo)

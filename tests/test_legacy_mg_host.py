@@ -12,7 +12,7 @@ import pytest
 from honei_b200 import _lib
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_DATA = "/root/reference/honei/math/testdata/"
+REF_DATA = os.path.join(os.environ.get("HONEI_REFERENCE", "/nonexistent"), "honei/math/testdata/")
 MIXED = [2, 1, 2, 1, 2, 2, 1, 2]
 CASES = {
     "A": dict(L=5, dtype=np.float64, kw=dict(n_max_iter=16), x0=None),
