@@ -510,9 +510,11 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cyc
     fp64 = hb.MGData.poisson_q1(MIN_LEVEL, level, aniso=aniso,
                                 params=hb.mg_params(max_iters=max_cycles, max_iters_coarse=COARSE_CAP, eps=1e-10,
                                                     coarse_exact=False))
+    # the inner MG's coarse CG stops at the inner eps, as the reference's one
+    # eps_relative does for both (math/mg.hh:585-594)
     inner = hb.MGData.poisson_q1(MIN_LEVEL, level, dtype=torch.float32, aniso=aniso,
                                  params=hb.mg_params(max_iters=max_cycles, max_iters_coarse=COARSE_CAP, eps=1e-3,
-                                                     coarse_eps=1e-10, coarse_exact=False, coarse_fp64=True))
+                                                     coarse_eps=1e-3, coarse_exact=False, coarse_fp64=True))
     x64 = hb.DenseVector(n)
     xir = hb.DenseVector(n)
 
@@ -739,11 +741,13 @@ def load_peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def variant_name(kind, rows_per_thread, windowed):
+def variant_name(kind, rows_per_thread, kernel):
     """Name of an ELL kernel variant as HB2_ELL_COMPACT spells it (plain, forceR,
-    patternR, patternwinR)."""
+    patternR, patternwinR, q1stencilR, q1gatherR, q1pair)."""
     if kind == 2:
-        return ("patternwin%d" if windowed else "pattern%d") % rows_per_thread
+        if int(kernel) == 4:
+            return "q1pair"
+        return ({1: "patternwin%d", 2: "q1stencil%d", 3: "q1gather%d"}.get(int(kernel), "pattern%d")) % rows_per_thread
     if kind == 1:
         return "force%d" % rows_per_thread
     return "plain"

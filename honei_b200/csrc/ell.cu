@@ -678,7 +678,10 @@ extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * ro
     const int l = A->layout[cls];
     if (layout) *layout = l;
     if (rows_per_thread) *rows_per_thread = (int)(ell_rows_per_block(A, cls == 1) / kEllThreads);
-    if (windowed) *windowed = l != kLayoutPattern ? 0 : (A->rpt[cls] & kPatWin) ? 1 : (A->rpt[cls] & kPatQ1) ? 2 : 0;
+    if (windowed)
+        *windowed = l != kLayoutPattern ? 0 : (A->rpt[cls] & kPatWin) ? 1 : (A->rpt[cls] & kPatQ1) ? 2
+                                                                      : (A->rpt[cls] & kPatQ1G) ? 3
+                                                                      : (A->rpt[cls] & kPatQ1P) ? 4 : 0;
     return HB2_OK;
 }
 

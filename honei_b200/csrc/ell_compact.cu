@@ -529,8 +529,10 @@ namespace hb2
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         if (A->pat && A->pat_win_m)
             for (int r : {1, 2}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatWin));
+        // the Q1 stencil kernel's gather form (its bulk-copy and pair forms measured
+        // slower on every level and precision: they stay available as pins)
         if (A->pat && A->q1_full >= 0)
-            for (int r : {2, 4, 8}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatQ1));
+            for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatQ1G));
         // Each candidate is timed as a burst of back-to-back launches (the way the
         // solvers issue them, and long enough for the event clock's granularity),
         // the candidates interleaved over several rounds so that clock or
@@ -600,14 +602,16 @@ namespace hb2
         st = ell_build_pattern(A, stream);
         if (st) return st;
         const char * v = getenv("HB2_ELL_COMPACT");
-        if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0 || strncmp(v, "q1stencil", 9) == 0))
+        if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0 || strncmp(v, "q1stencil", 9) == 0 ||
+                  strncmp(v, "q1gather", 8) == 0 || strncmp(v, "q1pair", 6) == 0))
         {
             // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
             // rows per thread; pattern[1|2|4]: the row-pattern layout (square
             // matrices that admit it; the others compressed, 2 rows per thread);
             // patternwin[1|2] its windowed kernel where the offsets allow;
             // q1stencil[2|4|8] the Q1 stencil kernel where the matrix holds the full
-            // nine-point stencil; no autotuning
+            // nine-point stencil, q1gather[1|2|4] its gather form, q1pair its pair
+            // form; no autotuning
             Choice c;
             if (v[0] == 'p' && A->pat)
             {
@@ -626,6 +630,20 @@ namespace hb2
                 c.layout[0] = c.layout[1] = kLayoutPattern;
                 c.rpt[0] = c.rpt[1] = (r == 4 || r == 8) ? r : 2;
                 if (A->q1_full >= 0) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatQ1;
+            }
+            else if (strncmp(v, "q1pair", 6) == 0 && A->pat)
+            {
+                // q1pair: the Q1 stencil kernel's pair form (two adjacent rows per thread)
+                c.layout[0] = c.layout[1] = kLayoutPattern;
+                c.rpt[0] = c.rpt[1] = 2 | (A->q1_full >= 0 ? kPatQ1P : 0);
+            }
+            else if (strncmp(v, "q1gather", 8) == 0 && A->pat)
+            {
+                // q1gather[1|2|4]: the Q1 stencil kernel's gather form
+                const int r = atoi(v + 8);
+                c.layout[0] = c.layout[1] = kLayoutPattern;
+                c.rpt[0] = c.rpt[1] = (r == 2 || r == 4) ? r : 1;
+                if (A->q1_full >= 0) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatQ1G;
             }
             else
             {

@@ -205,6 +205,301 @@ namespace hb2
         if (! fast) mbar_wait_bounded(&bar, 0, 1000000000ull);
     }
 
+    // ------------------------------------------------------------------
+    // Gather form: no shared memory, no block barrier, no bulk copies.  Each thread
+    // owns R rows interleaved over the block (coalesced) and issues every load of
+    // all of them before the first use: the pattern ids, rhs and Jacobi vector,
+    // and the nine x values of each row as three runs of three (x[i-m-1..i-m+1],
+    // x[i-1..i+1], x[i+m-1..i+m+1]: one base pointer per run, immediate offsets),
+    // which the L1 serves after the first lane of a warp brought the line in.
+    // Measured on B200: small bulk copies complete one after another within a CTA
+    // (about 0.57 us per copy of 4 or 8 KiB, whatever the number issued ahead), so
+    // a block that stages three x windows pays three serialised latencies; plain
+    // loads of all rows of all resident blocks are in flight together.
+    template <typename T, int MODE>
+    __device__ __forceinline__ void q1_epilogue(T * __restrict__ y, int64_t i, T acc, T xc, T ea, T ep, double & part,
+                                                float * __restrict__ y32 = nullptr, float * __restrict__ z32 = nullptr)
+    {
+        typedef Arith<T> M;
+        if (MODE == kDefectIR)
+        {
+            // the outer defect in FP64, handed to the FP32 inner solve as its
+            // right-hand side (round to nearest, as convert<> does), the inner
+            // guess cleared
+            const T d = M::sub(ea, acc);
+            y32[i] = (float)d;
+            if (z32) z32[i] = 0.f;
+            part = fma((double)d, (double)d, part);
+        }
+        else if (MODE == kPlain) y[i] = acc;
+        else if (MODE == kDefect)
+        {
+            const T d = M::sub(ea, acc);
+            y[i] = d;
+            part = fma((double)d, (double)d, part);
+        }
+        else if (MODE == kDot)
+        {
+            y[i] = acc;
+            part = fma((double)acc, (double)xc, part);
+        }
+        else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep, M::sub(ea, acc)));
+    }
+
+    template <typename T, int MODE, int R>
+    __global__ void __launch_bounds__(kEllThreads, R == 1 ? 8 : 1)
+    q1_gather_kernel(const __grid_constant__ Q1Stencil<T> s, const T * __restrict__ x, T * __restrict__ y,
+                     const T * __restrict__ aux, const T * __restrict__ aux2, ReduceSlot rs, double * red,
+                     int want_sqrt, int flags, float * __restrict__ y32, float * __restrict__ z32)
+    {
+        typedef Arith<T> M;
+        const int64_t n = s.n, m = s.m;
+        const int t = (int)threadIdx.x;
+        const int64_t blk = (flags & kReverse) ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
+        const int64_t i0 = blk * (kEllThreads * R) + t;
+        uint32_t p[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            p[k] = i < n ? (uint32_t)((flags & kKeepL2) ? __ldcg(s.pat + i) : __ldcs(s.pat + i)) : s.full;
+        }
+        pdl_entry();   // x, rhs and P may come from the previous kernel
+        T xv[R][9], ea[R], ep[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            // every neighbour of a row inside [m + 1, n - m - 1) exists; the full
+            // stencil's rows all lie there, the others read through the table below
+            if (i >= m + 1 && i + m + 1 < n)
+            {
+                const T * a = x + (i - m - 1), * b = x + (i - 1), * c = x + (i + m - 1);
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                {
+                    xv[k][q] = a[q];
+                    xv[k][3 + q] = b[q];
+                    xv[k][6 + q] = c[q];
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) xv[k][q] = T(0);
+            }
+            const bool ok = i < n;
+            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR)) ? aux[i] : T(0);
+            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+        }
+        double part = 0.0;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int64_t i = i0 + k * kEllThreads;
+            if (i >= n) break;
+            T acc, xc;
+            if (p[k] == s.full && i >= m + 1 && i + m + 1 < n)
+            {
+                acc = M::add(T(0), M::mul(s.v[0], xv[k][0]));
+#pragma unroll
+                for (int q = 1; q < 9; ++q) acc = M::add(acc, M::mul(s.v[q], xv[k][q]));
+                xc = xv[k][4];
+            }
+            else
+            {
+                acc = q1_any_row<T, 1>(s.tab + p[k] * 9u, x, i, nullptr, 0, 0, 0, false);
+                xc = (MODE == kJacobi || MODE == kDot) ? x[i] : T(0);
+            }
+            q1_epilogue<T, MODE>(y, i, acc, xc, ea[k], ep[k], part, y32, z32);
+        }
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        {
+            // one partial per block; q1_sum_partials_kernel adds them in block order
+            // after this launch (no fence or ticket on the block's way out)
+            __shared__ double scratch[32];
+            const double sum = block_sum(part, scratch);
+            if (t == 0) rs.partials[blockIdx.x] = sum;
+        }
+    }
+
+    // the fused reduction's second step: partials[0 .. G) summed in a fixed order
+    // (thread t adds t, t + 1024, t + 2048, ... in that order, eight independent
+    // loads in flight at a time; then the block tree), so the result depends on
+    // the data and the launch shape only
+    constexpr int kSumThreads = 1024;
+    __global__ void __launch_bounds__(kSumThreads) q1_sum_partials_kernel(const double * __restrict__ partials,
+                                                                          unsigned G, double * out, int want_sqrt)
+    {
+        __shared__ double scratch[32];
+        pdl_entry();
+        double s = 0.0;
+        for (unsigned b0 = threadIdx.x; b0 < G; b0 += 8 * kSumThreads)
+        {
+            double v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const unsigned b = b0 + q * kSumThreads;
+                v[q] = b < G ? partials[b] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) s += v[q];
+        }
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) out[0] = want_sqrt ? sqrt(s) : s;
+    }
+
+    // ------------------------------------------------------------------
+    // Pair form: each thread owns two adjacent rows i0 = 2g, i0 + 1 (a warp 64
+    // consecutive rows).  The two rows share their x values: per grid row of the
+    // stencil four consecutive elements, fetched as two aligned pairs (16 bytes in
+    // FP64, 8 in FP32: i0 - m - 1 and i0 + m - 1 are even because m is odd) or, for
+    // the centre row, an element, a pair and an element; rhs, P, the pattern ids and
+    // the output move as pairs too.  About ten loads per two rows instead of
+    // twenty-two, and one index computation: the kernel issues a third of the
+    // instructions of the one-row form.  Needs x, rhs, P and y aligned to the pair
+    // size (else the interleaved form with two rows per thread runs instead).
+    template <typename T> struct Pair;
+    template <> struct Pair<double> { typedef double2 type; };
+    template <> struct Pair<float> { typedef float2 type; };
+
+    template <typename T, int MODE>
+    __device__ __forceinline__ T q1_pair_out(T acc, T xc, T ea, T ep, double & part)
+    {
+        typedef Arith<T> M;
+        if (MODE == kPlain) return acc;
+        if (MODE == kDefect || MODE == kDefectIR)
+        {
+            const T d = M::sub(ea, acc);
+            part = fma((double)d, (double)d, part);
+            return d;
+        }
+        if (MODE == kDot)
+        {
+            part = fma((double)acc, (double)xc, part);
+            return acc;
+        }
+        return M::add(xc, M::mul(ep, M::sub(ea, acc)));   // kJacobi
+    }
+
+    template <typename T>
+    __device__ __forceinline__ T q1_row9(const Q1Stencil<T> & s, const T * a, const T * c, const T * d)
+    {
+        typedef Arith<T> M;
+        T acc = M::add(T(0), M::mul(s.v[0], a[0]));
+        acc = M::add(acc, M::mul(s.v[1], a[1]));
+        acc = M::add(acc, M::mul(s.v[2], a[2]));
+        acc = M::add(acc, M::mul(s.v[3], c[0]));
+        acc = M::add(acc, M::mul(s.v[4], c[1]));
+        acc = M::add(acc, M::mul(s.v[5], c[2]));
+        acc = M::add(acc, M::mul(s.v[6], d[0]));
+        acc = M::add(acc, M::mul(s.v[7], d[1]));
+        return M::add(acc, M::mul(s.v[8], d[2]));
+    }
+
+    template <typename T, int MODE>
+    __global__ void __launch_bounds__(kEllThreads)
+    q1_pair_kernel(const __grid_constant__ Q1Stencil<T> s, const T * __restrict__ x, T * __restrict__ y,
+                   const T * __restrict__ aux, const T * __restrict__ aux2, ReduceSlot rs, double * red, int flags,
+                   float * __restrict__ y32, float * __restrict__ z32)
+    {
+        typedef typename Pair<T>::type V;
+        const int n = (int)s.n, m = (int)s.m;
+        const int t = (int)threadIdx.x;
+        const int blk = (flags & kReverse) ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+        const int i0 = 2 * (blk * kEllThreads + t);
+        const bool any = i0 < n, two = i0 + 1 < n;
+        uint32_t p0 = s.full, p1 = s.full;
+        if (two)
+        {
+            const uint32_t pp = (uint32_t)((flags & kKeepL2) ? __ldcg((const unsigned short *)(s.pat + i0))
+                                                            : __ldcs((const unsigned short *)(s.pat + i0)));
+            p0 = pp & 0xffu;
+            p1 = pp >> 8;
+        }
+        else if (any) p0 = s.pat[i0];
+        pdl_entry();   // x, rhs and P may come from the previous kernel
+        // both rows' neighbours exist: x[i0 - m - 1 .. i0 + m + 2]
+        const bool inner = two && i0 >= m + 1 && i0 + m + 2 < n;
+        T a[4], c[4], d[4];
+        if (inner)
+        {
+            const V a01 = *(const V *)(x + (i0 - m - 1)), a23 = *(const V *)(x + (i0 - m + 1));
+            const V c12 = *(const V *)(x + i0);
+            const V d01 = *(const V *)(x + (i0 + m - 1)), d23 = *(const V *)(x + (i0 + m + 1));
+            c[0] = x[i0 - 1];
+            c[3] = x[i0 + 2];
+            a[0] = a01.x; a[1] = a01.y; a[2] = a23.x; a[3] = a23.y;
+            c[1] = c12.x; c[2] = c12.y;
+            d[0] = d01.x; d[1] = d01.y; d[2] = d23.x; d[3] = d23.y;
+        }
+        T ea0 = T(0), ea1 = T(0), ep0 = T(0), ep1 = T(0);
+        if (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR)
+        {
+            if (two) { const V v = *(const V *)(aux + i0); ea0 = v.x; ea1 = v.y; }
+            else if (any) ea0 = aux[i0];
+        }
+        if (MODE == kJacobi)
+        {
+            if (two) { const V v = *(const V *)(aux2 + i0); ep0 = v.x; ep1 = v.y; }
+            else if (any) ep0 = aux2[i0];
+        }
+        double part = 0.0;
+        T o0 = T(0), o1 = T(0);
+        if (any)
+        {
+            T acc, xc;
+            if (inner && p0 == s.full) { acc = q1_row9(s, a, c, d); xc = c[1]; }
+            else
+            {
+                acc = q1_any_row<T, 1>(s.tab + p0 * 9u, x, i0, nullptr, 0, 0, 0, false);
+                xc = (MODE == kJacobi || MODE == kDot) ? x[i0] : T(0);
+            }
+            o0 = q1_pair_out<T, MODE>(acc, xc, ea0, ep0, part);
+        }
+        if (two)
+        {
+            T acc, xc;
+            if (inner && p1 == s.full) { acc = q1_row9(s, a + 1, c + 1, d + 1); xc = c[2]; }
+            else
+            {
+                acc = q1_any_row<T, 1>(s.tab + p1 * 9u, x, i0 + 1, nullptr, 0, 0, 0, false);
+                xc = (MODE == kJacobi || MODE == kDot) ? x[i0 + 1] : T(0);
+            }
+            o1 = q1_pair_out<T, MODE>(acc, xc, ea1, ep1, part);
+        }
+        if (MODE == kDefectIR)
+        {
+            // the FP64 defect handed to the FP32 inner solve (round to nearest, as
+            // convert<> does), the inner guess cleared
+            if (two)
+            {
+                *(float2 *)(y32 + i0) = make_float2((float)o0, (float)o1);
+                if (z32) *(float2 *)(z32 + i0) = make_float2(0.f, 0.f);
+            }
+            else if (any)
+            {
+                y32[i0] = (float)o0;
+                if (z32) z32[i0] = 0.f;
+            }
+        }
+        else if (two)
+        {
+            V v;
+            v.x = o0;
+            v.y = o1;
+            *(V *)(y + i0) = v;
+        }
+        else if (any) y[i0] = o0;
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        {
+            __shared__ double scratch[32];
+            const double sum = block_sum(part, scratch);
+            if (t == 0) rs.partials[blockIdx.x] = sum;
+        }
+    }
+
     template <typename T, int R>
     static constexpr size_t q1_stencil_smem()
     {
@@ -247,21 +542,63 @@ namespace hb2
         s.n = (int64_t)A->rows;
         s.m = A->pat_win_m;
         s.full = (uint32_t)A->q1_full;
+        if (R & kPatQ1P)
+        {
+            // two adjacent rows per thread; the interleaved form where the vectors are
+            // not aligned to pairs (same rows per block)
+            // (the pairs of the x rows at -m and +m are aligned because m is odd)
+            const uintptr_t al = 2 * sizeof(T) - 1;
+            if ((((uintptr_t)x | (uintptr_t)y | (uintptr_t)aux | (uintptr_t)aux2) & al) == 0 && (A->pat_win_m & 1) &&
+                A->rows < (1ull << 31) - 4096)
+            {
+                launch_pdl(q1_pair_kernel<T, MODE>, grid, dim3(kEllThreads), 0, st, s, (const T *)x, (T *)y,
+                           (const T *)aux, (const T *)aux2, rs, red, flags, (float *)nullptr, (float *)nullptr);
+                if ((MODE == kDefect || MODE == kDot) && red)
+                {
+                    launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials,
+                               grid.x, red, want_sqrt);
+                    count_launches(1);
+                }
+                return;
+            }
+            R = kPatQ1G | 2;
+        }
+        if (R & kPatQ1G)
+        {
+            R &= ~kPatQ1G;
+#define HB2_Q1G(R_) launch_pdl(q1_gather_kernel<T, MODE, R_>, grid, dim3(kEllThreads), 0, st, s, (const T *)x, (T *)y, \
+                               (const T *)aux, (const T *)aux2, rs, red, want_sqrt, flags, (float *)nullptr,      \
+                               (float *)nullptr)
+            if (R == 1) HB2_Q1G(1);
+            else if (R == 2) HB2_Q1G(2);
+            else HB2_Q1G(4);
+#undef HB2_Q1G
+            if ((MODE == kDefect || MODE == kDot) && red)
+            {
+                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials, grid.x,
+                           red, want_sqrt);
+                count_launches(1);
+            }
+            return;
+        }
         if (R == 2) q1_stencil_launch<T, MODE, 2>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
         else if (R == 4) q1_stencil_launch<T, MODE, 4>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
         else q1_stencil_launch<T, MODE, 8>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
     }
 
-    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, const Batch & b)
+    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, int rpt, const Batch & b)
     {
+        // the windows' bulk copies need a 16-byte aligned x (the gather form needs nothing)
+        const bool aligned = (rpt & (kPatQ1G | kPatQ1P)) || ((uintptr_t)x & 15) == 0;
         return A->q1_full >= 0 && A->pat_win_m && A->K == 9 && ! b.list && b.nvec == 1 && ! b.active &&
-               (mode == kPlain || mode == kDefect || mode == kDot || mode == kJacobi) && ((uintptr_t)x & 15) == 0;
+               (mode == kPlain || mode == kDefect || mode == kDot || mode == kJacobi) && aligned;
     }
 
     void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                                const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
                                cudaStream_t stream, int flags, int R)
     {
+        // R: rows per thread, with kPatQ1G for the gather form, kPatQ1P for the pair form
 #define HB2_Q1S(T_, M_) q1_stencil_mode<T_, M_>(A, R, grid, stream, x, y, aux, aux2, rs, red, want_sqrt, flags)
         if (A->dtype == HB2_F64)
         {
@@ -278,6 +615,48 @@ namespace hb2
             else HB2_Q1S(float, kJacobi);
         }
 #undef HB2_Q1S
+    }
+
+    int launch_ir_defect(const hb2_ell_s * A, const double * x, const double * b, float * b32, float * x32,
+                         double * r64, double * red, const Workspace * ws, cudaStream_t stream)
+    {
+        const uint64_t n = A->rows;
+        const unsigned grid = ceil_div(n, kEllThreads);
+        if (A->dtype == HB2_F64 && A->q1_full >= 0 && A->pat && A->pat_win_m && A->K == 9 && n > 0 &&
+            grid <= ws->max_blocks)
+        {
+            Q1Stencil<double> s;
+            for (int k = 0; k < 9; ++k) s.v[k] = A->q1_val[k];
+            s.pat = A->pat;
+            s.tab = (const PatEnt<double> *)A->ptab;
+            s.n = (int64_t)n;
+            s.m = A->pat_win_m;
+            s.full = (uint32_t)A->q1_full;
+            const ReduceSlot rs = ws->slot();
+            const unsigned pgrid = ceil_div(n, 2 * kEllThreads);
+            if (((((uintptr_t)x | (uintptr_t)b) & 15) | (((uintptr_t)b32 | (uintptr_t)x32) & 7)) == 0 &&
+                (A->pat_win_m & 1) && n < (1ull << 31) - 4096)
+            {
+                launch_pdl(q1_pair_kernel<double, kDefectIR>, dim3(pgrid), dim3(kEllThreads), 0, stream, s, x,
+                           (double *)nullptr, b, (const double *)nullptr, rs, red, 0, b32, x32);
+                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials,
+                           pgrid, red, 1);
+                count_launches(2);
+                HB2_LAUNCH_CHECK("IR defect launch");
+                return HB2_OK;
+            }
+            launch_pdl(q1_gather_kernel<double, kDefectIR, 1>, dim3(grid), dim3(kEllThreads), 0, stream, s, x,
+                       (double *)nullptr, b, (const double *)nullptr, rs, red, 1, 0, b32, x32);
+            launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials, grid,
+                       red, 1);
+            count_launches(2);
+            HB2_LAUNCH_CHECK("IR defect launch");
+            return HB2_OK;
+        }
+        int st = launch_ell(A, kDefect, x, r64, b, 0, 0, red, 1, ws, stream);
+        if (! st) st = launch_convert(HB2_F32, b32, HB2_F64, r64, n, stream);
+        if (! st && x32) st = launch_fill(HB2_F32, x32, 0.0, n, stream);
+        return st;
     }
 
     // After the row-pattern layout is built: the pattern, if any, that holds the

@@ -140,7 +140,8 @@ namespace hb2
         kDot = 2,       // y = A x, red = <y, x>
         kAdd = 3,       // y = y + A x
         kJacobi = 4,    // y = x + P (.) (aux - A x) (ping-pong sweep)
-        kRestrict = 5   // y = A x, zero[0..rows) = 0
+        kRestrict = 5,  // y = A x, zero[0..rows) = 0
+        kDefectIR = 6   // FP64 r = aux - A x: (float) r and its ||r|| (the IR outer defect, Q1 kernels only)
     };
 
     // Pass flags of the ELL family: kReverse walks the row blocks from the end
@@ -196,7 +197,9 @@ namespace hb2
     constexpr int32_t kPatEmpty = (-2147483647 - 1);
     constexpr int kPatWin = 0x10;    // rpt flag: the windowed row-pattern kernel
     constexpr int kPatQ1 = 0x20;     // rpt flag: the Q1 stencil kernel (ell_q1.cu)
-    constexpr int kPatFlags = kPatWin | kPatQ1;
+    constexpr int kPatQ1G = 0x40;    // rpt flag: the Q1 stencil kernel's gather form (ell_q1.cu)
+    constexpr int kPatQ1P = 0x80;    // rpt flag: the Q1 stencil kernel's pair form (ell_q1.cu)
+    constexpr int kPatFlags = kPatWin | kPatQ1 | kPatQ1G | kPatQ1P;
     constexpr int kSubPatMax = 8;    // patterns of a small-level operator in the fused kernels
     int ell_small_patterns(hb2_ell_s * A);
 
@@ -222,7 +225,7 @@ namespace hb2
 
     // Q1 stencil kernel for row-pattern matrices with the full nine-point stencil (ell_q1.cu)
     void ell_find_q1_stencil(hb2_ell_s * A);
-    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, const Batch & b);
+    bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, int rpt, const Batch & b);
     void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                                const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
                                cudaStream_t stream, int flags, int R);
@@ -253,6 +256,11 @@ namespace hb2
     int launch_convert(int dst_dt, void * dst, int src_dt, const void * src, uint64_t n, cudaStream_t stream);
     // x64 += (double) c  (IR update, math/ir.hh:73-75)
     int launch_add_converted(void * x64, int c_dt, const void * c, uint64_t n, cudaStream_t stream);
+    // IR outer defect of an F64 matrix: r = b - A x, b32 = (float) r, x32 = 0 (x32
+    // nullable), red = ||r|| -- one pass on the Q1 stencil kernel, else a defect
+    // into r64, a conversion and a fill
+    int launch_ir_defect(const hb2_ell_s * A, const double * x, const double * b, float * b32, float * x32,
+                         double * r64, double * red, const Workspace * ws, cudaStream_t stream);
 
     // small levels of a V-cycle as cluster kernels (subcycle.cu)
     struct SubLevelDesc

@@ -79,6 +79,16 @@ struct hb2_mg_s
     bool sub_fused;          // levels 0..sub_top, coarse CG included, in one launch
     hb2_ell_s * coarse64;    // FP64 copy of the coarsest operator (F32 hierarchies with coarse_fp64)
     double * ir_r;           // outer FP64 defect of hb2_ir_solve (allocated on first use, kept)
+    // hb2_ir_solve as one CUDA graph, built for the outer operator and vectors of
+    // the last call (rebuilt when any of them or the loop parameters change)
+    cudaStream_t cap3 = 0;
+    cudaGraph_t ir_graph = 0;
+    cudaGraphExec_t ir_exec = 0;
+    const void * ir_key_A = 0, * ir_key_b = 0, * ir_key_x = 0;
+    double ir_key_eps = 0;
+    uint64_t ir_key_max = 0;
+    int ir_key_reset = -1;
+    uint64_t ir_body_kernels = 0, ir_inner_body_kernels = 0;
 };
 
 namespace hb2
@@ -485,6 +495,176 @@ namespace hb2
     }
 }
 
+namespace hb2
+{
+    // IRSolver loop control (math/ir.hh:55-75) on the device.  Scalars (the
+    // inner hierarchy's workspace): [16] ||r0||, [17] ||r|| at the last check,
+    // [18] outer index i, [19] last checked i, [20] inner cycles in all.
+    __global__ void ir_loop_init_kernel(double * sc, uint64_t max_iters, cudaGraphConditionalHandle h)
+    {
+        sc[17] = 1e16;
+        uint64_t * u = (uint64_t *)sc;
+        u[18] = 0;
+        u[19] = 0;
+        u[20] = 0;
+        cudaGraphSetConditional(h, max_iters > 0 ? 1u : 0u);
+    }
+
+    // after an inner solve, the update and the next defect: i += 1; the defect of
+    // index i is checked only while i < max_iters (the reference's loop runs its
+    // i-th defect at the top of iteration i)
+    __global__ void ir_loop_decide_kernel(double * sc, const double * norm, const uint64_t * inner_iters,
+                                          uint64_t max_iters, double eps, cudaGraphConditionalHandle h)
+    {
+        pdl_entry();
+        uint64_t * u = (uint64_t *)sc;
+        const uint64_t i = u[18] + 1;
+        u[18] = i;
+        u[20] += *inner_iters;
+        bool stop = i >= max_iters;
+        if (! stop)
+        {
+            const double rc = *norm;
+            sc[17] = rc;
+            u[19] = i;
+            stop = rc < eps * sc[16] || ! (rc == rc);
+        }
+        cudaGraphSetConditional(h, stop ? 0u : 1u);
+    }
+
+    // a conditional handle in the graph `s` is capturing into
+    static cudaError_t new_handle(cudaStream_t s, cudaGraphConditionalHandle * h)
+    {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t capg = 0;
+        const cudaGraphNode_t * deps = 0;
+        size_t ndeps = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, 0, &capg, &deps, &ndeps);
+        if (e != cudaSuccess) return e;
+        return cudaGraphConditionalHandleCreate(h, capg, 0, cudaGraphCondAssignDefault);
+    }
+
+    // a conditional WHILE node on handle h at the capture position of `s`: returns
+    // its body graph and makes the node `s`'s dependency
+    static cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t * body)
+    {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t capg = 0;
+        const cudaGraphNode_t * deps = 0;
+        size_t ndeps = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, 0, &capg, &deps, &ndeps);
+        if (e != cudaSuccess) return e;
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        e = cudaGraphAddNode(&node, capg, deps, ndeps, &cp);
+        if (e != cudaSuccess) return e;
+        *body = cp.conditional.phGraph_out[0];
+        return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    }
+
+    static int ir_capture_error(cudaError_t e, const char * what, hb2_mg_s * mg, int st = HB2_OK)
+    {
+        cudaGraph_t g = 0;
+        cudaStreamEndCapture(mg->cap3, &g);
+        if (g) { cudaGraphDestroy(g); g = 0; }
+        cudaStreamEndCapture(mg->cap2, &g);
+        if (g) { cudaGraphDestroy(g); g = 0; }
+        cudaStreamEndCapture(mg->cap, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (st) return st;
+        return cuda_status(e == cudaSuccess ? cudaErrorUnknown : e, what);
+    }
+
+    // The whole IRSolver (math/ir.hh:31-80) as one graph:
+    //   outer defect (FP64; fused: its FP32 copy into the inner rhs, the inner guess
+    //   cleared when reset_inner, ||r0||)
+    //   WHILE (outer):
+    //     inner MGSolver: its initial defect, WHILE (inner): V-cycle, norm, decide
+    //     x += (double) inner x
+    //     outer defect (fused as above), decide
+    //   statistics to pinned host memory
+    static int build_ir_graph(hb2_mg_s * mg, const hb2_ell_s * A, const double * b, double * x, double eps,
+                              uint64_t max_iters, int reset_inner)
+    {
+        if (mg->ir_exec) { cudaGraphExecDestroy(mg->ir_exec); mg->ir_exec = 0; }
+        if (mg->ir_graph) { cudaGraphDestroy(mg->ir_graph); mg->ir_graph = 0; }
+        if (! mg->cap3) HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap3, cudaStreamNonBlocking));
+        if (! mg->ir_r) HB2_CUDA(cudaMalloc(&mg->ir_r, A->rows * 8 + 16));
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        double * sc = mg->ws->scalars;
+        float * b32 = (float *)F.b, * x32 = reset_inner ? (float *)F.x : nullptr;
+        const uint64_t before = hb2_launch_count();
+        HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
+        cudaGraphConditionalHandle ho, hi;
+        cudaGraph_t obody = 0, ibody = 0;
+        reset_directions(mg);
+        cudaError_t e = new_handle(mg->cap, &ho);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR outer handle", mg);
+        ir_loop_init_kernel<<<1, 1, 0, mg->cap>>>(sc, max_iters, ho);
+        count_launches(1);
+        int st = launch_ir_defect(A, x, b, b32, x32, mg->ir_r, sc + 16, mg->ws, mg->cap);
+        if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+        e = add_while(mg->cap, ho, &obody);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(mg->cap2, obody, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR outer loop", mg);
+        const uint64_t obody0 = hb2_launch_count();
+        // the inner MGSolver on (F.b, F.x)
+        st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->r0_dev, 1, mg->ws, mg->cap2, F.pass(F.rev_A));
+        if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+        e = new_handle(mg->cap2, &hi);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR inner handle", mg);
+        mg_loop_init_kernel<<<1, 1, 0, mg->cap2>>>(mg->iters_dev, mg->prm.max_iters, hi);
+        count_launches(1);
+        e = add_while(mg->cap2, hi, &ibody);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(mg->cap3, ibody, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR inner loop", mg);
+        const uint64_t ibody0 = hb2_launch_count();
+        st = record_cycle(mg, mg->nlev - 1, mg->cap3);
+        if (! st) st = finest_norm(mg, mg->cap3);
+        if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+        launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap3, mg->norm_dev, mg->r0_dev, mg->iters_dev,
+                   mg->prm.max_iters, mg->prm.eps_relative, hi);
+        count_launches(1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return ir_capture_error(e, "IR inner decide", mg);
+        mg->ir_inner_body_kernels = hb2_launch_count() - ibody0;
+        e = cudaStreamEndCapture(mg->cap3, &ibody);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR inner body", mg);
+        // x += (double) inner x; the next outer defect; the decision
+        st = launch_add_converted(x, mg->dtype, F.x, F.n, mg->cap2);
+        if (! st) st = launch_ir_defect(A, x, b, b32, x32, mg->ir_r, sc + 21, mg->ws, mg->cap2);
+        if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+        launch_pdl(ir_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap2, sc, (const double *)(sc + 21),
+                   (const uint64_t *)mg->iters_dev, max_iters, eps, ho);
+        count_launches(1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return ir_capture_error(e, "IR decide", mg);
+        mg->ir_body_kernels = hb2_launch_count() - obody0 - mg->ir_inner_body_kernels;
+        e = cudaStreamEndCapture(mg->cap2, &obody);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR outer body", mg);
+        e = cudaMemcpyAsync(mg->ws->host_scalars + 16, sc + 16, 5 * sizeof(double), cudaMemcpyDeviceToHost, mg->cap);
+        if (e != cudaSuccess) return ir_capture_error(e, "IR statistics copy", mg);
+        cudaGraph_t g = 0;
+        e = cudaStreamEndCapture(mg->cap, &g);
+        set_launch_count(before);
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture (IR)");
+        mg->ir_graph = g;
+        e = cudaGraphInstantiate(&mg->ir_exec, g, 0);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate (IR)");
+        mg->ir_key_A = A;
+        mg->ir_key_b = b;
+        mg->ir_key_x = x;
+        mg->ir_key_eps = eps;
+        mg->ir_key_max = max_iters;
+        mg->ir_key_reset = reset_inner;
+        return HB2_OK;
+    }
+}
+
 using namespace hb2;
 
 extern "C" int hb2_mg_create(hb2_mg * out, uint32_t num_levels, const hb2_ell * A, const hb2_ell * prol,
@@ -546,6 +726,9 @@ extern "C" int hb2_mg_destroy(hb2_mg mg)
     if (mg->solve_graph) cudaGraphDestroy(mg->solve_graph);
     if (mg->cap) cudaStreamDestroy(mg->cap);
     if (mg->cap2) cudaStreamDestroy(mg->cap2);
+    if (mg->ir_exec) cudaGraphExecDestroy(mg->ir_exec);
+    if (mg->ir_graph) cudaGraphDestroy(mg->ir_graph);
+    if (mg->cap3) cudaStreamDestroy(mg->cap3);
     if (mg->coarse64) hb2_ell_destroy(mg->coarse64);
     if (mg->ir_r) cudaFree(mg->ir_r);
     if (mg->vec_block) cudaFree(mg->vec_block);
@@ -593,6 +776,35 @@ extern "C" int hb2_ir_solve(hb2_ell A, hb2_mg inner, const void * b, void * x, d
     if (A->dtype != HB2_F64) return fail(HB2_ERR_ARG, "hb2_ir_solve: the outer system must be F64");
     MgLevel & F = inner->lev[inner->nlev - 1];
     if (F.n != A->rows || A->rows != A->cols) return fail(HB2_ERR_SIZE, "hb2_ir_solve: VectorSizeDoesNotMatch (inner finest level)");
+    const char * loop = getenv("HB2_IR_LOOP");
+    if (! (loop && strcmp(loop, "host") == 0) && ! host_loop_requested())
+    {
+        // the whole solve as one graph launch and one synchronisation
+        if (! inner->ir_exec || inner->ir_key_A != A || inner->ir_key_b != b || inner->ir_key_x != x ||
+            inner->ir_key_eps != eps || inner->ir_key_max != max_iters || inner->ir_key_reset != reset_inner)
+        {
+            int st = build_ir_graph(inner, A, (const double *)b, (double *)x, eps, max_iters, reset_inner);
+            if (st) return st;
+        }
+        HB2_CUDA(cudaGraphLaunch(inner->ir_exec, stream));
+        HB2_CUDA(cudaStreamSynchronize(stream));
+        const double * h = inner->ws->host_scalars + 16;
+        uint64_t outer = 0, used = 0, inner_total = 0;
+        memcpy(&outer, h + 2, sizeof(uint64_t));
+        memcpy(&used, h + 3, sizeof(uint64_t));
+        memcpy(&inner_total, h + 4, sizeof(uint64_t));
+        count_launches(3 + outer * inner->ir_body_kernels + inner_total * inner->ir_inner_body_kernels);
+        const double r0 = h[0], rc = used ? h[1] : 1e16;
+        if (stats)
+        {
+            stats[0] = (double)used;
+            stats[1] = r0;
+            stats[2] = rc;
+            stats[3] = (double)inner_total;
+        }
+        if (! (rc == rc) || ! (r0 == r0)) return fail(HB2_ERR_NOT_FINITE, "hb2_ir_solve: NaN defect norm");
+        return HB2_OK;
+    }
     Workspace * ws = 0;
     int st = stream_workspace(stream, &ws);
     if (st) return st;

@@ -31,6 +31,19 @@ namespace hb2
                      :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
     }
 
+    // init without the fences (several barriers initialised by one thread; the
+    // caller fences once with mbar_init_fence)
+    __device__ __forceinline__ void mbar_init_only(uint64_t * bar, unsigned count)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
+    }
+
+    __device__ __forceinline__ void mbar_init_fence()
+    {
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+
     __device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, unsigned parity)
     {
         uint32_t ok;

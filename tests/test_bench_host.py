@@ -30,6 +30,9 @@ def test_mg_solve_bytes_counts_every_pass():
 def test_variant_names_and_committed_traffic():
     assert bench.variant_name(2, 2, False) == "pattern2"
     assert bench.variant_name(2, 1, True) == "patternwin1"
+    assert bench.variant_name(2, 4, 2) == "q1stencil4"
+    assert bench.variant_name(2, 2, 3) == "q1gather2"
+    assert bench.variant_name(2, 2, 4) == "q1pair"
     assert bench.variant_name(1, 4, False) == "force4"
     assert bench.variant_name(0, 2, False) == "plain"
     for v in ("pattern1", "pattern2", "pattern4", "patternwin1", "patternwin2"):

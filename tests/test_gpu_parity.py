@@ -449,7 +449,8 @@ def test_ir_mixed_fp64_coarse(oracle):
 
 
 @pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4", "patternwin1",
-                                    "patternwin2", "q1stencil2", "q1stencil4", "q1stencil8"])
+                                    "patternwin2", "q1stencil2", "q1stencil4", "q1stencil8", "q1gather1",
+                                    "q1gather2", "q1gather4", "q1pair"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     """Value-dictionary + 16-bit offset layout (forceR) and row-pattern layout (patternR,
@@ -463,10 +464,11 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     monkeypatch.setenv("HB2_Q1_TRANSFER", "0")      # the transfers on their stored layout too
     A = SparseMatrixELL.poisson_q1(L, dt)
     P, R = SparseMatrixELL.transfer(L, dt)
-    if layout.startswith("pattern") or layout.startswith("q1stencil"):
+    if layout.startswith("pattern") or layout.startswith("q1"):
         # two row patterns: interior stencil, Dirichlet identity row; 1 matrix byte per row
         assert A.layout() == (2, 2, 1)
-        want = (2, int(layout[-1]), 1 if layout.startswith("patternwin") else 2 if layout.startswith("q1") else 0)
+        kern = {"patternwin": 1, "q1stencil": 2, "q1gather": 3, "q1pai": 4}.get(layout[:-1], 0)
+        want = (2, 2 if layout == "q1pair" else int(layout[-1]), kern)
     else:
         assert A.layout() == (1, 3, 27)
         want = (1, int(layout[-1]), 0)

@@ -1,12 +1,13 @@
-"""The Q1 stencil kernel (honei_b200/csrc/ell_q1.cu) for row-pattern ELL matrices
-holding the full nine-point stencil, pinned with HB2_ELL_COMPACT=q1stencilR
-(R = 2, 4, 8 rows per thread).  Bit for bit against the oracle's ELL product
-(la/product.hh:148-206) in every mode it runs (y = A x, r = b - A x with the fused
+"""The Q1 stencil kernels (honei_b200/csrc/ell_q1.cu) for row-pattern ELL matrices
+holding the full nine-point stencil, pinned with HB2_ELL_COMPACT=q1stencilR (x
+windows staged by bulk copies, R = 2, 4, 8 rows per thread) and q1gatherR (x
+gathered by plain loads, R = 1, 2, 4).  Bit for bit against the oracle's ELL product
+(la/product.hh:148-206) in every mode they run (y = A x, r = b - A x with the fused
 ||r||^2, y = A x with <y, x>, the Jacobi sweep of math/ri.hh:97-133), at the
 levels where the layout applies (8..11), in both precisions; for the anisotropic
 operator (other stencil values), for a matrix with a second full-stencil pattern
-(its rows take the general slot loop), for an x that is not 16-byte aligned (the
-general kernel) and inside the MG solve (passes in alternating directions)."""
+(its rows take the general slot loop), for an x that is not 16-byte aligned and
+inside the MG solve (passes in alternating directions)."""
 import ctypes
 
 import numpy as np
@@ -66,31 +67,39 @@ def check_modes(oracle, A, ref, npdt, seed=3):
     assert same_bits(host(s), expect)
 
 
-@pytest.mark.parametrize("R", [2, 4, 8])
+VARIANTS = [("q1stencil", 2), ("q1stencil", 4), ("q1stencil", 8), ("q1gather", 1), ("q1gather", 2), ("q1gather", 4),
+            ("q1pair", 2)]
+KERNEL = {"q1stencil": 2, "q1gather": 3, "q1pair": 4}
+
+
+@pytest.mark.parametrize("kind,R", VARIANTS)
 @pytest.mark.parametrize("L", [8, 9, 10, 11])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
-def test_q1_stencil_modes_bit_exact(oracle, monkeypatch, dt, L, R):
+def test_q1_stencil_modes_bit_exact(oracle, monkeypatch, dt, L, kind, R):
     if L == 11 and dt == torch.float32 and R != 4:
-        pytest.skip("level 11 FP32: one shape is enough")
+        pytest.skip("level 11 FP32: one shape per kernel is enough")
     npdt = np.float64 if dt == torch.float64 else np.float32
-    monkeypatch.setenv("HB2_ELL_COMPACT", f"q1stencil{R}")
+    monkeypatch.setenv("HB2_ELL_COMPACT", kind if kind == "q1pair" else f"{kind}{R}")
     A = SparseMatrixELL.poisson_q1(L, dt)
-    assert A.layout_variant(0) == (2, R, 2) and A.layout_variant(1) == (2, R, 2)
+    want = (2, R, KERNEL[kind])
+    assert A.layout_variant(0) == want and A.layout_variant(1) == want
     check_modes(oracle, A, oracle.q1_ell(L, npdt), npdt)
 
 
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
 @pytest.mark.parametrize("aniso", [10.0, 100.0])
-def test_q1_stencil_anisotropic(oracle, monkeypatch, aniso):
-    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+def test_q1_stencil_anisotropic(oracle, monkeypatch, aniso, variant):
+    monkeypatch.setenv("HB2_ELL_COMPACT", variant)
     A = SparseMatrixELL.poisson_q1(9, aniso=aniso)
-    assert A.layout_variant(0)[2] == 2
+    assert A.layout_variant(0)[2] in (2, 3, 4)
     check_modes(oracle, A, oracle.q1_ell(9, aniso=aniso), np.float64)
 
 
-def test_q1_stencil_second_full_pattern(oracle, monkeypatch):
+@pytest.mark.parametrize("variant", ["q1stencil2", "q1gather1", "q1pair"])
+def test_q1_stencil_second_full_pattern(oracle, monkeypatch, variant):
     """Interior rows of one grid band carry other stencil values: a second
     full-stencil pattern, whose rows take the general slot loop."""
-    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil2")
+    monkeypatch.setenv("HB2_ELL_COMPACT", variant)
     ref = oracle.q1_ell(9)
     Ax = ref.Ax.copy().reshape(ref.K, ref.stride)
     m = (1 << 9) + 1
@@ -99,14 +108,17 @@ def test_q1_stencil_second_full_pattern(oracle, monkeypatch):
     Ax[:, rows[full]] *= 2.0
     Ax = Ax.reshape(-1)
     A = SparseMatrixELL.from_arrays(ref.rows, ref.cols, ref.stride, ref.K, ref.Aj, Ax, ref.Arl)
-    assert A.layout()[:2] == (2, 3) and A.layout_variant(0)[2] == 2
+    assert A.layout()[:2] == (2, 3) and A.layout_variant(0)[2] in (2, 3, 4)
     ref2 = oracle.Ell(ref.rows, ref.cols, ref.stride, ref.K, 1, ref.Aj, Ax, ref.Arl)
     check_modes(oracle, A, ref2, np.float64)
 
 
-def test_q1_stencil_unaligned_x(oracle, monkeypatch):
-    """x not 16-byte aligned: the general row-pattern kernel runs instead, same bits."""
-    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
+def test_q1_stencil_unaligned_x(oracle, monkeypatch, variant):
+    """x not 16-byte aligned: the bulk-copy form hands over to the general row-pattern
+    kernel, the pair form to the interleaved gather form, the gather form runs as it
+    is; same bits."""
+    monkeypatch.setenv("HB2_ELL_COMPACT", variant)
     L = 9
     A = SparseMatrixELL.poisson_q1(L)
     n = A.rows()
@@ -120,11 +132,12 @@ def test_q1_stencil_unaligned_x(oracle, monkeypatch):
     assert same_bits(host(y), oracle.ell_spmv(oracle.q1_ell(L), x))
 
 
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
-def test_q1_stencil_in_the_mg_solve(oracle, monkeypatch, dt):
-    """MG V(4,4) with every eligible level on the Q1 stencil kernel: the oracle's
+def test_q1_stencil_in_the_mg_solve(oracle, monkeypatch, dt, variant):
+    """MG V(4,4) with every eligible level on a Q1 stencil kernel: the oracle's
     iterates bit for bit (reference-order coarse CG), cycle count equal."""
-    monkeypatch.setenv("HB2_ELL_COMPACT", "q1stencil4")
+    monkeypatch.setenv("HB2_ELL_COMPACT", variant)
     npdt = np.float64 if dt == torch.float64 else np.float32
     L = 10
     A = oracle.q1_ell(L, npdt)
