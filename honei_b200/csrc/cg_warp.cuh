@@ -14,6 +14,10 @@ namespace hb2
     template <> struct Eps<double> { static __device__ __forceinline__ double v() { return DBL_EPSILON; } };
     template <> struct Eps<float> { static __device__ __forceinline__ float v() { return FLT_EPSILON; } };
 
+    template <typename T> struct Recip;
+    template <> struct Recip<double> { static __device__ __forceinline__ double rn(double v) { return __drcp_rn(v); } };
+    template <> struct Recip<float> { static __device__ __forceinline__ float rn(float v) { return __frcp_rn(v); } };
+
     template <typename T>
     __device__ __forceinline__ T guard(T d)
     {
@@ -142,6 +146,85 @@ namespace hb2
         const T initial = sqrt(alpha);
         T current = initial;
         uint64_t it = 0, used = 0;
+        if (! exact && max_iters > 0)
+        {
+            // Chronopoulos-Gear recurrence (the same iterates as the loop below in
+            // exact arithmetic): per iteration one product w = A r and both dots
+            // (r, r), (w, r) in one shuffle tree, so the chain of an iteration holds
+            // one reduction and one division instead of two of each; the
+            // reciprocals the next iteration needs are formed off that chain.
+            //   x += a p; r -= a s; w = A r; g = (r, r); d = (w, r);
+            //   b = g / g_old; a = g / (d - b g / a_old); p = r + b p; s = w + b s
+            T sr[RPL], wr[RPL];
+            spmv(wr);   // w0 = A r0 (sp holds r0 = p0)
+            T gam = alpha, del;
+            {
+                double s1 = 0.0;
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                    if (lane + 32 * j < n) s1 = fma((double)wr[j], (double)rr[j], s1);
+                del = (T)warp_sum(s1);
+            }
+            T a = M::div(gam, guard(del));
+            T inv_a = Recip<T>::rn(guard(a)), inv_g = Recip<T>::rn(guard(gam));
+            // the stop test on squared norms: no square root on the iteration's chain
+            const T thr = M::mul(eps, initial), thr2 = M::mul(thr, thr), eps2 = M::mul(eps, eps);
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) sr[j] = wr[j];
+            while (it < max_iters)
+            {
+                const T ma = -a;
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                {
+                    xr[j] = M::add(xr[j], M::mul(a, pr[j]));
+                    rr[j] = M::add(rr[j], M::mul(ma, sr[j]));
+                }
+                __syncwarp();   // every lane is done gathering the old r
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                    if (lane + 32 * j < n) sp[lane + 32 * j] = rr[j];
+                __syncwarp();
+                spmv(wr);
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                    if (lane + 32 * j < n)
+                    {
+                        s1 = fma((double)rr[j], (double)rr[j], s1);
+                        s2 = fma((double)wr[j], (double)rr[j], s2);
+                    }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                {
+                    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                }
+                const T g = (T)s1;
+                del = (T)s2;
+                ++it;
+                if (g < thr2 || g < eps2 || it == max_iters)
+                {
+                    current = sqrt(g);
+                    used = it;
+                    break;
+                }
+                // single-rounded reciprocals instead of IEEE divisions (this mode is
+                // not the reference's order anyway)
+                const T b = M::mul(g, inv_g);
+                a = M::mul(g, Recip<T>::rn(guard(M::sub(del, M::mul(M::mul(b, g), inv_a)))));
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                {
+                    pr[j] = M::add(rr[j], M::mul(b, pr[j]));
+                    sr[j] = M::add(wr[j], M::mul(b, sr[j]));
+                }
+                inv_a = Recip<T>::rn(guard(a));
+                inv_g = Recip<T>::rn(guard(g));
+                gam = g;
+            }
+            it = max_iters;   // done: skip the loop below
+        }
         while (it < max_iters)
         {
             spmv(vr);

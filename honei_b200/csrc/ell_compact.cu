@@ -516,10 +516,10 @@ namespace hb2
         if (st) return st;
         void * buf = 0;
         const size_t vb = ((std::max(A->rows, A->cols) * es + 255) / 256) * 256;
-        HB2_CUDA(cudaMalloc(&buf, 3 * vb + 256));
-        HB2_CUDA(cudaMemsetAsync(buf, 0, 3 * vb + 256, s));
-        void * xv = buf, * yv = (char *)buf + vb, * bv = (char *)buf + 2 * vb;
-        double * nrm = (double *)((char *)buf + 3 * vb);
+        HB2_CUDA(cudaMalloc(&buf, 4 * vb + 256));
+        HB2_CUDA(cudaMemsetAsync(buf, 0, 4 * vb + 256, s));
+        void * xv = buf, * yv = (char *)buf + vb, * bv = (char *)buf + 2 * vb, * pv = (char *)buf + 3 * vb;
+        double * nrm = (double *)((char *)buf + 4 * vb);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -555,9 +555,13 @@ namespace hb2
                     // the workspace are not candidates
                     if (cls == 1 && (uint64_t)ell_grid(A, true) > ws->max_blocks) continue;
                     cudaEventRecord(e0, s);
+                    // class 0 of a square matrix is timed on the Jacobi sweep (the
+                    // multigrid's eight passes per level and cycle), of a rectangular
+                    // one on the product
                     for (int b = 0; b < kBurst && ! st; ++b)
-                        st = cls == 0 ? launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s)
-                                      : launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s);
+                        st = cls == 1 ? launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s)
+                             : square ? launch_ell(A, kJacobi, xv, yv, bv, pv, 0, 0, 0, 0, s)
+                                      : launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s);
                     cudaEventRecord(e1, s);
                     if (st) break;
                     cudaEventSynchronize(e1);
