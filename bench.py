@@ -1,13 +1,16 @@
 #!/usr/bin/env python
 """Headline benchmark: Poisson solves/s to 1e-10 relative residual.
 
-Workload (one "step"): one full MG solve of the level-10 Q1 Poisson system
-(1025 x 1025 nodes, 1,050,625 unknowns, ELL FP64), V(4,4) with damped Jacobi
-(omega 0.7), bilinear prolongation / transposed restriction, coarsest level 3
-solved by CG (iteration cap 100, the reference's own MG test setting), stop at
-||r|| < 1e-10 ||r0||; b = A u*, u* ~ U[-1,1] (splitmix64, seed 42 + rank),
-x0 = 0.  Inputs are resident in HBM when a timed step starts; L2 is flushed
-(256 MiB write) before every step and the flush is outside the step's events.
+Workload (one "step"): one full MG solve of the level-11 Q1 Poisson system
+(2049 x 2049 nodes, 4,198,401 unknowns, ELL FP64; the largest single-GPU
+configuration, whose mixed-precision comparison is reported beside it), V(4,4)
+with damped Jacobi (omega 0.7), bilinear prolongation / transposed restriction,
+coarsest level 3 solved by CG (iteration cap 100, the reference's own MG test
+setting), stop at ||r|| < 1e-10 ||r0||; b = A u*, u* ~ U[-1,1] (splitmix64,
+seed 42 + rank), x0 = 0.  Inputs are resident in HBM when a timed step starts;
+L2 is flushed before every step (256 MiB written, then 256 MiB read, so that no
+dirty line of the flush is written back inside the step) and the flush is
+outside the step's events.  --level 10 runs the level-10 solve of config 1.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -36,6 +39,8 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "honei_ref")
 MIN_LEVEL = 3
 COARSE_CAP = 100
 MIXED_LEVEL = 11
+DEFAULT_LEVEL = 11
+SERVING_RATES = (50.0, 100.0, 200.0, 500.0, 1000.0, 2000.0)
 SUB_MAX_ROWS = 20000    # levels up to this many rows run in the fused small-level kernels
 
 
@@ -45,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--level", type=int, default=10)
+    ap.add_argument("--level", type=int, default=DEFAULT_LEVEL)
+    ap.add_argument("--serving-duration", type=float, default=10.0, help="seconds per serving rate")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
@@ -188,9 +194,9 @@ def barrier(world: int):
         dist.barrier()
 
 
-def reference_cpu(level: int, reps: int, warmup: int, tag: str, threads: int):
+def reference_cpu(level: int, reps: int, warmup: int, tag: str, threads: int, env=None):
     """Run the reference's own MG solver (oracle/_ref/honei_ref) and parse its RESULT line."""
-    env = dict(os.environ)
+    env = dict(os.environ, **(env or {}))
     with tempfile.NamedTemporaryFile("w", suffix=".honeirc", delete=False) as f:
         f.write(f"mc::num_threads = {threads}\nlog::categories = none\nlog::output = /dev/null\n")
         env["HONEI_CONFIG"] = f.name
@@ -210,12 +216,14 @@ def oracle_port_cpu(level: int, reps: int):
     from oracle import oracle as o
     A = o.q1_ell(level)
     b = o.ell_spmv(A, uniform(A.rows, 42))
+    import numpy as np
     t = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        _, it, _ = o.mg_q1(level, b, max_iters_coarse=COARSE_CAP)
+        x, it, _ = o.mg_q1(level, b, max_iters_coarse=COARSE_CAP)
         t.append(time.perf_counter() - t0)
-    return {"seconds_per_solve": sum(t) / len(t), "iters": it, "tag": "oracle-port"}
+    relres = float(np.linalg.norm(b - o.ell_spmv(A, x)) / np.linalg.norm(b))
+    return {"seconds_per_solve": sum(t) / len(t), "iters": it, "tag": "oracle-port", "x": x, "relres": relres}
 
 
 def run_reference_arm(args, rank, world):
@@ -248,8 +256,55 @@ def workload_config(args, world):
     return {"workload": f"mg-v44-fp64-q1-level{args.level}", "level": args.level,
             "unknowns": ((1 << args.level) + 1) ** 2, "matrix": "SparseMatrixELL (9 slots, int32 columns on device)",
             "coarse_level": MIN_LEVEL, "coarse_solver": f"CG, cap {COARSE_CAP}, tree-ordered dots", "smoother": "Jacobi omega 0.7, 4+4",
-            "tol": 1e-10, "l2": "flushed (256 MiB write) before every step, flush outside the step events",
+            "tol": 1e-10, "l2": "flushed before every step (256 MiB written, then 256 MiB read), flush outside the step "
+                                "events; the level's vectors alone exceed L2 at level 11",
             "parallelism": f"{world} independent systems (one per GPU)" if world > 1 else "single system"}
+
+
+ROW_BYTES = {"jacobi": 4, "spmv": 2, "defect": 3}   # vector accesses per row (8 B each in FP64)
+
+
+def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None):
+    """One ELL kernel of the level-`level` operator on the layout A runs on, timed in
+    its steady state: 40 launches captured in one CUDA graph, rotating over sets of
+    input and output vectors of more than 2x L2 in all (every launch reads its vectors
+    from DRAM), CUDA events around each replay on the launching stream, the mean
+    launch time the median over replays.  achieved = algorithmic bytes per launch
+    (matrix bytes per row of the layout + the vector accesses) / that time."""
+    import numpy as np
+    import torch
+    from honei_b200.kernel_bench import graph_time
+    n = A.rows()
+    P = hb.RISmoother.jacobi_precon(A, 0.7)
+    ms = graph_time(kind, A, P, n, torch.float64, np.float64, dev, reps)
+    kind_l, table_size, rb = A.layout()
+    vk, vr, vw = A.layout_variant(1 if kind == "defect" else 0)
+    variant = variant_name(vk, vr, vw)
+    nbytes = n * (rb + 8 * ROW_BYTES[kind])
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    key = f"{variant}:{kind}:L{level}"
+    return {"bound": "hbm", "kernel": label or f"{kind} on {variant}", "variant": variant, "level": level,
+            "layout": layout_text(kind_l, table_size, rb), "achieved": achieved, "peak": peak[0], "unit": "GB/s",
+            "frac": achieved / peak[0], "peak_source": peak[1], "traffic": load_traffic(key), "traffic_key": key,
+            "algorithmic_bytes": nbytes, "bytes_per_row": rb + 8 * ROW_BYTES[kind], "launch_us": 1000 * ms,
+            "timing": "CUDA graph of 40 launches over rotating vector sets (> 2x L2), events around each replay"}
+
+
+def time_solves(hb, data, b, x, flush, steps, warmup, stream):
+    """CUDA-event times of `steps` MG solves (x = 0 each time), L2 flushed before each"""
+    import torch
+    ts = []
+    for i in range(warmup + steps):
+        flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hb.fill(x, 0.0)
+        hb.MGSolver.value(data, b, x)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            ts.append(e0.elapsed_time(e1))
+    return ts
 
 
 def main():
@@ -260,12 +315,11 @@ def main():
         barrier(world)
         return rc
 
-    import numpy as np
     import torch
 
     import honei_b200 as hb
-    from honei_b200 import _lib
     from honei_b200.inputs import uniform
+    from honei_b200.kernel_bench import L2Flush
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -280,7 +334,7 @@ def main():
     b = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
     hb.Product.value(b, A, u)
     x = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
-    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    flush = L2Flush(dev)
 
     def one_solve():
         hb.fill(x, 0.0)
@@ -299,7 +353,7 @@ def main():
     with Clocks(local) as clk:
         t_wall0 = time.perf_counter()
         for i in range(args.steps):
-            flush.zero_()
+            flush()
             ev[i][0].record(stream)
             one_solve()
             ev[i][1].record(stream)
@@ -328,7 +382,7 @@ def main():
     x_host = torch.empty(n, dtype=torch.float64).pin_memory()
     e2e_ms = []
     for i in range(args.warmup + args.steps):
-        flush.zero_()
+        flush()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         b_dev = b_host.to(dev, non_blocking=True)
@@ -342,30 +396,9 @@ def main():
     e2e_mean = max_over_ranks(statistics.mean(e2e_ms), world, dev)
 
     # ---------------------------------------------------------------- dominant kernel
-    P = hb.RISmoother.jacobi_precon(A, 0.7)
-    xa = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
-    xb = hb.DenseVector(torch.zeros(n, dtype=torch.float64, device=dev))
-    kms = []
-    for i in range(args.warmup + max(args.steps, 30)):
-        flush.zero_()
-        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k0.record(stream)
-        _lib.call("hb2_jacobi_sweep_ell", A.handle, P.ptr, b.ptr, xa.ptr, xb.ptr,
-                  ctypes_stream(stream))
-        k1.record(stream)
-        k1.synchronize()
-        if i >= args.warmup:
-            kms.append(k0.elapsed_time(k1))
-        xa, xb = xb, xa
-    k_ms = statistics.mean(kms)
-    kind, table_size, row_bytes = A.layout()
-    k_bytes = (row_bytes + 4 * 8) * n
-    achieved = k_bytes / (k_ms * 1e-3) / 1e9
     peaks = load_peaks()
-    vkind, vrpt, vwin = A.layout_variant(0)
-    variant = variant_name(vkind, vrpt, vwin)
-    traffic = load_traffic(variant)
-
+    roof = kernel_roofline(hb, "jacobi", A, L, peaks, dev,
+                           label=f"fused Jacobi sweep x' = x + P (b - A x), level {L}, FP64")
     solve_bytes = mg_solve_bytes(L, int(statistics.median(cycles)),
                                  layout_row_bytes(hb, torch.float64, range(MIN_LEVEL, L + 1)))
     line = {
@@ -377,30 +410,33 @@ def main():
         "latency_ms": {"p50": percentile(step_ms, 50), "p99": percentile(step_ms, 99), "max": max(step_ms)},
         "cycles": int(statistics.median(cycles)), "relres": relres,
         "wall_ms_per_step_incl_flush": 1000 * t_wall / args.steps,
-        "roofline": {"bound": "hbm", "kernel": "%s, Jacobi mode, %d rows per thread (fused Jacobi sweep, level %d)" % (
-                         "ell_pattern_win_kernel" if vwin else KERNEL_OF_LAYOUT[kind], vrpt, L),
-                     "variant": variant,
-                     "layout": layout_text(kind, table_size, row_bytes + 32),
-                     "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
-                     "peak_source": peaks[1], "traffic": traffic, "algorithmic_bytes": k_bytes,
-                     "launch_us": 1000 * k_ms},
+        "roofline": roof,
         "e2e": {"value": world * 1000.0 / e2e_mean, "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": gpu_launches,
         "clocks": clk.summary(),
     }
-    if not args.no_mixed:
-        line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5), min(args.warmup, 2),
-                                              rank)
-        line["mixed_vs_fp64"]["anisotropic"] = anisotropic_probe(hb, dev, flush, MIXED_LEVEL, rank)
-    if not args.no_batch:
-        line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
-    if not args.no_serving:
-        line["serving"] = serving_loop(rank)
-    if not args.no_next:
-        line["next_rows"] = next_rows(hb, dev, flush, rank)
+    # the single-GPU characterisation beside the headline (replica runs skip it)
+    keep = {}
+    if world == 1:
+        line["roofline_extra"] = roofline_extra(hb, A, L, peaks, dev)
+        if L != 10:
+            line["config1_level10"] = level10_solve(hb, dev, flush, args, stream)
+        if not args.no_mixed:
+            line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5),
+                                                  min(args.warmup, 2), rank, keep=keep)
+            line["mixed_vs_fp64"]["anisotropic"] = anisotropic_probe(hb, dev, flush, MIXED_LEVEL, rank)
+        if not args.no_batch:
+            line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
+        if not args.no_serving:
+            line["serving"] = serving_loop(rank, duration=args.serving_duration)
+        if not args.no_next:
+            line["next_rows"] = next_rows(hb, dev, flush, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(L)
+        line["cpu_baseline"] = cpu_baseline(L, keep if L == MIXED_LEVEL else None)
+        errors = line["cpu_baseline"].pop("errors", None)
+        if errors and "mixed_vs_fp64" in line:
+            line["mixed_vs_fp64"].update(errors)
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)
@@ -408,6 +444,50 @@ def main():
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def roofline_extra(hb, A, L, peaks, dev):
+    """The other kernels' steady-state rooflines: the SpMV and the fused defect + norm
+    on the tuned layout at level L; the level-10 sweep on its tuned layout; and, on the
+    plain ELL arrays (FP64 values + int32 columns read with 128-bit loads: 124 / 132
+    B/row), the SpMV and defect at level L."""
+    out = [kernel_roofline(hb, "spmv", A, L, peaks, dev, label=f"y = A x, level {L}, tuned layout"),
+           kernel_roofline(hb, "defect", A, L, peaks, dev, label=f"r = b - A x with ||r||^2, level {L}, tuned layout")]
+    if L != 10:
+        A10 = hb.SparseMatrixELL.poisson_q1(10)
+        out.append(kernel_roofline(hb, "jacobi", A10, 10, peaks, dev, label="fused Jacobi sweep, level 10, tuned layout"))
+        del A10
+    old = os.environ.get("HB2_ELL_COMPACT")
+    os.environ["HB2_ELL_COMPACT"] = "0"        # the plain layout (read when a matrix is created)
+    try:
+        Ap = hb.SparseMatrixELL.poisson_q1(L)
+    finally:
+        if old is None:
+            del os.environ["HB2_ELL_COMPACT"]
+        else:
+            os.environ["HB2_ELL_COMPACT"] = old
+    out.append(kernel_roofline(hb, "spmv", Ap, L, peaks, dev, label=f"y = A x, level {L}, plain ELL"))
+    out.append(kernel_roofline(hb, "defect", Ap, L, peaks, dev, label=f"r = b - A x with ||r||^2, level {L}, plain ELL"))
+    return out
+
+
+def level10_solve(hb, dev, flush, args, stream):
+    """Config 1: the level-10 MG solve (1,050,625 unknowns), same parameters and timing."""
+    import torch
+    from honei_b200.inputs import uniform
+    L = 10
+    n = ((1 << L) + 1) ** 2
+    A = hb.SparseMatrixELL.poisson_q1(L)
+    data = hb.MGData.poisson_q1(MIN_LEVEL, L, params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10,
+                                                                    coarse_exact=False))
+    b = hb.DenseVector(n)
+    hb.Product.value(b, A, hb.DenseVector(torch.from_numpy(uniform(n, 42)).to(dev)))
+    x = hb.DenseVector(n)
+    ts = time_solves(hb, data, b, x, flush, args.steps, args.warmup, stream)
+    r = hb.DenseVector(n)
+    hb.Defect.value(r, b, A, x)
+    return {"level": L, "unknowns": n, "ms_per_solve": statistics.mean(ts), "solves_per_s": 1000.0 / statistics.mean(ts),
+            "p99_ms": percentile(ts, 99), "cycles": data.used_iters, "relres": hb.Norm.value(r) / hb.Norm.value(b)}
 
 
 def next_rows(hb, dev, flush, rank, reps=3):
@@ -427,7 +507,7 @@ def next_rows(hb, dev, flush, rank, reps=3):
         fn()
         ts = []
         for _ in range(reps):
-            flush.zero_()
+            flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             r = fn()
@@ -490,13 +570,16 @@ def finite_or_text(v):
     return v if math.isfinite(v) else str(v)
 
 
-def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cycles=100, max_outer=100):
+def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cycles=100, max_outer=100, keep=None):
     """Config 2: level-11 Q1 Poisson (4,198,401 unknowns) to 1e-10 relative residual,
     plain FP64 MG vs iterative refinement (FP64 defect / update / norm around an FP32
-    MG V(4,4) inner solve to 1e-3, restarted from zero each outer step, coarse CG
-    cap 100 at eps 1e-10).  Times are CUDA-event times per solve, L2 flushed before each.
-    aniso scales the x-coupling of every level's operator (the anisotropic variant);
-    max_cycles caps the MG cycles of both solvers, max_outer the IR steps."""
+    MG V(4,4) inner solve to 1e-3, restarted from zero each outer step, its coarse CG
+    (FP64 arithmetic) cap 100 at the same eps 1e-3, the reference's one eps_relative
+    for both).  The whole IR solve is one CUDA graph.  Times are CUDA-event times per
+    solve, L2 flushed before each.  aniso scales the x-coupling of every level's
+    operator (the anisotropic variant); max_cycles caps the MG cycles of both solvers,
+    max_outer the IR steps.  keep (dict): receives host copies of both solutions, for
+    the error against the reference's FP64 solution (cpu_baseline)."""
     import statistics
 
     import torch
@@ -521,7 +604,7 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cyc
     def timed(fn):
         ts = []
         for i in range(warmup + steps):
-            flush.zero_()
+            flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             fn()
@@ -565,8 +648,12 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cyc
     res = {"level": level, "unknowns": n, "fp64_mg_ms": t64, "fp64_cycles": fp64.used_iters,
            "fp64_relres": finite_or_text(rel64), "mixed_ir_ms": tir, "ir_outer_iters": info["outer"],
            "ir_inner_fp32_cycles": info["inner"], "mixed_relres": finite_or_text(relir),
-           "mixed_rel_error_vs_fp64": finite_or_text(err), "speedup_mixed_over_fp64": t64 / tir,
-           "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-10"}
+           "mixed_rel_error_vs_fp64_gpu": finite_or_text(err), "speedup_mixed_over_fp64": t64 / tir,
+           "inner": "FP32 ELL MG V(4,4) to 1e-3 (restart from zero), FP64 coarse CG cap 100 / eps 1e-3"}
+    if keep is not None:
+        keep["x64"], keep["xir"] = x64.elements.cpu().numpy(), xir.elements.cpu().numpy()
+        keep["b"] = b.elements.cpu().numpy()
+        keep["relres_mixed"], keep["relres_fp64"] = relir, rel64
     if aniso != 1.0:
         res["x_coupling"] = aniso
         res["cycle_cap"], res["outer_cap"] = max_cycles, max_outer
@@ -633,7 +720,7 @@ def batched_solves(hb, dev, flush, steps, warmup, rank):
     def timed(fn):
         ts = []
         for i in range(warmup + steps):
-            flush.zero_()
+            flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             fn()
@@ -668,21 +755,32 @@ def batched_solves(hb, dev, flush, steps, warmup, rank):
             bj = hb.DenseVector(dev_b[s][j].clone())
             hb.Defect.value(r, bj, A, hb.DenseVector(x[j].clone()))
             worst = max(worst, hb.Norm.value(r) / hb.Norm.value(bj))
-    # the loop of the single-system solver: per-level median solve time x RHS count
-    per_level = {}
+    # the loop of the single-system solver over every right-hand side of the batch:
+    # one FP64 MG hierarchy per level (built before the loop), each RHS solved from
+    # x = 0 in turn, the whole loop between two CUDA events (L2 flushed before it)
     params = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-8, coarse_exact=False)
-    for level in sorted({l for l, _ in systems}):
-        data = hb.MGData.poisson_q1(MIN_LEVEL, level, params=params)
-        s = next(i for i, (l, _) in enumerate(systems) if l == level)
-        b = hb.DenseVector(dev_b[s][0].clone())
-        x = hb.DenseVector(B.unknowns(level))
+    hier = {level: hb.MGData.poisson_q1(MIN_LEVEL, level, params=params) for level in sorted({l for l, _ in systems})}
+    xs = {level: hb.DenseVector(B.unknowns(level)) for level in hier}
+    loop_cycles = []
 
-        def one():
-            hb.fill(x, 0.0)
-            hb.MGSolver.value(data, b, x)
-        per_level[level] = timed(one)
-        del data
-    t_loop = sum(per_level[l] * k for l, k in systems)
+    def loop():
+        for s, (level, k) in enumerate(systems):
+            for j in range(k):
+                hb.fill(xs[level], 0.0)
+                hb.MGSolver.value(hier[level], hb.DenseVector(dev_b[s][j]), xs[level])
+                loop_cycles.append(hier[level].used_iters)
+    for level in hier:                              # warm-up: one solve per level
+        s0 = next(i for i, (l, _) in enumerate(systems) if l == level)
+        hb.fill(xs[level], 0.0)
+        hb.MGSolver.value(hier[level], hb.DenseVector(dev_b[s0][0]), xs[level])
+    flush()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loop()
+    e1.record()
+    e1.synchronize()
+    t_loop = e0.elapsed_time(e1)
+    del hier
     return {"systems": len(systems), "rhs": nvec, "levels": "U{4..9}", "multi_rhs_systems": sum(k > 1 for _, k in systems),
             "device_ms": t_dev, "rhs_per_s": nvec * 1000.0 / t_dev,
             "e2e_ms": t_e2e, "e2e_rhs_per_s": nvec * 1000.0 / t_e2e,
@@ -691,34 +789,41 @@ def batched_solves(hb, dev, flush, steps, warmup, rank):
             "max_rel_defect": max(rels), "worst_true_relres_sampled": worst,
             "launches_per_step": info["launches_per_step"], "launches_per_solve": launches,
             "device_bytes": info["device_bytes"],
-            "loop_fp64_mg_ms_projected": t_loop, "loop_ms_per_level": per_level,
+            "loop_fp64_mg_ms": t_loop, "loop_solves": nvec, "loop_mean_cycles": statistics.mean(loop_cycles),
+            "loop": "config 1's single-system FP64 MG solver (V(4,4), coarse CG cap 100) to 1e-8 over all "
+                    f"{nvec} right-hand sides in turn, one resident hierarchy per level, timed as one loop",
             "speedup_vs_loop": t_loop / t_dev,
             "method": "CG VAR (FP64) + one FP32 MG V(4,4) preconditioner, FP64 coarse CG cap 100; tol 1e-8"}
 
 
-def serving_loop(rank, rates=(100.0, 500.0), duration=5.0):
-    """Config 4, short form: Poisson arrivals for `duration` s per rate, levels log-uniform
-    in 5..11, tolerance 1e-8 / 1e-10 50/50, seeded U[-1,1] RHS; slot pool sized under a
-    120 GB budget.  Latency = host clock from arrival to the solution in pinned host
-    memory.  The FP64 comparison serves the same arrivals one at a time with resident
-    FP64 MG hierarchies.  (python -m honei_b200.serving runs the full 60 s sweep.)"""
+def serving_loop(rank, rates=SERVING_RATES, duration=10.0, fp64_max_rate=200.0):
+    """Config 4: Poisson arrivals for `duration` s per rate (50 ... 2000 req/s), levels
+    log-uniform in 5..11, tolerance 1e-8 / 1e-10 50/50, seeded U[-1,1] RHS; slot pool
+    sized under a 120 GB budget.  Latency = host clock from arrival to the solution in
+    pinned host memory.  Three servers on the same arrivals: the hybrid one (FP64 MG
+    when idle, continuous batching otherwise), the batched engine alone, and FP64 MG one
+    request at a time (up to fp64_max_rate: above its ~380 req/s capacity its queue
+    only grows).  python -m honei_b200.serving runs the same sweep for 60 s per rate."""
     from honei_b200 import serving
+    keys = ("rate_req_s", "arrived", "finished", "solves_per_s", "p50_ms", "p99_ms", "max_rel_defect_1e-8",
+            "max_rel_defect_1e-10")
     pool = serving.RhsPool(seed=rank)
     srv = serving.PoissonServer(budget_bytes=120e9)
-    serving.run(srv, 200, 1.0, pool, seed=99)
-    out = {"budget_bytes": 120e9, "device_bytes": srv.device_bytes, "slots": srv.slots, "duration_s": duration,
-           "batched_mixed": [], "fp64_sequential": []}
-    for rate in rates:
-        s, _ = serving.run(srv, rate, duration, pool, seed=rank)
-        out["batched_mixed"].append({k: s[k] for k in ("rate_req_s", "finished", "solves_per_s", "p50_ms", "p99_ms",
-                                                         "max_rel_defect_1e-8", "max_rel_defect_1e-10")})
-    del srv
     seq = serving.FP64SequentialServer()
-    serving.run(seq, 50, 1.0, pool, seed=99)
+    hyb = serving.HybridServer(srv, seq)
+    serving.run(srv, 200, 1.0, pool, seed=99)
+    serving.run(hyb, 50, 1.0, pool, seed=99)
+    out = {"budget_bytes": 120e9, "device_bytes": srv.device_bytes, "slots": srv.slots, "duration_s": duration,
+           "hybrid": [], "batched_mixed": [], "fp64_sequential": []}
     for rate in rates:
-        s, _ = serving.run(seq, rate, duration, pool, seed=rank)
-        out["fp64_sequential"].append({k: s[k] for k in ("rate_req_s", "finished", "solves_per_s", "p50_ms", "p99_ms",
-                                                           "max_rel_defect_1e-8", "max_rel_defect_1e-10")})
+        hyb.routed.clear()
+        s, _ = serving.run(hyb, rate, duration, pool, seed=rank)
+        out["hybrid"].append(dict({k: s[k] for k in keys}, routed=dict(hyb.routed)))
+        s, _ = serving.run(srv, rate, duration, pool, seed=rank)
+        out["batched_mixed"].append({k: s[k] for k in keys})
+        if rate <= fp64_max_rate:
+            s, _ = serving.run(seq, rate, duration, pool, seed=rank)
+            out["fp64_sequential"].append({k: s[k] for k in keys})
     return out
 
 
@@ -753,31 +858,70 @@ def variant_name(kind, rows_per_thread, kernel):
     return "plain"
 
 
-def load_traffic(variant):
-    """DRAM bytes per launch of the dominant kernel, for the variant the autotuner
-    chose, from the committed ncu summary (None when that variant was not captured)."""
-    path = os.path.join(ROOT, "profiles", "ell_jacobi_sweep_fp64_level10.md")
-    key = "traffic_bytes_per_launch[%s]:" % variant
-    try:
-        for line in open(path):
-            if line.startswith(key):
-                return float(line.split(":", 1)[1])
-    except Exception:
-        pass
+def load_traffic(key):
+    """DRAM bytes (read + write) per launch of a kernel, from the committed ncu
+    summaries: a line `traffic_bytes_per_launch[<variant>:<kernel>:L<level>]: <bytes>`
+    in any file under profiles/ (None when that kernel was not captured)."""
+    import glob
+    tag = "traffic_bytes_per_launch[%s]:" % key
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        try:
+            for line in open(path):
+                if line.startswith(tag):
+                    return float(line[len(tag):])
+        except Exception:
+            pass
     return None
 
 
-def cpu_baseline(level):
-    reps = 2
+def q1_lambda_min(level):
+    """smallest eigenvalue of the Q1 stencil (8/3 centre, -1/3 neighbours) on the
+    interior nodes of the (2^L + 1)^2 grid: 1 / ||A^-1|| for the error bound"""
+    import math
+    c = math.cos(math.pi / (1 << level))
+    return (8.0 - 4.0 * c - 4.0 * c * c) / 3.0
+
+
+def solution_errors(level, keep, x_ref, ref_relres, ref_what):
+    """The GPU solutions (FP64 MG and mixed IR) against the reference's own FP64 CPU
+    solution of the same system, with the bound the two residuals allow:
+    ||x - x_ref|| <= ||A^-1|| (||r|| + ||r_ref||)."""
+    import numpy as np
+    nx = float(np.linalg.norm(x_ref))
+    bound = (keep["relres_mixed"] + ref_relres) * float(np.linalg.norm(keep["b"])) / (q1_lambda_min(level) * nx)
+    return {"mixed_rel_error_vs_reference_fp64": float(np.linalg.norm(keep["xir"] - x_ref)) / nx,
+            "fp64_gpu_rel_error_vs_reference_fp64": float(np.linalg.norm(keep["x64"] - x_ref)) / nx,
+            "mixed_error_bound_from_residuals": bound, "reference_fp64_relres": ref_relres,
+            "reference_fp64_solution": ref_what}
+
+
+def cpu_baseline(level, keep=None):
+    """The reference's own tags::CPU::SSE MG solver on one host core (oracle/_ref), one
+    solve of the headline's system; when `keep` holds the GPU solutions (level 11),
+    the reference's solution is dumped and the GPU results' errors are stated
+    against it."""
+    import numpy as np
+    reps = 1
+    dump = os.path.join(tempfile.gettempdir(), "hb2_ref_x_%d.bin" % os.getpid())
     try:
-        res = reference_cpu(level, reps, 0, "sse", 1)
-        return {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "reference",
-                "sample": f"{reps} MG solves at level {level} (reference tags::CPU::SSE, 1 thread)",
-                "iters": res["iters"]}
+        res = reference_cpu(level, reps, 0, "sse", 1, env={"HONEI_DUMP_X": dump} if keep else None)
+        out = {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "reference",
+               "sample": f"{reps} MG solve at level {level} (reference tags::CPU::SSE, 1 thread)",
+               "iters": res["iters"]}
+        if keep and os.path.exists(dump):
+            x_ref = np.fromfile(dump, dtype=np.float64)
+            os.unlink(dump)
+            if x_ref.size == keep["xir"].size:
+                out["errors"] = solution_errors(level, keep, x_ref, float(res["relres"]),
+                                                "reference tags::CPU::SSE MGSolver (oracle/_ref)")
+        return out
     except Exception as e:  # binary absent: the oracle port
         res = oracle_port_cpu(level, 1)
-        return {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "port",
-                "sample": f"1 MG solve at level {level} (oracle C port; reference binary unavailable: {e})"}
+        out = {"value": 1.0 / res["seconds_per_solve"], "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"1 MG solve at level {level} (oracle C port; reference binary unavailable: {e})"}
+        if keep and "x" in res:
+            out["errors"] = solution_errors(level, keep, res["x"], res["relres"], "oracle port of the MGSolver")
+        return out
 
 
 if __name__ == "__main__":

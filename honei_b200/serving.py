@@ -24,7 +24,10 @@ request is admitted only into a free slot.
 ``FP64SequentialServer`` is the comparison point: resident FP64 MG hierarchies per
 level (the single-system solver), requests served one at a time in arrival order.
 
-    python -m honei_b200.serving --rates 50,200,1000,2000 --duration 60
+``HybridServer`` routes a request that arrives at an idle server to the FP64 MG
+hierarchy and batches the rest.
+
+    python -m honei_b200.serving --rates 50,200,1000,2000 --duration 60 [--hybrid] [--fp64]
 """
 from __future__ import annotations
 
@@ -214,6 +217,39 @@ class FP64SequentialServer:
         return [req]
 
 
+class HybridServer:
+    """Continuous batching with a fast path for an idle server.  A request that
+    arrives while nothing is in flight or waiting is solved at once by the resident
+    FP64 MG hierarchy of its level (one graph launch: at low load a single MG solve
+    has the lower latency, while a batched PCG step costs a fixed ~0.5 ms and a
+    request needs several); requests that find others in flight or waiting join the
+    batched mixed-precision engine.  Either way a result meets its tolerance; which
+    path served it depends on the load (``routed`` counts them)."""
+
+    def __init__(self, batched: PoissonServer, direct: FP64SequentialServer):
+        self.batched, self.direct = batched, direct
+        self.waiting = collections.deque()
+        self.routed = collections.Counter()
+
+    def submit(self, req):
+        self.waiting.append(req)
+
+    def pending(self):
+        return len(self.waiting) + self.batched.pending() + self.direct.pending()
+
+    def poll(self, clock, steps=1):
+        idle = not self.batched.active and not any(self.batched.queue.values())
+        if idle and len(self.waiting) == 1:
+            req = self.waiting.popleft()
+            self.direct.submit(req)
+            self.routed["fp64_mg"] += 1
+            return self.direct.poll(clock)
+        while self.waiting:
+            self.batched.submit(self.waiting.popleft())
+            self.routed["batched"] += 1
+        return self.batched.poll(clock, steps)
+
+
 def run(server, rate, duration, pool, seed=0, drain_limit=60.0):
     """Drive `server` with Poisson arrivals at `rate` req/s for `duration` s (host clock);
     returns the latency / throughput summary and the finished requests."""
@@ -258,6 +294,7 @@ def main(argv=None):
     ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--fp64", action="store_true", help="also run the FP64 sequential server")
+    ap.add_argument("--hybrid", action="store_true", help="also run the hybrid server (FP64 MG when idle)")
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args(argv)
     pool = RhsPool(seed=a.seed)
@@ -269,6 +306,15 @@ def main(argv=None):
         summary, _ = run(server, rate, a.duration, pool, seed=a.seed)
         summary["server"] = "batched mixed-precision PCG (continuous batching)"
         print(json.dumps(summary), flush=True)
+    if a.hybrid:
+        hyb = HybridServer(server, FP64SequentialServer())
+        run(hyb, 50, 1.0, pool, seed=a.seed + 99)
+        for rate in [float(r) for r in a.rates.split(",")]:
+            hyb.routed.clear()
+            summary, _ = run(hyb, rate, a.duration, pool, seed=a.seed)
+            summary["server"] = "hybrid: FP64 MG when idle, else batched mixed-precision PCG"
+            summary["routed"] = dict(hyb.routed)
+            print(json.dumps(summary), flush=True)
     if a.fp64:
         seq = FP64SequentialServer()
         run(seq, 50, 1.0, pool, seed=a.seed + 99)

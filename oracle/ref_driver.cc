@@ -370,6 +370,18 @@ namespace
                 relres = rel_residual(h.A.back(), h.b.back(), data.x.back());
             }
             std::sort(times.begin(), times.end());
+            // HONEI_DUMP_X=<file>: the solution, raw doubles (the checker of other solvers' results)
+            if (const char * dump = getenv("HONEI_DUMP_X"))
+                if (FILE * f = fopen(dump, "wb"))
+                {
+                    const DenseVector<double> & xs(h.x.back());   // shared with the solver's MGData
+                    for (unsigned long i(0); i < xs.size(); ++i)
+                    {
+                        const double v(xs[i]);
+                        fwrite(&v, sizeof(double), 1, f);
+                    }
+                    fclose(f);
+                }
             printf("RESULT {\"which\": \"mg\", \"tag\": \"%s\", \"level\": %u, \"reps\": %u, \"seconds_per_solve\": %.6g, "
                    "\"min_s\": %.6g, \"max_s\": %.6g, \"iters\": %lu, \"relres\": %.6g, \"setup_s\": %.3g, "
                    "\"coarse_cap\": %lu}\n", tagname, L, reps, secs / reps, times.front(), times.back(), iters, relres,

@@ -36,10 +36,26 @@ def test_variant_names_and_committed_traffic():
     assert bench.variant_name(1, 4, False) == "force4"
     assert bench.variant_name(0, 2, False) == "plain"
     for v in ("pattern1", "pattern2", "pattern4", "patternwin1", "patternwin2"):
-        t = bench.load_traffic(v)
+        t = bench.load_traffic(f"{v}:jacobi:L10")
         # DRAM bytes of one level-10 sweep: about the 25 B/row the kernel must read
         assert t is not None and 25 * 1_050_625 <= t <= 25.1 * 1_050_625
-    assert bench.load_traffic("force8") is None
+    assert bench.load_traffic("force8:jacobi:L10") is None
+    # the level-11 kernels the bench reports
+    for key in ("q1gather1:jacobi:L11", "plain:spmv:L11", "plain:defect:L11"):
+        assert bench.load_traffic(key) is not None, key
+
+
+def test_error_bound_from_residuals():
+    """the Q1 operator's smallest eigenvalue (smooth interior mode) and the bound on
+    the distance of two solutions from their residuals"""
+    import numpy as np
+    lam = bench.q1_lambda_min(11)
+    assert abs(lam - 4.706e-6) < 1e-8
+    keep = {"xir": np.ones(4) * 1.0 + 1e-9, "x64": np.ones(4), "b": np.ones(4) * 2.0, "relres_mixed": 1e-11}
+    e = bench.solution_errors(11, keep, np.ones(4), 2e-11, "test")
+    assert abs(e["mixed_rel_error_vs_reference_fp64"] - 1e-9) < 1e-15
+    assert e["fp64_gpu_rel_error_vs_reference_fp64"] == 0.0
+    assert abs(e["mixed_error_bound_from_residuals"] - 3e-11 * 4.0 / (lam * 2.0)) < 1e-12
 
 
 def test_diverged_numbers_stay_strict_json():

@@ -70,3 +70,19 @@ def test_queue_waits_for_a_free_slot():
     # one slot: requests finish strictly one after another, in arrival order
     done = [got[i].done for i in range(3)]
     assert done[0] < done[1] < done[2]
+
+
+def test_hybrid_server_routes_by_load(oracle):
+    """An idle server solves a lone request on the FP64 MG hierarchy; requests that find
+    others waiting go to the batched engine.  Every result meets its tolerance on the
+    oracle's FP64 operator, whichever path served it."""
+    hyb = serving.HybridServer(serving.PoissonServer(slots=SLOTS, budget_bytes=4e9, keep_results=True),
+                               serving.FP64SequentialServer(levels=(5, 6, 7), keep_results=True))
+    got = serve(hyb, [[make(0, 6, 1e-8)], [], [make(1, 7, 1e-10), make(2, 5, 1e-8), make(3, 6, 1e-10)]])
+    assert sorted(got) == [0, 1, 2, 3]
+    assert hyb.routed["fp64_mg"] == 1 and hyb.routed["batched"] == 3
+    for r in got.values():
+        A = oracle.q1_ell(r.level)
+        b = r.rhs.numpy()[0]
+        res = b - oracle.ell_spmv(A, r.x.numpy()[0])
+        assert np.linalg.norm(res) <= 1.05 * r.tol * np.linalg.norm(b), r.rid

@@ -30,3 +30,38 @@ def test_slot_pool_fits_the_budget():
         assert need <= 0.8 * budget or all(k == 1 for k in slots.values())
         assert set(slots) == set(range(5, 12))
     assert serving.default_slots(120e9)[5] == 32
+
+
+class _FakeBatched:
+    def __init__(self):
+        self.active, self.queue, self.got = {}, {5: collections.deque()}, []
+
+    def submit(self, r):
+        self.got.append(r)
+
+    def pending(self):
+        return 0
+
+    def poll(self, clock, steps=1):
+        return []
+
+
+class _FakeDirect(_FakeBatched):
+    def poll(self, clock, steps=1):
+        return [self.got.pop()] if self.got else []
+
+
+def test_hybrid_routing_rule():
+    """a lone request at an idle server goes to the FP64 MG path, a burst to the batch"""
+    b, d = _FakeBatched(), _FakeDirect()
+    hyb = serving.HybridServer(b, d)
+    hyb.submit("a")
+    assert hyb.poll(lambda: 0.0) == ["a"] and hyb.routed["fp64_mg"] == 1
+    for r in ("b", "c"):
+        hyb.submit(r)
+    hyb.poll(lambda: 0.0)
+    assert b.got == ["b", "c"] and hyb.routed["batched"] == 2
+    b.active = {0: "b"}          # something in flight: even a lone request is batched
+    hyb.submit("d")
+    hyb.poll(lambda: 0.0)
+    assert b.got[-1] == "d" and hyb.routed["fp64_mg"] == 1
