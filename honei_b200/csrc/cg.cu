@@ -263,12 +263,16 @@ namespace hb2
     {
         if (nvec == 0) return HB2_OK;
         bool ok;
+        // the batched preconditioner keeps the standard recurrence: inside the outer
+        // PCG the one-reduction form left some right-hand sides of the 512-system
+        // batch short of their tolerance after 100 steps
+        const int mode = kCgTreeStandard;
         if (A->dtype == HB2_F64 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
+            ok = launch_warp_reg<double, float>(A, b, x, max_iters, eps, mode, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else if (A->dtype == HB2_F64 && vec_dtype == HB2_F64)
-            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
+            ok = launch_warp_reg<double, double>(A, b, x, max_iters, eps, mode, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else if (A->dtype == HB2_F32 && vec_dtype == HB2_F32)
-            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, 0, 0, 0, stream, nvec, vstride, active, list, count, cap);
+            ok = launch_warp_reg<float, float>(A, b, x, max_iters, eps, mode, 0, 0, stream, nvec, vstride, active, list, count, cap);
         else return fail(HB2_ERR_ARG, "batched coarse CG: unsupported element types");
         if (! ok) return fail(HB2_ERR_UNSUPPORTED, "batched coarse CG: the coarsest level needs <= 128 rows and 9 slots");
         count_launches(1);

@@ -14,6 +14,13 @@ namespace hb2
     template <> struct Eps<double> { static __device__ __forceinline__ double v() { return DBL_EPSILON; } };
     template <> struct Eps<float> { static __device__ __forceinline__ float v() { return FLT_EPSILON; } };
 
+    // the `exact` argument of the coarse CG: the reference's sequential fma order
+    // (bit-identical to it); the standard recurrence with tree-ordered dots; the
+    // Chronopoulos-Gear recurrence with one fused reduction per iteration
+    constexpr int kCgTreeOneReduction = 0;
+    constexpr int kCgExact = 1;
+    constexpr int kCgTreeStandard = 2;
+
     template <typename T> struct Recip;
     template <> struct Recip<double> { static __device__ __forceinline__ double rn(double v) { return __drcp_rn(v); } };
     template <> struct Recip<float> { static __device__ __forceinline__ float rn(float v) { return __frcp_rn(v); } };
@@ -110,7 +117,7 @@ namespace hb2
         };
         // dot of per-lane register vectors a, b over the valid rows
         auto dot = [&](const T (&a)[RPL], const T (&bb)[RPL]) -> T {
-            if (exact)
+            if (exact == kCgExact)
             {
 #pragma unroll
                 for (int j = 0; j < RPL; ++j)
@@ -146,7 +153,7 @@ namespace hb2
         const T initial = sqrt(alpha);
         T current = initial;
         uint64_t it = 0, used = 0;
-        if (! exact && max_iters > 0)
+        if (exact == kCgTreeOneReduction && max_iters > 0)
         {
             // Chronopoulos-Gear recurrence (the same iterates as the loop below in
             // exact arithmetic): per iteration one product w = A r and both dots
