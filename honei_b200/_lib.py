@@ -126,6 +126,7 @@ SIGNATURES = {
     "hb2_convert": (_int, [_int, _vp, _int, _vp, _u64, _vp]),
     "hb2_dot": (_int, [_int, _vp, _vp, _u64, _vp, _vp, _vp]),
     "hb2_norm_l2": (_int, [_int, _vp, _u64, _int, _vp, _vp, _vp]),
+    "hb2_dot_ordered": (_int, [_int, _vp, _vp, _u64, _int, _vp, _vp, _vp]),
     "hb2_prolongation": (_int, [_int, _vp, _u64, _vp, _u64, _vp, _vp]),
     "hb2_restriction": (_int, [_int, _vp, _u64, _vp, _u64, _vp, _vp]),
     "hb2_jacobi_ell": (_int, [_vp, _vp, _vp, _vp, _vp, _u64, _vp]),

@@ -150,15 +150,46 @@ namespace hb2
         return launch_dot(dt, x, x, n, root, dev_out, ws, stream);
     }
 
+    // The dot in the reference's tags::CPU order (la/dot_product.hh:72-89: one
+    // sequential chain result += x[i] * y[i], contracted to fma by its compiler, in
+    // the element type), sqrt in the element type for the rooted norm
+    // (la/norm.hh:363-381).  One thread: for callers that need the reference's bits
+    // (the tag binding's exact mode), not for speed.
+    template <typename T>
+    __global__ void dot_ordered_kernel(const T * __restrict__ x, const T * __restrict__ y, uint64_t n, double * out,
+                                       int root)
+    {
+        if (threadIdx.x != 0 || blockIdx.x != 0) return;
+        T s = T(0);
+        uint64_t i = 0;
+        for (; i + 8 <= n; i += 8)
+        {
+            T a[8], b[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { a[k] = x[i + k]; b[k] = y[i + k]; }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s = Arith<T>::fma(a[k], b[k], s);
+        }
+        for (; i < n; ++i) s = Arith<T>::fma(x[i], y[i], s);
+        *out = root ? (double)sqrt(s) : (double)s;
+    }
+
     static int reduce_api(int dt, const void * x, const void * y, uint64_t n, int root, double * dev_out,
-                          double * host_out, cudaStream_t stream)
+                          double * host_out, cudaStream_t stream, bool ordered = false)
     {
         if ((n > 0 && (! x || ! y)) || (! dev_out && ! host_out)) return fail(HB2_ERR_ARG, "reduction: null argument");
         Workspace * ws = 0;
         int st = stream_workspace(stream, &ws);
         if (st) return st;
         double * target = dev_out ? dev_out : ws->scalars;
-        st = launch_dot(dt, x, y, n, root, target, ws, stream);
+        if (ordered)
+        {
+            if (dt == HB2_F64) dot_ordered_kernel<double><<<1, 32, 0, stream>>>((const double *)x, (const double *)y, n, target, root);
+            else dot_ordered_kernel<float><<<1, 32, 0, stream>>>((const float *)x, (const float *)y, n, target, root);
+            count_launches(1);
+            HB2_LAUNCH_CHECK("ordered dot launch");
+        }
+        else st = launch_dot(dt, x, y, n, root, target, ws, stream);
         if (st) return st;
         if (host_out)
         {
@@ -210,3 +241,7 @@ extern "C" int hb2_dot(hb2_dtype dt, const void * x, const void * y, uint64_t n,
 extern "C" int hb2_norm_l2(hb2_dtype dt, const void * x, uint64_t n, int root, double * dev_out, double * host_out,
                            cudaStream_t s)
 { return reduce_api(dt, x, x, n, root, dev_out, host_out, s); }
+
+extern "C" int hb2_dot_ordered(hb2_dtype dt, const void * x, const void * y, uint64_t n, int root, double * dev_out,
+                               double * host_out, cudaStream_t s)
+{ return reduce_api(dt, x, y, n, root, dev_out, host_out, s, true); }

@@ -238,6 +238,13 @@ HB2_API int hb2_dot(hb2_dtype dt, const void *x, const void *y, uint64_t n, doub
             cudaStream_t stream);
 HB2_API int hb2_norm_l2(hb2_dtype dt, const void *x, uint64_t n, int root, double *dev_out, double *host_out,
                 cudaStream_t stream);
+/* DotProduct<tags::CPU> / Norm<vnt_l_two, root, tags::CPU> in the reference's own
+ * summation order (la/dot_product.hh:72-89: one sequential fma chain in the element
+ * type; la/norm.hh:363-381: sqrt in the element type): its bits, at the speed of one
+ * thread.  For bit-for-bit comparisons with the reference; hb2_dot / hb2_norm_l2 are
+ * the fast (tree-ordered) reductions.  Same outputs as hb2_dot. */
+HB2_API int hb2_dot_ordered(hb2_dtype dt, const void *x, const void *y, uint64_t n, int root, double *dev_out,
+                            double *host_out, cudaStream_t stream);
 
 /* ---------------------------------------------------------------- grid transfer */
 /* Matrix-free Prolongation<Tag, NONE> (math/prolongation.hh:42-139) and

@@ -16,11 +16,14 @@ REF      ?= $(HONEI_REFERENCE)
 ifeq ($(strip $(REF)),)
 $(error set REF=<reference checkout> or HONEI_REFERENCE)
 endif
-OUT      := oracle/_ref
+# OUT / OVERLAY: honei_b200/binding/binding.mk builds the same library into its own
+# directory with a header overlay (a directory searched before the tree)
+OUT      ?= oracle/_ref
+OVERLAY  ?=
 OBJ      := $(OUT)/obj
 CXX      ?= g++
 CXXFLAGS := -std=gnu++98 -O3 -march=x86-64-v3 -DHONEI_SSE -fpermissive -w -fPIC \
-            -I$(REF) -DHONEI_SOURCEDIR='"$(REF)"'
+            $(if $(OVERLAY),-I$(OVERLAY)) -I$(REF) -DHONEI_SOURCEDIR='"$(REF)"'
 
 UTIL_SRC := assertion barrier benchmark_info condition_variable configuration exception \
             lock log memory_arbiter memory_backend memory_pool mutex partitioner \
@@ -71,7 +74,9 @@ $(OUT)/honei_oracle.o: oracle/honei_oracle.c oracle/honei_oracle.h | $(OBJ)
 $(OUT)/honei_ref: $(OUT)/ref_driver.o $(OUT)/honei_oracle.o $(OUT)/libhonei_ref.a
 	$(CXX) -o $@ $(OUT)/ref_driver.o $(OUT)/honei_oracle.o -Wl,--whole-archive $(OUT)/libhonei_ref.a -Wl,--no-whole-archive -lpthread -lm
 
+lib: $(OUT)/libhonei_ref.a
+
 clean:
 	rm -rf $(OUT)
 
-.PHONY: all clean
+.PHONY: all lib clean
