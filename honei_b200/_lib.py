@@ -86,9 +86,12 @@ SIGNATURES = {
     "hb2_ell_export": (_int, [_vp, _vp, _vp, _vp]),
     "hb2_ell_layout": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "hb2_ell_layout_variant": (_int, [_vp, _int, ctypes.POINTER(_int), ctypes.POINTER(_int), ctypes.POINTER(_int)]),
+    "hb2_ell_launch_shape": (_int, [_vp, _int, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "hb2_ell_read": (_int, [_pvp, ctypes.c_char_p, _int, _vp]),
     "hb2_ell_write": (_int, [_vp, ctypes.c_char_p]),
     "hb2_ell_transpose": (_int, [_pvp, _vp, _vp]),
+    "hb2_ell_create_bf16": (_int, [_pvp, _vp, _int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                   _vp]),
     "hb2_lmg_create": (_int, [_pvp, ctypes.c_uint, ctypes.c_uint, _vp, _vp, _vp]),
     "hb2_lmg_destroy": (_int, [_vp]),
     "hb2_lmg_solve": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),

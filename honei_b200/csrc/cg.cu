@@ -484,9 +484,10 @@ extern "C" int hb2_cg_solve(hb2_ell A, const void * b, void * x, uint64_t max_it
     else
     {
         void * tmp = 0;
-        HB2_CUDA(cudaMallocAsync(&tmp, 3 * n * es + 64, stream));
+        const size_t vb = (n * es + 255) / 256 * 256;   // each vector 256-byte aligned
+        HB2_CUDA(cudaMallocAsync(&tmp, 3 * vb + 64, stream));
         char * base = (char *)tmp;
-        void * r = base, * p = base + n * es, * v = base + 2 * n * es;
+        void * r = base, * p = base + vb, * v = base + 2 * vb;
         int dev = 0, per_sm = 0;
         cudaGetDevice(&dev);
         if (A->dtype == HB2_F64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_coop_kernel<double>, kCoopThreads, 0);

@@ -57,9 +57,14 @@ namespace hb2
         }
     }
 
-    // One thread: R consecutive rows; KT = compile-time slot count (0: runtime).
-    template <typename T, int KT, int MODE>
-    __global__ void __launch_bounds__(kEllThreads)
+    // One thread (TPR = 1) or a pair of adjacent lanes (TPR = 2): R consecutive
+    // rows; KT = compile-time slot count (0: runtime).  With two lanes per row
+    // the lanes load alternate slots (the even lane 0, 2, 4, ..., the odd one
+    // 1, 3, 5, ...) and form their products; the odd lane's products move to the
+    // even lane by shuffle, which adds all of them in slot order, so the sums are
+    // the one-lane kernel's bit for bit.  The even lane runs the epilogue.
+    template <typename T, int KT, int MODE, int TPR>
+    __global__ void __launch_bounds__(kEllMaxThreads)
     ell_kernel(EllView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
                const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
                int flags, Batch bt)
@@ -85,11 +90,14 @@ namespace hb2
         const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
         const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
         const bool keep = (flags & kKeepL2) != 0;
-        const uint64_t r0 = (blk * blockDim.x + threadIdx.x) * R;
+        const uint64_t r0 = (blk * (blockDim.x / TPR) + threadIdx.x / TPR) * R;
         const int K = KT > 0 ? KT : (int)A.K;
+        const int lane2 = TPR == 2 ? (int)(threadIdx.x & 1) : 0;
         T acc[R];
 #pragma unroll
         for (int i = 0; i < R; ++i) acc[i] = T(0);
+        if constexpr (TPR == 1)
+        {
         if (r0 < A.rows)
         {
             const T * vp = A.val + r0;
@@ -122,12 +130,51 @@ namespace hb2
                 }
             }
         }
+        }
+        else
+        {
+            // both lanes of a pair run every shuffle (the whole warp does: r0 and K
+            // are the same for the pair, the loads are guarded instead)
+            const bool live = r0 < A.rows;
+            const T * vp = A.val + (live ? r0 : 0);
+            const int32_t * cp = A.col + (live ? r0 : 0);
+            constexpr int KH = KT > 0 ? (KT + 1) / 2 : 1;
+            const int kh = (K + 1) / 2;
+#pragma unroll (KT > 0 ? KH : 1)
+            for (int h = 0; h < kh; ++h)
+            {
+                const int k = 2 * h + lane2;
+                T v[R], pr[R];
+                int c[R];
+                if (live && k < K) load_slot<T, R>(vp + (uint64_t)k * A.ld, cp + (uint64_t)k * A.ld, v, c, keep);
+                else
+                {
+#pragma unroll
+                    for (int i = 0; i < R; ++i) { v[i] = T(0); c[i] = -1; }
+                }
+                unsigned ok = 0;
+#pragma unroll
+                for (int i = 0; i < R; ++i)
+                {
+                    pr[i] = c[i] >= 0 ? M::mul(v[i], __ldg(x + c[i])) : T(0);
+                    ok |= c[i] >= 0 ? 1u << i : 0u;
+                }
+                const unsigned ok_odd = __shfl_down_sync(0xffffffffu, ok, 1);
+#pragma unroll
+                for (int i = 0; i < R; ++i)
+                {
+                    const T odd = __shfl_down_sync(0xffffffffu, pr[i], 1);
+                    if (ok & (1u << i)) acc[i] = M::add(acc[i], pr[i]);             // slot 2h
+                    if (ok_odd & (1u << i)) acc[i] = M::add(acc[i], odd);           // slot 2h + 1
+                }
+            }
+        }
         double part = 0.0;
 #pragma unroll
         for (int i = 0; i < R; ++i)
         {
             const uint64_t r = r0 + i;
-            if (r >= A.rows) break;
+            if (r >= A.rows || lane2) break;
             if (MODE == kPlain) y[r] = acc[i];
             else if (MODE == kDefect)
             {
@@ -153,38 +200,47 @@ namespace hb2
         }
     }
 
-    template <typename T, int MODE>
-    static void launch_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
-                            void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
-                            int flags, Batch b)
+    template <typename T, int MODE, int TPR>
+    static void launch_shape(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
+                             void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
+                             int flags, Batch b, unsigned bs)
     {
         EllView<T> v = A->view<T>();
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         if (A->K == 9)
-            launch_pdl(ell_kernel<T, 9, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+            launch_pdl(ell_kernel<T, 9, MODE, TPR>, grid, dim3(bs), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
                        (T *)zero, rs, red, want_sqrt, flags, b);
         else if (A->K == 4)
-            launch_pdl(ell_kernel<T, 4, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+            launch_pdl(ell_kernel<T, 4, MODE, TPR>, grid, dim3(bs), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
                        (T *)zero, rs, red, want_sqrt, flags, b);
         else
-            launch_pdl(ell_kernel<T, 0, MODE>, grid, dim3(kEllThreads), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
+            launch_pdl(ell_kernel<T, 0, MODE, TPR>, grid, dim3(bs), 0, s, v, xp, yp, (const T *)aux, (const T *)aux2,
                        (T *)zero, rs, red, want_sqrt, flags, b);
+    }
+
+    template <typename T, int MODE>
+    static void launch_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
+                            void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
+                            int flags, Batch b, unsigned bs, int tpr)
+    {
+        if (tpr == 2) launch_shape<T, MODE, 2>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, flags, b, bs);
+        else launch_shape<T, MODE, 1>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, flags, b, bs);
     }
 
     template <typename T>
     static void launch_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                              const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs,
-                             dim3 grid, cudaStream_t s, int f, Batch b)
+                             dim3 grid, cudaStream_t s, int f, Batch b, unsigned bs, int tpr)
     {
         switch (mode)
         {
-            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kPlain: launch_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
+            case kDefect: launch_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
+            case kDot: launch_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
+            case kAdd: launch_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
+            case kJacobi: launch_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
+            case kRestrict: launch_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, tpr); break;
         }
     }
 
@@ -203,12 +259,31 @@ namespace hb2
         return cap;
     }
 
-    uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)
+    // rows per block of a launch of bs threads on the class's layout
+    static uint64_t rows_per_block(const hb2_ell_s * A, int cls, uint64_t bs)
+    {
+        if (A->layout[cls] == kLayoutPattern) return bs * (A->rpt[cls] & ~kPatFlags);
+        if (A->layout[cls] == kLayoutCompact) return bs * (cls ? A->compact_rpt_red : A->compact_rpt);
+        if (A->layout[cls] == kLayoutBF16) return bs * A->rpt[cls];
+        return bs / A->tpr[cls] * (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
+    }
+
+    // the tuned block size where the class's kernel takes one (plain, compressed,
+    // the Q1 gather form), else 256
+    bool ell_shape_tunable(const hb2_ell_s * A, int cls)
+    {
+        return A->layout[cls] != kLayoutPattern || (A->rpt[cls] & kPatQ1G);
+    }
+
+    unsigned ell_block(const hb2_ell_s * A, bool reducing)
     {
         const int cls = reducing ? 1 : 0;
-        if (A->layout[cls] == kLayoutPattern) return (uint64_t)kEllThreads * (A->rpt[cls] & ~kPatFlags);
-        if (A->layout[cls] == kLayoutCompact) return (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt);
-        return (uint64_t)kEllThreads * (A->dtype == HB2_F64 ? RowsPerThread<double>::value : RowsPerThread<float>::value);
+        return ell_shape_tunable(A, cls) ? (unsigned)A->bs[cls] : (unsigned)kEllThreads;
+    }
+
+    uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)
+    {
+        return rows_per_block(A, reducing ? 1 : 0, ell_block(A, reducing));
     }
 
     unsigned ell_grid(const hb2_ell_s * A, bool reducing) { return ceil_div(A->rows, ell_rows_per_block(A, reducing)); }
@@ -232,7 +307,12 @@ namespace hb2
             if (red) HB2_CUDA(cudaMemsetAsync(red, 0, sizeof(double), stream));
             return HB2_OK;
         }
-        const unsigned gx = ell_grid(A, red != 0);
+        // the launch shape: the class's tuned one, except where a Q1 gather layout
+        // hands this launch to the general row-pattern kernel (256 threads)
+        const int cls = red != 0;
+        unsigned bs = ell_block(A, red != 0);
+        if (A->layout[cls] == kLayoutPattern && ! ell_q1_stencil_applies(A, mode, x, A->rpt[cls], b)) bs = kEllThreads;
+        const unsigned gx = (unsigned)ceil_div(A->rows, rows_per_block(A, cls, bs));
         if (b.nvec == 0 || b.nvec > 65535) return fail(HB2_ERR_ARG, "ELL batch: 1..65535 vectors");
         dim3 grid(gx, b.nvec);
         if (b.list)
@@ -259,13 +339,15 @@ namespace hb2
         if (A->q1_transfer && ! red && b.nvec == 1 && ! b.list && ! b.active &&
             (mode == kPlain || mode == kAdd || mode == kRestrict) && q1_transfer_kernels_enabled())
             return launch_q1_transfer(A, mode, x, y, zero, stream);
-        const int cls = red != 0;
         if (A->layout[cls] == kLayoutPattern)
-            launch_ell_pattern(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, A->rpt[cls]);
+            launch_ell_pattern(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, A->rpt[cls], bs);
         else if (A->layout[cls] == kLayoutCompact)
-            launch_ell_compact(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
-        else if (A->dtype == HB2_F64) launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
-        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+            launch_ell_compact(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs);
+        else if (A->layout[cls] == kLayoutBF16)
+            launch_ell_bf16(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs);
+        else if (A->dtype == HB2_F64)
+            launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs, A->tpr[cls]);
+        else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs, A->tpr[cls]);
         count_launches(1);
         HB2_LAUNCH_CHECK("ell kernel launch");
         return HB2_OK;
@@ -502,17 +584,20 @@ extern "C" int hb2_ell_create(hb2_ell * out, hb2_dtype dtype, uint64_t rows, uin
     cudaError_t e = cudaSuccess;
     if (host_ptrs && rows > 0)
     {
-        size_t bytes = nslots * 8 + nslots * es + rows * 8;
+        // Aj | Ax | Arl, each part 256-byte aligned (an F32 Ax of an odd slot count
+        // would leave the uint64 Arl 4-byte aligned)
+        const size_t ax_off = nslots * 8, arl_off = (ax_off + nslots * es + 255) / 256 * 256;
+        size_t bytes = arl_off + rows * 8;
         e = cudaMalloc(&tmp, bytes);
         if (e == cudaSuccess)
         {
             char * p = (char *)tmp;
             cudaMemcpyAsync(p, Aj, nslots * 8, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(p + nslots * 8, Ax, nslots * es, cudaMemcpyHostToDevice, stream);
-            e = cudaMemcpyAsync(p + nslots * 8 + nslots * es, Arl, rows * 8, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(p + ax_off, Ax, nslots * es, cudaMemcpyHostToDevice, stream);
+            e = cudaMemcpyAsync(p + arl_off, Arl, rows * 8, cudaMemcpyHostToDevice, stream);
             dAj = (const uint64_t *)p;
-            dAx = p + nslots * 8;
-            dArl = (const uint64_t *)(p + nslots * 8 + nslots * es);
+            dAx = p + ax_off;
+            dArl = (const uint64_t *)(p + arl_off);
         }
     }
     if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int));
@@ -642,6 +727,7 @@ extern "C" int hb2_ell_destroy(hb2_ell A)
     cudaFree(A->col);
     ell_free_compact(A);
     ell_free_pattern(A);
+    ell_free_bf16(A);
     cudaFree(A->spat);
     cudaFree(A->sptab);
     delete A;
@@ -657,7 +743,7 @@ extern "C" int hb2_ell_info(hb2_ell A, uint64_t * rows, uint64_t * cols, uint64_
     if (stride) *stride = A->ref_stride;
     if (K) *K = A->ref_K;
     if (threads) *threads = A->ref_T;
-    if (device_bytes) *device_bytes = A->bytes + A->compact_bytes + A->pattern_bytes;
+    if (device_bytes) *device_bytes = A->bytes + A->compact_bytes + A->pattern_bytes + A->bf16_bytes;
     return HB2_OK;
 }
 
@@ -667,7 +753,11 @@ extern "C" int hb2_ell_layout(hb2_ell A, int * layout, uint32_t * table_size, ui
     const int l = A->layout[0];
     if (layout) *layout = l;
     if (table_size) *table_size = l == kLayoutPattern ? A->npat : (l == kLayoutCompact ? A->ntable : 0u);
-    if (row_bytes) *row_bytes = l == kLayoutPattern ? 1u : A->K * (l == kLayoutCompact ? 3u : (uint32_t)(dtype_size(A->dtype) + 4));
+    if (row_bytes)
+        *row_bytes = l == kLayoutPattern   ? 1u
+                     : l == kLayoutBF16    ? A->K * (A->bform == 0 ? 4u : 6u) + (A->bdiag ? 4u : 0u)
+                     : l == kLayoutCompact ? A->K * 3u
+                                           : A->K * (uint32_t)(dtype_size(A->dtype) + 4);
     return HB2_OK;
 }
 
@@ -677,7 +767,7 @@ extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * ro
     if (cls != 0 && cls != 1) return fail(HB2_ERR_ARG, "hb2_ell_layout_variant: class must be 0 or 1");
     const int l = A->layout[cls];
     if (layout) *layout = l;
-    if (rows_per_thread) *rows_per_thread = (int)(ell_rows_per_block(A, cls == 1) / kEllThreads);
+    if (rows_per_thread) *rows_per_thread = (int)(ell_rows_per_block(A, cls == 1) * A->tpr[cls] / ell_block(A, cls == 1));
     if (windowed)
         *windowed = l != kLayoutPattern ? 0 : (A->rpt[cls] & kPatWin) ? 1 : (A->rpt[cls] & kPatQ1) ? 2
                                                                       : (A->rpt[cls] & kPatQ1G) ? 3
@@ -685,12 +775,23 @@ extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * ro
     return HB2_OK;
 }
 
+extern "C" int hb2_ell_launch_shape(hb2_ell A, int cls, int * block_threads, int * threads_per_row)
+{
+    if (! A) return fail(HB2_ERR_ARG, "hb2_ell_launch_shape: null matrix");
+    if (cls != 0 && cls != 1) return fail(HB2_ERR_ARG, "hb2_ell_launch_shape: class must be 0 or 1");
+    if (block_threads) *block_threads = (int)ell_block(A, cls == 1);
+    if (threads_per_row) *threads_per_row = A->layout[cls] == kLayoutPlain ? A->tpr[cls] : 1;
+    return HB2_OK;
+}
+
 extern "C" int hb2_ell_export(hb2_ell A, uint64_t * Aj, void * Ax, uint64_t * Arl)
 {
     if (! A || ! Aj || ! Ax || ! Arl) return fail(HB2_ERR_ARG, "hb2_ell_export: null argument");
     size_t nslots = A->ref_K * A->ref_stride, es = dtype_size(A->dtype);
+    // Aj | Ax | Arl in one buffer, Arl 256-byte aligned
+    const size_t arl_off = (nslots * 8 + nslots * es + 255) / 256 * 256;
     void * d = 0;
-    HB2_CUDA(cudaMalloc(&d, nslots * 8 + nslots * es + A->rows * 8 + 16));
+    HB2_CUDA(cudaMalloc(&d, arl_off + A->rows * 8 + 16));
     char * p = (char *)d;
     cudaError_t e = cudaMemset(p, 0, nslots * 8 + nslots * es);
     if (e == cudaSuccess && A->rows > 0)
@@ -699,17 +800,17 @@ extern "C" int hb2_ell_export(hb2_ell A, uint64_t * Aj, void * Ax, uint64_t * Ar
         if (A->dtype == HB2_F64)
             ell_to_ref_kernel<double><<<grid, 256>>>((const double *)A->val, A->col, A->rows, A->ld, A->K, A->ref_stride,
                                                      A->ref_T, (uint64_t *)p, (double *)(p + nslots * 8),
-                                                     (uint64_t *)(p + nslots * 8 + nslots * es));
+                                                     (uint64_t *)(p + arl_off));
         else
             ell_to_ref_kernel<float><<<grid, 256>>>((const float *)A->val, A->col, A->rows, A->ld, A->K, A->ref_stride,
                                                     A->ref_T, (uint64_t *)p, (float *)(p + nslots * 8),
-                                                    (uint64_t *)(p + nslots * 8 + nslots * es));
+                                                    (uint64_t *)(p + arl_off));
         count_launches(1);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(Aj, p, nslots * 8, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(Ax, p + nslots * 8, nslots * es, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && A->rows > 0) e = cudaMemcpy(Arl, p + nslots * 8 + nslots * es, A->rows * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && A->rows > 0) e = cudaMemcpy(Arl, p + arl_off, A->rows * 8, cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) return cuda_status(e, "hb2_ell_export");
     return HB2_OK;

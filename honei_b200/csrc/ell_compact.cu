@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -30,6 +31,7 @@ namespace hb2
     constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
     constexpr int kCompactRowsMax = 8;                // rows per thread: 2, 4 or 8 (autotuned)
     constexpr uint64_t kCompactMinRows = 32768;       // smaller matrices stay plain
+    constexpr uint64_t kShapeMinRows = 4096;          // smaller ones also keep the default launch shape
 
     template <typename T> __device__ __forceinline__ unsigned long long key_of(T v);
     template <> __device__ __forceinline__ unsigned long long key_of<double>(double v) { return (unsigned long long)__double_as_longlong(v); }
@@ -163,7 +165,7 @@ namespace hb2
     }
 
     template <typename T, int KT, int MODE, int R>
-    __global__ void __launch_bounds__(kEllThreads)
+    __global__ void __launch_bounds__(kEllMaxThreads)
     ell_compact_kernel(EllCompactView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
                        const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
                        int flags, Batch bt)
@@ -272,7 +274,7 @@ namespace hb2
     template <typename T, int MODE>
     static void compact_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
                              void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
-                             int flags, Batch b)
+                             int flags, Batch b, unsigned bs)
     {
         EllCompactView<T> v;
         v.code = A->code;
@@ -290,7 +292,7 @@ namespace hb2
         const T * a2 = (const T *)aux2;
         T * zp = (T *)zero;
 #define HB2_COMPACT_LAUNCH(KT_, R_)                                                                          \
-        launch_pdl(ell_compact_kernel<T, KT_, MODE, R_>, grid, dim3(kEllThreads), 0, s, v, xp, yp, ap, a2, zp, rs, \
+        launch_pdl(ell_compact_kernel<T, KT_, MODE, R_>, grid, dim3(bs), 0, s, v, xp, yp, ap, a2, zp, rs, \
                    red, want_sqrt, flags, b)
         const int R = red ? A->compact_rpt_red : A->compact_rpt;
         if (A->K == 9) { if (R == 2) HB2_COMPACT_LAUNCH(9, 2); else if (R == 4) HB2_COMPACT_LAUNCH(9, 4); else HB2_COMPACT_LAUNCH(9, 8); }
@@ -302,30 +304,25 @@ namespace hb2
     template <typename T>
     static void compact_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                               const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                              cudaStream_t s, int f, Batch b)
+                              cudaStream_t s, int f, Batch b, unsigned bs)
     {
         switch (mode)
         {
-            case kPlain: compact_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kDefect: compact_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kDot: compact_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kAdd: compact_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kJacobi: compact_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
-            case kRestrict: compact_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b); break;
+            case kPlain: compact_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kDefect: compact_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kDot: compact_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kAdd: compact_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kJacobi: compact_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kRestrict: compact_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
         }
-    }
-
-    unsigned compact_grid(const hb2_ell_s * A, bool reducing)
-    {
-        return ceil_div(A->rows, (uint64_t)kEllThreads * (reducing ? A->compact_rpt_red : A->compact_rpt));
     }
 
     void launch_ell_compact(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                             const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                            cudaStream_t stream, int flags, Batch b)
+                            cudaStream_t stream, int flags, Batch b, unsigned bs)
     {
-        if (A->dtype == HB2_F64) compact_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
-        else compact_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b);
+        if (A->dtype == HB2_F64) compact_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs);
+        else compact_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs);
     }
 
     static bool compact_enabled()
@@ -415,10 +412,12 @@ namespace hb2
 
     // Autotuner: time y = A x and the defect with its fused norm on every layout
     // the matrix admits -- plain; compressed with 2, 4 or 8 rows per thread;
-    // row patterns with 1, 2 or 4 rows per thread -- (three timed launches
-    // each, after one warm-up) and keep the fastest for each of the two kernel
-    // classes; the arrays of a layout neither class uses are freed.  Runs once
-    // per matrix shape and process, at creation, on `stream`.
+    // row patterns with 1, 2 or 4 rows per thread (and the Q1 gather form) --
+    // and keep the fastest for each of the two kernel classes; then time the
+    // winner's launch shape: blocks of 128, 256 or 512 threads where its kernel
+    // takes them (plain, compressed, Q1 gather), and on the plain layout one or
+    // two threads per row.  The arrays of a layout neither class uses are
+    // freed.  Runs once per matrix shape and process, at creation, on `stream`.
     //
     // The decision is kept per (device, element type, shape, slots, table size)
     // for the life of the process: matrices of one shape always run the same
@@ -429,15 +428,16 @@ namespace hb2
         int device, dtype;
         uint64_t rows, cols;
         uint32_t K, ntable, npat;
+        uint32_t kind;   // 0, or for the BF16 layout 1 + 2 * form + compensated
         bool operator<(const TuneKey & o) const
         {
-            return std::tie(device, dtype, rows, cols, K, ntable, npat) <
-                   std::tie(o.device, o.dtype, o.rows, o.cols, o.K, o.ntable, o.npat);
+            return std::tie(device, dtype, rows, cols, K, ntable, npat, kind) <
+                   std::tie(o.device, o.dtype, o.rows, o.cols, o.K, o.ntable, o.npat, o.kind);
         }
     };
     struct Choice
     {
-        int layout[2], rpt[2];
+        int layout[2], rpt[2], bs[2], tpr[2];
     };
     static std::mutex g_tune_mutex;
     static std::map<TuneKey, Choice> g_tune;
@@ -458,8 +458,9 @@ namespace hb2
         TuneKey k;
         Choice c;
         unsigned long long rows, cols;
-        while (fscanf(f, "%d %d %llu %llu %u %u %u %d %d %d %d", &k.device, &k.dtype, &rows, &cols, &k.K, &k.ntable,
-                      &k.npat, &c.layout[0], &c.rpt[0], &c.layout[1], &c.rpt[1]) == 11)
+        while (fscanf(f, "%d %d %llu %llu %u %u %u %u %d %d %d %d %d %d %d %d", &k.device, &k.dtype, &rows, &cols,
+                      &k.K, &k.ntable, &k.npat, &k.kind, &c.layout[0], &c.rpt[0], &c.layout[1], &c.rpt[1], &c.bs[0],
+                      &c.tpr[0], &c.bs[1], &c.tpr[1]) == 16)
         {
             k.rows = rows;
             k.cols = cols;
@@ -474,9 +475,31 @@ namespace hb2
         if (! path || ! *path) return;
         FILE * f = fopen(path, "a");
         if (! f) return;
-        fprintf(f, "%d %d %llu %llu %u %u %u %d %d %d %d\n", k.device, k.dtype, (unsigned long long)k.rows,
-                (unsigned long long)k.cols, k.K, k.ntable, k.npat, c.layout[0], c.rpt[0], c.layout[1], c.rpt[1]);
+        fprintf(f, "%d %d %llu %llu %u %u %u %u %d %d %d %d %d %d %d %d\n", k.device, k.dtype,
+                (unsigned long long)k.rows, (unsigned long long)k.cols, k.K, k.ntable, k.npat, k.kind, c.layout[0],
+                c.rpt[0], c.layout[1], c.rpt[1], c.bs[0], c.tpr[0], c.bs[1], c.tpr[1]);
         fclose(f);
+    }
+
+    // HB2_ELL_BLOCK=128|256|512 and HB2_ELL_TPR=1|2 override the tuned launch
+    // shape (threads per row on the plain layout only); read at each matrix
+    // creation
+    static int shape_pin(const char * name, int a, int b, int c)
+    {
+        const char * v = getenv(name);
+        const int p = v && *v ? atoi(v) : 0;
+        return (p == a || p == b || p == c) ? p : 0;
+    }
+
+    static void apply_shape_pins(hb2_ell_s * A)
+    {
+        const int bs = shape_pin("HB2_ELL_BLOCK", 128, 256, 512), tpr = shape_pin("HB2_ELL_TPR", 1, 2, 1);
+        for (int cls = 0; cls < 2; ++cls)
+        {
+            if (bs) A->bs[cls] = bs;
+            if (tpr && A->layout[cls] == kLayoutPlain) A->tpr[cls] = tpr;
+            if (A->layout[cls] != kLayoutPlain) A->tpr[cls] = 1;
+        }
     }
 
     static void apply_choice(hb2_ell_s * A, const Choice & c)
@@ -485,6 +508,8 @@ namespace hb2
         {
             A->layout[cls] = c.layout[cls];
             A->rpt[cls] = c.rpt[cls];
+            A->bs[cls] = c.bs[cls];
+            A->tpr[cls] = c.tpr[cls];
         }
         if (c.layout[0] == kLayoutCompact) A->compact_rpt = c.rpt[0];
         if (c.layout[1] == kLayoutCompact) A->compact_rpt_red = c.rpt[1];
@@ -494,11 +519,13 @@ namespace hb2
             A->compact_bytes = 0;
         }
         if (c.layout[0] != kLayoutPattern && c.layout[1] != kLayoutPattern) ell_free_pattern(A);
+        apply_shape_pins(A);
     }
 
     static int autotune(hb2_ell_s * A, cudaStream_t s)
     {
-        const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable, A->npat};
+        const TuneKey key = {A->device, A->dtype, A->rows, A->cols, A->K, A->ntable, A->npat,
+                             A->bval ? 1u + 2u * (uint32_t)A->bform + (A->bdiag ? 1u : 0u) : 0u};
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
             tune_file_load();
@@ -514,17 +541,29 @@ namespace hb2
         Workspace * ws = 0;
         int st = square ? stream_workspace(s, &ws) : HB2_OK;
         if (st) return st;
+        // One launch reads and writes a set of four vectors.  Where a set fills half
+        // of L2 or more, consecutive launches in a solver find little of it in L2, so
+        // the bursts rotate over enough sets to exceed twice L2 and the candidates
+        // are timed against DRAM; smaller sets stay L2-resident in the solvers and are
+        // timed that way (one set).
         void * buf = 0;
         const size_t vb = ((std::max(A->rows, A->cols) * es + 255) / 256) * 256;
-        HB2_CUDA(cudaMalloc(&buf, 4 * vb + 256));
-        HB2_CUDA(cudaMemsetAsync(buf, 0, 4 * vb + 256, s));
-        void * xv = buf, * yv = (char *)buf + vb, * bv = (char *)buf + 2 * vb, * pv = (char *)buf + 3 * vb;
-        double * nrm = (double *)((char *)buf + 4 * vb);
+        int l2 = 0;
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, A->device);
+        const size_t set = 4 * vb, l2b = l2 > 0 ? (size_t)l2 : ((size_t)126 << 20);
+        const int nsets = set >= l2b / 2 ? (int)std::min<size_t>(8, (2 * l2b + set - 1) / set) : 1;
+        HB2_CUDA(cudaMalloc(&buf, nsets * set + 256));
+        HB2_CUDA(cudaMemsetAsync(buf, 0, nsets * set + 256, s));
+        double * nrm = (double *)((char *)buf + nsets * set);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        std::vector<std::pair<int, int>> variants = {{kLayoutPlain, 0}, {kLayoutCompact, 2}, {kLayoutCompact, 4},
-                                                     {kLayoutCompact, 8}};
+        // a BF16 matrix runs on its BF16 arrays (1, 2, 4 or 8 rows per thread)
+        std::vector<std::pair<int, int>> variants = {{A->bval ? (int)kLayoutBF16 : (int)kLayoutPlain, A->bval ? 1 : 0}};
+        if (A->bval)
+            for (int r : {2, 4, 8}) variants.push_back(std::make_pair((int)kLayoutBF16, r));
+        if (A->code)
+            for (int r : {2, 4, 8}) variants.push_back(std::make_pair((int)kLayoutCompact, r));
         if (A->pat)
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         if (A->pat && A->pat_win_m)
@@ -538,19 +577,12 @@ namespace hb2
         // the candidates interleaved over several rounds so that clock or
         // neighbour drift hits all of them; a candidate's time is its best round.
         constexpr int kRounds = 4, kBurst = 8;
-        Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}};
-        for (int cls = 0; cls < (square ? 2 : 1) && ! st; ++cls)
-        {
-            std::vector<float> best(variants.size(), 1e30f);
-            auto select = [&](const std::pair<int, int> & v) {
-                A->layout[cls] = v.first;
-                A->rpt[cls] = v.second;
-                if (v.first == kLayoutCompact) (cls ? A->compact_rpt_red : A->compact_rpt) = v.second;
-            };
+        auto fastest = [&](int cls, size_t count, const std::function<void(size_t)> & select) -> size_t {
+            std::vector<float> best(count, 1e30f);
             for (int round = 0; round <= kRounds && ! st; ++round)   // round 0 warms up
-                for (size_t vi = 0; vi < variants.size() && ! st; ++vi)
+                for (size_t vi = 0; vi < count && ! st; ++vi)
                 {
-                    select(variants[vi]);
+                    select(vi);
                     // a fused reduction needs one partial per row block: shapes beyond
                     // the workspace are not candidates
                     if (cls == 1 && (uint64_t)ell_grid(A, true) > ws->max_blocks) continue;
@@ -559,9 +591,13 @@ namespace hb2
                     // multigrid's eight passes per level and cycle), of a rectangular
                     // one on the product
                     for (int b = 0; b < kBurst && ! st; ++b)
+                    {
+                        char * v = (char *)buf + (b % nsets) * set;
+                        void * xv = v, * yv = v + vb, * bv = v + 2 * vb, * pv = v + 3 * vb;
                         st = cls == 1 ? launch_ell(A, kDefect, xv, yv, bv, 0, 0, nrm, 0, ws, s)
                              : square ? launch_ell(A, kJacobi, xv, yv, bv, pv, 0, 0, 0, 0, s)
                                       : launch_ell(A, kPlain, xv, yv, 0, 0, 0, 0, 0, 0, s);
+                    }
                     cudaEventRecord(e1, s);
                     if (st) break;
                     cudaEventSynchronize(e1);
@@ -569,14 +605,38 @@ namespace hb2
                     cudaEventElapsedTime(&ms, e0, e1);
                     if (round > 0 && ms < best[vi]) best[vi] = ms;
                 }
-            float best_ms = 1e30f;
-            for (size_t vi = 0; vi < variants.size(); ++vi)
-                if (best[vi] < best_ms)
-                {
-                    best_ms = best[vi];
-                    c.layout[cls] = variants[vi].first;
-                    c.rpt[cls] = variants[vi].second;
-                }
+            size_t w = 0;
+            for (size_t vi = 1; vi < count; ++vi)
+                if (best[vi] < best[w]) w = vi;
+            return w;
+        };
+        Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}, {kEllThreads, kEllThreads}, {1, 1}};
+        for (int cls = 0; cls < (square ? 2 : 1) && ! st; ++cls)
+        {
+            // stage 1: layout and rows per thread, 256 threads per block, one per row
+            A->bs[cls] = kEllThreads;
+            A->tpr[cls] = 1;
+            auto select = [&](const std::pair<int, int> & v) {
+                A->layout[cls] = v.first;
+                A->rpt[cls] = v.second;
+                if (v.first == kLayoutCompact) (cls ? A->compact_rpt_red : A->compact_rpt) = v.second;
+            };
+            const size_t w = variants.size() > 1 ? fastest(cls, variants.size(), [&](size_t i) { select(variants[i]); }) : 0;
+            select(variants[w]);
+            c.layout[cls] = variants[w].first;
+            c.rpt[cls] = variants[w].second;
+            // stage 2: the winner's launch shape
+            if (st || ! ell_shape_tunable(A, cls)) continue;   // a kernel of fixed shape
+            std::vector<std::pair<int, int>> shapes;
+            for (int bs : {128, 256, 512})
+                for (int tpr : {1, 2})
+                    if (tpr == 1 || A->layout[cls] == kLayoutPlain) shapes.push_back(std::make_pair(bs, tpr));
+            const size_t sw = fastest(cls, shapes.size(), [&](size_t i) {
+                A->bs[cls] = shapes[i].first;
+                A->tpr[cls] = shapes[i].second;
+            });
+            c.bs[cls] = shapes[sw].first;
+            c.tpr[cls] = shapes[sw].second;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -587,6 +647,8 @@ namespace hb2
         {
             c.layout[1] = c.layout[0];
             c.rpt[1] = c.rpt[0];
+            c.bs[1] = c.bs[0];
+            c.tpr[1] = c.tpr[0];
         }
         {
             std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -598,11 +660,40 @@ namespace hb2
         return HB2_OK;
     }
 
+    int ell_autotune(hb2_ell_s * A, cudaStream_t stream)
+    {
+        // HB2_ELL_COMPACT=bf16r1|bf16r2|bf16r4|bf16r8: a BF16 matrix with that many rows per
+        // thread, no timing
+        const char * v = getenv("HB2_ELL_COMPACT");
+        if (A->bval && v && strncmp(v, "bf16r", 5) == 0)
+        {
+            const int r = atoi(v + 5);
+            A->rpt[0] = A->rpt[1] = (r == 1 || r == 2 || r == 8) ? r : 4;
+            apply_shape_pins(A);
+            return HB2_OK;
+        }
+        if (A->rows < kShapeMinRows)
+        {
+            apply_shape_pins(A);
+            return HB2_OK;
+        }
+        return autotune(A, stream);
+    }
+
     int ell_build_compact(hb2_ell_s * A, cudaStream_t stream)
     {
-        if (! compact_enabled() || A->rows < kCompactMinRows) return HB2_OK;
+        // HB2_ELL_COMPACT=0 and matrices below kShapeMinRows: the plain layout in its
+        // default (or pinned) shape, no timing; below kCompactMinRows, or without a
+        // compressed form: the plain layout's shape is timed
+        if (! compact_enabled() || A->rows < kShapeMinRows)
+        {
+            apply_shape_pins(A);
+            return HB2_OK;
+        }
+        if (A->rows < kCompactMinRows) return autotune(A, stream);
         int st = A->dtype == HB2_F64 ? build_compact_typed<double>(A, stream) : build_compact_typed<float>(A, stream);
-        if (st || ! A->code) return st;
+        if (st) return st;
+        if (! A->code) return autotune(A, stream);
         st = ell_build_pattern(A, stream);
         if (st) return st;
         const char * v = getenv("HB2_ELL_COMPACT");
@@ -615,8 +706,8 @@ namespace hb2
             // patternwin[1|2] its windowed kernel where the offsets allow;
             // q1stencil[2|4|8] the Q1 stencil kernel where the matrix holds the full
             // nine-point stencil, q1gather[1|2|4] its gather form, q1pair its pair
-            // form; no autotuning
-            Choice c;
+            // form; no autotuning (the default launch shape, or HB2_ELL_BLOCK / HB2_ELL_TPR)
+            Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}, {kEllThreads, kEllThreads}, {1, 1}};
             if (v[0] == 'p' && A->pat)
             {
                 // patternwin[1|2]: the windowed kernel where the matrix admits it

@@ -414,7 +414,7 @@ namespace hb2
     template <typename T, int MODE>
     static void pattern_mode(const hb2_ell_s * A, const void * x, void * y, const void * aux, const void * aux2,
                              void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid, cudaStream_t s,
-                             int flags, Batch b, int R)
+                             int flags, Batch b, int R, unsigned bs)
     {
         EllPatternView<T> v;
         v.pat = A->pat;
@@ -425,7 +425,7 @@ namespace hb2
         if ((R & (kPatQ1 | kPatQ1G)) && ell_q1_stencil_applies(A, MODE, x, R, b))
         {
             launch_ell_q1_stencil(A, MODE, x, y, aux, aux2, red, want_sqrt, rs, grid, s, flags,
-                                  (R & ~kPatFlags) | (R & kPatQ1G));
+                                  (R & ~kPatFlags) | (R & kPatQ1G), bs);
             return;
         }
         // the window copies need a 16-byte aligned x
@@ -460,25 +460,25 @@ namespace hb2
     template <typename T>
     static void pattern_typed(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                               const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                              cudaStream_t s, int f, Batch b, int R)
+                              cudaStream_t s, int f, Batch b, int R, unsigned bs)
     {
         switch (mode)
         {
-            case kPlain: pattern_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
-            case kDefect: pattern_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
-            case kDot: pattern_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
-            case kAdd: pattern_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
-            case kJacobi: pattern_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
-            case kRestrict: pattern_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R); break;
+            case kPlain: pattern_mode<T, kPlain>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kDefect: pattern_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kDot: pattern_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kAdd: pattern_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kJacobi: pattern_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kRestrict: pattern_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
         }
     }
 
     void launch_ell_pattern(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                             const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                            cudaStream_t stream, int flags, Batch b, int R)
+                            cudaStream_t stream, int flags, Batch b, int R, unsigned bs)
     {
-        if (A->dtype == HB2_F64) pattern_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R);
-        else pattern_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R);
+        if (A->dtype == HB2_F64) pattern_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R, bs);
+        else pattern_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, R, bs);
     }
 
     // ------------------------------------------------------------------ build

@@ -246,8 +246,10 @@ namespace hb2
         else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep, M::sub(ea, acc)));
     }
 
+    // blocks of 128, 256 or 512 threads (autotuned); one row per thread keeps 2,048
+    // threads resident per SM (32 registers)
     template <typename T, int MODE, int R>
-    __global__ void __launch_bounds__(kEllThreads, R == 1 ? 8 : 1)
+    __global__ void __launch_bounds__(kEllMaxThreads, R == 1 ? 2048 / kEllMaxThreads : 1)
     q1_gather_kernel(const __grid_constant__ Q1Stencil<T> s, const T * __restrict__ x, T * __restrict__ y,
                      const T * __restrict__ aux, const T * __restrict__ aux2, ReduceSlot rs, double * red,
                      int want_sqrt, int flags, float * __restrict__ y32, float * __restrict__ z32)
@@ -256,12 +258,13 @@ namespace hb2
         const int64_t n = s.n, m = s.m;
         const int t = (int)threadIdx.x;
         const int64_t blk = (flags & kReverse) ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
-        const int64_t i0 = blk * (kEllThreads * R) + t;
+        const int64_t nt = (int64_t)blockDim.x;
+        const int64_t i0 = blk * (nt * R) + t;
         uint32_t p[R];
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
-            const int64_t i = i0 + k * kEllThreads;
+            const int64_t i = i0 + k * nt;
             p[k] = i < n ? (uint32_t)((flags & kKeepL2) ? __ldcg(s.pat + i) : __ldcs(s.pat + i)) : s.full;
         }
         pdl_entry();   // x, rhs and P may come from the previous kernel
@@ -269,7 +272,7 @@ namespace hb2
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
-            const int64_t i = i0 + k * kEllThreads;
+            const int64_t i = i0 + k * nt;
             // every neighbour of a row inside [m + 1, n - m - 1) exists; the full
             // stencil's rows all lie there, the others read through the table below
             if (i >= m + 1 && i + m + 1 < n)
@@ -296,7 +299,7 @@ namespace hb2
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
-            const int64_t i = i0 + k * kEllThreads;
+            const int64_t i = i0 + k * nt;
             if (i >= n) break;
             T acc, xc;
             if (p[k] == s.full && i >= m + 1 && i + m + 1 < n)
@@ -533,7 +536,7 @@ namespace hb2
     template <typename T, int MODE>
     static void q1_stencil_mode(const hb2_ell_s * A, int R, dim3 grid, cudaStream_t st, const void * x, void * y,
                                 const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
-                                int flags)
+                                int flags, unsigned bs)
     {
         Q1Stencil<T> s;
         for (int k = 0; k < 9; ++k) s.v[k] = (T)A->q1_val[k];
@@ -566,7 +569,7 @@ namespace hb2
         if (R & kPatQ1G)
         {
             R &= ~kPatQ1G;
-#define HB2_Q1G(R_) launch_pdl(q1_gather_kernel<T, MODE, R_>, grid, dim3(kEllThreads), 0, st, s, (const T *)x, (T *)y, \
+#define HB2_Q1G(R_) launch_pdl(q1_gather_kernel<T, MODE, R_>, grid, dim3(bs), 0, st, s, (const T *)x, (T *)y, \
                                (const T *)aux, (const T *)aux2, rs, red, want_sqrt, flags, (float *)nullptr,      \
                                (float *)nullptr)
             if (R == 1) HB2_Q1G(1);
@@ -596,10 +599,10 @@ namespace hb2
 
     void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                                const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                               cudaStream_t stream, int flags, int R)
+                               cudaStream_t stream, int flags, int R, unsigned bs)
     {
         // R: rows per thread, with kPatQ1G for the gather form, kPatQ1P for the pair form
-#define HB2_Q1S(T_, M_) q1_stencil_mode<T_, M_>(A, R, grid, stream, x, y, aux, aux2, rs, red, want_sqrt, flags)
+#define HB2_Q1S(T_, M_) q1_stencil_mode<T_, M_>(A, R, grid, stream, x, y, aux, aux2, rs, red, want_sqrt, flags, bs)
         if (A->dtype == HB2_F64)
         {
             if (mode == kPlain) HB2_Q1S(double, kPlain);

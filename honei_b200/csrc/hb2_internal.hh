@@ -14,6 +14,10 @@ namespace hb2
     // kRowsPerThread consecutive rows (one 128-bit load of values per slot for
     // FP64, two rows; four rows for FP32).
     constexpr int kEllThreads = 256;
+    // The plain, compressed and Q1 gather kernels also run as blocks of 128 or 512
+    // threads, and the plain one with two threads per row: the autotuner times
+    // those shapes (their launch bounds are sized for the largest block).
+    constexpr int kEllMaxThreads = 512;
     constexpr uint32_t kMaxReduceBlocks = 1u << 16;
 
     // Launch with programmatic dependent launch (pdl_entry in the kernel) when
@@ -95,6 +99,18 @@ struct hb2_ell_s
     // (rpt | kPatQ1, ell_q1.cu)
     int q1_full = -1;
     double q1_val[9] = {};
+    // optional BF16 layout (ell_bf16.cu, F32 matrices made by hb2_ell_create_bf16):
+    // bform 0: per slot one 32-bit word (BF16 bits of s * a, 16-bit column offset)
+    // in chunks of 32 rows, the chunk's slots one after another; bform 1: BF16
+    // values and int32 columns (bidx) slot-major.  With the row-sum compensated
+    // form, the diagonal in FP32 (bdiag), its slot marked in the index.  val / col
+    // hold the same operator in FP32 (a = q / s) for the paths that read them.
+    void * bval = nullptr;
+    void * bidx = nullptr;
+    float * bdiag = nullptr;
+    float bscale = 1.f;
+    int bform = 0;
+    uint64_t bf16_bytes = 0;
     // row patterns of a small square matrix for the fused small-level kernels
     // (subcycle.cu), built on the host when the matrix joins a hierarchy
     uint8_t * spat = nullptr;
@@ -105,6 +121,11 @@ struct hb2_ell_s
     // its rows per thread
     int layout[2] = {0, 0};
     int rpt[2] = {2, 2};
+    // threads per block (128, 256 or 512) and, on the plain layout, threads per
+    // row (1 or 2) of each kernel class: autotuned where the kernel takes them
+    // (hb2::ell_block), else 256 and 1
+    int bs[2] = {hb2::kEllThreads, hb2::kEllThreads};
+    int tpr[2] = {1, 1};
     // the Q1 transfer matrices of hb2_ell_create_transfer: +L for the prolongation
     // into fine level L, -L for its transposition, the restriction; 0 otherwise.
     // Their products run on kernels that know the rows' columns and weights
@@ -207,36 +228,49 @@ namespace hb2
     {
         kLayoutPlain = 0,
         kLayoutCompact = 1,
-        kLayoutPattern = 2
+        kLayoutPattern = 2,
+        kLayoutBF16 = 3
     };
     constexpr int kPatMax = 32;     // patterns per matrix
     constexpr int kPatMaxK = 16;    // slots per row of the pattern layout
 
-    // row blocks of one launch on A for the kernel class (reducing or not)
+    // row blocks of one launch on A for the kernel class (reducing or not), its
+    // block size and rows per block, for the kernel of the class's layout (the
+    // Q1 gather form where the layout names it)
     unsigned ell_grid(const hb2_ell_s * A, bool reducing);
+    unsigned ell_block(const hb2_ell_s * A, bool reducing);
+    bool ell_shape_tunable(const hb2_ell_s * A, int cls);   // the class's kernel takes a tuned block size
     uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing);
 
     // row-pattern layout (ell_pattern.cu)
     int ell_build_pattern(hb2_ell_s * A, cudaStream_t stream);
     void ell_free_pattern(hb2_ell_s * A);
+    // bs: threads per block of the Q1 gather form (the other pattern kernels run 256)
     void launch_ell_pattern(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                             const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                            cudaStream_t stream, int flags, Batch b, int R);
+                            cudaStream_t stream, int flags, Batch b, int R, unsigned bs);
 
     // Q1 stencil kernel for row-pattern matrices with the full nine-point stencil (ell_q1.cu)
     void ell_find_q1_stencil(hb2_ell_s * A);
     bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, int rpt, const Batch & b);
     void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                                const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                               cudaStream_t stream, int flags, int R);
+                               cudaStream_t stream, int flags, int R, unsigned bs);
 
     // compressed ELL layout (ell_compact.cu)
     int ell_build_compact(hb2_ell_s * A, cudaStream_t stream);
     void ell_free_compact(hb2_ell_s * A);
-    unsigned compact_grid(const hb2_ell_s * A, bool reducing);
     void launch_ell_compact(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                             const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
-                            cudaStream_t stream, int flags, Batch b);
+                            cudaStream_t stream, int flags, Batch b, unsigned bs);
+
+    // BF16 layout (ell_bf16.cu)
+    void ell_free_bf16(hb2_ell_s * A);
+    void launch_ell_bf16(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
+                         const void * aux2, void * zero, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
+                         cudaStream_t stream, int flags, Batch b, unsigned bs);
+    // time the layouts and launch shapes the matrix admits, keep the fastest (ell_compact.cu)
+    int ell_autotune(hb2_ell_s * A, cudaStream_t stream);
 
     // BLAS-1 helpers (blas1.cu) usable from other translation units.
     int launch_fill(int dt, void * x, double value, uint64_t n, cudaStream_t stream);

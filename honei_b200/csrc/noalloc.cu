@@ -82,19 +82,22 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
         return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: " + std::to_string(A->rows) +
                     " rows exceed the static scratch limit of " + std::to_string(max_rows) +
                     " rows for this element type; use hb2_defect_ell");
-    // The kernel runs on the matrix's tuned layout unless that layout's row
-    // blocks outnumber the scratch partials (the row-pattern layout at one row
+    // The kernel runs on the matrix's tuned layout, in blocks of 256 threads,
+    // unless that layout's row blocks outnumber the scratch partials (the row-pattern layout at one row
     // per thread, or the compressed one at two in FP32): then on the same layout
     // with enough rows per thread.  Every variant forms the same products and
     // slot-ordered sums, so the defect vector is the same bit for bit; the norm's
     // block partials follow the launch shape.
     hb2_ell_s V = *A;
+    V.bs[1] = kEllThreads;   // the default launch shape: 256 threads, one per row
+    V.tpr[1] = 1;
     const int base = V.rpt[1] & ~kPatFlags, kflags = V.rpt[1] & kPatFlags;
     for (int r = 2; r <= 8 && ell_grid(&V, true) > kNoAllocMaxBlocks; r *= 2)
     {
         if (V.layout[1] == kLayoutPattern && r > base && (r <= 4 || (kflags & kPatQ1)))
             V.rpt[1] = r | (kflags & (kPatQ1 | kPatQ1G)) | (r <= 2 ? (kflags & (kPatWin | kPatQ1P)) : 0);
         else if (V.layout[1] == kLayoutCompact && r > V.compact_rpt_red) V.compact_rpt_red = r;
+        else if (V.layout[1] == kLayoutBF16 && r > V.rpt[1]) V.rpt[1] = r;
     }
     if (ell_grid(&V, true) > kNoAllocMaxBlocks)
         return fail(HB2_ERR_UNSUPPORTED, "hb2_defect_ell_noalloc: no layout variant fits the static scratch");

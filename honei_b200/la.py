@@ -148,6 +148,21 @@ class SparseMatrixELL:
         m._dtype = self._dtype
         return m
 
+    def to_bf16(self, compensate: bool = False, stream=None) -> "SparseMatrixELL":
+        """A BF16-stored copy (hb2_ell_create_bf16): entries bf16(s * a) with one
+        scale s per matrix, FP32 accumulation and one division by s per row; with
+        compensate=True the diagonal in FP32, absorbing the row's off-diagonal
+        rounding errors (row sums kept).  An F32 matrix; ``scale`` and
+        ``max_rel_error`` describe the rounding."""
+        h = ctypes.c_void_p()
+        s, e = ctypes.c_double(), ctypes.c_double()
+        call("hb2_ell_create_bf16", ctypes.byref(h), self._h, 1 if compensate else 0, ctypes.byref(s),
+             ctypes.byref(e), _stream(stream))
+        m = SparseMatrixELL(h.value)
+        m._dtype = dtype_code(torch.float32)
+        m.scale, m.max_rel_error, m.compensated = s.value, e.value, bool(compensate)
+        return m
+
     def converted(self, dtype, stream=None) -> "SparseMatrixELL":
         h = ctypes.c_void_p()
         call("hb2_ell_convert", ctypes.byref(h), self._h, dtype_code(dtype), _stream(stream))
@@ -179,6 +194,14 @@ class SparseMatrixELL:
         k, r, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hb2_ell_layout_variant", self._h, cls, ctypes.byref(k), ctypes.byref(r), ctypes.byref(w))
         return k.value, r.value, w.value
+
+    def launch_shape(self, cls: int = 0):
+        """(threads_per_block, threads_per_row) of that kernel: the autotuner's
+        choice among 128 / 256 / 512 threads (plain, compressed and Q1 gather
+        kernels; 256 for the others) and 1 or 2 threads per row (plain layout)."""
+        b, t = ctypes.c_int(), ctypes.c_int()
+        call("hb2_ell_launch_shape", self._h, cls, ctypes.byref(b), ctypes.byref(t))
+        return b.value, t.value
 
     def stride(self) -> int:
         return self._stride

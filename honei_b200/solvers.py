@@ -274,6 +274,35 @@ class MGData:
              ctypes.byref(params), _stream(stream))
         return cls(params=params, _handle=h)
 
+    @classmethod
+    def q1_coefficient(cls, k, min_level: int, dtype=torch.float64, params: MgParams | None = None,
+                       bf16: str | None = None, stream=None):
+        """The hierarchy of the variable-coefficient Q1 operator with per-cell
+        coefficients k ((2^L)^2 cells, inputs.q1_coefficient_operator), rediscretised
+        on the coarser levels with the cells' mean coefficients, and the Q1 grid
+        transfers.  bf16 = "pure" / "compensated" (F32 only): every level above the
+        coarsest stored in BF16 (SparseMatrixELL.to_bf16)."""
+        from .inputs import coarsen_coefficients, q1_coefficient_operator
+        npdt = np.float64 if dtype == torch.float64 else np.float32
+        if bf16 not in (None, "pure", "compensated") or (bf16 and dtype != torch.float32):
+            raise ValueError("bf16: None, 'pure' or 'compensated', for an F32 hierarchy")
+        L = int(np.log2(k.shape[0]))
+        ks = [np.asarray(k, np.float64)]
+        for _ in range(L - min_level):
+            ks.append(coarsen_coefficients(ks[-1]))
+        ks.reverse()                                   # coarsest first
+        A, P, R = [], [], []
+        for i, kl in enumerate(ks):
+            m = SparseMatrixELL.from_arrays(*q1_coefficient_operator(kl, npdt), stream=stream)
+            if bf16 and i > 0:
+                m = m.to_bf16(compensate=bf16 == "compensated", stream=stream)
+            A.append(m)
+            if i > 0:
+                p, r = SparseMatrixELL.transfer(min_level + i, dtype, stream=stream)
+                P.append(p)
+                R.append(r)
+        return cls(A, P, R, params=params, stream=stream)
+
     @property
     def handle(self):
         return self._h

@@ -114,15 +114,25 @@ HB2_API int hb2_ell_info(hb2_ell A, uint64_t *rows, uint64_t *cols, uint64_t *st
  *             1  compressed: 1-byte value codes into a table of *table_size
  *                distinct values + 16-bit column offsets from the row;
  *             2  row patterns (square matrices): a 1-byte pattern id per row into
- *                a table of *table_size patterns of (value, column - row) slots.
+ *                a table of *table_size patterns of (value, column - row) slots;
+ *             3  BF16 values + 16-bit offsets or int32 columns (hb2_ell_create_bf16).
  * *row_bytes = matrix bytes read per row.  Every layout gives the same bits.
  * No counterpart in the reference (its device copy is the raw arrays). */
 HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_t *row_bytes);
 /* The kernel behind that choice, per kernel class (cls 0: products, sweeps and
  * transfers; 1: defects with a fused norm): its layout (as above), rows per thread,
- * and *windowed = 1 for the row-pattern kernel that stages x in shared-memory
- * windows.  No counterpart in the reference. */
+ * and *windowed = the kernel kind on the row-pattern layout (0 general, 1 x staged
+ * in shared-memory windows, 2 / 3 / 4 the Q1 stencil kernel's bulk-copy, gather and
+ * pair forms).  No counterpart in the reference. */
 HB2_API int hb2_ell_layout_variant(hb2_ell A, int cls, int *layout, int *rows_per_thread, int *windowed);
+/* Launch shape of that kernel: threads per block (128, 256 or 512; timed by the
+ * autotuner for the plain, compressed and Q1 gather kernels, 256 for the others)
+ * and threads per row (1, or 2 on the plain layout).  HB2_ELL_BLOCK and
+ * HB2_ELL_TPR override the tuned values for matrices created while they are set.
+ * The reference's counterparts are its block-size settings
+ * (honei/honeirc:50-51) and the T threads per row of the ELL kernel
+ * (backends/cuda/product.cu:148-200); every shape gives the same bits. */
+HB2_API int hb2_ell_launch_shape(hb2_ell A, int cls, int *block_threads, int *threads_per_row);
 /* Download the matrix in the reference layout (host arrays of K*stride, K*stride
  * and rows elements); Arl as the reference computes it. */
 HB2_API int hb2_ell_export(hb2_ell A, uint64_t *Aj, void *Ax, uint64_t *Arl);
@@ -137,6 +147,20 @@ HB2_API int hb2_ell_write(hb2_ell A, const char *path);
  * reference (each row's entries in ascending column order); MGUtil::load_data
  * builds every restriction matrix this way from its prolongation. */
 HB2_API int hb2_ell_transpose(hb2_ell *out, hb2_ell A, cudaStream_t stream);
+/* A BF16-stored copy of A for the FP32 inner solve of mixed-precision iterative
+ * refinement: every entry stored as q = bf16(s * a) (one rounding from the double
+ * s * a, to nearest, ties to even), s the first of 1, 3, ..., 15 with the smallest
+ * largest relative rounding error of the stored entries (3 for the Q1 operator:
+ * 8, -1 and 3 exactly), column offsets in 16 bits where they fit.  compensate = 1
+ * (square matrices): the diagonal in FP32, each row's diagonal absorbing the
+ * rounding errors of its off-diagonal entries, d = s a_ii + sum (s a_ij - q_ij),
+ * so the row sums of s * A are kept.  Products accumulate in FP32 (fmaf, slot
+ * order) and divide by s once per row; the vectors are F32 and *out is an F32
+ * matrix (hb2_ell_layout reports layout 3) usable wherever an F32 ELL matrix is,
+ * its plain arrays holding q / s.  *scale and *max_rel_error (nullable): s and
+ * that largest error.  No counterpart in the reference. */
+HB2_API int hb2_ell_create_bf16(hb2_ell *out, hb2_ell A, int compensate, double *scale, double *max_rel_error,
+                                cudaStream_t stream);
 
 /* SparseMatrixCSR<DT>(blocksize, rows, columns, Aj, Ax, Ar, used) (la/sparse_matrix_csr-impl.hh:40-71,
  * 140-145): Ar[rows + 1] block offsets, Aj[Ar[rows]] first column of each block,

@@ -1108,3 +1108,105 @@ uint64_t hbo_lmg_mixed(unsigned lmin, unsigned lmax, const float *const *bands, 
     if (inner_total) *inner_total = inner;
     return outer;
 }
+
+/* ------------------------------------------------------------------------ */
+/* BF16-stored matrix of the FP32 inner solve (no counterpart in the         */
+/* reference): the storage and product of hb2_ell_create_bf16 restated       */
+/* ------------------------------------------------------------------------ */
+/* to nearest BF16 (8 significant bits, exponent range of float), ties to even:
+ * scale the magnitude so that the BF16 spacing of its binade is 1, round to an
+ * integer in the current (nearest-even) mode, scale back */
+double hbo_bf16_round(double t)
+{
+    if (t != t || t == 0.0 || isinf(t)) return t;
+    const double a = fabs(t);
+    int e;
+    frexp(a, &e);                          /* a = m 2^e, 1/2 <= m < 1 */
+    int q = e - 8;                         /* spacing of the binade [2^(e-1), 2^e) */
+    if (q < -133) q = -133;                /* the subnormal spacing */
+    double v = ldexp(nearbyint(ldexp(a, -q)), q);
+    if (v >= 0x1p128) v = INFINITY;
+    return t < 0 ? -v : v;
+}
+
+void hbo_bf16_round_array(uint64_t n, const double *t, double *out)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = hbo_bf16_round(t[i]);
+}
+
+/* row r's diagonal slot in visiting order (the first with Aj == r), or -1 */
+static int64_t bf16_diag(uint64_t r, uint64_t stride, uint64_t T, const uint64_t *Aj, const uint64_t *Arl)
+{
+    for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)
+        for (uint64_t t = 0; t < T; ++t)
+            if (Aj[j + t] == r) return (int64_t)(j + t);
+    return -1;
+}
+
+#define DEFINE_ELL_BF16(T_, SFX)                                                             \
+void hbo_ell_bf16_scale_##SFX(uint64_t rows, uint64_t stride, uint64_t T, const uint64_t *Aj,   \
+                              const T_ *Ax, const uint64_t *Arl, int compensate, double *err)   \
+{                                                                                            \
+    for (int c = 0; c < 8; ++c) err[c] = 0.0;                                                \
+    for (uint64_t r = 0; r < rows; ++r) {                                                    \
+        const int64_t dj = compensate ? bf16_diag(r, stride, T, Aj, Arl) : -1;               \
+        for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)                  \
+            for (uint64_t t = 0; t < T; ++t) {                                               \
+                const double a = (double)Ax[j + t];                                          \
+                if ((int64_t)(j + t) == dj || a == 0.0) continue;                            \
+                for (int c = 0; c < 8; ++c) {                                                \
+                    const double v = a * (double)(2 * c + 1);                                \
+                    const double e = fabs(hbo_bf16_round(v) - v) / fabs(v);                  \
+                    if (e > err[c]) err[c] = e;                                              \
+                }                                                                            \
+            }                                                                                \
+    }                                                                                        \
+}                                                                                            \
+/* d of row r (compensated form) */                                                          \
+static float bf16_d_##SFX(uint64_t r, uint64_t stride, uint64_t T, const uint64_t *Aj,       \
+                          const T_ *Ax, const uint64_t *Arl, double s, int64_t dj)           \
+{                                                                                            \
+    double comp = 0.0;                                                                       \
+    for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)                      \
+        for (uint64_t t = 0; t < T; ++t) {                                                   \
+            if ((int64_t)(j + t) == dj) continue;                                            \
+            const double v = (double)Ax[j + t] * s;                                          \
+            comp += v - hbo_bf16_round(v);                                                   \
+        }                                                                                    \
+    return (float)((double)Ax[dj] * s + comp);                                               \
+}                                                                                            \
+void hbo_ell_bf16_spmv_##SFX(uint64_t rows, uint64_t stride, uint64_t T, const uint64_t *Aj,    \
+                             const T_ *Ax, const uint64_t *Arl, double s, int compensate,    \
+                             const float *x, float *y)                                       \
+{                                                                                            \
+    for (uint64_t r = 0; r < rows; ++r) {                                                    \
+        const int64_t dj = compensate ? bf16_diag(r, stride, T, Aj, Arl) : -1;               \
+        const float d = dj >= 0 ? bf16_d_##SFX(r, stride, T, Aj, Ax, Arl, s, dj) : 0.f;      \
+        float acc = 0.f;                                                                     \
+        for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)                  \
+            for (uint64_t t = 0; t < T; ++t) {                                               \
+                const float v = (int64_t)(j + t) == dj ? d                                   \
+                                : (float)hbo_bf16_round((double)Ax[j + t] * s);              \
+                acc = fmaf(v, x[Aj[j + t]], acc);                                            \
+            }                                                                                \
+        y[r] = s == 1.0 ? acc : acc / (float)s;                                              \
+    }                                                                                        \
+}                                                                                            \
+void hbo_ell_bf16_values_##SFX(uint64_t rows, uint64_t stride, uint64_t T, uint64_t K,       \
+                               const uint64_t *Aj, const T_ *Ax, const uint64_t *Arl,        \
+                               double s, int compensate, float *val32)                       \
+{                                                                                            \
+    memset(val32, 0, K * stride * sizeof(float));                                            \
+    for (uint64_t r = 0; r < rows; ++r) {                                                    \
+        const int64_t dj = compensate ? bf16_diag(r, stride, T, Aj, Arl) : -1;               \
+        for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)                  \
+            for (uint64_t t = 0; t < T; ++t) {                                               \
+                const double q = (int64_t)(j + t) == dj                                      \
+                    ? (double)bf16_d_##SFX(r, stride, T, Aj, Ax, Arl, s, dj)                 \
+                    : hbo_bf16_round((double)Ax[j + t] * s);                                 \
+                val32[j + t] = (float)(q / s);                                               \
+            }                                                                                \
+    }                                                                                        \
+}
+DEFINE_ELL_BF16(double, f64)
+DEFINE_ELL_BF16(float, f32)

@@ -84,6 +84,15 @@ def lib():
         L.hbo_ir_q1.restype = _u64
         L.hbo_ir_q1.argtypes = [ctypes.c_uint, ctypes.c_uint, _dbl, _dbl, _u64, _u64, _u64, _u64, _dbl, _dbl,
                                 _u64, _dbl, ctypes.c_int, _ptr, _ptr, _ptr]
+        L.hbo_bf16_round.restype = _dbl
+        L.hbo_bf16_round.argtypes = [_dbl]
+        L.hbo_bf16_round_array.argtypes = [_u64, _ptr, _ptr]
+        for sfx in ("f64", "f32"):
+            getattr(L, "hbo_ell_bf16_scale_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, ctypes.c_int, _ptr]
+            getattr(L, "hbo_ell_bf16_spmv_" + sfx).argtypes = [_u64, _u64, _u64, _ptr, _ptr, _ptr, _dbl, ctypes.c_int,
+                                                               _ptr, _ptr]
+            getattr(L, "hbo_ell_bf16_values_" + sfx).argtypes = [_u64, _u64, _u64, _u64, _ptr, _ptr, _ptr, _dbl,
+                                                                 ctypes.c_int, _ptr]
     return _lib
 
 
@@ -193,6 +202,40 @@ def ell_defect(A: Ell, rhs: np.ndarray, x: np.ndarray) -> np.ndarray:
     getattr(lib(), "hbo_ell_defect_" + _sfx(A.dtype))(
         _u64(A.rows), _u64(A.stride), _u64(A.T), _p(A.Aj), _p(A.Ax), _p(A.Arl), _p(rhs), _p(x), _p(r))
     return r
+
+
+def bf16_round(t: np.ndarray) -> np.ndarray:
+    """to nearest BF16 value, ties to even, from double (one rounding)"""
+    t = np.ascontiguousarray(t, np.float64)
+    out = np.empty_like(t)
+    lib().hbo_bf16_round_array(_u64(t.size), _p(t), _p(out))
+    return out
+
+
+def ell_bf16_scale(A: Ell, compensate: bool):
+    """(s, largest relative rounding error) of the BF16-stored copy: the first of
+    s = 1, 3, ..., 15 with the smallest largest error"""
+    err = np.zeros(8)
+    getattr(lib(), "hbo_ell_bf16_scale_" + _sfx(A.dtype))(
+        _u64(A.rows), _u64(A.stride), _u64(A.T), _p(A.Aj), _p(A.Ax), _p(A.Arl), int(compensate), _p(err))
+    c = int(np.argmin(err))     # the first minimum
+    return float(2 * c + 1), float(err[c])
+
+
+def ell_bf16_spmv(A: Ell, s: float, compensate: bool, x: np.ndarray) -> np.ndarray:
+    y = np.empty(A.rows, np.float32)
+    getattr(lib(), "hbo_ell_bf16_spmv_" + _sfx(A.dtype))(
+        _u64(A.rows), _u64(A.stride), _u64(A.T), _p(A.Aj), _p(A.Ax), _p(A.Arl), _dbl(s), int(compensate),
+        _p(np.ascontiguousarray(x, np.float32)), _p(y))
+    return y
+
+
+def ell_bf16_values(A: Ell, s: float, compensate: bool) -> np.ndarray:
+    out = np.empty(A.K * A.stride, np.float32)
+    getattr(lib(), "hbo_ell_bf16_values_" + _sfx(A.dtype))(
+        _u64(A.rows), _u64(A.stride), _u64(A.T), _u64(A.K), _p(A.Aj), _p(A.Ax), _p(A.Arl), _dbl(s), int(compensate),
+        _p(out))
+    return out
 
 
 def ell_row_length(A: Ell) -> np.ndarray:

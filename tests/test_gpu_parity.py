@@ -85,6 +85,18 @@ def test_upload_reference_arrays_roundtrip(oracle, T):
     assert same_bits(host(y), oracle.ell_spmv(ref, x))
 
 
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_upload_and_export_with_an_odd_slot_count(oracle, dt):
+    """stride * num_cols_per_row odd (stride = rows of a (2^L + 1)^2 grid): the
+    uint64 row lengths after F32 values stay 8-byte aligned on the way in and out"""
+    from honei_b200 import inputs
+    rows, cols, stride, K, Aj, Ax, Arl = inputs.q1_coefficient_operator(inputs.element_coefficients(5, 3), dt)
+    assert (K * stride) % 2 == 1
+    A = SparseMatrixELL.from_arrays(rows, cols, stride, K, Aj, Ax, Arl)
+    Aj2, Ax2, Arl2 = A.export()
+    assert same_bits(Aj2, Aj) and same_bits(Ax2, Ax) and same_bits(Arl2, Arl)
+
+
 def test_upload_rejects_bad_columns(oracle):
     ref = oracle.q1_ell(3)
     Aj = ref.Aj.copy()
