@@ -264,7 +264,7 @@ def workload_config(args, world):
 ROW_BYTES = {"jacobi": 4, "spmv": 2, "defect": 3}   # vector accesses per row (8 B each in FP64)
 
 
-def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None):
+def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None, dtype=None):
     """One ELL kernel of the level-`level` operator on the layout A runs on, timed in
     its steady state: 40 launches captured in one CUDA graph, rotating over sets of
     input and output vectors of more than 2x L2 in all (every launch reads its vectors
@@ -274,19 +274,22 @@ def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None):
     import numpy as np
     import torch
     from honei_b200.kernel_bench import graph_time
+    dtype = dtype or torch.float64
+    es = 8 if dtype == torch.float64 else 4
     n = A.rows()
     P = hb.RISmoother.jacobi_precon(A, 0.7)
-    ms = graph_time(kind, A, P, n, torch.float64, np.float64, dev, reps)
+    ms = graph_time(kind, A, P, n, dtype, np.float64 if es == 8 else np.float32, dev, reps)
     kind_l, table_size, rb = A.layout()
     vk, vr, vw = A.layout_variant(1 if kind == "defect" else 0)
     variant = variant_name(vk, vr, vw)
-    nbytes = n * (rb + 8 * ROW_BYTES[kind])
+    nbytes = n * (rb + es * ROW_BYTES[kind])
     achieved = nbytes / (ms * 1e-3) / 1e9
     key = f"{variant}:{kind}:L{level}"
     return {"bound": "hbm", "kernel": label or f"{kind} on {variant}", "variant": variant, "level": level,
             "layout": layout_text(kind_l, table_size, rb), "achieved": achieved, "peak": peak[0], "unit": "GB/s",
             "frac": achieved / peak[0], "peak_source": peak[1], "traffic": load_traffic(key), "traffic_key": key,
-            "algorithmic_bytes": nbytes, "bytes_per_row": rb + 8 * ROW_BYTES[kind], "launch_us": 1000 * ms,
+            "algorithmic_bytes": nbytes, "bytes_per_row": rb + es * ROW_BYTES[kind], "launch_us": 1000 * ms,
+            "launch_shape": list(A.launch_shape(1 if kind == "defect" else 0)),
             "timing": "CUDA graph of 40 launches over rotating vector sets (> 2x L2), events around each replay"}
 
 
@@ -426,6 +429,7 @@ def main():
             line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5),
                                                   min(args.warmup, 2), rank, keep=keep)
             line["mixed_vs_fp64"]["anisotropic"] = anisotropic_probe(hb, dev, flush, MIXED_LEVEL, rank)
+            line["mixed_vs_fp64"]["bf16_inner"] = bf16_variant(hb, dev, flush, MIXED_LEVEL, peaks, rank)
         if not args.no_batch:
             line["batched"] = batched_solves(hb, dev, flush, min(args.steps, 3), min(args.warmup, 1), rank)
         if not args.no_serving:
@@ -664,6 +668,90 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cyc
     return res
 
 
+def bf16_variant(hb, dev, flush, level, peaks, rank):
+    """The BF16-stored inner matrices (hb2_ell_create_bf16) against FP32-stored ones in
+    the mixed-precision refinement at `level`, on two operators:
+    * "q1": the Q1 operator of config 2.  s = 3 makes 8/3, -1/3 and 1 exact in BF16.
+      The tuned FP32 levels run the Q1 stencil kernel (one byte per row); the BF16
+      ones run the BF16 layout.
+    * "coefficients": the Q1 finite-element operator with per-cell coefficients of
+      contrast 4 (seeded), rediscretised on the coarse levels.  No two rows repeat,
+      so every FP32 level runs on the plain layout; BF16 pure and with row-sum
+      compensated diagonals.
+    Per operator: IRSolver.choose_inner over the candidates (FP32 first), i.e. each
+    IR solve to 1e-10 with its outer steps, inner cycles, best-of-2 time and `kept`
+    (converged with inner cycles within 10 % of the FP32-stored solve's -- the rule
+    for keeping a BF16 variant) and the choice; each solution's true relative
+    residual and its error against the FP64 MG solution of the same system; and the
+    level's Jacobi sweep on each inner matrix (graph-timed, algorithmic bytes)."""
+    import numpy as np
+    import torch
+
+    from honei_b200 import inputs
+    n = ((1 << level) + 1) ** 2
+    out = {"level": level, "unknowns": n,
+           "rule": "kept when converged with inner MG cycles <= 1.1 x the FP32-stored inner solve's"}
+    inner_prm = hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-3, coarse_eps=1e-3, coarse_exact=False,
+                             coarse_fp64=True)
+    u = torch.from_numpy(inputs.uniform(n, 42 + rank)).to(dev)
+    for op in ("q1", "coefficients"):
+        k = np.ones((1 << level, 1 << level)) if op == "q1" else inputs.element_coefficients(level, 7)
+        if op == "q1":
+            A64 = hb.SparseMatrixELL.poisson_q1(level)
+            fp64 = hb.MGData.poisson_q1(MIN_LEVEL, level, params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10,
+                                                                                 coarse_exact=False))
+            cands = {"fp32": hb.MGData.poisson_q1(MIN_LEVEL, level, dtype=torch.float32, params=inner_prm),
+                     "bf16": hb.MGData.q1_coefficient(k, MIN_LEVEL, torch.float32, params=inner_prm, bf16="pure")}
+        else:
+            A64 = hb.SparseMatrixELL.from_arrays(*inputs.q1_coefficient_operator(k))
+            fp64 = hb.MGData.q1_coefficient(k, MIN_LEVEL, torch.float64,
+                                           params=hb.mg_params(max_iters_coarse=COARSE_CAP, eps=1e-10,
+                                                               coarse_exact=False))
+            cands = {"fp32": hb.MGData.q1_coefficient(k, MIN_LEVEL, torch.float32, params=inner_prm),
+                     "bf16_compensated": hb.MGData.q1_coefficient(k, MIN_LEVEL, torch.float32, params=inner_prm,
+                                                                  bf16="compensated"),
+                     "bf16_pure": hb.MGData.q1_coefficient(k, MIN_LEVEL, torch.float32, params=inner_prm,
+                                                           bf16="pure")}
+        b = hb.DenseVector(n)
+        hb.Product.value(b, A64, hb.DenseVector(u))
+        x64 = hb.DenseVector(n)
+        hb.MGSolver.value(fp64, b, x64)
+        xr = x64.numpy().copy()
+        nb = float(torch.linalg.norm(b.elements))
+        choice, rep = hb.IRSolver.choose_inner(A64, b, cands)
+        x = hb.DenseVector(n)
+        r = hb.DenseVector(n)
+        for name, inner in cands.items():
+            if not rep[name]["converged"]:
+                continue
+            hb.fill(x, 0.0)
+            hb.IRSolver.value(A64, b, x, inner, eps=1e-10, reset_inner=True)
+            hb.Defect.value(r, b, A64, x)
+            rep[name]["relres"] = float(torch.linalg.norm(r.elements)) / nb
+            rep[name]["rel_error_vs_fp64_mg"] = float(np.linalg.norm(x.numpy() - xr) / np.linalg.norm(xr))
+        # the finest level's inner matrix of each candidate: its Jacobi sweep
+        finest = {"fp32": hb.SparseMatrixELL.poisson_q1(level, torch.float32) if op == "q1" else
+                  hb.SparseMatrixELL.from_arrays(*inputs.q1_coefficient_operator(k, np.float32))}
+        if op == "q1":
+            finest["bf16"] = hb.SparseMatrixELL.from_arrays(*inputs.q1_coefficient_operator(k, np.float32)).to_bf16()
+        else:
+            finest["bf16_compensated"] = finest["fp32"].to_bf16(compensate=True)
+            finest["bf16_pure"] = finest["fp32"].to_bf16()
+        for name, M in finest.items():
+            kr = kernel_roofline(hb, "jacobi", M, level, peaks, dev, dtype=torch.float32,
+                                 label=f"fused Jacobi sweep, level {level}, {op} operator, {name} inner matrix")
+            rep[name]["sweep"] = {key: kr[key] for key in ("variant", "launch_shape", "bytes_per_row", "launch_us",
+                                                           "achieved", "frac")}
+            if hasattr(M, "scale"):
+                rep[name]["scale"], rep[name]["max_rel_rounding_error"] = M.scale, M.max_rel_error
+        rep["fp64_mg_cycles"] = fp64.used_iters
+        rep["choice"] = choice
+        out[op] = rep
+        del cands, fp64, finest, A64
+        torch.cuda.synchronize()
+    return out
+
+
 def anisotropic_probe(hb, dev, flush, level, rank):
     """Config 2's anisotropic variant: every level's x-coupling (DL/DU) scaled by a
     factor, the diagonal raised to keep zero interior row sums.  The reference's
@@ -848,11 +936,14 @@ def load_peaks():
 
 def variant_name(kind, rows_per_thread, kernel):
     """Name of an ELL kernel variant as HB2_ELL_COMPACT spells it (plain, forceR,
-    patternR, patternwinR, q1stencilR, q1gatherR, q1pair)."""
+    patternR, patternwinR, q1stencilR, q1gatherR, q1pair, q1stripR, bf16rR)."""
+    if kind == 3:
+        return "bf16r%d" % rows_per_thread
     if kind == 2:
         if int(kernel) == 4:
             return "q1pair"
-        return ({1: "patternwin%d", 2: "q1stencil%d", 3: "q1gather%d"}.get(int(kernel), "pattern%d")) % rows_per_thread
+        return ({1: "patternwin%d", 2: "q1stencil%d", 3: "q1gather%d", 5: "q1strip%d"}.get(int(kernel), "pattern%d")
+                % rows_per_thread)
     if kind == 1:
         return "force%d" % rows_per_thread
     return "plain"

@@ -272,7 +272,7 @@ namespace hb2
     // the Q1 gather form), else 256
     bool ell_shape_tunable(const hb2_ell_s * A, int cls)
     {
-        return A->layout[cls] != kLayoutPattern || (A->rpt[cls] & kPatQ1G);
+        return A->layout[cls] != kLayoutPattern || (A->rpt[cls] & (kPatQ1G | kPatQ1S));
     }
 
     unsigned ell_block(const hb2_ell_s * A, bool reducing)
@@ -286,7 +286,19 @@ namespace hb2
         return rows_per_block(A, reducing ? 1 : 0, ell_block(A, reducing));
     }
 
-    unsigned ell_grid(const hb2_ell_s * A, bool reducing) { return ceil_div(A->rows, ell_rows_per_block(A, reducing)); }
+    // blocks of a launch of bs threads with the class's kernel (q1: the Q1 stencil
+    // kernel runs it, where the layout names one)
+    static unsigned grid_blocks(const hb2_ell_s * A, int cls, unsigned bs, bool q1)
+    {
+        if (q1 && A->layout[cls] == kLayoutPattern && (A->rpt[cls] & kPatQ1S))
+            return q1_strip_grid(A, A->rpt[cls] & ~kPatFlags, bs);
+        return ceil_div(A->rows, rows_per_block(A, cls, bs));
+    }
+
+    unsigned ell_grid(const hb2_ell_s * A, bool reducing)
+    {
+        return grid_blocks(A, reducing ? 1 : 0, ell_block(A, reducing), true);
+    }
 
     // HB2_Q1_TRANSFER=0 runs the Q1 transfer matrices on their stored layout instead
     // (read at every launch, so a process can compare both)
@@ -311,8 +323,9 @@ namespace hb2
         // hands this launch to the general row-pattern kernel (256 threads)
         const int cls = red != 0;
         unsigned bs = ell_block(A, red != 0);
-        if (A->layout[cls] == kLayoutPattern && ! ell_q1_stencil_applies(A, mode, x, A->rpt[cls], b)) bs = kEllThreads;
-        const unsigned gx = (unsigned)ceil_div(A->rows, rows_per_block(A, cls, bs));
+        const bool q1 = A->layout[cls] == kLayoutPattern && ell_q1_stencil_applies(A, mode, x, A->rpt[cls], b);
+        if (A->layout[cls] == kLayoutPattern && ! q1) bs = kEllThreads;
+        const unsigned gx = grid_blocks(A, cls, bs, q1);
         if (b.nvec == 0 || b.nvec > 65535) return fail(HB2_ERR_ARG, "ELL batch: 1..65535 vectors");
         dim3 grid(gx, b.nvec);
         if (b.list)
@@ -771,7 +784,8 @@ extern "C" int hb2_ell_layout_variant(hb2_ell A, int cls, int * layout, int * ro
     if (windowed)
         *windowed = l != kLayoutPattern ? 0 : (A->rpt[cls] & kPatWin) ? 1 : (A->rpt[cls] & kPatQ1) ? 2
                                                                       : (A->rpt[cls] & kPatQ1G) ? 3
-                                                                      : (A->rpt[cls] & kPatQ1P) ? 4 : 0;
+                                                                      : (A->rpt[cls] & kPatQ1P) ? 4
+                                                                      : (A->rpt[cls] & kPatQ1S) ? 5 : 0;
     return HB2_OK;
 }
 

@@ -568,8 +568,8 @@ namespace hb2
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r));
         if (A->pat && A->pat_win_m)
             for (int r : {1, 2}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatWin));
-        // the Q1 stencil kernel's gather form (its bulk-copy and pair forms measured
-        // slower on every level and precision: they stay available as pins)
+        // the Q1 stencil kernel's gather form (its bulk-copy, pair and strip forms
+        // measured slower on every level and precision: they stay available as pins)
         if (A->pat && A->q1_full >= 0)
             for (int r : {1, 2, 4}) variants.push_back(std::make_pair((int)kLayoutPattern, r | kPatQ1G));
         // Each candidate is timed as a burst of back-to-back launches (the way the
@@ -577,7 +577,12 @@ namespace hb2
         // the candidates interleaved over several rounds so that clock or
         // neighbour drift hits all of them; a candidate's time is its best round.
         constexpr int kRounds = 4, kBurst = 8;
-        auto fastest = [&](int cls, size_t count, const std::function<void(size_t)> & select) -> size_t {
+        // the fastest candidate; with `incumbent` set, that one unless another beats it
+        // by more than kMargin (launch shapes that differ by less than the timing's
+        // scatter keep the default)
+        constexpr float kMargin = 0.97f;
+        auto fastest = [&](int cls, size_t count, const std::function<void(size_t)> & select,
+                           long incumbent = -1) -> size_t {
             std::vector<float> best(count, 1e30f);
             for (int round = 0; round <= kRounds && ! st; ++round)   // round 0 warms up
                 for (size_t vi = 0; vi < count && ! st; ++vi)
@@ -608,6 +613,8 @@ namespace hb2
             size_t w = 0;
             for (size_t vi = 1; vi < count; ++vi)
                 if (best[vi] < best[w]) w = vi;
+            if (incumbent >= 0 && best[incumbent] < 1e30f && best[w] > kMargin * best[incumbent])
+                w = (size_t)incumbent;
             return w;
         };
         Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}, {kEllThreads, kEllThreads}, {1, 1}};
@@ -628,13 +635,18 @@ namespace hb2
             // stage 2: the winner's launch shape
             if (st || ! ell_shape_tunable(A, cls)) continue;   // a kernel of fixed shape
             std::vector<std::pair<int, int>> shapes;
+            long incumbent = -1;
             for (int bs : {128, 256, 512})
                 for (int tpr : {1, 2})
-                    if (tpr == 1 || A->layout[cls] == kLayoutPlain) shapes.push_back(std::make_pair(bs, tpr));
+                    if (tpr == 1 || A->layout[cls] == kLayoutPlain)
+                    {
+                        if (bs == kEllThreads && tpr == 1) incumbent = (long)shapes.size();
+                        shapes.push_back(std::make_pair(bs, tpr));
+                    }
             const size_t sw = fastest(cls, shapes.size(), [&](size_t i) {
                 A->bs[cls] = shapes[i].first;
                 A->tpr[cls] = shapes[i].second;
-            });
+            }, incumbent);
             c.bs[cls] = shapes[sw].first;
             c.tpr[cls] = shapes[sw].second;
         }
@@ -698,7 +710,7 @@ namespace hb2
         if (st) return st;
         const char * v = getenv("HB2_ELL_COMPACT");
         if (v && (strncmp(v, "force", 5) == 0 || strncmp(v, "pattern", 7) == 0 || strncmp(v, "q1stencil", 9) == 0 ||
-                  strncmp(v, "q1gather", 8) == 0 || strncmp(v, "q1pair", 6) == 0))
+                  strncmp(v, "q1gather", 8) == 0 || strncmp(v, "q1pair", 6) == 0 || strncmp(v, "q1strip", 7) == 0))
         {
             // HB2_ELL_COMPACT=force[2|4|8]: the compressed layout with that many
             // rows per thread; pattern[1|2|4]: the row-pattern layout (square
@@ -706,7 +718,7 @@ namespace hb2
             // patternwin[1|2] its windowed kernel where the offsets allow;
             // q1stencil[2|4|8] the Q1 stencil kernel where the matrix holds the full
             // nine-point stencil, q1gather[1|2|4] its gather form, q1pair its pair
-            // form; no autotuning (the default launch shape, or HB2_ELL_BLOCK / HB2_ELL_TPR)
+            // form, q1strip[2|4|8] its strip form; no autotuning (the default launch shape, or HB2_ELL_BLOCK / HB2_ELL_TPR)
             Choice c = {{kLayoutPlain, kLayoutPlain}, {2, 2}, {kEllThreads, kEllThreads}, {1, 1}};
             if (v[0] == 'p' && A->pat)
             {
@@ -731,6 +743,15 @@ namespace hb2
                 // q1pair: the Q1 stencil kernel's pair form (two adjacent rows per thread)
                 c.layout[0] = c.layout[1] = kLayoutPattern;
                 c.rpt[0] = c.rpt[1] = 2 | (A->q1_full >= 0 ? kPatQ1P : 0);
+            }
+            else if (strncmp(v, "q1strip", 7) == 0 && A->pat)
+            {
+                // q1strip[2|4|8]: the Q1 stencil kernel's strip form (that many grid rows
+                // per thread)
+                const int r = atoi(v + 7);
+                c.layout[0] = c.layout[1] = kLayoutPattern;
+                c.rpt[0] = c.rpt[1] = (r == 2 || r == 8) ? r : 4;
+                if (A->q1_full >= 0) c.rpt[0] = c.rpt[1] = c.rpt[0] | kPatQ1S;
             }
             else if (strncmp(v, "q1gather", 8) == 0 && A->pat)
             {

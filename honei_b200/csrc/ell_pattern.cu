@@ -422,10 +422,10 @@ namespace hb2
         v.rows = A->rows;
         v.K = A->K;
         v.npat = A->npat;
-        if ((R & (kPatQ1 | kPatQ1G)) && ell_q1_stencil_applies(A, MODE, x, R, b))
+        if ((R & (kPatQ1 | kPatQ1G | kPatQ1S)) && ell_q1_stencil_applies(A, MODE, x, R, b))
         {
             launch_ell_q1_stencil(A, MODE, x, y, aux, aux2, red, want_sqrt, rs, grid, s, flags,
-                                  (R & ~kPatFlags) | (R & kPatQ1G), bs);
+                                  (R & ~kPatFlags) | (R & (kPatQ1G | kPatQ1S)), bs);
             return;
         }
         // the window copies need a 16-byte aligned x

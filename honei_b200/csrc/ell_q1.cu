@@ -533,6 +533,90 @@ namespace hb2
                    (const T *)aux, (const T *)aux2, rs, red, want_sqrt, flags);
     }
 
+    // ------------------------------------------------------------------
+    // Strip form (a pin, HB2_ELL_COMPACT=q1stripS; measured slower than the gather
+    // form on B200 at every level, precision, strip length and block size, so the
+    // autotuner does not time it): thread g (of m * ceil(m / S)) owns grid column j = g % m and the
+    // S grid rows r = S (g / m) .. S (g / m) + S - 1 of that column, node i = r m + j.
+    // The three x values a node takes from each stencil row (flattened indices
+    // r' m + j - 1, r' m + j, r' m + j + 1 for r' = r - 1, r, r + 1) stay in registers
+    // as the strip moves down: each node loads the three of the row below it, not
+    // nine.  A warp's 32 threads are 32 consecutive columns (contiguous loads).  The
+    // registers hold exactly the values the gather form reads at i - m - 1 ..
+    // i + m + 1 (loads outside [0, n) give 0 and are used by no full-stencil row), so
+    // the sums are the gather form's bit for bit; rows of other patterns take the
+    // general slot loop.  The per-block partial of a fused reduction goes to
+    // rs.partials as in the gather form.
+    template <typename T>
+    __device__ __forceinline__ void q1_strip_row(const T * __restrict__ x, int64_t b, int64_t n, bool keep,
+                                                 T (&v)[3])
+    {
+        // x[b - 1], x[b], x[b + 1], 0 outside [0, n)
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+            const int64_t g = b - 1 + q;
+            v[q] = (g >= 0 && g < n) ? (keep ? __ldcg(x + g) : __ldg(x + g)) : T(0);
+        }
+    }
+
+    template <typename T, int MODE, int S>
+    __global__ void __launch_bounds__(kEllMaxThreads)
+    q1_strip_kernel(const __grid_constant__ Q1Stencil<T> s, const T * __restrict__ x, T * __restrict__ y,
+                    const T * __restrict__ aux, const T * __restrict__ aux2, ReduceSlot rs, double * red, int flags,
+                    float * __restrict__ y32, float * __restrict__ z32)
+    {
+        const int64_t n = s.n, m = s.m;
+        const int64_t strips = (m + S - 1) / S;
+        const int64_t blk = (flags & kReverse) ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
+        const int64_t g = blk * blockDim.x + threadIdx.x;
+        const bool keep = (flags & kKeepL2) != 0;
+        pdl_entry();   // x, rhs and P may come from the previous kernel
+        double part = 0.0;
+        if (g < m * strips)
+        {
+            const int64_t j = g % m, r0 = (g / m) * S;
+            T up[3], mid[3];
+            q1_strip_row<T>(x, (r0 - 1) * m + j, n, keep, up);
+            q1_strip_row<T>(x, r0 * m + j, n, keep, mid);
+#pragma unroll
+            for (int t = 0; t < S; ++t)
+            {
+                const int64_t r = r0 + t;
+                if (r >= m) break;
+                const int64_t i = r * m + j;
+                T lo[3];
+                q1_strip_row<T>(x, i + m, n, keep, lo);
+                const uint32_t p = keep ? __ldcg(s.pat + i) : __ldcs(s.pat + i);
+                const T ea = (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR) ? aux[i] : T(0);
+                const T ep = MODE == kJacobi ? aux2[i] : T(0);
+                T acc;
+                if (p == s.full && i >= m + 1 && i + m + 1 < n) acc = q1_row9<T>(s, up, mid, lo);
+                else acc = q1_any_row<T, 1>(s.tab + p * 9u, x, i, nullptr, 0, 0, 0, false);
+                q1_epilogue<T, MODE>(y, i, acc, mid[1], ea, ep, part, y32, z32);
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                {
+                    up[q] = mid[q];
+                    mid[q] = lo[q];
+                }
+            }
+        }
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        {
+            __shared__ double scratch[32];
+            const double sum = block_sum(part, scratch);
+            if (threadIdx.x == 0) rs.partials[blockIdx.x] = sum;
+        }
+    }
+
+    // blocks of a strip-form launch
+    unsigned q1_strip_grid(const hb2_ell_s * A, int S, unsigned bs)
+    {
+        const uint64_t m = (uint64_t)A->pat_win_m, strips = (m + S - 1) / S;
+        return ceil_div(m * strips, bs);
+    }
+
     template <typename T, int MODE>
     static void q1_stencil_mode(const hb2_ell_s * A, int R, dim3 grid, cudaStream_t st, const void * x, void * y,
                                 const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
@@ -566,6 +650,23 @@ namespace hb2
             }
             R = kPatQ1G | 2;
         }
+        if (R & kPatQ1S)
+        {
+            R &= ~kPatQ1S;
+#define HB2_Q1S_(S_) launch_pdl(q1_strip_kernel<T, MODE, S_>, grid, dim3(bs), 0, st, s, (const T *)x, (T *)y,      \
+                                (const T *)aux, (const T *)aux2, rs, red, flags, (float *)nullptr, (float *)nullptr)
+            if (R == 2) HB2_Q1S_(2);
+            else if (R == 4) HB2_Q1S_(4);
+            else HB2_Q1S_(8);
+#undef HB2_Q1S_
+            if ((MODE == kDefect || MODE == kDot) && red)
+            {
+                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials, grid.x,
+                           red, want_sqrt);
+                count_launches(1);
+            }
+            return;
+        }
         if (R & kPatQ1G)
         {
             R &= ~kPatQ1G;
@@ -592,7 +693,7 @@ namespace hb2
     bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, int rpt, const Batch & b)
     {
         // the windows' bulk copies need a 16-byte aligned x (the gather form needs nothing)
-        const bool aligned = (rpt & (kPatQ1G | kPatQ1P)) || ((uintptr_t)x & 15) == 0;
+        const bool aligned = (rpt & (kPatQ1G | kPatQ1P | kPatQ1S)) || ((uintptr_t)x & 15) == 0;
         return A->q1_full >= 0 && A->pat_win_m && A->K == 9 && ! b.list && b.nvec == 1 && ! b.active &&
                (mode == kPlain || mode == kDefect || mode == kDot || mode == kJacobi) && aligned;
     }

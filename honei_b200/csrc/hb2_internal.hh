@@ -220,7 +220,8 @@ namespace hb2
     constexpr int kPatQ1 = 0x20;     // rpt flag: the Q1 stencil kernel (ell_q1.cu)
     constexpr int kPatQ1G = 0x40;    // rpt flag: the Q1 stencil kernel's gather form (ell_q1.cu)
     constexpr int kPatQ1P = 0x80;    // rpt flag: the Q1 stencil kernel's pair form (ell_q1.cu)
-    constexpr int kPatFlags = kPatWin | kPatQ1 | kPatQ1G | kPatQ1P;
+    constexpr int kPatQ1S = 0x100;   // rpt flag: the Q1 stencil kernel's strip form (ell_q1.cu)
+    constexpr int kPatFlags = kPatWin | kPatQ1 | kPatQ1G | kPatQ1P | kPatQ1S;
     constexpr int kSubPatMax = 8;    // patterns of a small-level operator in the fused kernels
     int ell_small_patterns(hb2_ell_s * A);
 
@@ -253,6 +254,7 @@ namespace hb2
     // Q1 stencil kernel for row-pattern matrices with the full nine-point stencil (ell_q1.cu)
     void ell_find_q1_stencil(hb2_ell_s * A);
     bool ell_q1_stencil_applies(const hb2_ell_s * A, int mode, const void * x, int rpt, const Batch & b);
+    unsigned q1_strip_grid(const hb2_ell_s * A, int S, unsigned bs);   // blocks of a strip-form launch
     void launch_ell_q1_stencil(const hb2_ell_s * A, int mode, const void * x, void * y, const void * aux,
                                const void * aux2, double * red, int want_sqrt, ReduceSlot rs, dim3 grid,
                                cudaStream_t stream, int flags, int R, unsigned bs);

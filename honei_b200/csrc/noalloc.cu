@@ -95,7 +95,7 @@ extern "C" int hb2_defect_ell_noalloc(hb2_ell A, const void * rhs, const void * 
     for (int r = 2; r <= 8 && ell_grid(&V, true) > kNoAllocMaxBlocks; r *= 2)
     {
         if (V.layout[1] == kLayoutPattern && r > base && (r <= 4 || (kflags & kPatQ1)))
-            V.rpt[1] = r | (kflags & (kPatQ1 | kPatQ1G)) | (r <= 2 ? (kflags & (kPatWin | kPatQ1P)) : 0);
+            V.rpt[1] = r | (kflags & (kPatQ1 | kPatQ1G | kPatQ1S)) | (r <= 2 ? (kflags & (kPatWin | kPatQ1P)) : 0);
         else if (V.layout[1] == kLayoutCompact && r > V.compact_rpt_red) V.compact_rpt_red = r;
         else if (V.layout[1] == kLayoutBF16 && r > V.rpt[1]) V.rpt[1] = r;
     }

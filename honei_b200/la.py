@@ -190,7 +190,8 @@ class SparseMatrixELL:
         kernel 1 for the row-pattern kernel that stages x in shared-memory windows,
         2 for the Q1 stencil kernel (row patterns holding the full nine-point
         stencil, x windows staged by bulk copies), 3 for its gather form (plain
-        loads), 4 for its pair form (two adjacent rows per thread), 0 otherwise."""
+        loads), 4 for its pair form (two adjacent rows per thread), 5 for its strip
+        form (rows_per_thread grid rows of one column per thread), 0 otherwise."""
         k, r, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hb2_ell_layout_variant", self._h, cls, ctypes.byref(k), ctypes.byref(r), ctypes.byref(w))
         return k.value, r.value, w.value

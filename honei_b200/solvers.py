@@ -351,6 +351,47 @@ class IRSolver:
             raise
         return x, int(stats[0]), list(stats)
 
+    @staticmethod
+    def choose_inner(A: SparseMatrixELL, b, candidates, eps=1e-10, max_iters=100, growth=0.10, reps=2,
+                     stream=None):
+        """Pick the inner hierarchy for repeated solves with A: solve A x = b once per
+        candidate (``candidates``: name -> MGData; the first is the reference, e.g. the
+        FP32-stored levels, the others e.g. BF16-stored ones), each from x = 0 with the
+        inner guess reset, best of ``reps`` CUDA-event timings.  A candidate is kept
+        when it converged and its inner cycles are at most (1 + growth) times the
+        reference's (the BF16-matrix rule: iterations may grow by 10 % at most); the
+        fastest kept one is chosen.  Returns (name, report), report[name] = {"outer",
+        "inner_cycles", "ms", "kept", "converged"}."""
+        b = _vec(b)
+        x = DenseVector(b.size(), dtype=torch.float64)
+        report, ref_cycles = {}, None
+        for i, (name, inner) in enumerate(candidates.items()):
+            r = {"converged": False}
+            best = float("inf")
+            for _ in range(reps):
+                x.elements.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                try:
+                    _, outer, st = IRSolver.value(A, b, x, inner, eps=eps, max_iters=max_iters, reset_inner=True,
+                                                  stream=stream)
+                except NotFinite as e:
+                    r.update(outer=int(e.stats[0]), inner_cycles=int(e.stats[3]), error="NotFinite")
+                    break
+                e1.record()
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+                r.update(outer=outer, inner_cycles=int(st[3]), converged=st[2] <= eps * st[1])
+            r["ms"] = best if r["converged"] else None
+            if i == 0:
+                ref_cycles = r.get("inner_cycles")
+            r["kept"] = bool(r["converged"] and ref_cycles is not None and
+                             r["inner_cycles"] <= (1.0 + growth) * ref_cycles)
+            report[name] = r
+        kept = [n for n, r in report.items() if r["kept"]]
+        choice = min(kept, key=lambda n: report[n]["ms"]) if kept else next(iter(candidates))
+        return choice, report
+
 
 def batch_params(max_iters=100, eps=1e-8, n_pre=4, n_post=4, max_iters_coarse=100, coarse_eps=1e-10,
                  omega=0.7) -> _lib.BatchParams:

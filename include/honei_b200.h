@@ -122,8 +122,8 @@ HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_
 /* The kernel behind that choice, per kernel class (cls 0: products, sweeps and
  * transfers; 1: defects with a fused norm): its layout (as above), rows per thread,
  * and *windowed = the kernel kind on the row-pattern layout (0 general, 1 x staged
- * in shared-memory windows, 2 / 3 / 4 the Q1 stencil kernel's bulk-copy, gather and
- * pair forms).  No counterpart in the reference. */
+ * in shared-memory windows, 2 / 3 / 4 / 5 the Q1 stencil kernel's bulk-copy, gather,
+ * pair and strip forms).  No counterpart in the reference. */
 HB2_API int hb2_ell_layout_variant(hb2_ell A, int cls, int *layout, int *rows_per_thread, int *windowed);
 /* Launch shape of that kernel: threads per block (128, 256 or 512; timed by the
  * autotuner for the plain, compressed and Q1 gather kernels, 256 for the others)

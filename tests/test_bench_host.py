@@ -33,6 +33,8 @@ def test_variant_names_and_committed_traffic():
     assert bench.variant_name(2, 4, 2) == "q1stencil4"
     assert bench.variant_name(2, 2, 3) == "q1gather2"
     assert bench.variant_name(2, 2, 4) == "q1pair"
+    assert bench.variant_name(2, 4, 5) == "q1strip4"
+    assert bench.variant_name(3, 1, 0) == "bf16r1"
     assert bench.variant_name(1, 4, False) == "force4"
     assert bench.variant_name(0, 2, False) == "plain"
     for v in ("pattern1", "pattern2", "pattern4", "patternwin1", "patternwin2"):

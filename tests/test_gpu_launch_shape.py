@@ -134,7 +134,7 @@ def test_plain_shapes_runtime_slot_count(oracle, monkeypatch, bs, tpr, T):
     assert same_bits(host(y), oracle.ell_spmv(ref, x))
 
 
-@pytest.mark.parametrize("layout", ["force2", "force8", "q1gather1", "q1gather4"])
+@pytest.mark.parametrize("layout", ["force2", "force8", "q1gather1", "q1gather4", "q1strip4"])
 @pytest.mark.parametrize("bs", [128, 512])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_compressed_and_q1_gather_shapes(oracle, monkeypatch, dt, layout, bs):
@@ -207,8 +207,9 @@ def test_tuner_times_the_shape_and_records_it(oracle, monkeypatch, tmp_path):
         assert bs in (128, 256, 512) and tpr in (1, 2)
     lines = [l.split() for l in path.read_text().splitlines()]
     mine = [l for l in lines if l[2] == "9001" and l[3] == "9001"]
-    assert len(mine) == 1 and len(mine[0]) == 15
-    assert (int(mine[0][11]), int(mine[0][12])) == A.launch_shape(0)
+    # device dtype rows cols K table patterns kind | layout rpt (x2) | block tpr (x2)
+    assert len(mine) == 1 and len(mine[0]) == 16
+    assert (int(mine[0][12]), int(mine[0][13])) == A.launch_shape(0)
     x = oracle.uniform(ref.cols, 9)
     y = dvec(np.zeros(ref.rows))
     hb.Product.value(y, A, dvec(x))
@@ -217,5 +218,5 @@ def test_tuner_times_the_shape_and_records_it(oracle, monkeypatch, tmp_path):
     kind, _, kernel = B.layout_variant(0)
     bs, tpr = B.launch_shape(0)
     assert tpr == 1 and bs in (128, 256, 512)
-    if kind == 2 and kernel != 3:
-        assert bs == 256      # row-pattern kernels other than the Q1 gather form
+    if kind == 2 and kernel not in (3, 5):
+        assert bs == 256      # row-pattern kernels other than the Q1 gather and strip forms

@@ -462,7 +462,7 @@ def test_ir_mixed_fp64_coarse(oracle):
 
 @pytest.mark.parametrize("layout", ["force2", "force4", "force8", "pattern1", "pattern2", "pattern4", "patternwin1",
                                     "patternwin2", "q1stencil2", "q1stencil4", "q1stencil8", "q1gather1",
-                                    "q1gather2", "q1gather4", "q1pair"])
+                                    "q1gather2", "q1gather4", "q1pair", "q1strip2", "q1strip8"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     """Value-dictionary + 16-bit offset layout (forceR) and row-pattern layout (patternR,
@@ -479,7 +479,7 @@ def test_compressed_layout_matches_plain(oracle, monkeypatch, dt, layout):
     if layout.startswith("pattern") or layout.startswith("q1"):
         # two row patterns: interior stencil, Dirichlet identity row; 1 matrix byte per row
         assert A.layout() == (2, 2, 1)
-        kern = {"patternwin": 1, "q1stencil": 2, "q1gather": 3, "q1pai": 4}.get(layout[:-1], 0)
+        kern = {"patternwin": 1, "q1stencil": 2, "q1gather": 3, "q1pai": 4, "q1strip": 5}.get(layout[:-1], 0)
         want = (2, 2 if layout == "q1pair" else int(layout[-1]), kern)
     else:
         assert A.layout() == (1, 3, 27)

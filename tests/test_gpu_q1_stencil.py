@@ -1,7 +1,8 @@
 """The Q1 stencil kernels (honei_b200/csrc/ell_q1.cu) for row-pattern ELL matrices
 holding the full nine-point stencil, pinned with HB2_ELL_COMPACT=q1stencilR (x
-windows staged by bulk copies, R = 2, 4, 8 rows per thread) and q1gatherR (x
-gathered by plain loads, R = 1, 2, 4).  Bit for bit against the oracle's ELL product
+windows staged by bulk copies, R = 2, 4, 8 rows per thread), q1gatherR (x
+gathered by plain loads, R = 1, 2, 4), q1pair (two adjacent rows per thread) and
+q1stripR (a vertical strip of R grid rows per thread, x rows kept in registers).  Bit for bit against the oracle's ELL product
 (la/product.hh:148-206) in every mode they run (y = A x, r = b - A x with the fused
 ||r||^2, y = A x with <y, x>, the Jacobi sweep of math/ri.hh:97-133), at the
 levels where the layout applies (8..11), in both precisions; for the anisotropic
@@ -68,8 +69,8 @@ def check_modes(oracle, A, ref, npdt, seed=3):
 
 
 VARIANTS = [("q1stencil", 2), ("q1stencil", 4), ("q1stencil", 8), ("q1gather", 1), ("q1gather", 2), ("q1gather", 4),
-            ("q1pair", 2)]
-KERNEL = {"q1stencil": 2, "q1gather": 3, "q1pair": 4}
+            ("q1pair", 2), ("q1strip", 2), ("q1strip", 4), ("q1strip", 8)]
+KERNEL = {"q1stencil": 2, "q1gather": 3, "q1pair": 4, "q1strip": 5}
 
 
 @pytest.mark.parametrize("kind,R", VARIANTS)
@@ -86,16 +87,16 @@ def test_q1_stencil_modes_bit_exact(oracle, monkeypatch, dt, L, kind, R):
     check_modes(oracle, A, oracle.q1_ell(L, npdt), npdt)
 
 
-@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair", "q1strip4"])
 @pytest.mark.parametrize("aniso", [10.0, 100.0])
 def test_q1_stencil_anisotropic(oracle, monkeypatch, aniso, variant):
     monkeypatch.setenv("HB2_ELL_COMPACT", variant)
     A = SparseMatrixELL.poisson_q1(9, aniso=aniso)
-    assert A.layout_variant(0)[2] in (2, 3, 4)
+    assert A.layout_variant(0)[2] in (2, 3, 4, 5)
     check_modes(oracle, A, oracle.q1_ell(9, aniso=aniso), np.float64)
 
 
-@pytest.mark.parametrize("variant", ["q1stencil2", "q1gather1", "q1pair"])
+@pytest.mark.parametrize("variant", ["q1stencil2", "q1gather1", "q1pair", "q1strip8"])
 def test_q1_stencil_second_full_pattern(oracle, monkeypatch, variant):
     """Interior rows of one grid band carry other stencil values: a second
     full-stencil pattern, whose rows take the general slot loop."""
@@ -108,12 +109,12 @@ def test_q1_stencil_second_full_pattern(oracle, monkeypatch, variant):
     Ax[:, rows[full]] *= 2.0
     Ax = Ax.reshape(-1)
     A = SparseMatrixELL.from_arrays(ref.rows, ref.cols, ref.stride, ref.K, ref.Aj, Ax, ref.Arl)
-    assert A.layout()[:2] == (2, 3) and A.layout_variant(0)[2] in (2, 3, 4)
+    assert A.layout()[:2] == (2, 3) and A.layout_variant(0)[2] in (2, 3, 4, 5)
     ref2 = oracle.Ell(ref.rows, ref.cols, ref.stride, ref.K, 1, ref.Aj, Ax, ref.Arl)
     check_modes(oracle, A, ref2, np.float64)
 
 
-@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair", "q1strip2"])
 def test_q1_stencil_unaligned_x(oracle, monkeypatch, variant):
     """x not 16-byte aligned: the bulk-copy form hands over to the general row-pattern
     kernel, the pair form to the interleaved gather form, the gather form runs as it
@@ -132,7 +133,7 @@ def test_q1_stencil_unaligned_x(oracle, monkeypatch, variant):
     assert same_bits(host(y), oracle.ell_spmv(oracle.q1_ell(L), x))
 
 
-@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair"])
+@pytest.mark.parametrize("variant", ["q1stencil4", "q1gather2", "q1pair", "q1strip4"])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_q1_stencil_in_the_mg_solve(oracle, monkeypatch, dt, variant):
     """MG V(4,4) with every eligible level on a Q1 stencil kernel: the oracle's
