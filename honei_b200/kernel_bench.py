@@ -3,6 +3,7 @@
     python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect|
                                                 cgvar|bicgstab|coarse_cg]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
+                                      [--operator q1|coefficients] [--storage native|bf16|bf16c]
 
 Each launch is preceded by an L2 flush (256 MiB written, then 256 MiB read, so
 that no dirty line of the flush is written back during the launch; --flush write
@@ -113,6 +114,11 @@ def main(argv=None) -> int:
     ap.add_argument("--level", type=int, default=10)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--operator", default="q1", choices=["q1", "coefficients"],
+                    help="q1: the Q1 Poisson operator; coefficients: the Q1 finite-element operator with per-cell "
+                         "coefficients of contrast 4 (seed 7), no two rows alike")
+    ap.add_argument("--storage", default="native", choices=["native", "bf16", "bf16c"],
+                    help="bf16 / bf16c: the matrix stored in BF16 (pure / row-sum compensated), FP32 vectors")
     ap.add_argument("--flush", default="clean", choices=["clean", "write", "none", "graph"],
                     help="clean: write then read 256 MiB before each launch; write: the write only; none: "
                          "bursts of 8 back-to-back launches, no flush (warm L2), time per launch; graph: "
@@ -133,7 +139,15 @@ def main(argv=None) -> int:
     def vec(m, seed):
         return DenseVector(torch.from_numpy(uniform(m, seed, dtype=npdt)).to(dev))
 
-    A = SparseMatrixELL.poisson_q1(L, dt)
+    if a.storage != "native" and a.dtype != "f32":
+        ap.error("--storage bf16 / bf16c needs --dtype f32")
+    if a.operator == "q1":
+        A = SparseMatrixELL.poisson_q1(L, dt)
+    else:
+        from .inputs import element_coefficients, q1_coefficient_operator
+        A = SparseMatrixELL.from_arrays(*q1_coefficient_operator(element_coefficients(L, 7), npdt))
+    if a.storage != "native":
+        A = A.to_bf16(compensate=a.storage == "bf16c")
     rb = A.layout()[2]              # matrix bytes per row of the layout in use
     x, b, y, y2 = vec(n, 1), vec(n, 2), vec(n, 3), vec(n, 4)
     _lib.call("hb2_product_ell", A.handle, x.ptr, b.ptr, stream)        # b = A x (setup)
@@ -247,8 +261,10 @@ def main(argv=None) -> int:
             ms = graph_time(name, A, P, n, dt, npdt, dev, a.iters)
             nbytes = kernels[name][1]
             gbs = nbytes / (ms * 1e-3) / 1e9
-            print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "rows": n, "layout": A.layout()[0],
+            print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "operator": a.operator,
+                              "storage": a.storage, "rows": n, "layout": A.layout()[0],
                               "variant": list(A.layout_variant(0 if name != "defect" else 1)) if name != "copy" else None,
+                              "launch_shape": list(A.launch_shape(0 if name != "defect" else 1)),
                               "flush": "graph", "matrix_bytes_per_row": rb, "launch_us": 1000 * ms,
                               "algorithmic_bytes": nbytes, "gbs": gbs, "frac_of_measured_peak": gbs / peak}), flush=True)
         return 0
