@@ -86,7 +86,7 @@ namespace hb2
         T * __restrict__ y = y_ + vo;
         const T * __restrict__ aux = aux_ ? aux_ + vo : aux_;
         T * __restrict__ zero = zero_ ? zero_ + (uint64_t)j * bt.zstride : zero_;
-        double * red = red_ ? red_ + j : red_;   // grid_sum_finish offsets its partials / counters itself
+        double * red = red_ ? red_ + j : red_;   // the block reduction offsets its partials / counters itself
         const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
         const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
         const bool keep = (flags & kKeepL2) != 0;
@@ -194,8 +194,7 @@ namespace hb2
         if ((MODE == kDefect || MODE == kDot) && red != 0)
         {
             __shared__ double scratch[32];
-            double s = block_sum(part, scratch);
-            grid_sum_finish(s, rs, red, want_sqrt, scratch);
+            ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
         }
         }
     }
@@ -352,6 +351,10 @@ namespace hb2
         if (A->q1_transfer && ! red && b.nvec == 1 && ! b.list && ! b.active &&
             (mode == kPlain || mode == kAdd || mode == kRestrict) && q1_transfer_kernels_enabled())
             return launch_q1_transfer(A, mode, x, y, zero, stream);
+        // the fused reduction split into per-block partials and a second launch: always
+        // on the Q1 stencil kernels, elsewhere from kSplitSumMinBlocks blocks
+        const bool split = red && (q1 || (uint64_t)gx * b.nvec >= kSplitSumMinBlocks);
+        if (split) flags |= kSplitSum;
         if (A->layout[cls] == kLayoutPattern)
             launch_ell_pattern(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, A->rpt[cls], bs);
         else if (A->layout[cls] == kLayoutCompact)
@@ -362,6 +365,7 @@ namespace hb2
             launch_typed<double>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs, A->tpr[cls]);
         else launch_typed<float>(A, mode, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, stream, flags, b, bs, A->tpr[cls]);
         count_launches(1);
+        if (split) launch_sum_partials(rs.partials, gx, b.nvec, red, want_sqrt, stream);
         HB2_LAUNCH_CHECK("ell kernel launch");
         return HB2_OK;
     }

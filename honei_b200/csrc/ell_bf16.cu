@@ -16,17 +16,18 @@
 // Row-sum compensated form.  Rounding every entry of a diffusion operator on its
 // own breaks its zero row sums; the error then reaches the smooth modes that the
 // operator barely damps, and the outer refinement stalls as the grid is refined.
-// The compensated form keeps the diagonal in FP32 and adds to it the rounding
-// errors of the row's off-diagonal entries (in double, slot order):
-//   d = s * a_ii + sum_j!=i (s * a_ij - q_ij),   stored as (float) d,
+// The compensated form gives the diagonal (the row's first slot with column ==
+// row) the rounding errors of the row's off-diagonal entries (in double, slot
+// order):  d = (float)(s * a_ii + sum_j!=i (s * a_ij - q_ij)),
 // so s * A and the stored matrix have the same row sums up to d's one rounding.
-// The diagonal is the row's first slot with column == row; its slot is marked in
-// the index stream (offset kBfDiag / column kColDiag) and its value read from d.
+// d is stored as its BF16 part h = bf16(d) in the diagonal's slot (an ordinary
+// slot) and the rest l = d - h (exact in FP32) in a per-row FP32 array.
 //
-// Products.  y_i = (sum over the row's slots in order of fmaf(v, x_j, acc)) / s,
-// FP32 accumulation, v = q (exact in FP32) or d, and one correctly rounded
-// division by s per row (none for s = 1).  The plain arrays of the new matrix
-// hold (float)(q / s) (and (float)(d / s)) for the paths that read FP32 values
+// Products.  acc = fmaf chain over the row's slots in order (v = q, exact in
+// FP32), then acc = fmaf(l, x_i, acc) in the compensated form, then
+// y_i = acc * fl(1/s) (the factor 1/s once per row, in the accumulator; no
+// multiply for s = 1).  The plain arrays of the new matrix hold (float)(q / s)
+// (and (float)(d / s) at the diagonal) for the paths that read FP32 values
 // (small fused levels, CG, export).
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
@@ -39,10 +40,9 @@
 
 namespace hb2
 {
-    constexpr int16_t kBfEmpty = -32768;   // slot past the row's length
-    constexpr int16_t kBfDiag = -32767;    // the row's diagonal slot (compensated form)
-    constexpr int32_t kColDiag = -2;
-    constexpr int kBfScales = 8;           // s = 1, 3, ..., 15
+    constexpr int16_t kBfEmpty = -32768;          // offset of a slot past the row's length
+    constexpr uint32_t kBfEmptyWord = 0x80000000u;  // form 0: that slot's word (value 0)
+    constexpr int kBfScales = 8;                  // s = 1, 3, ..., 15
 
     // double -> BF16 bits, rounded to nearest, ties to even, in one rounding:
     // truncate to float, record any discarded bits in the last place (round to
@@ -94,7 +94,7 @@ namespace hb2
                 const int32_t cj = col[(uint64_t)k * ld + r];
                 if (cj < 0) continue;
                 const int64_t d = (int64_t)cj - (int64_t)r;
-                if (d < -32766 || d > 32767) *wide = 1;
+                if (d < -32767 || d > 32767) *wide = 1;
                 if (compensate && diag_slot(col, ld, r, k)) continue;
                 const double a = (double)val[(uint64_t)k * ld + r];
                 if (a == 0.0) continue;
@@ -123,8 +123,9 @@ namespace hb2
         }
     }
 
-    // one thread per row: BF16 values, indices, the compensated diagonal and the
-    // FP32 rendering (val32 / col32 of the new matrix, same layout as the source)
+    // one thread per row: BF16 values, indices, the compensated diagonal's FP32
+    // remainder and the FP32 rendering (val32 / col32 of the new matrix, same
+    // layout as the source)
     // form 0: word index of (row r, slot k) in the chunked layout
     __host__ __device__ __forceinline__ uint64_t bf16_word(uint64_t r, uint32_t k, uint32_t K)
     {
@@ -134,7 +135,7 @@ namespace hb2
     __device__ __forceinline__ void bf16_put(int form, void * bval, void * bidx, uint64_t r, uint32_t k, uint32_t K,
                                              uint64_t i, uint16_t q, int16_t off, int32_t col)
     {
-        if (form == 0) ((uint32_t *)bval)[bf16_word(r, k, K)] = (uint32_t)q | ((uint32_t)(uint16_t)off << 16);
+        if (form == 0) ((uint32_t *)bval)[bf16_word(r, k, K)] = (uint32_t)q | ((uint32_t)(uint16_t)off << 16);   // empty: q = 0, off = kBfEmpty
         else
         {
             ((uint16_t *)bval)[i] = q;
@@ -145,7 +146,7 @@ namespace hb2
     template <typename T>
     __global__ void bf16_build_kernel(const T * __restrict__ val, const int32_t * __restrict__ col, uint64_t rows,
                                       uint64_t ld, uint32_t K, double s, int compensate, int form, void * bval,
-                                      void * bidx, float * bdiag, float * val32, int32_t * col32)
+                                      void * bidx, float * bdlo, float * val32, int32_t * col32)
     {
         const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= ld) return;
@@ -166,9 +167,8 @@ namespace hb2
             const double t = (double)val[i] * s;
             if (compensate && dslot < 0 && cj == (int32_t)r)
             {
-                dslot = (int64_t)k;
+                dslot = (int64_t)k;      // written once the row's errors are summed
                 dval = t;
-                bf16_put(form, bval, bidx, r, k, K, i, 0, kBfDiag, kColDiag);
                 continue;
             }
             const uint16_t q = bf16_rne(t);
@@ -177,11 +177,19 @@ namespace hb2
             bf16_put(form, bval, bidx, r, k, K, i, q, (int16_t)((int64_t)cj - (int64_t)r), cj);
             val32[i] = (float)(qd / s);
         }
-        if (bdiag)
+        if (bdlo)
         {
-            const float d = dslot >= 0 ? (float)(dval + comp) : 0.f;
-            bdiag[r] = d;
-            if (dslot >= 0) val32[(uint64_t)dslot * ld + r] = (float)((double)d / s);
+            float lo = 0.f;
+            if (dslot >= 0)
+            {
+                const float d = (float)(dval + comp);
+                const uint16_t h = bf16_rne((double)d);
+                lo = d - bf16_float(h);           // exact: h is d to 8 bits
+                const uint64_t i = (uint64_t)dslot * ld + r;
+                bf16_put(form, bval, bidx, r, (uint32_t)dslot, K, i, h, 0, (int32_t)r);
+                val32[i] = (float)((double)d / s);
+            }
+            bdlo[r] = lo;
         }
     }
 
@@ -190,10 +198,10 @@ namespace hb2
     {
         const void * val;     // form 0: packed words; form 1: BF16 values
         const int32_t * idx;  // form 1: columns
-        const float * diag;   // null: no compensated diagonal
+        const float * dlo;    // compensated form: the diagonal's FP32 remainder per row (else null)
         uint64_t rows, ld;
         uint32_t K;
-        float scale;
+        float inv;            // fl(1 / s); 1: no multiply
     };
 
     template <int R> struct BfWide;
@@ -201,8 +209,7 @@ namespace hb2
     template <> struct BfWide<4> { typedef uint2 V; typedef int4 C; };
     template <> struct BfWide<8> { typedef uint4 V; typedef int4 C; };   // columns: two loads
 
-    // slot k of rows r0 .. r0 + R - 1: BF16 bits and column (-1 empty, kColDiag the
-    // compensated diagonal)
+    // slot k of rows r0 .. r0 + R - 1: BF16 bits and column (-1: empty)
     template <int R, int FORM>
     __device__ __forceinline__ void bf16_slot(const EllBf16View & A, uint32_t K, uint32_t k, uint64_t r0, bool keep,
                                               uint32_t (&q)[R], int (&c)[R])
@@ -234,9 +241,8 @@ namespace hb2
 #pragma unroll
             for (int j = 0; j < R; ++j)
             {
-                const int16_t h = (int16_t)(w[j] >> 16);
                 q[j] = w[j] & 0xffffu;
-                c[j] = h == kBfEmpty ? -1 : h == kBfDiag ? kColDiag : (int)((int64_t)r0 + j + h);
+                c[j] = w[j] == kBfEmptyWord ? -1 : (int)r0 + j + (int)(int16_t)(w[j] >> 16);
             }
         }
         else
@@ -311,18 +317,13 @@ namespace hb2
         for (int i = 0; i < R; ++i) acc[i] = 0.f;
         if (r0 < A.rows)
         {
-            float d[R];
+            float lo[R];
 #pragma unroll
-            for (int i = 0; i < R; ++i) d[i] = A.diag ? A.diag[r0 + i] : 0.f;
+            for (int i = 0; i < R; ++i) lo[i] = A.dlo ? A.dlo[r0 + i] : 0.f;
             auto slot = [&](const uint32_t (&q)[R], const int (&c)[R]) {
 #pragma unroll
                 for (int i = 0; i < R; ++i)
-                {
-                    if (c[i] == -1) continue;
-                    const bool dg = c[i] == kColDiag;
-                    const float v = dg ? d[i] : bf16_float(q[i]);
-                    acc[i] = M::fma(v, __ldg(x + (dg ? (int64_t)(r0 + i) : (int64_t)c[i])), acc[i]);
-                }
+                    if (c[i] >= 0) acc[i] = M::fma(bf16_float(q[i]), __ldg(x + c[i]), acc[i]);
             };
             if constexpr (KT > 0)
             {
@@ -343,9 +344,12 @@ namespace hb2
                     slot(q, c);
                 }
             }
-            if (A.scale != 1.f)
+            if (A.dlo)
 #pragma unroll
-                for (int i = 0; i < R; ++i) acc[i] = M::div(acc[i], A.scale);
+                for (int i = 0; i < R; ++i) acc[i] = M::fma(lo[i], __ldg(x + r0 + i), acc[i]);
+            if (A.inv != 1.f)
+#pragma unroll
+                for (int i = 0; i < R; ++i) acc[i] = M::mul(acc[i], A.inv);
         }
         double part = 0.0;
 #pragma unroll
@@ -372,8 +376,7 @@ namespace hb2
         if ((MODE == kDefect || MODE == kDot) && red != 0)
         {
             __shared__ double scratch[32];
-            const double sum = block_sum(part, scratch);
-            grid_sum_finish(sum, rs, red, want_sqrt, scratch);
+            ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
         }
         }
     }
@@ -386,11 +389,11 @@ namespace hb2
         EllBf16View v;
         v.val = A->bval;
         v.idx = (const int32_t *)A->bidx;
-        v.diag = A->bdiag;
+        v.dlo = A->bdiag;
         v.rows = A->rows;
         v.ld = A->ld;
         v.K = A->K;
-        v.scale = A->bscale;
+        v.inv = A->bscale == 1.f ? 1.f : (float)(1.0 / (double)A->bscale);
         const float * xp = (const float *)x;
         float * yp = (float *)y;
         const float * ap = (const float *)aux;

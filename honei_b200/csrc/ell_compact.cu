@@ -191,7 +191,7 @@ namespace hb2
         T * __restrict__ y = y_ + vo;
         const T * __restrict__ aux = aux_ ? aux_ + vo : aux_;
         T * __restrict__ zero = zero_ ? zero_ + (uint64_t)j * bt.zstride : zero_;
-        double * red = red_ ? red_ + j : red_;   // grid_sum_finish offsets its partials / counters itself
+        double * red = red_ ? red_ + j : red_;   // the block reduction offsets its partials / counters itself
         const uint64_t bx = listed ? item % bt.gx : blockIdx.x;
         const uint64_t blk = (flags & kReverse) ? (gridDim.x - 1 - bx) : bx;
         const bool keep = (flags & kKeepL2) != 0;
@@ -265,8 +265,7 @@ namespace hb2
         if ((MODE == kDefect || MODE == kDot) && red != 0)
         {
             __shared__ double scratch[32];
-            double s = block_sum(part, scratch);
-            grid_sum_finish(s, rs, red, want_sqrt, scratch);
+            ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
         }
         }
     }

@@ -222,8 +222,7 @@ namespace hb2
             if ((MODE == kDefect || MODE == kDot) && red != 0)
             {
                 __shared__ double scratch[32];
-                const double s = block_sum(part, scratch);
-                grid_sum_finish(s, rs, red, want_sqrt, scratch);
+                ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
             }
         }
     }
@@ -268,7 +267,7 @@ namespace hb2
     __global__ void __launch_bounds__(kEllThreads)
     ell_pattern_win_kernel(EllPatternView<T> A, int64_t m, const T * __restrict__ x, T * __restrict__ y,
                            const T * __restrict__ aux, const T * __restrict__ aux2, T * __restrict__ zero,
-                           ReduceSlot rs, double * red, int want_sqrt)
+                           ReduceSlot rs, double * red, int want_sqrt, int flags)
     {
         typedef Arith<T> M;
         constexpr int K = 9;
@@ -404,8 +403,7 @@ namespace hb2
         if ((MODE == kDefect || MODE == kDot) && red != 0)
         {
             __shared__ double scratch[32];
-            const double sum = block_sum(part, scratch);
-            grid_sum_finish(sum, rs, red, want_sqrt, scratch);
+            ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
         }
         // copies still in flight must land before the block's shared memory is reused
         if (! fast) mbar_wait_bounded(&bar, 0, 1000000000ull);
@@ -435,10 +433,10 @@ namespace hb2
             const int Rw = R & ~kPatWin;
             if (Rw == 1)
                 launch_pdl(ell_pattern_win_kernel<T, MODE, 1>, grid, dim3(kEllThreads), 0, s, v, A->pat_win_m,
-                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt);
+                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags);
             else
                 launch_pdl(ell_pattern_win_kernel<T, MODE, 2>, grid, dim3(kEllThreads), 0, s, v, A->pat_win_m,
-                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt);
+                           (const T *)x, (T *)y, (const T *)aux, (const T *)aux2, (T *)zero, rs, red, want_sqrt, flags);
             return;
         }
         R &= ~kPatFlags;

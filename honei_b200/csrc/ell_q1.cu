@@ -198,8 +198,7 @@ namespace hb2
         if ((MODE == kDefect || MODE == kDot) && red != 0)
         {
             __shared__ double scratch[32];
-            const double sum = block_sum(part, scratch);
-            grid_sum_finish(sum, rs, red, want_sqrt, scratch);
+            ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
         }
         // copies still in flight must land before the block's shared memory is reused
         if (! fast) mbar_wait_bounded(&bar, 0, 1000000000ull);
@@ -318,23 +317,25 @@ namespace hb2
         }
         if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
         {
-            // one partial per block; q1_sum_partials_kernel adds them in block order
-            // after this launch (no fence or ticket on the block's way out)
+            // one partial per block; sum_partials_kernel adds them in block order after
+            // this launch (no fence or ticket on the block's way out)
             __shared__ double scratch[32];
             const double sum = block_sum(part, scratch);
             if (t == 0) rs.partials[blockIdx.x] = sum;
         }
     }
 
-    // the fused reduction's second step: partials[0 .. G) summed in a fixed order
-    // (thread t adds t, t + 1024, t + 2048, ... in that order, eight independent
-    // loads in flight at a time; then the block tree), so the result depends on
-    // the data and the launch shape only
+    // the fused reduction's second step: for vector j = blockIdx.x, partials[j G ..
+    // j G + G) summed in a fixed order (thread t adds t, t + 1024, t + 2048, ... in
+    // that order, eight independent loads in flight at a time; then the block
+    // tree), so the result depends on the data and the launch shape only
     constexpr int kSumThreads = 1024;
-    __global__ void __launch_bounds__(kSumThreads) q1_sum_partials_kernel(const double * __restrict__ partials,
-                                                                          unsigned G, double * out, int want_sqrt)
+    __global__ void __launch_bounds__(kSumThreads) sum_partials_kernel(const double * __restrict__ partials,
+                                                                       unsigned G, double * out, int want_sqrt)
     {
         __shared__ double scratch[32];
+        partials += (uint64_t)blockIdx.x * G;
+        out += blockIdx.x;
         pdl_entry();
         double s = 0.0;
         for (unsigned b0 = threadIdx.x; b0 < G; b0 += 8 * kSumThreads)
@@ -351,6 +352,13 @@ namespace hb2
         }
         s = block_sum(s, scratch);
         if (threadIdx.x == 0) out[0] = want_sqrt ? sqrt(s) : s;
+    }
+
+    void launch_sum_partials(const double * partials, unsigned G, unsigned nvec, double * out, int want_sqrt,
+                             cudaStream_t stream)
+    {
+        launch_pdl(sum_partials_kernel, dim3(nvec), dim3(kSumThreads), 0, stream, partials, G, out, want_sqrt);
+        count_launches(1);
     }
 
     // ------------------------------------------------------------------
@@ -640,12 +648,6 @@ namespace hb2
             {
                 launch_pdl(q1_pair_kernel<T, MODE>, grid, dim3(kEllThreads), 0, st, s, (const T *)x, (T *)y,
                            (const T *)aux, (const T *)aux2, rs, red, flags, (float *)nullptr, (float *)nullptr);
-                if ((MODE == kDefect || MODE == kDot) && red)
-                {
-                    launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials,
-                               grid.x, red, want_sqrt);
-                    count_launches(1);
-                }
                 return;
             }
             R = kPatQ1G | 2;
@@ -659,12 +661,6 @@ namespace hb2
             else if (R == 4) HB2_Q1S_(4);
             else HB2_Q1S_(8);
 #undef HB2_Q1S_
-            if ((MODE == kDefect || MODE == kDot) && red)
-            {
-                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials, grid.x,
-                           red, want_sqrt);
-                count_launches(1);
-            }
             return;
         }
         if (R & kPatQ1G)
@@ -677,12 +673,6 @@ namespace hb2
             else if (R == 2) HB2_Q1G(2);
             else HB2_Q1G(4);
 #undef HB2_Q1G
-            if ((MODE == kDefect || MODE == kDot) && red)
-            {
-                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, st, (const double *)rs.partials, grid.x,
-                           red, want_sqrt);
-                count_launches(1);
-            }
             return;
         }
         if (R == 2) q1_stencil_launch<T, MODE, 2>(s, grid, st, x, y, aux, aux2, rs, red, want_sqrt, flags);
@@ -743,7 +733,7 @@ namespace hb2
             {
                 launch_pdl(q1_pair_kernel<double, kDefectIR>, dim3(pgrid), dim3(kEllThreads), 0, stream, s, x,
                            (double *)nullptr, b, (const double *)nullptr, rs, red, 0, b32, x32);
-                launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials,
+                launch_pdl(sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials,
                            pgrid, red, 1);
                 count_launches(2);
                 HB2_LAUNCH_CHECK("IR defect launch");
@@ -751,7 +741,7 @@ namespace hb2
             }
             launch_pdl(q1_gather_kernel<double, kDefectIR, 1>, dim3(grid), dim3(kEllThreads), 0, stream, s, x,
                        (double *)nullptr, b, (const double *)nullptr, rs, red, 1, 0, b32, x32);
-            launch_pdl(q1_sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials, grid,
+            launch_pdl(sum_partials_kernel, dim3(1), dim3(kSumThreads), 0, stream, (const double *)rs.partials, grid,
                        red, 1);
             count_launches(2);
             HB2_LAUNCH_CHECK("IR defect launch");

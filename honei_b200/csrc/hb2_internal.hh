@@ -103,8 +103,9 @@ struct hb2_ell_s
     // bform 0: per slot one 32-bit word (BF16 bits of s * a, 16-bit column offset)
     // in chunks of 32 rows, the chunk's slots one after another; bform 1: BF16
     // values and int32 columns (bidx) slot-major.  With the row-sum compensated
-    // form, the diagonal in FP32 (bdiag), its slot marked in the index.  val / col
-    // hold the same operator in FP32 (a = q / s) for the paths that read them.
+    // form, bdiag holds each row's diagonal remainder (FP32, the BF16 part sits in
+    // the diagonal's slot).  val / col hold the same operator in FP32 (a = q / s)
+    // for the paths that read them.
     void * bval = nullptr;
     void * bidx = nullptr;
     float * bdiag = nullptr;
@@ -169,11 +170,36 @@ namespace hb2
     // (consecutive passes over one matrix in alternating directions start where
     // the previous pass left its lines in L2); kKeepL2 caches the matrix stream
     // in L2 (ld.cg) instead of marking it evict-first (ld.cs).
+    // kSplitSum (set by launch_ell): the fused reduction only stores one partial per
+    // block, partials[blockIdx.y * gridDim.x + blockIdx.x], and a second launch
+    // (launch_sum_partials) adds them; for launches of many blocks, where the fence
+    // and ticket every block of grid_sum_finish waits for before it exits cost more
+    // than that launch.
     enum EllFlags
     {
         kReverse = 1,
-        kKeepL2 = 2
+        kKeepL2 = 2,
+        kSplitSum = 4
     };
+    constexpr uint64_t kSplitSumMinBlocks = 4096;
+
+    // end of a fused reduction in an ELL kernel: the block's sum, then its partial
+    // (kSplitSum) or the two-level finish of grid_sum_finish
+    __device__ __forceinline__ void ell_block_reduce(double part, ReduceSlot rs, double * red, int want_sqrt, int flags,
+                                                     double * scratch)
+    {
+        const double s = block_sum(part, scratch);
+        if (flags & kSplitSum)
+        {
+            if (threadIdx.x == 0) rs.partials[(uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+        }
+        else grid_sum_finish(s, rs, red, want_sqrt, scratch);
+    }
+
+    // out[j] (sqrt when asked) = the sum of partials[j * G .. j * G + G) in a fixed
+    // order, j < nvec; one block of 1,024 threads per vector (ell.cu)
+    void launch_sum_partials(const double * partials, unsigned G, unsigned nvec, double * out, int want_sqrt,
+                             cudaStream_t stream);
 
     // Batch dimension of the ELL family: nvec vectors stored one after another
     // (vector j of y / aux at element offset j * vstride, of x at j * xstride

@@ -1179,17 +1179,20 @@ void hbo_ell_bf16_spmv_##SFX(uint64_t rows, uint64_t stride, uint64_t T, const u
                              const T_ *Ax, const uint64_t *Arl, double s, int compensate,    \
                              const float *x, float *y)                                       \
 {                                                                                            \
+    const float inv = (float)(1.0 / s);                                                      \
     for (uint64_t r = 0; r < rows; ++r) {                                                    \
         const int64_t dj = compensate ? bf16_diag(r, stride, T, Aj, Arl) : -1;               \
         const float d = dj >= 0 ? bf16_d_##SFX(r, stride, T, Aj, Ax, Arl, s, dj) : 0.f;      \
+        const float h = (float)hbo_bf16_round((double)d), l = d - h;                         \
         float acc = 0.f;                                                                     \
         for (uint64_t col = 0, j = r * T; col < Arl[r]; ++col, j += stride)                  \
             for (uint64_t t = 0; t < T; ++t) {                                               \
-                const float v = (int64_t)(j + t) == dj ? d                                   \
+                const float v = (int64_t)(j + t) == dj ? h                                   \
                                 : (float)hbo_bf16_round((double)Ax[j + t] * s);              \
                 acc = fmaf(v, x[Aj[j + t]], acc);                                            \
             }                                                                                \
-        y[r] = s == 1.0 ? acc : acc / (float)s;                                              \
+        if (dj >= 0) acc = fmaf(l, x[r], acc);                                               \
+        y[r] = s == 1.0 ? acc : acc * inv;                                                   \
     }                                                                                        \
 }                                                                                            \
 void hbo_ell_bf16_values_##SFX(uint64_t rows, uint64_t stride, uint64_t T, uint64_t K,       \
