@@ -264,7 +264,7 @@ def workload_config(args, world):
 ROW_BYTES = {"jacobi": 4, "spmv": 2, "defect": 3}   # vector accesses per row (8 B each in FP64)
 
 
-def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None, dtype=None):
+def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None, dtype=None, key_suffix=""):
     """One ELL kernel of the level-`level` operator on the layout A runs on, timed in
     its steady state: 40 launches captured in one CUDA graph, rotating over sets of
     input and output vectors of more than 2x L2 in all (every launch reads its vectors
@@ -284,7 +284,7 @@ def kernel_roofline(hb, kind, A, level, peak, dev, reps=12, label=None, dtype=No
     variant = variant_name(vk, vr, vw)
     nbytes = n * (rb + es * ROW_BYTES[kind])
     achieved = nbytes / (ms * 1e-3) / 1e9
-    key = f"{variant}:{kind}:L{level}"
+    key = f"{variant}:{kind}:L{level}{key_suffix}"
     return {"bound": "hbm", "kernel": label or f"{kind} on {variant}", "variant": variant, "level": level,
             "layout": layout_text(kind_l, table_size, rb), "achieved": achieved, "peak": peak[0], "unit": "GB/s",
             "frac": achieved / peak[0], "peak_source": peak[1], "traffic": load_traffic(key), "traffic_key": key,
@@ -739,9 +739,11 @@ def bf16_variant(hb, dev, flush, level, peaks, rank):
             finest["bf16_pure"] = finest["fp32"].to_bf16()
         for name, M in finest.items():
             kr = kernel_roofline(hb, "jacobi", M, level, peaks, dev, dtype=torch.float32,
-                                 label=f"fused Jacobi sweep, level {level}, {op} operator, {name} inner matrix")
+                                 label=f"fused Jacobi sweep, level {level}, {op} operator, {name} inner matrix",
+                                 key_suffix="" if op == "q1" else
+                                 ":coefficients" + ("" if name == "fp32" else "-" + name.split("_")[1]))
             rep[name]["sweep"] = {key: kr[key] for key in ("variant", "launch_shape", "bytes_per_row", "launch_us",
-                                                           "achieved", "frac")}
+                                                           "achieved", "frac", "traffic", "traffic_key")}
             if hasattr(M, "scale"):
                 rep[name]["scale"], rep[name]["max_rel_rounding_error"] = M.scale, M.max_rel_error
         rep["fp64_mg_cycles"] = fp64.used_iters

@@ -43,7 +43,8 @@ def test_variant_names_and_committed_traffic():
         assert t is not None and 25 * 1_050_625 <= t <= 25.1 * 1_050_625
     assert bench.load_traffic("force8:jacobi:L10") is None
     # the level-11 kernels the bench reports
-    for key in ("q1gather1:jacobi:L11", "plain:spmv:L11", "plain:defect:L11"):
+    for key in ("q1gather1:jacobi:L11", "plain:spmv:L11", "plain:defect:L11", "plain:jacobi:L11:coefficients",
+                "bf16r2:jacobi:L11:coefficients-compensated"):
         assert bench.load_traffic(key) is not None, key
 
 
