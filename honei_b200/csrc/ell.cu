@@ -188,10 +188,16 @@ namespace hb2
                 part = fma((double)acc[i], (double)x[r], part);
             }
             else if (MODE == kAdd) y[r] = M::add(y[r], acc[i]);
-            else if (MODE == kJacobi) y[r] = M::add(x[r], M::mul(aux2[r], M::sub(aux[r], acc[i])));
+            else if (MODE == kJacobi)
+            {
+                // the sweep's defect b - A x, and its square for a fused norm
+                const T d = M::sub(aux[r], acc[i]);
+                y[r] = M::add(x[r], M::mul(aux2[r], d));
+                part = fma((double)d, (double)d, part);
+            }
             else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
         }
-        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);

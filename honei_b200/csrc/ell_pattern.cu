@@ -216,10 +216,15 @@ namespace hb2
                     part = fma((double)acc[i], (double)ex[i], part);
                 }
                 else if (MODE == kAdd) y[r] = M::add(ex[i], acc[i]);
-                else if (MODE == kJacobi) y[r] = M::add(ex[i], M::mul(ep[i], M::sub(ea[i], acc[i])));
+                else if (MODE == kJacobi)
+                {
+                    const T d = M::sub(ea[i], acc[i]);
+                    y[r] = M::add(ex[i], M::mul(ep[i], d));
+                    part = fma((double)d, (double)d, part);
+                }
                 else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
             }
-            if ((MODE == kDefect || MODE == kDot) && red != 0)
+            if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
             {
                 __shared__ double scratch[32];
                 ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -397,10 +402,15 @@ namespace hb2
                 part = fma((double)acc, (double)xc, part);
             }
             else if (MODE == kAdd) y[i] = M::add(ey[k], acc);
-            else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep[k], M::sub(ea[k], acc)));
+            else if (MODE == kJacobi)
+            {
+                const T d = M::sub(ea[k], acc);
+                y[i] = M::add(xc, M::mul(ep[k], d));
+                part = fma((double)d, (double)d, part);
+            }
             else if (MODE == kRestrict) { y[i] = acc; zero[i] = T(0); }
         }
-        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);

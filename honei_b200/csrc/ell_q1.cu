@@ -193,9 +193,14 @@ namespace hb2
                 y[i] = acc;
                 part = fma((double)acc, (double)xc, part);
             }
-            else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep[k], M::sub(ea[k], acc)));
+            else if (MODE == kJacobi)
+            {
+                const T d = M::sub(ea[k], acc);
+                y[i] = M::add(xc, M::mul(ep[k], d));
+                part = fma((double)d, (double)d, part);
+            }
         }
-        if ((MODE == kDefect || MODE == kDot) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -242,7 +247,12 @@ namespace hb2
             y[i] = acc;
             part = fma((double)acc, (double)xc, part);
         }
-        else if (MODE == kJacobi) y[i] = M::add(xc, M::mul(ep, M::sub(ea, acc)));
+        else if (MODE == kJacobi)
+        {
+            const T d = M::sub(ea, acc);
+            y[i] = M::add(xc, M::mul(ep, d));
+            part = fma((double)d, (double)d, part);
+        }
     }
 
     // blocks of 128, 256 or 512 threads (autotuned); one row per thread keeps 2,048
@@ -315,7 +325,7 @@ namespace hb2
             }
             q1_epilogue<T, MODE>(y, i, acc, xc, ea[k], ep[k], part, y32, z32);
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
         {
             // one partial per block; sum_partials_kernel adds them in block order after
             // this launch (no fence or ticket on the block's way out)
@@ -391,7 +401,9 @@ namespace hb2
             part = fma((double)acc, (double)xc, part);
             return acc;
         }
-        return M::add(xc, M::mul(ep, M::sub(ea, acc)));   // kJacobi
+        const T d = M::sub(ea, acc);                       // kJacobi
+        part = fma((double)d, (double)d, part);
+        return M::add(xc, M::mul(ep, d));
     }
 
     template <typename T>
@@ -503,7 +515,7 @@ namespace hb2
             *(V *)(y + i0) = v;
         }
         else if (any) y[i0] = o0;
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
         {
             __shared__ double scratch[32];
             const double sum = block_sum(part, scratch);
@@ -610,7 +622,7 @@ namespace hb2
                 }
             }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
         {
             __shared__ double scratch[32];
             const double sum = block_sum(part, scratch);

@@ -81,7 +81,7 @@ struct hb2_mg_s
     double * ir_r;           // outer FP64 defect of hb2_ir_solve (allocated on first use, kept)
     // hb2_ir_solve as one CUDA graph, built for the outer operator and vectors of
     // the last call (rebuilt when any of them or the loop parameters change)
-    cudaStream_t cap3 = 0;
+    cudaStream_t cap3 = 0, cap4 = 0;
     cudaGraph_t ir_graph = 0;
     cudaGraphExec_t ir_exec = 0;
     const void * ir_key_A = 0, * ir_key_b = 0, * ir_key_x = 0;
@@ -89,6 +89,21 @@ struct hb2_mg_s
     uint64_t ir_key_max = 0;
     int ir_key_reset = -1;
     uint64_t ir_body_kernels = 0, ir_inner_body_kernels = 0;
+    // The convergence test's norm ||b - A x|| fused into the next cycle's first
+    // finest-level Jacobi sweep, which computes that defect anyway (fused_norm: the
+    // finest level outside the cluster kernels, at least one pre-smoothing sweep):
+    // the loop body is that sweep with its norm, the decision, and the rest of the
+    // cycle under a conditional IF node.  When the loop stops, x is the last cycle's
+    // (the sweep wrote the other Jacobi buffer).  One finest-level defect pass less
+    // per cycle, one discarded sweep per solve.  The host loop runs the two parts as
+    // graphs of their own.  Off by default (HB2_MG_FUSED_NORM=1 turns it on): measured
+    // on B200 the second conditional node per cycle costs about what the defect pass
+    // saves (level 9 +5 us, level 10 +2 us, level 11 -6 us per cycle).
+    bool fused_norm = false;
+    cudaGraph_t first_graph = 0, rest_graph = 0;
+    cudaGraphExec_t first_exec = 0, rest_exec = 0;
+    uint64_t pro_kernels = 0, first_kernels = 0, rest_kernels = 0;
+    uint64_t ir_first_kernels = 0, ir_rest_kernels = 0;
 };
 
 namespace hb2
@@ -99,10 +114,11 @@ namespace hb2
         return v && *v ? strtoull(v, 0, 10) : dflt;
     }
 
-    static int smooth(hb2_mg_s * mg, MgLevel & L, uint64_t sweeps, cudaStream_t s)
+    // `sweeps` Jacobi sweeps on level L; done = 1: the first one already ran (x -> tmp)
+    static int smooth(hb2_mg_s * mg, MgLevel & L, uint64_t sweeps, cudaStream_t s, uint64_t done = 0)
     {
-        void * cur = L.x, * nxt = L.tmp;
-        for (uint64_t k = 0; k < sweeps; ++k)
+        void * cur = done ? L.tmp : L.x, * nxt = done ? L.x : L.tmp;
+        for (uint64_t k = done; k < sweeps; ++k)
         {
             int st = launch_ell(L.A, kJacobi, cur, nxt, L.b, L.jac, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
             if (st) return st;
@@ -152,14 +168,15 @@ namespace hb2
         return st;
     }
 
-    // MGCycleCreation::_build_cycle (math/mg.hh:577-640)
-    static int record_cycle(hb2_mg_s * mg, uint32_t i, cudaStream_t s)
+    // MGCycleCreation::_build_cycle (math/mg.hh:577-640); first_done: the level's
+    // first pre-smoothing sweep already ran (the fused loop)
+    static int record_cycle(hb2_mg_s * mg, uint32_t i, cudaStream_t s, bool first_done = false)
     {
         MgLevel & L = mg->lev[i];
         if ((int)i == mg->sub_top) return record_small_levels(mg, s);
         if (i == 0) return coarse_solve(mg, s);
         MgLevel & C = mg->lev[i - 1];
-        int st = smooth(mg, L, mg->prm.n_pre_smooth, s);
+        int st = smooth(mg, L, mg->prm.n_pre_smooth, s, first_done ? 1 : 0);
         if (! st) st = launch_ell(L.A, kDefect, L.x, L.store, L.b, 0, 0, 0, 0, mg->ws, s, L.pass(L.rev_A));
         if (! st) st = launch_ell(L.R, kRestrict, L.store, C.b, 0, 0, C.x, 0, 0, mg->ws, s, L.pass(L.rev_R));
         if (! st) st = record_cycle(mg, i - 1, s);
@@ -175,6 +192,14 @@ namespace hb2
     {
         MgLevel & F = mg->lev[mg->nlev - 1];
         return launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->norm_dev, 1, mg->ws, s, F.pass(F.rev_A));
+    }
+
+    // the fused loop's first part: the finest level's first pre-smoothing sweep
+    // (x -> tmp) with the norm of its defect b - A x into norm_dev
+    static int first_sweep_norm(hb2_mg_s * mg, cudaStream_t s)
+    {
+        MgLevel & F = mg->lev[mg->nlev - 1];
+        return launch_ell(F.A, kJacobi, F.x, F.tmp, F.b, F.jac, 0, mg->norm_dev, 1, mg->ws, s, F.pass(F.rev_A));
     }
 
     static void reset_directions(hb2_mg_s * mg)
@@ -201,13 +226,70 @@ namespace hb2
         cudaGraphSetConditional(h, stop ? 0u : 1u);
     }
 
+    // the fused loop's decision, after the first sweep of the cycle that would be
+    // number k + 1 (k = cycles done): for k >= 1 the sweep's norm is ||b - A x|| after
+    // cycle k, and the stop test of mg_loop_decide_kernel applies to it; k = 0 always
+    // runs (the loop is entered only when max_iters > 0).  Sets both the IF node over
+    // the rest of the cycle and the loop's WHILE node.
+    __global__ void mg_loop_decide_pre_kernel(const double * norm, const double * r0, uint64_t * iters,
+                                              uint64_t max_iters, double eps, cudaGraphConditionalHandle hw,
+                                              cudaGraphConditionalHandle hif)
+    {
+        pdl_entry();
+        const uint64_t k = *iters;
+        const double rc = *norm;
+        const bool run = k == 0 || ! (rc < eps * *r0 || ! (rc == rc) || k >= max_iters);
+        if (run) *iters = k + 1;
+        cudaGraphSetConditional(hif, run ? 1u : 0u);
+        cudaGraphSetConditional(hw, run ? 1u : 0u);
+    }
+
     static int capture_error(cudaError_t e, const char * what, hb2_mg_s * mg)
     {
         cudaGraph_t g = 0;
+        if (mg->cap3) { cudaStreamEndCapture(mg->cap3, &g); if (g) { cudaGraphDestroy(g); g = 0; } }
         cudaStreamEndCapture(mg->cap2, &g);
+        if (g) { cudaGraphDestroy(g); g = 0; }
         cudaStreamEndCapture(mg->cap, &g);
         if (g) cudaGraphDestroy(g);
         return cuda_status(e, what);
+    }
+
+    static cudaError_t new_handle(cudaStream_t s, cudaGraphConditionalHandle * h);
+    static cudaError_t add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType t,
+                                       cudaGraph_t * body);
+
+    // the fused loop body on `s` (capturing into the WHILE node's body graph, handle
+    // hw): first sweep + norm, decision, IF (rest of the cycle), the IF body captured
+    // on mg->cap3; the kernel counts of the two parts into *first / *rest
+    static int record_fused_body(hb2_mg_s * mg, cudaStream_t s, cudaGraphConditionalHandle hw, uint64_t * first,
+                                 uint64_t * rest)
+    {
+        if (! mg->cap3) HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap3, cudaStreamNonBlocking));
+        const uint64_t c0 = hb2_launch_count();
+        int st = first_sweep_norm(mg, s);
+        if (st) return st;
+        cudaGraphConditionalHandle hif;
+        cudaError_t e = new_handle(s, &hif);
+        if (e != cudaSuccess) return cuda_status(e, "MG loop: IF handle");
+        launch_pdl(mg_loop_decide_pre_kernel, dim3(1), dim3(1), 0, s, mg->norm_dev, mg->r0_dev, mg->iters_dev,
+                   mg->prm.max_iters, mg->prm.eps_relative, hw, hif);
+        count_launches(1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_status(e, "MG loop: decide kernel");
+        *first = hb2_launch_count() - c0;
+        cudaGraph_t ifbody = 0;
+        e = add_conditional(s, hif, cudaGraphCondTypeIf, &ifbody);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(mg->cap3, ifbody, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_status(e, "MG loop: IF node");
+        const uint64_t c1 = hb2_launch_count();
+        st = record_cycle(mg, mg->nlev - 1, mg->cap3, true);
+        *rest = hb2_launch_count() - c1;
+        cudaGraph_t g = ifbody;
+        e = cudaStreamEndCapture(mg->cap3, &g);
+        if (st) return st;
+        if (e != cudaSuccess) return cuda_status(e, "MG loop: IF body");
+        return HB2_OK;
     }
 
     static int build_solve_graph(hb2_mg_s * mg)
@@ -228,6 +310,7 @@ namespace hb2
         int st = launch_ell(F.A, kDefect, F.x, mg->rfine, F.b, 0, 0, mg->r0_dev, 1, mg->ws, mg->cap, F.pass(F.rev_A));
         if (st) { capture_error(cudaSuccess, "", mg); return st; }
         mg_loop_init_kernel<<<1, 1, 0, mg->cap>>>(mg->iters_dev, mg->prm.max_iters, h);
+        count_launches(1);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(mg->cap, &cs, 0, &capg, &deps, &ndeps);
         if (e != cudaSuccess) return capture_error(e, "capture (loop init)", mg);
@@ -243,18 +326,27 @@ namespace hb2
         if (e == cudaSuccess)
             e = cudaStreamBeginCaptureToGraph(mg->cap2, body, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return capture_error(e, "capture of the loop body", mg);
+        mg->pro_kernels = hb2_launch_count() - before;
         const uint64_t body0 = hb2_launch_count();
-        st = record_cycle(mg, mg->nlev - 1, mg->cap2);
-        if (! st) st = finest_norm(mg, mg->cap2);
-        if (! st)
+        if (mg->fused_norm)
         {
-            launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap2, mg->norm_dev, mg->r0_dev, mg->iters_dev,
-                       mg->prm.max_iters, mg->prm.eps_relative, h);
-            count_launches(1);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return capture_error(e, "decide kernel", mg);
+            st = record_fused_body(mg, mg->cap2, h, &mg->first_kernels, &mg->rest_kernels);
+            if (st) { capture_error(cudaSuccess, "", mg); return st; }
         }
-        if (st) { capture_error(cudaSuccess, "", mg); return st; }
+        else
+        {
+            st = record_cycle(mg, mg->nlev - 1, mg->cap2);
+            if (! st) st = finest_norm(mg, mg->cap2);
+            if (! st)
+            {
+                launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap2, mg->norm_dev, mg->r0_dev,
+                           mg->iters_dev, mg->prm.max_iters, mg->prm.eps_relative, h);
+                count_launches(1);
+                e = cudaGetLastError();
+                if (e != cudaSuccess) return capture_error(e, "decide kernel", mg);
+            }
+            if (st) { capture_error(cudaSuccess, "", mg); return st; }
+        }
         mg->body_kernels = hb2_launch_count() - body0;
         e = cudaStreamEndCapture(mg->cap2, &body);
         if (e != cudaSuccess) return capture_error(e, "cudaStreamEndCapture (body)", mg);
@@ -292,6 +384,34 @@ namespace hb2
         mg->graph = g;
         e = cudaGraphInstantiate(&mg->exec, g, 0);
         if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+        if (! mg->fused_norm) return HB2_OK;
+        // the fused loop on the host: (first sweep + norm, its copy to the host) and
+        // (the rest of the cycle) as two graphs, the pass directions continuing from
+        // one to the other as in the device loop's body
+        reset_directions(mg);
+        HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
+        st = first_sweep_norm(mg, mg->cap);
+        if (! st)
+        {
+            e = cudaMemcpyAsync(mg->ws->host_scalars, mg->norm_dev, sizeof(double), cudaMemcpyDeviceToHost, mg->cap);
+            if (e != cudaSuccess) st = cuda_status(e, "capture D2H");
+        }
+        g = 0;
+        e = cudaStreamEndCapture(mg->cap, &g);
+        if (st) { if (g) cudaGraphDestroy(g); set_launch_count(before); return st; }
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture (first sweep)");
+        mg->first_graph = g;
+        HB2_CUDA(cudaStreamBeginCapture(mg->cap, cudaStreamCaptureModeThreadLocal));
+        st = record_cycle(mg, mg->nlev - 1, mg->cap, true);
+        g = 0;
+        e = cudaStreamEndCapture(mg->cap, &g);
+        set_launch_count(before);
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture (rest of the cycle)");
+        mg->rest_graph = g;
+        e = cudaGraphInstantiate(&mg->first_exec, mg->first_graph, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&mg->rest_exec, mg->rest_graph, 0);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate (fused loop)");
         return HB2_OK;
     }
 
@@ -378,6 +498,8 @@ namespace hb2
             HB2_CUDA(cudaStreamSynchronize(stream));
         }
         HB2_CUDA(cudaStreamSynchronize(stream));
+        mg->fused_norm = mg->nlev >= 2 && mg->sub_top < (int)mg->nlev - 1 && mg->prm.n_pre_smooth >= 1 &&
+                         env_u64("HB2_MG_FUSED_NORM", 0) != 0;
         mg->sub_fused = mg->sub_top >= 1 && env_u64("HB2_SUB_FUSED", 0) != 0 &&
                         subvcycle_supported(mg->lev[0].A, mg->coarse64);
         // prime the coarse kernel's shared-memory attribute outside the capture
@@ -442,15 +564,31 @@ namespace hb2
         const double r0 = mg->ws->host_scalars[0];
         double rc = 1e16;
         uint64_t used = 0;
-        for (uint64_t i = 0; i < mg->prm.max_iters; ++i)
+        if (mg->fused_norm)
         {
-            HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
-            count_launches(mg->graph_kernels);
-            HB2_CUDA(cudaStreamSynchronize(stream));
-            rc = mg->ws->host_scalars[0];
-            used = i + 1;
-            if (rc < mg->prm.eps_relative * r0 || ! (rc == rc)) break;
+            // the device loop's steps: first sweep + norm, decision, rest of the cycle
+            for (uint64_t k = 0; mg->prm.max_iters > 0; ++k)
+            {
+                HB2_CUDA(cudaGraphLaunch(mg->first_exec, stream));
+                count_launches(mg->first_kernels - 1);
+                HB2_CUDA(cudaStreamSynchronize(stream));
+                rc = mg->ws->host_scalars[0];
+                if (k > 0 && (rc < mg->prm.eps_relative * r0 || ! (rc == rc) || k >= mg->prm.max_iters)) break;
+                HB2_CUDA(cudaGraphLaunch(mg->rest_exec, stream));
+                count_launches(mg->rest_kernels);
+                used = k + 1;
+            }
         }
+        else
+            for (uint64_t i = 0; i < mg->prm.max_iters; ++i)
+            {
+                HB2_CUDA(cudaGraphLaunch(mg->exec, stream));
+                count_launches(mg->graph_kernels);
+                HB2_CUDA(cudaStreamSynchronize(stream));
+                rc = mg->ws->host_scalars[0];
+                used = i + 1;
+                if (rc < mg->prm.eps_relative * r0 || ! (rc == rc)) break;
+            }
         if (stats)
         {
             uint64_t cu = 0;
@@ -482,7 +620,10 @@ namespace hb2
         memcpy(&used, h + 4, sizeof(uint64_t));
         memcpy(&cu, h + 1, sizeof(uint64_t));
         const double r0 = h[3], rc = used ? h[0] : 1e16;
-        count_launches(2 + used * mg->body_kernels);
+        if (! mg->fused_norm) count_launches(mg->pro_kernels + used * mg->body_kernels);
+        else if (mg->prm.max_iters > 0)
+            count_launches(mg->pro_kernels + (used + 1) * mg->first_kernels + used * mg->rest_kernels);
+        else count_launches(mg->pro_kernels);
         if (stats)
         {
             stats[0] = (double)used;
@@ -544,9 +685,10 @@ namespace hb2
         return cudaGraphConditionalHandleCreate(h, capg, 0, cudaGraphCondAssignDefault);
     }
 
-    // a conditional WHILE node on handle h at the capture position of `s`: returns
-    // its body graph and makes the node `s`'s dependency
-    static cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t * body)
+    // a conditional node (WHILE or IF) on handle h at the capture position of `s`:
+    // returns its body graph and makes the node `s`'s dependency
+    static cudaError_t add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType t,
+                                       cudaGraph_t * body)
     {
         cudaStreamCaptureStatus cs;
         cudaGraph_t capg = 0;
@@ -556,7 +698,7 @@ namespace hb2
         if (e != cudaSuccess) return e;
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.type = t;
         cp.conditional.size = 1;
         cudaGraphNode_t node;
         e = cudaGraphAddNode(&node, capg, deps, ndeps, &cp);
@@ -565,9 +707,15 @@ namespace hb2
         return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
     }
 
+    static cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t * body)
+    {
+        return add_conditional(s, h, cudaGraphCondTypeWhile, body);
+    }
+
     static int ir_capture_error(cudaError_t e, const char * what, hb2_mg_s * mg, int st = HB2_OK)
     {
         cudaGraph_t g = 0;
+        if (mg->cap4) { cudaStreamEndCapture(mg->cap4, &g); if (g) { cudaGraphDestroy(g); g = 0; } }
         cudaStreamEndCapture(mg->cap3, &g);
         if (g) { cudaGraphDestroy(g); g = 0; }
         cudaStreamEndCapture(mg->cap2, &g);
@@ -623,14 +771,26 @@ namespace hb2
         if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(mg->cap3, ibody, 0, 0, 0, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return ir_capture_error(e, "IR inner loop", mg);
         const uint64_t ibody0 = hb2_launch_count();
-        st = record_cycle(mg, mg->nlev - 1, mg->cap3);
-        if (! st) st = finest_norm(mg, mg->cap3);
-        if (st) return ir_capture_error(cudaSuccess, "", mg, st);
-        launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap3, mg->norm_dev, mg->r0_dev, mg->iters_dev,
-                   mg->prm.max_iters, mg->prm.eps_relative, hi);
-        count_launches(1);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return ir_capture_error(e, "IR inner decide", mg);
+        if (mg->fused_norm)
+        {
+            // the inner body captured on cap3, its IF body on cap4
+            if (! mg->cap4) HB2_CUDA(cudaStreamCreateWithFlags(&mg->cap4, cudaStreamNonBlocking));
+            std::swap(mg->cap3, mg->cap4);
+            st = record_fused_body(mg, mg->cap4, hi, &mg->ir_first_kernels, &mg->ir_rest_kernels);
+            std::swap(mg->cap3, mg->cap4);
+            if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+        }
+        else
+        {
+            st = record_cycle(mg, mg->nlev - 1, mg->cap3);
+            if (! st) st = finest_norm(mg, mg->cap3);
+            if (st) return ir_capture_error(cudaSuccess, "", mg, st);
+            launch_pdl(mg_loop_decide_kernel, dim3(1), dim3(1), 0, mg->cap3, mg->norm_dev, mg->r0_dev, mg->iters_dev,
+                       mg->prm.max_iters, mg->prm.eps_relative, hi);
+            count_launches(1);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return ir_capture_error(e, "IR inner decide", mg);
+        }
         mg->ir_inner_body_kernels = hb2_launch_count() - ibody0;
         e = cudaStreamEndCapture(mg->cap3, &ibody);
         if (e != cudaSuccess) return ir_capture_error(e, "IR inner body", mg);
@@ -729,6 +889,11 @@ extern "C" int hb2_mg_destroy(hb2_mg mg)
     if (mg->ir_exec) cudaGraphExecDestroy(mg->ir_exec);
     if (mg->ir_graph) cudaGraphDestroy(mg->ir_graph);
     if (mg->cap3) cudaStreamDestroy(mg->cap3);
+    if (mg->cap4) cudaStreamDestroy(mg->cap4);
+    if (mg->first_exec) cudaGraphExecDestroy(mg->first_exec);
+    if (mg->rest_exec) cudaGraphExecDestroy(mg->rest_exec);
+    if (mg->first_graph) cudaGraphDestroy(mg->first_graph);
+    if (mg->rest_graph) cudaGraphDestroy(mg->rest_graph);
     if (mg->coarse64) hb2_ell_destroy(mg->coarse64);
     if (mg->ir_r) cudaFree(mg->ir_r);
     if (mg->vec_block) cudaFree(mg->vec_block);

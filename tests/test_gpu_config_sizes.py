@@ -172,3 +172,55 @@ def test_ir_graph_matches_the_host_loop(oracle, monkeypatch, L):
     assert np.linalg.norm(xg - xh) <= 1e-13 * np.linalg.norm(xh)
     assert abs(stg[2] - sth[2]) <= 1e-10 * sth[2]
     assert np.linalg.norm(b - oracle.ell_spmv(A0, xg)) < 1e-10 * np.linalg.norm(b) * 1.001
+
+
+@pytest.mark.parametrize("L", [9, 11])
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_fused_convergence_norm(oracle, monkeypatch, L, dt):
+    """The MG loop with its convergence norm ||b - A x|| taken from the next cycle's
+    first finest-level sweep (HB2_MG_FUSED_NORM=1) against a separate defect pass per
+    cycle (the default); on the device loop and on the host loop (HB2_MG_LOOP=host):
+    the same cycles, the same solution bits, the final norms within 1e-12 relative, and
+    in the reference-order mode the oracle's iterates bit for bit."""
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    A = oracle.q1_ell(L, npdt)
+    b = oracle.ell_spmv(A, oracle.uniform(A.rows, 42, npdt))
+    eps = 1e-10 if dt == torch.float64 else 1e-5
+    out = {}
+    for fused in ("1", "0"):
+        for loop in (None, "host"):
+            monkeypatch.setenv("HB2_MG_FUSED_NORM", fused)
+            if loop:
+                monkeypatch.setenv("HB2_MG_LOOP", loop)
+            else:
+                monkeypatch.delenv("HB2_MG_LOOP", raising=False)
+            data = hb.MGData.poisson_q1(3, L, dtype=dt,
+                                        params=hb.mg_params(max_iters_coarse=100, eps=eps, coarse_exact=True))
+            x = dvec(np.zeros(A.rows, npdt))
+            hb.MGSolver.value(data, dvec(b), x)
+            out[(fused, loop)] = (host(x), data.used_iters, data.rnorm_final)
+    ref = out[("0", None)]
+    for key, (x, it, rn) in out.items():
+        assert it == ref[1], key
+        assert same_bits(x, ref[0]), key
+        assert abs(rn - ref[2]) <= 1e-12 * ref[2], key
+    if L == 9:
+        xo, ito, _ = oracle.mg_q1(L, b, max_iters_coarse=100, eps=eps)
+        assert ref[1] == ito and same_bits(ref[0], xo)
+
+
+def test_fused_norm_stops_at_the_cycle_cap(monkeypatch):
+    """max_iters cycles: the loop runs exactly that many, with or without the fused norm"""
+    L = 9
+    n = ((1 << L) + 1) ** 2
+    b = DenseVector(torch.rand(n, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(7)))
+    res = []
+    for fused in ("1", "0"):
+        monkeypatch.setenv("HB2_MG_FUSED_NORM", fused)
+        data = hb.MGData.poisson_q1(3, L, params=hb.mg_params(max_iters=3, max_iters_coarse=100, eps=1e-14))
+        x = DenseVector(torch.zeros(n, dtype=torch.float64, device="cuda"))
+        hb.MGSolver.value(data, b, x)
+        res.append((host(x), data.used_iters, data.rnorm_final))
+    assert res[0][1] == res[1][1] == 3
+    assert same_bits(res[0][0], res[1][0])
+    assert abs(res[0][2] - res[1][2]) <= 1e-12 * res[1][2]
