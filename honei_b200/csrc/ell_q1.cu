@@ -27,6 +27,7 @@
 #include "hb2_internal.hh"
 #include "tma.cuh"
 
+#include <cstdlib>
 #include <vector>
 
 namespace hb2
@@ -39,7 +40,14 @@ namespace hb2
         const PatEnt<T> * tab;   // npat * 9 (value, column - row) entries
         int64_t n, m;
         uint32_t full;           // pattern id of the full stencil row
+        int64_t pf = 0;          // gather form: L2 prefetch distance in rows (0: none)
     };
+
+    // a hint: the line of `p` (a generic address of global memory) into L2
+    __device__ __forceinline__ void prefetch_l2(const void * p)
+    {
+        asm volatile("prefetch.L2 [%0];" :: "l"(p));
+    }
 
     // diagnostic: set when a block's window copies did not complete in time
     __device__ int g_q1_stencil_timeout = 0;
@@ -277,6 +285,19 @@ namespace hb2
             p[k] = i < n ? (uint32_t)((flags & kKeepL2) ? __ldcg(s.pat + i) : __ldcs(s.pat + i)) : s.full;
         }
         pdl_entry();   // x, rhs and P may come from the previous kernel
+        if (s.pf)
+        {
+            // the rows a later wave of blocks will take (in the pass's direction): their
+            // pattern ids, x, rhs and P into L2 while this wave's loads are in flight
+            const int64_t j = (flags & kReverse) ? i0 - s.pf : i0 + s.pf;
+            if (j >= 0 && j < n)
+            {
+                if ((t & 31) == 0) prefetch_l2(s.pat + j);
+                prefetch_l2(x + j);
+                if (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR) prefetch_l2(aux + j);
+                if (MODE == kJacobi) prefetch_l2(aux2 + j);
+            }
+        }
         T xv[R][9], ea[R], ep[R];
 #pragma unroll
         for (int k = 0; k < R; ++k)
@@ -637,6 +658,18 @@ namespace hb2
         return ceil_div(m * strips, bs);
     }
 
+    // gather form's L2 prefetch distance in rows: half a wave of resident rows (2,048
+    // per SM) ahead in FP64, none in FP32 -- measured (graph-timed, levels 10 and 11):
+    // FP64 sweep 25.9 -> 24.0 us at level 11, 0.25-0.75 waves within 2 % of that, no
+    // gain at any distance in FP32.  HB2_Q1_PREFETCH=<waves> overrides (0: none); read
+    // at each launch.
+    static int64_t q1_prefetch_rows(size_t elem)
+    {
+        const char * v = getenv("HB2_Q1_PREFETCH");
+        const double w = v && *v ? atof(v) : (elem == 8 ? 0.5 : 0.0);
+        return w > 0 ? (int64_t)(w * num_sms() * 2048.0) : 0;
+    }
+
     template <typename T, int MODE>
     static void q1_stencil_mode(const hb2_ell_s * A, int R, dim3 grid, cudaStream_t st, const void * x, void * y,
                                 const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
@@ -649,6 +682,7 @@ namespace hb2
         s.n = (int64_t)A->rows;
         s.m = A->pat_win_m;
         s.full = (uint32_t)A->q1_full;
+        s.pf = (R & kPatQ1G) ? q1_prefetch_rows(sizeof(T)) : 0;
         if (R & kPatQ1P)
         {
             // two adjacent rows per thread; the interleaved form where the vectors are
