@@ -43,11 +43,6 @@ namespace hb2
         int64_t pf = 0;          // gather form: L2 prefetch distance in rows (0: none)
     };
 
-    // a hint: the line of `p` (a generic address of global memory) into L2
-    __device__ __forceinline__ void prefetch_l2(const void * p)
-    {
-        asm volatile("prefetch.L2 [%0];" :: "l"(p));
-    }
 
     // diagnostic: set when a block's window copies did not complete in time
     __device__ int g_q1_stencil_timeout = 0;
@@ -658,18 +653,6 @@ namespace hb2
         return ceil_div(m * strips, bs);
     }
 
-    // gather form's L2 prefetch distance in rows: half a wave of resident rows (2,048
-    // per SM) ahead in FP64, none in FP32 -- measured (graph-timed, levels 10 and 11):
-    // FP64 sweep 25.9 -> 24.0 us at level 11, 0.25-0.75 waves within 2 % of that, no
-    // gain at any distance in FP32.  HB2_Q1_PREFETCH=<waves> overrides (0: none); read
-    // at each launch.
-    static int64_t q1_prefetch_rows(size_t elem)
-    {
-        const char * v = getenv("HB2_Q1_PREFETCH");
-        const double w = v && *v ? atof(v) : (elem == 8 ? 0.5 : 0.0);
-        return w > 0 ? (int64_t)(w * num_sms() * 2048.0) : 0;
-    }
-
     template <typename T, int MODE>
     static void q1_stencil_mode(const hb2_ell_s * A, int R, dim3 grid, cudaStream_t st, const void * x, void * y,
                                 const void * aux, const void * aux2, ReduceSlot rs, double * red, int want_sqrt,
@@ -682,7 +665,7 @@ namespace hb2
         s.n = (int64_t)A->rows;
         s.m = A->pat_win_m;
         s.full = (uint32_t)A->q1_full;
-        s.pf = (R & kPatQ1G) ? q1_prefetch_rows(sizeof(T)) : 0;
+        s.pf = (R & kPatQ1G) ? l2_prefetch_rows(sizeof(T)) : 0;
         if (R & kPatQ1P)
         {
             // two adjacent rows per thread; the interleaved form where the vectors are

@@ -316,4 +316,19 @@ namespace hb2
 
     extern int g_num_sms;
     int num_sms();
+
+    // a hint: the line of `p` (a generic address of global memory) into L2
+    __device__ __forceinline__ void prefetch_l2(const void * p)
+    {
+        asm volatile("prefetch.L2 [%0];" :: "l"(p));
+    }
+
+    // L2 prefetch distance of the streaming one-row-per-thread kernels, in rows: half a
+    // wave of resident rows (2,048 per SM) ahead -- for the Q1 stencil kernel's gather
+    // form in FP64 only (graph-timed, level 11: FP64 sweep 25.9 -> 23.7 us, 0.25-0.75
+    // waves within 2 % of that; no gain at any distance in FP32), for the Q1 transfer
+    // kernels in both precisions (level-11 prolongation 26.2 -> 23.0 us FP64, 23.9 ->
+    // 21.4 us FP32; restriction 10.8 -> 10.1 us FP64).  HB2_Q1_PREFETCH=<waves>
+    // overrides (0: none); read at each launch (runtime.cu).
+    int64_t l2_prefetch_rows(size_t elem, bool fp32 = false);
 }

@@ -10,6 +10,8 @@
 #include "hb2_common.cuh"
 #include "hb2_internal.hh"
 
+#include <cstdlib>
+
 namespace hb2
 {
     struct Mask
@@ -141,26 +143,62 @@ namespace hb2
     // as the ELL kernels sum it (0 + v0 x0 + v1 x1 ..., products and sums rounded
     // separately; q1_prolong_row / q1_restrict_row), so the results are bit-identical
     // to the matrix products.
-    template <typename T, int MODE>
+    // R fine rows per thread, interleaved over the block (every access coalesced); the
+    // rows' y loads (kAdd) issued before their coarse gathers
+    template <typename T, int MODE, int R>
     __global__ void __launch_bounds__(256)
-    q1_prolong_kernel(const T * __restrict__ c, T * __restrict__ y, uint32_t mf, uint32_t mc, uint64_t nf)
+    q1_prolong_kernel(const T * __restrict__ c, T * __restrict__ y, uint32_t mf, uint32_t mc, uint64_t nf,
+                      int64_t pf)
     {
         typedef Arith<T> M;
         pdl_entry();
-        const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        if (r >= nf) return;
-        const T acc = q1_prolong_row<T, false>(r, c, mf, mc);
-        y[r] = MODE == kAdd ? M::add(y[r], acc) : acc;
+        const uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x * R + threadIdx.x;
+        T yv[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const uint64_t r = r0 + (uint64_t)k * blockDim.x;
+            yv[k] = (MODE == kAdd && r < nf) ? y[r] : T(0);
+            // the fine vector of a later wave of blocks into L2 (y += P c reads it)
+            if (MODE == kAdd && pf && r + pf < nf) prefetch_l2(y + r + pf);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const uint64_t r = r0 + (uint64_t)k * blockDim.x;
+            if (r >= nf) break;
+            const T acc = q1_prolong_row<T, false>(r, c, mf, mc);
+            y[r] = MODE == kAdd ? M::add(yv[k], acc) : acc;
+        }
+    }
+
+    // rows per thread of the prolongation kernel: 2 (graph-timed, level 11, with the
+    // L2 prefetch: FP64 19.8 / 18.1 / 21.3 us for 1 / 2 / 4 rows, FP32 18.9 / 16.1 /
+    // 16.1 us; the first form, one row and y loaded after the gathers, 26.2 / 23.9 us);
+    // HB2_Q1_PROLONG_R (1, 2 or 4) overrides
+    static int prolong_rows()
+    {
+        const char * v = getenv("HB2_Q1_PROLONG_R");
+        const int r = v && *v ? atoi(v) : 2;
+        return (r == 1 || r == 4) ? r : 2;
     }
 
     template <typename T, int MODE>
     __global__ void __launch_bounds__(256)
     q1_restrict_kernel(const T * __restrict__ x, T * __restrict__ y, T * __restrict__ zero, uint32_t mf,
-                       uint32_t mc, uint64_t nc)
+                       uint32_t mc, uint64_t nc, int64_t pf)
     {
         pdl_entry();
         const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= nc) return;
+        if (pf && r + pf < nc)
+        {
+            // the three fine grid rows a later wave's coarse row reads, into L2
+            const uint64_t rr = r + pf, I = rr / mc, J = rr - I * mc, f = 2 * I * mf + 2 * J, nf = (uint64_t)mf * mf;
+            if (f >= mf) prefetch_l2(x + f - mf);
+            prefetch_l2(x + f);
+            if (f + mf < nf) prefetch_l2(x + f + mf);
+        }
         y[r] = q1_restrict_row<T, false>(r, x, mf, mc);
         if (MODE == kRestrict) zero[r] = T(0);
     }
@@ -174,16 +212,26 @@ namespace hb2
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         const dim3 grid(ceil_div(A->rows, 256));
+        const int64_t pf = l2_prefetch_rows(sizeof(T), true);
         if (A->q1_transfer > 0)
         {
-            if (mode == kAdd) launch_pdl(q1_prolong_kernel<T, kAdd>, grid, dim3(256), 0, s, xp, yp, mf, mc, A->rows);
-            else launch_pdl(q1_prolong_kernel<T, kPlain>, grid, dim3(256), 0, s, xp, yp, mf, mc, A->rows);
+            const int R = prolong_rows();
+            const dim3 pgrid(ceil_div(A->rows, 256 * R));
+#define HB2_PROL(R_)                                                                                                   \
+            if (mode == kAdd) launch_pdl(q1_prolong_kernel<T, kAdd, R_>, pgrid, dim3(256), 0, s, xp, yp, mf, mc, A->rows, pf); \
+            else launch_pdl(q1_prolong_kernel<T, kPlain, R_>, pgrid, dim3(256), 0, s, xp, yp, mf, mc, A->rows, pf)
+            if (R == 4) { HB2_PROL(4); }
+            else if (R == 2) { HB2_PROL(2); }
+            else { HB2_PROL(1); }
+#undef HB2_PROL
         }
         else
         {
             if (mode == kRestrict)
-                launch_pdl(q1_restrict_kernel<T, kRestrict>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows);
-            else launch_pdl(q1_restrict_kernel<T, kPlain>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows);
+                launch_pdl(q1_restrict_kernel<T, kRestrict>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows,
+                           pf);
+            else launch_pdl(q1_restrict_kernel<T, kPlain>, grid, dim3(256), 0, s, xp, yp, (T *)zero, mf, mc, A->rows,
+                            pf);
         }
         return HB2_OK;
     }

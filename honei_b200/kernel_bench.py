@@ -82,6 +82,12 @@ def graph_time(name, A, P, n, dt, npdt, dev, reps, launches=40):
         elif name == "defect":
             _lib.call("hb2_defect_ell", A.handle, ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x.data_ptr()),
                       ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(nrm.data_ptr()), st)
+        elif name == "prolong":
+            # A = the prolongation: b (fine) += A x[:coarse]
+            _lib.call("hb2_product_add_ell", A.handle, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(b.data_ptr()), st)
+        elif name == "restrict":
+            # A = the restriction: y[:coarse] = A x (fine)
+            _lib.call("hb2_product_ell", A.handle, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()), st)
         else:
             y.copy_(x)
 
@@ -256,15 +262,16 @@ def main(argv=None) -> int:
     peak = peak_gbs()
     if a.flush == "graph":
         for name in names:
-            if name not in ("jacobi", "spmv", "defect", "copy"):
+            if name not in ("jacobi", "spmv", "defect", "copy", "prolong", "restrict"):
                 continue
-            ms = graph_time(name, A, P, n, dt, npdt, dev, a.iters)
+            M = A if name not in ("prolong", "restrict") else (Pm if name == "prolong" else Rm)
+            ms = graph_time(name, M, P, n, dt, npdt, dev, a.iters)
             nbytes = kernels[name][1]
             gbs = nbytes / (ms * 1e-3) / 1e9
             print(json.dumps({"kernel": name, "level": L, "dtype": a.dtype, "operator": a.operator,
-                              "storage": a.storage, "rows": n, "layout": A.layout()[0],
-                              "variant": list(A.layout_variant(0 if name != "defect" else 1)) if name != "copy" else None,
-                              "launch_shape": list(A.launch_shape(0 if name != "defect" else 1)),
+                              "storage": a.storage, "rows": n, "layout": M.layout()[0],
+                              "variant": list(M.layout_variant(0 if name != "defect" else 1)) if name != "copy" else None,
+                              "launch_shape": list(M.launch_shape(0 if name != "defect" else 1)),
                               "flush": "graph", "matrix_bytes_per_row": rb, "launch_us": 1000 * ms,
                               "algorithmic_bytes": nbytes, "gbs": gbs, "frac_of_measured_peak": gbs / peak}), flush=True)
         return 0
