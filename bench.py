@@ -461,6 +461,20 @@ def roofline_extra(hb, A, L, peaks, dev):
         A10 = hb.SparseMatrixELL.poisson_q1(10)
         out.append(kernel_roofline(hb, "jacobi", A10, 10, peaks, dev, label="fused Jacobi sweep, level 10, tuned layout"))
         del A10
+    # the same sweep with the L2 prefetch option (half a wave of rows ahead; off in the
+    # solvers, where it cost 1-4 %: a level's vectors partly stay in L2 between passes)
+    old_pf = os.environ.get("HB2_Q1_PREFETCH")
+    os.environ["HB2_Q1_PREFETCH"] = "0.5"
+    try:
+        e = kernel_roofline(hb, "jacobi", A, L, peaks, dev,
+                            label=f"fused Jacobi sweep, level {L}, tuned layout, L2 prefetch option (HB2_Q1_PREFETCH=0.5)")
+    finally:
+        if old_pf is None:
+            del os.environ["HB2_Q1_PREFETCH"]
+        else:
+            os.environ["HB2_Q1_PREFETCH"] = old_pf
+    e["traffic"], e["traffic_key"] = None, None
+    out.append(e)
     old = os.environ.get("HB2_ELL_COMPACT")
     os.environ["HB2_ELL_COMPACT"] = "0"        # the plain layout (read when a matrix is created)
     try:

@@ -323,12 +323,14 @@ namespace hb2
         asm volatile("prefetch.L2 [%0];" :: "l"(p));
     }
 
-    // L2 prefetch distance of the streaming one-row-per-thread kernels, in rows: half a
-    // wave of resident rows (2,048 per SM) ahead -- for the Q1 stencil kernel's gather
-    // form in FP64 only (graph-timed, level 11: FP64 sweep 25.9 -> 23.7 us, 0.25-0.75
-    // waves within 2 % of that; no gain at any distance in FP32), for the Q1 transfer
-    // kernels in both precisions (level-11 prolongation 26.2 -> 23.0 us FP64, 23.9 ->
-    // 21.4 us FP32; restriction 10.8 -> 10.1 us FP64).  HB2_Q1_PREFETCH=<waves>
-    // overrides (0: none); read at each launch (runtime.cu).
-    int64_t l2_prefetch_rows(size_t elem, bool fp32 = false);
+    // L2 prefetch distance of the streaming one-row-per-thread kernels (the Q1 stencil
+    // kernel's gather form, the Q1 transfer kernels), in rows: HB2_Q1_PREFETCH=<waves>
+    // of resident rows (2,048 per SM) ahead, read at each launch (runtime.cu); none by
+    // default.  Measured: with every launch reading its vectors from DRAM (graph-timed,
+    // vector sets of more than twice L2) half a wave ahead takes the level-11 FP64
+    // sweep from 25.9 to 23.7 us (0.82 -> 0.90 of measured HBM; no gain in FP32) and
+    // the prolongation from 26.2 to 23.0 us; inside the MG solve, where a level's
+    // vectors partly stay in L2 from pass to pass and the kernels are issue-bound, it
+    // made the solves 1-4 % slower at levels 9-11.
+    int64_t l2_prefetch_rows(size_t elem);
 }

@@ -32,10 +32,10 @@ namespace hb2
     // off by default: inside CUDA graphs on B200 the launch gaps are already
     // hidden (measured: MG level 10 3.349 ms with, 3.343 ms without; level 11
     // 6.73 / 6.51 ms); HB2_PDL=1 turns it on
-    int64_t l2_prefetch_rows(size_t elem, bool fp32)
+    int64_t l2_prefetch_rows(size_t)
     {
         const char * v = getenv("HB2_Q1_PREFETCH");
-        const double w = v && *v ? atof(v) : ((elem == 8 || fp32) ? 0.5 : 0.0);
+        const double w = v && *v ? atof(v) : 0.0;
         return w > 0 ? (int64_t)(w * num_sms() * 2048.0) : 0;
     }
 

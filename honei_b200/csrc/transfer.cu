@@ -172,15 +172,17 @@ namespace hb2
         }
     }
 
-    // rows per thread of the prolongation kernel: 2 (graph-timed, level 11, with the
-    // L2 prefetch: FP64 19.8 / 18.1 / 21.3 us for 1 / 2 / 4 rows, FP32 18.9 / 16.1 /
-    // 16.1 us; the first form, one row and y loaded after the gathers, 26.2 / 23.9 us);
+    // rows per thread of the prolongation kernel: 2 for fine grids of 2^21 rows or more,
+    // else 1 (graph-timed at level 11 with an L2 prefetch: FP64 19.8 / 18.1 / 21.3 us for
+    // 1 / 2 / 4 rows, FP32 18.9 / 16.1 / 16.1 us; the first form, one row and y loaded
+    // after the gathers, 26.2 / 23.9 us; inside the MG solves two rows helped at level 11
+    // and cost 0.5 % at levels 9 and 10, where the grid of blocks is small);
     // HB2_Q1_PROLONG_R (1, 2 or 4) overrides
-    static int prolong_rows()
+    static int prolong_rows(uint64_t nf)
     {
         const char * v = getenv("HB2_Q1_PROLONG_R");
-        const int r = v && *v ? atoi(v) : 2;
-        return (r == 1 || r == 4) ? r : 2;
+        const int r = v && *v ? atoi(v) : (nf >= (1u << 21) ? 2 : 1);
+        return (r == 2 || r == 4) ? r : 1;
     }
 
     template <typename T, int MODE>
@@ -212,10 +214,10 @@ namespace hb2
         const T * xp = (const T *)x;
         T * yp = (T *)y;
         const dim3 grid(ceil_div(A->rows, 256));
-        const int64_t pf = l2_prefetch_rows(sizeof(T), true);
+        const int64_t pf = l2_prefetch_rows(sizeof(T));
         if (A->q1_transfer > 0)
         {
-            const int R = prolong_rows();
+            const int R = prolong_rows(A->rows);
             const dim3 pgrid(ceil_div(A->rows, 256 * R));
 #define HB2_PROL(R_)                                                                                                   \
             if (mode == kAdd) launch_pdl(q1_prolong_kernel<T, kAdd, R_>, pgrid, dim3(256), 0, s, xp, yp, mf, mc, A->rows, pf); \
