@@ -370,7 +370,7 @@ namespace hb2
                 part = fma((double)acc[i], (double)x[r], part);
             }
             else if (MODE == kAdd) y[r] = M::add(y[r], acc[i]);
-            else if (MODE == kJacobi)
+            else if (is_jacobi(MODE))
             {
                 const float d = M::sub(aux[r], acc[i]);
                 y[r] = M::add(x[r], M::mul(aux2[r], d));
@@ -378,7 +378,7 @@ namespace hb2
             }
             else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = 0.f; }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -444,7 +444,10 @@ namespace hb2
             case kDefect: bf16_mode<kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R); break;
             case kDot: bf16_mode<kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R); break;
             case kAdd: bf16_mode<kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R); break;
-            case kJacobi: bf16_mode<kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R); break;
+            case kJacobi:
+                if (red) bf16_mode<kJacobiNorm>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R);
+                else bf16_mode<kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R);
+                break;
             case kRestrict: bf16_mode<kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs, R); break;
         }
     }

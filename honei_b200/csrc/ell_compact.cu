@@ -259,7 +259,7 @@ namespace hb2
                 part = fma((double)acc[i], (double)x[r], part);
             }
             else if (MODE == kAdd) y[r] = M::add(y[r], acc[i]);
-            else if (MODE == kJacobi)
+            else if (is_jacobi(MODE))
             {
                 // the sweep's defect b - A x, and its square for a fused norm
                 const T d = M::sub(aux[r], acc[i]);
@@ -268,7 +268,7 @@ namespace hb2
             }
             else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -317,7 +317,10 @@ namespace hb2
             case kDefect: compact_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
             case kDot: compact_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
             case kAdd: compact_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
-            case kJacobi: compact_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
+            case kJacobi:
+                if (red) compact_mode<T, kJacobiNorm>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs);
+                else compact_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs);
+                break;
             case kRestrict: compact_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, bs); break;
         }
     }

@@ -168,8 +168,8 @@ namespace hb2
                 const bool ok = r < A.rows;
                 p[i] = ok ? (uint32_t)__ldcs(A.pat + r) : 0u;
                 acc[i] = T(0);
-                if (MODE == kDefect || MODE == kJacobi) ea[i] = ok ? aux[r] : T(0);
-                if (MODE == kJacobi) { ep[i] = ok ? aux2[r] : T(0); ex[i] = ok ? x[r] : T(0); }
+                if (MODE == kDefect || is_jacobi(MODE)) ea[i] = ok ? aux[r] : T(0);
+                if (is_jacobi(MODE)) { ep[i] = ok ? aux2[r] : T(0); ex[i] = ok ? x[r] : T(0); }
                 if (MODE == kDot) ex[i] = ok ? x[r] : T(0);
                 if (MODE == kAdd) ex[i] = ok ? y[r] : T(0);
             }
@@ -216,7 +216,7 @@ namespace hb2
                     part = fma((double)acc[i], (double)ex[i], part);
                 }
                 else if (MODE == kAdd) y[r] = M::add(ex[i], acc[i]);
-                else if (MODE == kJacobi)
+                else if (is_jacobi(MODE))
                 {
                     const T d = M::sub(ea[i], acc[i]);
                     y[r] = M::add(ex[i], M::mul(ep[i], d));
@@ -224,7 +224,7 @@ namespace hb2
                 }
                 else if (MODE == kRestrict) { y[r] = acc[i]; zero[r] = T(0); }
             }
-            if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
+            if ((MODE == kDefect || MODE == kDot || MODE == kJacobiNorm) && red != 0)
             {
                 __shared__ double scratch[32];
                 ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -316,8 +316,8 @@ namespace hb2
         {
             const int64_t i = r0 + (int64_t)k * kEllThreads + t;
             const bool ok = i < n;
-            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi)) ? aux[i] : T(0);
-            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+            ea[k] = (ok && (MODE == kDefect || is_jacobi(MODE))) ? aux[i] : T(0);
+            ep[k] = (ok && is_jacobi(MODE)) ? aux2[i] : T(0);
             ey[k] = (ok && MODE == kAdd) ? y[i] : T(0);
         }
         if (t == 0)
@@ -388,7 +388,7 @@ namespace hb2
                     acc = M::add(acc, M::mul(e.val, xv));
                 }
             }
-            const T xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[(i - wbase[1]) + W] : x[i]) : T(0);
+            const T xc = (is_jacobi(MODE) || MODE == kDot) ? (fast ? win[(i - wbase[1]) + W] : x[i]) : T(0);
             if (MODE == kPlain) y[i] = acc;
             else if (MODE == kDefect)
             {
@@ -402,7 +402,7 @@ namespace hb2
                 part = fma((double)acc, (double)xc, part);
             }
             else if (MODE == kAdd) y[i] = M::add(ey[k], acc);
-            else if (MODE == kJacobi)
+            else if (is_jacobi(MODE))
             {
                 const T d = M::sub(ea[k], acc);
                 y[i] = M::add(xc, M::mul(ep[k], d));
@@ -410,7 +410,7 @@ namespace hb2
             }
             else if (MODE == kRestrict) { y[i] = acc; zero[i] = T(0); }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -476,7 +476,10 @@ namespace hb2
             case kDefect: pattern_mode<T, kDefect>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
             case kDot: pattern_mode<T, kDot>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
             case kAdd: pattern_mode<T, kAdd>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
-            case kJacobi: pattern_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
+            case kJacobi:
+                if (red) pattern_mode<T, kJacobiNorm>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs);
+                else pattern_mode<T, kJacobi>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs);
+                break;
             case kRestrict: pattern_mode<T, kRestrict>(A, x, y, aux, aux2, zero, red, want_sqrt, rs, grid, s, f, b, R, bs); break;
         }
     }

@@ -117,8 +117,8 @@ namespace hb2
         {
             const int64_t i = i0 + k * kEllThreads;
             const bool ok = i < n;
-            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi)) ? aux[i] : T(0);
-            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+            ea[k] = (ok && (MODE == kDefect || is_jacobi(MODE))) ? aux[i] : T(0);
+            ep[k] = (ok && is_jacobi(MODE)) ? aux2[i] : T(0);
         }
         int64_t lo[3], hi[3], alo[3], ahi[3];
 #pragma unroll
@@ -182,7 +182,7 @@ namespace hb2
             else
             {
                 acc = q1_any_row<T, W>(s.tab + p[k] * 9u, x, i, win, alo[0], alo[1], alo[2], fast);
-                xc = (MODE == kJacobi || MODE == kDot) ? (fast ? win[o1 + l + 1] : x[i]) : T(0);
+                xc = (is_jacobi(MODE) || MODE == kDot) ? (fast ? win[o1 + l + 1] : x[i]) : T(0);
             }
             if (MODE == kPlain) y[i] = acc;
             else if (MODE == kDefect)
@@ -196,14 +196,14 @@ namespace hb2
                 y[i] = acc;
                 part = fma((double)acc, (double)xc, part);
             }
-            else if (MODE == kJacobi)
+            else if (is_jacobi(MODE))
             {
                 const T d = M::sub(ea[k], acc);
                 y[i] = M::add(xc, M::mul(ep[k], d));
                 part = fma((double)d, (double)d, part);
             }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             ell_block_reduce(part, rs, red, want_sqrt, flags, scratch);
@@ -250,7 +250,7 @@ namespace hb2
             y[i] = acc;
             part = fma((double)acc, (double)xc, part);
         }
-        else if (MODE == kJacobi)
+        else if (is_jacobi(MODE))
         {
             const T d = M::sub(ea, acc);
             y[i] = M::add(xc, M::mul(ep, d));
@@ -289,8 +289,8 @@ namespace hb2
             {
                 if ((t & 31) == 0) prefetch_l2(s.pat + j);
                 prefetch_l2(x + j);
-                if (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR) prefetch_l2(aux + j);
-                if (MODE == kJacobi) prefetch_l2(aux2 + j);
+                if (MODE == kDefect || is_jacobi(MODE) || MODE == kDefectIR) prefetch_l2(aux + j);
+                if (is_jacobi(MODE)) prefetch_l2(aux2 + j);
             }
         }
         T xv[R][9], ea[R], ep[R];
@@ -317,8 +317,8 @@ namespace hb2
                 for (int q = 0; q < 9; ++q) xv[k][q] = T(0);
             }
             const bool ok = i < n;
-            ea[k] = (ok && (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR)) ? aux[i] : T(0);
-            ep[k] = (ok && MODE == kJacobi) ? aux2[i] : T(0);
+            ea[k] = (ok && (MODE == kDefect || is_jacobi(MODE) || MODE == kDefectIR)) ? aux[i] : T(0);
+            ep[k] = (ok && is_jacobi(MODE)) ? aux2[i] : T(0);
         }
         double part = 0.0;
 #pragma unroll
@@ -337,11 +337,11 @@ namespace hb2
             else
             {
                 acc = q1_any_row<T, 1>(s.tab + p[k] * 9u, x, i, nullptr, 0, 0, 0, false);
-                xc = (MODE == kJacobi || MODE == kDot) ? x[i] : T(0);
+                xc = (is_jacobi(MODE) || MODE == kDot) ? x[i] : T(0);
             }
             q1_epilogue<T, MODE>(y, i, acc, xc, ea[k], ep[k], part, y32, z32);
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobiNorm) && red != 0)
         {
             // one partial per block; sum_partials_kernel adds them in block order after
             // this launch (no fence or ticket on the block's way out)
@@ -474,12 +474,12 @@ namespace hb2
             d[0] = d01.x; d[1] = d01.y; d[2] = d23.x; d[3] = d23.y;
         }
         T ea0 = T(0), ea1 = T(0), ep0 = T(0), ep1 = T(0);
-        if (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR)
+        if (MODE == kDefect || is_jacobi(MODE) || MODE == kDefectIR)
         {
             if (two) { const V v = *(const V *)(aux + i0); ea0 = v.x; ea1 = v.y; }
             else if (any) ea0 = aux[i0];
         }
-        if (MODE == kJacobi)
+        if (is_jacobi(MODE))
         {
             if (two) { const V v = *(const V *)(aux2 + i0); ep0 = v.x; ep1 = v.y; }
             else if (any) ep0 = aux2[i0];
@@ -493,7 +493,7 @@ namespace hb2
             else
             {
                 acc = q1_any_row<T, 1>(s.tab + p0 * 9u, x, i0, nullptr, 0, 0, 0, false);
-                xc = (MODE == kJacobi || MODE == kDot) ? x[i0] : T(0);
+                xc = (is_jacobi(MODE) || MODE == kDot) ? x[i0] : T(0);
             }
             o0 = q1_pair_out<T, MODE>(acc, xc, ea0, ep0, part);
         }
@@ -504,7 +504,7 @@ namespace hb2
             else
             {
                 acc = q1_any_row<T, 1>(s.tab + p1 * 9u, x, i0 + 1, nullptr, 0, 0, 0, false);
-                xc = (MODE == kJacobi || MODE == kDot) ? x[i0 + 1] : T(0);
+                xc = (is_jacobi(MODE) || MODE == kDot) ? x[i0 + 1] : T(0);
             }
             o1 = q1_pair_out<T, MODE>(acc, xc, ea1, ep1, part);
         }
@@ -531,7 +531,7 @@ namespace hb2
             *(V *)(y + i0) = v;
         }
         else if (any) y[i0] = o0;
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             const double sum = block_sum(part, scratch);
@@ -624,8 +624,8 @@ namespace hb2
                 T lo[3];
                 q1_strip_row<T>(x, i + m, n, keep, lo);
                 const uint32_t p = keep ? __ldcg(s.pat + i) : __ldcs(s.pat + i);
-                const T ea = (MODE == kDefect || MODE == kJacobi || MODE == kDefectIR) ? aux[i] : T(0);
-                const T ep = MODE == kJacobi ? aux2[i] : T(0);
+                const T ea = (MODE == kDefect || is_jacobi(MODE) || MODE == kDefectIR) ? aux[i] : T(0);
+                const T ep = is_jacobi(MODE) ? aux2[i] : T(0);
                 T acc;
                 if (p == s.full && i >= m + 1 && i + m + 1 < n) acc = q1_row9<T>(s, up, mid, lo);
                 else acc = q1_any_row<T, 1>(s.tab + p * 9u, x, i, nullptr, 0, 0, 0, false);
@@ -638,7 +638,7 @@ namespace hb2
                 }
             }
         }
-        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobi) && red != 0)
+        if ((MODE == kDefect || MODE == kDot || MODE == kDefectIR || MODE == kJacobiNorm) && red != 0)
         {
             __shared__ double scratch[32];
             const double sum = block_sum(part, scratch);
@@ -728,6 +728,7 @@ namespace hb2
             if (mode == kPlain) HB2_Q1S(double, kPlain);
             else if (mode == kDefect) HB2_Q1S(double, kDefect);
             else if (mode == kDot) HB2_Q1S(double, kDot);
+            else if (red) HB2_Q1S(double, kJacobiNorm);
             else HB2_Q1S(double, kJacobi);
         }
         else
@@ -735,6 +736,7 @@ namespace hb2
             if (mode == kPlain) HB2_Q1S(float, kPlain);
             else if (mode == kDefect) HB2_Q1S(float, kDefect);
             else if (mode == kDot) HB2_Q1S(float, kDot);
+            else if (red) HB2_Q1S(float, kJacobiNorm);
             else HB2_Q1S(float, kJacobi);
         }
 #undef HB2_Q1S

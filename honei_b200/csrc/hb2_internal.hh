@@ -163,8 +163,12 @@ namespace hb2
         kAdd = 3,       // y = y + A x
         kJacobi = 4,    // y = x + P (.) (aux - A x) (ping-pong sweep)
         kRestrict = 5,  // y = A x, zero[0..rows) = 0
-        kDefectIR = 6   // FP64 r = aux - A x: (float) r and its ||r|| (the IR outer defect, Q1 kernels only)
+        kDefectIR = 6,  // FP64 r = aux - A x: (float) r and its ||r|| (the IR outer defect, Q1 kernels only)
+        kJacobiNorm = 7 // kJacobi with ||aux - A x||^2 into red: the kernels' template mode when a Jacobi
+                        // launch asks for the norm, so that the plain sweep carries no reduction code
     };
+
+    __host__ __device__ constexpr bool is_jacobi(int mode) { return mode == kJacobi || mode == kJacobiNorm; }
 
     // Pass flags of the ELL family: kReverse walks the row blocks from the end
     // (consecutive passes over one matrix in alternating directions start where
