@@ -238,7 +238,7 @@ namespace hb2
                                 uint64_t vstride = 0, const uint8_t * active = nullptr,
                                 const uint32_t * list = nullptr, const uint32_t * count = nullptr, uint64_t cap = 0)
     {
-        if (A->K != 9 || A->rows > 128) return false;
+        if (A->K == 0 || A->K > 9 || A->rows > 128) return false;
         const int rpl = (int)((A->rows + 31) / 32);
         const size_t smem = 3 * A->rows * sizeof(T) + 16;
         EllView<T> v = A->view<T>();
@@ -280,14 +280,17 @@ namespace hb2
         return HB2_OK;
     }
 
-    bool cg_mixed_supported(const hb2_ell_s * A64) { return A64->dtype == HB2_F64 && A64->K == 9 && A64->rows <= 128; }
+    bool cg_mixed_supported(const hb2_ell_s * A64)
+    {
+        return A64->dtype == HB2_F64 && A64->K >= 1 && A64->K <= 9 && A64->rows <= 128;
+    }
 
     // coarsest solve of an FP32 level in FP64: A64 is the FP64 operator, b / x are FP32
     int launch_cg_small_f32io(const hb2_ell_s * A64, const void * b32, void * x32, uint64_t max_iters, double eps,
                               int exact, uint64_t * used_dev, double * defect_dev, cudaStream_t stream)
     {
         if (! launch_warp_reg<double, float>(A64, b32, x32, max_iters, eps, exact, used_dev, defect_dev, stream))
-            return fail(HB2_ERR_UNSUPPORTED, "FP64 coarse solve of an FP32 level needs <= 128 rows and 9 slots");
+            return fail(HB2_ERR_UNSUPPORTED, "FP64 coarse solve of an FP32 level needs <= 128 rows and 1-9 slots");
         count_launches(1);
         HB2_LAUNCH_CHECK("cg_warp_reg_kernel (FP32 vectors, FP64 arithmetic)");
         return HB2_OK;
@@ -326,7 +329,9 @@ namespace hb2
             HB2_CUDA(cudaFuncSetAttribute(cg_warp_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemLimit + 64));
             attr_set = true;
         }
-        const bool reg = A->dtype == HB2_F64
+        // the register kernel for the 9-slot operators; others take the shared-memory one
+        const bool reg = A->K != 9 ? false
+                       : A->dtype == HB2_F64
                              ? launch_warp_reg<double, double>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream)
                              : launch_warp_reg<float, float>(A, b, x, max_iters, eps, exact, used_dev, defect_dev, stream);
         if (reg)

@@ -97,8 +97,9 @@ namespace hb2
 #pragma unroll
             for (int k = 0; k < K; ++k)
             {
-                av[j][k] = ok ? Ag.val[(uint64_t)k * Ag.ld + row] : T(0);
-                ac[j][k] = ok ? Ag.col[(uint64_t)k * Ag.ld + row] : -1;
+                const bool okk = ok && k < (int)Ag.K;     // up to 9 slots; the missing ones are skipped
+                av[j][k] = okk ? Ag.val[(uint64_t)k * Ag.ld + row] : T(0);
+                ac[j][k] = okk ? Ag.col[(uint64_t)k * Ag.ld + row] : -1;
             }
             xr[j] = ok ? T(xg[row]) : T(0);
             if (ok) sp[row] = xr[j];

@@ -494,7 +494,7 @@ namespace hb2
             st = hb2_ell_convert(&c64, mg->lev[0].A, HB2_F64, stream);
             if (st) return st;
             mg->coarse64 = c64;
-            if (! cg_mixed_supported(c64)) return fail(HB2_ERR_UNSUPPORTED, "coarse_fp64: coarsest level has more than 128 rows");
+            if (! cg_mixed_supported(c64)) return fail(HB2_ERR_UNSUPPORTED, "coarse_fp64: the coarsest level needs <= 128 rows and 1-9 slots");
             HB2_CUDA(cudaStreamSynchronize(stream));
         }
         HB2_CUDA(cudaStreamSynchronize(stream));

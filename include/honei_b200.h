@@ -380,7 +380,7 @@ typedef struct
     int no_fused_levels;                    /* 1: one kernel per operator on every level (0: levels below
                                                ~20k rows run as two thread-block-cluster kernels per cycle) */
     int coarse_fp64;                        /* F32 hierarchies: 1 runs the coarsest CG in FP64 on an FP64 copy
-                                               of the coarse operator (<= 128 rows); 0: FP32 as the reference */
+                                               of the coarse operator (<= 128 rows, 1-9 slots); 0: FP32 as the reference */
     int cycle;                              /* 0: V-cycle (MGCycleCreation<V::STATIC>, math/mg.hh:567-656);
                                                1: W-cycle (MGCycleCreation<W::STATIC>, math/mg.hh:658-740) */
 } hb2_mg_params;

@@ -210,3 +210,45 @@ def ell_hierarchy(oracle, k, min_level):
         P.append(p)
         R.append(r)
     return A, P, R
+
+
+def test_ir_on_the_feast_hierarchy_with_bf16_inner(feast, oracle, tmp_path):
+    """The reference's own FEAST Q1 matrices (math/mg_TEST.cc:398-463, levels 1-6, read
+    by MatrixIO): FP64 refinement of A_6 x = rhs_6 with an inner FP32 MG V(4,4) to 1e-3
+    over the FP32-read hierarchy (FP64 coarse CG on A_1, 9 rows and 7 slots), its levels
+    2-6 FP32-stored, BF16 with compensated diagonals, or BF16 pure.  Their entries are
+    multiples of 1/3, so BF16 at scale 3 holds them as exactly as FP32 does and all three
+    take the same steps.  Each reaches 1e-10 on the FP64 operator; the error against
+    the dense FP64 solution is within cond(A_6) times the relative residual, and the
+    solution meets the reference test's 8e-3 against its stored sol_6."""
+    def read(name, dt):
+        return hb.MatrixIO.read_matrix(feast.write(tmp_path, name), dtype=dt)
+
+    A64 = read("A_6", torch.float64)
+    b = feast.z["rhs_6"].astype(np.float64)
+    ref = feast.ell(oracle, "A_6")
+    D = np.zeros((ref.rows, ref.cols))
+    for k in range(ref.K):
+        j, v = ref.Aj[k * ref.stride:k * ref.stride + ref.rows], ref.Ax[k * ref.stride:k * ref.stride + ref.rows]
+        m = v != 0
+        D[np.nonzero(m)[0], j[m].astype(np.int64)] += v[m]
+    xd = np.linalg.solve(D, b)
+    kappa = np.linalg.cond(D)
+    nb = np.linalg.norm(b)
+    prm = hb.mg_params(max_iters_coarse=100, eps=1e-3, coarse_eps=1e-3, coarse_exact=False, coarse_fp64=True)
+    P = [read(f"prol_{i}", torch.float32) for i in range(2, 7)]
+    R = [p.transposed() for p in P]
+    out = {}
+    for mode in (None, "compensated", "pure"):
+        A = [read(f"A_{i}", torch.float32) for i in range(1, 7)]
+        if mode:
+            A = A[:1] + [a.to_bf16(compensate=mode == "compensated") for a in A[1:]]
+            assert all(a.scale == 3.0 for a in A[1:])
+        inner = hb.MGData(A, P, R, params=prm)
+        x, it, st = ir_solve(A64, b, inner)
+        rel = np.linalg.norm(b - oracle.ell_spmv(ref, x)) / nb
+        out[mode] = (it, int(st[3]))
+        assert rel < 1e-10, (mode, rel)
+        assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= kappa * rel, mode
+        assert np.abs(x - feast.z["sol_6"]).max() < 8e-3
+    assert out["compensated"] == out[None] and out["pure"] == out[None], out
