@@ -63,8 +63,11 @@ namespace hb2
     // 1, 3, 5, ...) and form their products; the odd lane's products move to the
     // even lane by shuffle, which adds all of them in slot order, so the sums are
     // the one-lane kernel's bit for bit.  The even lane runs the epilogue.
+    // One thread per row takes blocks of up to 256 threads, two up to 512: bounded
+    // at 512 the one-thread FP64 kernel got 44 registers instead of 32 (defect: 64
+    // instead of 40) and the level-11 SpMV ran 20 % slower.
     template <typename T, int KT, int MODE, int TPR>
-    __global__ void __launch_bounds__(kEllMaxThreads)
+    __global__ void __launch_bounds__(TPR == 1 ? kEllThreads : kEllMaxThreads)
     ell_kernel(EllView<T> A, const T * __restrict__ x_, T * __restrict__ y_, const T * __restrict__ aux_,
                const T * __restrict__ aux2, T * __restrict__ zero_, ReduceSlot rs, double * red_, int want_sqrt,
                int flags, Batch bt)
@@ -286,7 +289,10 @@ namespace hb2
     unsigned ell_block(const hb2_ell_s * A, bool reducing)
     {
         const int cls = reducing ? 1 : 0;
-        return ell_shape_tunable(A, cls) ? (unsigned)A->bs[cls] : (unsigned)kEllThreads;
+        if (! ell_shape_tunable(A, cls)) return kEllThreads;
+        // the plain kernel with one thread per row is bounded at 256 threads
+        if (A->layout[cls] == kLayoutPlain && A->tpr[cls] == 1) return std::min(A->bs[cls], kEllThreads);
+        return (unsigned)A->bs[cls];
     }
 
     uint64_t ell_rows_per_block(const hb2_ell_s * A, bool reducing)

@@ -423,8 +423,8 @@ namespace hb2
     // row patterns with 1, 2 or 4 rows per thread (and the Q1 gather form) --
     // and keep the fastest for each of the two kernel classes; then time the
     // winner's launch shape: blocks of 128, 256 or 512 threads where its kernel
-    // takes them (plain, compressed, Q1 gather), and on the plain layout one or
-    // two threads per row.  The arrays of a layout neither class uses are
+    // takes them (plain, compressed, Q1 gather; the plain one with one thread per
+    // row up to 256), and on the plain layout one or two threads per row.  The arrays of a layout neither class uses are
     // freed.  Runs once per matrix shape and process, at creation, on `stream`.
     //
     // The decision is kept per (device, element type, shape, slots, table size)
@@ -646,7 +646,8 @@ namespace hb2
             long incumbent = -1;
             for (int bs : {128, 256, 512})
                 for (int tpr : {1, 2})
-                    if (tpr == 1 || A->layout[cls] == kLayoutPlain)
+                    if ((tpr == 1 || A->layout[cls] == kLayoutPlain) &&
+                        ! (A->layout[cls] == kLayoutPlain && tpr == 1 && bs > kEllThreads))
                     {
                         if (bs == kEllThreads && tpr == 1) incumbent = (long)shapes.size();
                         shapes.push_back(std::make_pair(bs, tpr));

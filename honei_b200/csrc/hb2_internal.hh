@@ -16,7 +16,8 @@ namespace hb2
     constexpr int kEllThreads = 256;
     // The plain, compressed and Q1 gather kernels also run as blocks of 128 or 512
     // threads, and the plain one with two threads per row: the autotuner times
-    // those shapes (their launch bounds are sized for the largest block).
+    // those shapes (their launch bounds are sized for the largest block; the
+    // plain kernel with one thread per row takes at most 256).
     constexpr int kEllMaxThreads = 512;
     constexpr uint32_t kMaxReduceBlocks = 1u << 16;
 

@@ -1,6 +1,7 @@
 """Launch shapes of the ELL kernels: blocks of 128, 256 or 512 threads (plain,
-compressed and Q1 gather kernels) and one or two threads per row (plain layout),
-pinned with HB2_ELL_BLOCK / HB2_ELL_TPR or chosen by the autotuner.
+compressed and Q1 gather kernels; the plain kernel with one thread per row up to
+256) and one or two threads per row (plain layout), pinned with HB2_ELL_BLOCK /
+HB2_ELL_TPR or chosen by the autotuner.
 
 Every shape forms the same products and slot-ordered sums, so every kernel mode is
 the oracle's ELL product (la/product.hh:148-206) bit for bit; the fused norms
@@ -18,7 +19,7 @@ from honei_b200 import DenseVector, SparseMatrixELL, _lib
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(128, 1), (128, 2), (256, 2), (512, 1), (512, 2)]
+SHAPES = [(128, 1), (128, 2), (256, 2), (512, 2)]
 
 
 def dvec(a):
@@ -106,6 +107,17 @@ def test_plain_shapes_transfers(oracle, monkeypatch, bs, tpr):
     assert same_bits(host(yp), pc)
     assert same_bits(host(ya), y0 + pc)
     assert same_bits(host(cc), oracle.ell_spmv(Rr, f))
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_plain_one_thread_per_row_takes_at_most_256(oracle, monkeypatch, dt):
+    """A pin of 512 threads with one thread per row runs the plain kernel in blocks
+    of 256 (its launch bound), bit for bit"""
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    pin(monkeypatch, "0", 512, 1)
+    A = SparseMatrixELL.poisson_q1(7, dt)
+    assert A.layout()[0] == 0 and A.launch_shape(0) == (256, 1) and A.launch_shape(1) == (256, 1)
+    check_square(oracle, A, oracle.q1_ell(7, npdt), npdt)
 
 
 def random_ell(oracle, rows, cols, seed, T=1):
