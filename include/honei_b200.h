@@ -126,8 +126,9 @@ HB2_API int hb2_ell_layout(hb2_ell A, int *layout, uint32_t *table_size, uint32_
  * pair and strip forms).  No counterpart in the reference. */
 HB2_API int hb2_ell_layout_variant(hb2_ell A, int cls, int *layout, int *rows_per_thread, int *windowed);
 /* Launch shape of that kernel: threads per block (128, 256 or 512; timed by the
- * autotuner for the plain, compressed and Q1 gather kernels, 256 for the others)
- * and threads per row (1, or 2 on the plain layout).  HB2_ELL_BLOCK and
+ * autotuner for the plain, compressed and Q1 gather kernels, 256 for the others;
+ * at most 256 for the plain kernel with one thread per row) and threads per row
+ * (1, or 2 on the plain layout).  HB2_ELL_BLOCK and
  * HB2_ELL_TPR override the tuned values for matrices created while they are set.
  * The reference's counterparts are its block-size settings
  * (honei/honeirc:50-51) and the T threads per row of the ELL kernel
