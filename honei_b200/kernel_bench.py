@@ -1,7 +1,7 @@
 """Per-kernel timing of the hot kernels on one Q1 level.
 
     python -m honei_b200.kernel_bench [--kernel all|jacobi|spmv|defect|q1|restrict|prolong|csr_spmv|csr_defect|
-                                                cgvar|bicgstab|coarse_cg]
+                                                cgvar|bicgstab|coarse_cg|solves]
                                       [--level 10] [--iters 20] [--dtype f64|f32]
                                       [--operator q1|coefficients] [--storage native|bf16|bf16c]
 
@@ -114,6 +114,49 @@ def graph_time(name, A, P, n, dt, npdt, dev, reps, launches=40):
     return statistics.median(ts)
 
 
+def solves(level: int, runs: int) -> int:
+    """--kernel solves: the two solves the benchmark times at `level` -- FP64 MG
+    (V(4,4), coarse level 3, coarse CG cap 100 with tree-ordered dots) to 1e-10, then
+    IR to 1e-10 around an FP32 inner MG to 1e-3 whose FP64 coarse CG stops at 1e-3 --
+    of b = A u, u ~ U[-1,1] (seed 42), each `runs` times from x = 0 (no L2 flush).
+    Prints the last run's times (CUDA events) and its launch counts: under a profiler,
+    the launch list of one solve of each kind (HB2_MG_LOOP=host HB2_IR_LOOP=host turn
+    the device-side loops into plain launches)."""
+    import honei_b200 as hb
+    dev = torch.device("cuda")
+    n = ((1 << level) + 1) ** 2
+    A = SparseMatrixELL.poisson_q1(level)
+    b = DenseVector(n)
+    hb.Product.value(b, A, DenseVector(torch.from_numpy(uniform(n, 42)).to(dev)))
+    fp64 = hb.MGData.poisson_q1(3, level, params=hb.mg_params(max_iters_coarse=100, eps=1e-10, coarse_exact=False))
+    inner = hb.MGData.poisson_q1(3, level, dtype=torch.float32,
+                                 params=hb.mg_params(max_iters_coarse=100, eps=1e-3, coarse_eps=1e-3,
+                                                     coarse_exact=False, coarse_fp64=True))
+    x = DenseVector(n)
+    out = {"kernel": "solves", "level": level, "runs": runs}
+    ir = {}
+
+    def run_ir():
+        _, ir["outer"], st = hb.IRSolver.value(A, b, x, inner, eps=1e-10, reset_inner=True)
+        ir["inner"] = int(st[3])
+
+    for name, fn in (("fp64_mg", lambda: hb.MGSolver.value(fp64, b, x)), ("mixed_ir", run_ir)):
+        for _ in range(runs):
+            hb.fill(x, 0.0)
+            torch.cuda.synchronize()
+            c0 = hb.launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            out[name + "_ms"] = e0.elapsed_time(e1)
+            out[name + "_launches"] = hb.launch_count() - c0
+    out.update(fp64_cycles=fp64.used_iters, ir_outer=ir["outer"], ir_inner_cycles=ir["inner"])
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="all")
@@ -131,6 +174,8 @@ def main(argv=None) -> int:
                          "40 launches in one CUDA graph rotating over vector sets of more than 2x L2 in all "
                          "(every launch reads its vectors from DRAM), time per launch")
     a = ap.parse_args(argv)
+    if a.kernel == "solves":
+        return solves(a.level, max(1, a.iters))
     dt = torch.float64 if a.dtype == "f64" else torch.float32
     s = 8 if a.dtype == "f64" else 4
     import numpy as np
