@@ -10,7 +10,7 @@ setting), stop at ||r|| < 1e-10 ||r0||; b = A u*, u* ~ U[-1,1] (splitmix64,
 seed 42 + rank), x0 = 0.  Inputs are resident in HBM when a timed step starts;
 L2 is flushed before every step (256 MiB written, then 256 MiB read, so that no
 dirty line of the flush is written back inside the step) and the flush is
-outside the step's events.  --level 10 runs the level-10 solve of config 1.
+outside the step's events.  --level 10 runs the level-10 solve (1,050,625 unknowns).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -424,7 +424,7 @@ def main():
     if world == 1:
         line["roofline_extra"] = roofline_extra(hb, A, L, peaks, dev)
         if L != 10:
-            line["config1_level10"] = level10_solve(hb, dev, flush, args, stream)
+            line["level10_solve"] = level10_solve(hb, dev, flush, args, stream)
         if not args.no_mixed:
             line["mixed_vs_fp64"] = mixed_vs_fp64(hb, dev, flush, MIXED_LEVEL, min(args.steps, 5),
                                                   min(args.warmup, 2), rank, keep=keep)
@@ -490,7 +490,7 @@ def roofline_extra(hb, A, L, peaks, dev):
 
 
 def level10_solve(hb, dev, flush, args, stream):
-    """Config 1: the level-10 MG solve (1,050,625 unknowns), same parameters and timing."""
+    """The level-10 MG solve (1,050,625 unknowns), same parameters and timing."""
     import torch
     from honei_b200.inputs import uniform
     L = 10
@@ -589,7 +589,7 @@ def finite_or_text(v):
 
 
 def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cycles=100, max_outer=100, keep=None):
-    """Config 2: level-11 Q1 Poisson (4,198,401 unknowns) to 1e-10 relative residual,
+    """Level-11 Q1 Poisson (4,198,401 unknowns) to 1e-10 relative residual,
     plain FP64 MG vs iterative refinement (FP64 defect / update / norm around an FP32
     MG V(4,4) inner solve to 1e-3, restarted from zero each outer step, its coarse CG
     (FP64 arithmetic) cap 100 at the same eps 1e-3, the reference's one eps_relative
@@ -685,7 +685,7 @@ def mixed_vs_fp64(hb, dev, flush, level, steps, warmup, rank, aniso=1.0, max_cyc
 def bf16_variant(hb, dev, flush, level, peaks, rank):
     """The BF16-stored inner matrices (hb2_ell_create_bf16) against FP32-stored ones in
     the mixed-precision refinement at `level`, on two operators:
-    * "q1": the Q1 operator of config 2.  s = 3 makes 8/3, -1/3 and 1 exact in BF16.
+    * "q1": the level-11 Q1 Poisson operator.  s = 3 makes 8/3, -1/3 and 1 exact in BF16.
       The tuned FP32 levels run the Q1 stencil kernel (one byte per row); the BF16
       ones run the BF16 layout.
     * "coefficients": the Q1 finite-element operator with per-cell coefficients of
@@ -769,7 +769,7 @@ def bf16_variant(hb, dev, flush, level, peaks, rank):
 
 
 def anisotropic_probe(hb, dev, flush, level, rank):
-    """Config 2's anisotropic variant: every level's x-coupling (DL/DU) scaled by a
+    """The level-11 system's anisotropic variant: every level's x-coupling (DL/DU) scaled by a
     factor, the diagonal raised to keep zero interior row sums.  The reference's
     method (V(4,4) damped Jacobi on rediscretised coarse operators, coarse CG)
     diverges for the factor 100 -- in FP64, and on the CPU oracle as well -- and
@@ -783,7 +783,7 @@ def anisotropic_probe(hb, dev, flush, level, rank):
 
 
 def batch_workload(seed, nsys=512, lo=4, hi=9, multi_frac=0.25, multi_rhs=8):
-    """Config 3: levels uniform in lo..hi, exactly multi_frac of the systems with multi_rhs RHS."""
+    """The batched workload: levels uniform in lo..hi, exactly multi_frac of the systems with multi_rhs RHS."""
     import numpy as np
     rng = np.random.default_rng(seed)
     levels = rng.integers(lo, hi + 1, nsys)
@@ -793,7 +793,7 @@ def batch_workload(seed, nsys=512, lo=4, hi=9, multi_frac=0.25, multi_rhs=8):
 
 
 def batched_solves(hb, dev, flush, steps, warmup, rank):
-    """Config 3: 512 Q1 systems (levels U{4..9}, 25 % with 8 RHS, RHS ~ U[-1,1]) solved
+    """The batched workload: 512 Q1 systems (levels U{4..9}, 25 % with 8 RHS, RHS ~ U[-1,1]) solved
     together by the batched mixed-precision MG-preconditioned CG to 1e-8, against
     looping the single-system FP64 MG solver (V(4,4), coarse CG cap 100) to 1e-8 over
     the same right-hand sides.  Device time per batch solve with CUDA events (L2
@@ -894,14 +894,14 @@ def batched_solves(hb, dev, flush, steps, warmup, rank):
             "launches_per_step": info["launches_per_step"], "launches_per_solve": launches,
             "device_bytes": info["device_bytes"],
             "loop_fp64_mg_ms": t_loop, "loop_solves": nvec, "loop_mean_cycles": statistics.mean(loop_cycles),
-            "loop": "config 1's single-system FP64 MG solver (V(4,4), coarse CG cap 100) to 1e-8 over all "
+            "loop": "the level-10 single-system FP64 MG solver (V(4,4), coarse CG cap 100) to 1e-8 over all "
                     f"{nvec} right-hand sides in turn, one resident hierarchy per level, timed as one loop",
             "speedup_vs_loop": t_loop / t_dev,
             "method": "CG VAR (FP64) + one FP32 MG V(4,4) preconditioner, FP64 coarse CG cap 100; tol 1e-8"}
 
 
 def serving_loop(rank, rates=SERVING_RATES, duration=10.0, fp64_max_rate=200.0):
-    """Config 4: Poisson arrivals for `duration` s per rate (50 ... 2000 req/s), levels
+    """The serving workload: Poisson arrivals for `duration` s per rate (50 ... 2000 req/s), levels
     log-uniform in 5..11, tolerance 1e-8 / 1e-10 50/50, seeded U[-1,1] RHS; slot pool
     sized under a 120 GB budget.  Latency = host clock from arrival to the solution in
     pinned host memory.  Three servers on the same arrivals: the hybrid one (FP64 MG

@@ -644,8 +644,8 @@ namespace honei_b200
         }
     };
 
-    /* MG parameters of the headline configuration (V(4,4), omega 0.7, coarse CG in the
-     * reference's dot order) */
+    /* MG parameters of the reference's Poisson solves (V(4,4), omega 0.7, coarse CG in
+     * the reference's dot order) */
     inline hb2_mg_params mg_params(double eps = 1e-10, uint64_t max_iters = 100, uint64_t max_iters_coarse = 100)
     {
         hb2_mg_params p;

@@ -247,7 +247,7 @@ namespace
             delete R;
         }
 
-        // CG, FP64, b = A u*, x0 = 0, rel. tol 1e-8 (config 0 shape at L = 5, 7)
+        // CG, FP64, b = A u*, x0 = 0, rel. tol 1e-8 (the CPU-sized CG workload at L = 5, 7)
         for (unsigned L(5); L <= 7; L += 2)
         {
             SparseMatrixELL<double> A(q1_ell_assembled<double>(L));

@@ -5,9 +5,9 @@ The reference has no anisotropic generator.  This build's variant scales the
 x-coupling (bands DL and DU, the left and right neighbours in a grid row) of the
 Q1 stencil by a factor a and raises the diagonal to (6 + 2a) / 3, so interior row
 sums stay zero; Dirichlet rows stay identity rows.  The MG method of the headline
-configs (V(4,4), damped Jacobi omega 0.7, rediscretised coarse operators, coarse
+workloads (V(4,4), damped Jacobi omega 0.7, rediscretised coarse operators, coarse
 CG) converges on it up to a factor of about 10 and diverges from about 20: at
-100, the factor that the mixed-precision config names, the defect grows by orders
+100, the factor of the mixed-precision stability probe, the defect grows by orders
 of magnitude per cycle even without a coarse solve."""
 import numpy as np
 import pytest

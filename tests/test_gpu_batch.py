@@ -50,7 +50,7 @@ def test_batch_true_residual(oracle):
 
 
 def test_every_rhs_of_the_512_system_batch_converges():
-    """Config 3's workload (512 systems, levels 4..9, a quarter with 8 right-hand
+    """The batched workload (512 systems, levels 4..9, a quarter with 8 right-hand
     sides: 1,408 in all): every right-hand side reaches 1e-8 within a few PCG steps.
     (A coarse solve whose recurrence differs from the standard one between calls once
     left some of them short of the tolerance after 100 steps.)"""

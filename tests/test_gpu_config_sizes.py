@@ -1,6 +1,6 @@
-"""Parity at the configs' own sizes and on the exact paths the benchmark times.
+"""Parity at the benchmark workloads' own sizes and on the exact paths the benchmark times.
 
-* Config 1 (Q1 level 10, 1,050,625 unknowns) with the benchmark's MG parameters:
+* Q1 level 10 (1,050,625 unknowns) with the benchmark's MG parameters:
   V(4,4), omega 0.7, coarse level 3, coarse CG capped at 100 iterations with
   tree-ordered dots (coarse_exact=False), stop at 1e-10.  Against the oracle
   (math/mg.hh:1094-1127 restated, reference-order coarse dots): cycle count within
@@ -8,7 +8,7 @@
   1e-8 relative of the oracle's.  (Each of the two solutions is about 5e-7 from the
   exact solution at this stop; the 1e-8 bound says they are the same iterate up
   to the coarse solve's rounding.)
-* Config 2 (level 11, 4,198,401 unknowns): FP64 MG with the reference-order coarse
+* Q1 level 11 (4,198,401 unknowns): FP64 MG with the reference-order coarse
   solve bit for bit against the oracle; with the benchmark's coarse mode as above;
   mixed-precision IR (math/ir.hh:31-80) with its true residual below 1e-10 and its
   error stated against the oracle's FP64 MG solution, bounded by what the two

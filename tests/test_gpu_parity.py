@@ -56,8 +56,8 @@ def test_transfer_assembly_on_device(oracle, L):
 
 
 @pytest.mark.parametrize("L", [10, 11])
-def test_assembly_at_config_levels(oracle, L):
-    """The config levels 10 and 11 (1,050,625 and 4,198,401 rows): operator and transfer
+def test_assembly_at_levels_10_and_11(oracle, L):
+    """The benchmark levels 10 and 11 (1,050,625 and 4,198,401 rows): operator and transfer
     matrices assembled on the device are the reference's arrays, bit for bit."""
     ref = oracle.q1_ell(L)
     A = SparseMatrixELL.poisson_q1(L)
@@ -305,8 +305,8 @@ def test_jacobi_bit_exact(oracle, L, sweeps):
 
 
 @pytest.mark.parametrize("L", [5, 7])
-def test_cg_config0(oracle, golden, L):
-    """Plain CG FP64, b = A u*, x0 = 0, tol 1e-8 (config 0 at L = 7)."""
+def test_cg_fp64_golden(oracle, golden, L):
+    """Plain CG FP64, b = A u*, x0 = 0, tol 1e-8 (the CPU-sized CG workload, at L = 7)."""
     A = SparseMatrixELL.poisson_q1(L)
     b = golden.array(f"cg_L{L}.b") if L == 5 else oracle.ell_spmv(oracle.q1_ell(L), oracle.uniform(A.rows(), 42))
     x = dvec(np.zeros(A.rows()))
@@ -353,8 +353,8 @@ def test_mg_bit_exact_with_reference(oracle, golden, L):
     assert golden.matches(f"mg_L{L}.x", host(x))
 
 
-def test_mg_config1_level10(oracle):
-    """Config 1: L10, V(4,4), omega 0.7, coarse level 3 (cap 100), eps 1e-10."""
+def test_mg_level10(oracle):
+    """Level 10, V(4,4), omega 0.7, coarse level 3 (cap 100), eps 1e-10."""
     L = 10
     A = oracle.q1_ell(L)
     b = oracle.ell_spmv(A, oracle.uniform(A.rows, 42))
@@ -443,7 +443,7 @@ def test_mg_fused_small_levels_identical(dt):
 
 
 def test_ir_mixed_fp64_coarse(oracle):
-    """Mixed IR with the north_star's FP64 coarsest solve inside the FP32 inner MG:
+    """Mixed IR with an FP64 coarsest-level solve inside the FP32 inner MG:
     converges to the FP64 stop and agrees with the FP64 MG solution."""
     L = 7
     Ao = oracle.q1_ell(L)

@@ -94,7 +94,7 @@ def test_jacobi(golden, oracle, L):
 
 @pytest.mark.parametrize("L", [5, 7])
 def test_cg(golden, oracle, L):
-    """Config-0 shape: plain CG, b = A u*, x0 = 0, rel. tol 1e-8; iterates bit-identical."""
+    """The CPU-sized CG workload: plain CG, b = A u*, x0 = 0, rel. tol 1e-8; iterates bit-identical."""
     A = oracle.q1_ell(L)
     b = oracle.ell_spmv(A, oracle.uniform(A.rows, 42))
     assert golden.matches(f"cg_L{L}.b", b)
