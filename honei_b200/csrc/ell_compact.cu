@@ -549,17 +549,18 @@ namespace hb2
         Workspace * ws = 0;
         int st = square ? stream_workspace(s, &ws) : HB2_OK;
         if (st) return st;
-        // One launch reads and writes a set of four vectors.  Where a set fills half
-        // of L2 or more, consecutive launches in a solver find little of it in L2, so
-        // the bursts rotate over enough sets to exceed twice L2 and the candidates
-        // are timed against DRAM; smaller sets stay L2-resident in the solvers and are
-        // timed that way (one set).
+        // One launch reads and writes a set of four vectors.  Where a set fills an
+        // eighth of L2 or more, the bursts rotate over up to eight sets (more than L2 in
+        // all) and the candidates are timed against DRAM; smaller sets are timed
+        // L2-resident (one set).  Inside a V-cycle a level's passes alternate with the
+        // other levels' ones: timed on one 17 MB set, the FP32 level-10 sweep took two
+        // rows per thread, and the level-11 mixed solve ran 3.5 % slower than with one.
         void * buf = 0;
         const size_t vb = ((std::max(A->rows, A->cols) * es + 255) / 256) * 256;
         int l2 = 0;
         cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, A->device);
         const size_t set = 4 * vb, l2b = l2 > 0 ? (size_t)l2 : ((size_t)126 << 20);
-        const int nsets = set >= l2b / 2 ? (int)std::min<size_t>(8, (2 * l2b + set - 1) / set) : 1;
+        const int nsets = set >= l2b / 8 ? (int)std::min<size_t>(8, (2 * l2b + set - 1) / set) : 1;
         HB2_CUDA(cudaMalloc(&buf, nsets * set + 256));
         HB2_CUDA(cudaMemsetAsync(buf, 0, nsets * set + 256, s));
         double * nrm = (double *)((char *)buf + nsets * set);
