@@ -86,3 +86,21 @@ def test_bf16_product_error_against_fp64(oracle, comp):
     reach = oracle.ell_spmv(absA, ax) + (ax * oracle.ell_spmv(absA, np.ones(A.cols)) if comp else 0.0)
     bound = reach * (err + 12 * np.finfo(np.float32).eps)
     assert np.all(np.abs(y - ref) <= bound + 1e-30)
+
+
+@pytest.mark.parametrize("level", [1, 2, 4, 6])
+def test_feast_matrices_are_exact_in_bf16_at_scale_three(oracle, feast, level):
+    """The reference's FEAST Q1 matrices (math/mg_TEST.cc:398-463, its ELL files):
+    3 a is within 1e-7 of an integer of magnitude at most 12 for every entry, so the
+    FP32 copies stored at s = 3 round no further than FP32 already did (largest
+    relative error 2^-25), pure and compensated alike, and the stored values read back
+    in FP32 are (float)(k / 3) -- why the BF16 inner hierarchies take the FP32 one's
+    steps on the FEAST system (tests/test_gpu_bf16.py)."""
+    A = feast.ell(oracle, f"A_{level}")
+    k = np.round(3 * A.Ax)
+    assert np.abs(3 * A.Ax - k).max() < 1e-7 and np.abs(k).max() <= 12
+    A32 = oracle.Ell(A.rows, A.cols, A.stride, A.K, A.T, A.Aj, A.Ax.astype(np.float32), A.Arl)
+    for comp in (False, True):
+        s, err = oracle.ell_bf16_scale(A32, comp)
+        assert s == 3.0 and err <= 2.0 ** -25
+    assert np.array_equal(oracle.ell_bf16_values(A32, 3.0, False), (k / 3).astype(np.float32))
