@@ -490,8 +490,8 @@ namespace hb2
     }
 
     // HB2_ELL_BLOCK=128|256|512 and HB2_ELL_TPR=1|2 override the tuned launch
-    // shape (threads per row on the plain layout only); read at each matrix
-    // creation
+    // shape (threads per row on the plain layout only; the plain kernel with one
+    // thread per row runs 512 as 256); read at each matrix creation
     static int shape_pin(const char * name, int a, int b, int c)
     {
         const char * v = getenv(name);

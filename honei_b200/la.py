@@ -199,7 +199,8 @@ class SparseMatrixELL:
     def launch_shape(self, cls: int = 0):
         """(threads_per_block, threads_per_row) of that kernel: the autotuner's
         choice among 128 / 256 / 512 threads (plain, compressed and Q1 gather
-        kernels; 256 for the others) and 1 or 2 threads per row (plain layout)."""
+        kernels, the plain one with one thread per row up to 256; 256 for the
+        others) and 1 or 2 threads per row (plain layout)."""
         b, t = ctypes.c_int(), ctypes.c_int()
         call("hb2_ell_launch_shape", self._h, cls, ctypes.byref(b), ctypes.byref(t))
         return b.value, t.value
